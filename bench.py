@@ -1,0 +1,345 @@
+"""Benchmark: FP64 residual + matrix-free Jacobian action (GDOF/s) of 3-D quasi-static isotropic
+linear elasticity on an unstructured P1 tetrahedral box mesh of ~1.2 M cells (Delaunay of seeded
+uniform-random interior points plus a jittered regular boundary grid, box [-6,6]x[-6,6]x[-9,0] km,
+per-cell log-normal Vs with median 3000 m/s and sigma_log 0.2, Vp = sqrt(3) Vs, density 2700
+kg/m^3 +-5%).
+
+One step = one residual F(u) and one Jacobian action J v, each over the whole mesh
+(2 applications x N_dof). value = 2 * N_dof * steps / (device time of the applications).
+The L2 cache (126 MB) is flushed (256 MiB write) before every application, because the
+application's working set (~53 MB) would otherwise stay cached between applications.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pylith_b200|reference]
+
+Under torchrun (N > 1) every rank runs the same workload on its own GPU (weak scaling, its own
+seeded mesh); the slowest rank's device time defines the step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TARGET_CELLS = 1_200_000
+METRIC = "GDOF/s residual+Jv (FP64), % of HBM roofline"
+UNIT = "GDOF/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_mesh(cells: int, seed: int):
+    """The seeded benchmark mesh, cached under the temp directory between processes."""
+    from pylith_b200 import meshing as M
+
+    cache = os.path.join(tempfile.gettempdir(), "pylith_b200_mesh_cache")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, f"tet_{cells}_{seed}_v1.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        return M.Mesh(M.CELL_TET4, d["coords"], d["cells"])
+    t0 = time.time()
+    mesh = M.box_tet_delaunay(cells, seed=seed)
+    log(f"mesh: {mesh.num_cells} tets, {mesh.num_nodes} nodes in {time.time() - t0:.1f} s")
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, coords=mesh.coords, cells=mesh.cells)
+    os.replace(tmp, path)
+    return mesh
+
+
+def algorithmic_bytes(mesh) -> int:
+    """Unique HBM bytes of one application with perfect on-chip reuse: connectivity (4 int32)
+    and material (mu, K as FP64) per cell; coordinates, input and output (3 FP64 each) per node."""
+    return mesh.num_cells * (16 + 16) + mesh.num_nodes * (24 + 24 + 24)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(mesh):
+    """DRAM bytes per residual launch from the committed ncu summary, scaled to this mesh."""
+    path = os.path.join(ROOT, "profiles", "tet4_residual_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return float(d["dram_bytes_per_cell"]) * mesh.num_cells
+
+
+def cpu_baseline(mesh, mat, source: str, budget_s: float = 12.0):
+    """Oracle cell loop on every host core: residual F(u) plus a second pass of the same loop
+    standing in for J v (linear elasticity: F(u) = J u), repeated within a time budget."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the checker; timed here as the CPU baseline only
+
+    if source == "ref" and not O.ref_available():
+        source = "oracle"
+    aux = O.AuxFields([(mat.density[:, None], "cell"), (mat.shear_modulus[:, None], "cell"),
+                       (mat.bulk_modulus[:, None], "cell")])
+    u = np.random.default_rng(0).standard_normal(mesh.num_nodes * 3)
+    cores = os.cpu_count() or 1
+    f1 = "IsotropicLinearElasticity3D::f1v_infinitesimalStrain"
+    O.residual(mesh, u, aux, f1=f1, source=source, nthreads=cores)  # warm-up
+    apps = 0
+    t0 = time.perf_counter()
+    while True:
+        O.residual(mesh, u, aux, f1=f1, source=source, nthreads=cores)
+        apps += 1
+        if time.perf_counter() - t0 > budget_s or apps >= 40:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": mesh.num_dof * apps / dt / 1e9, "unit": UNIT, "cores": cores,
+            "kind": "reference" if source == "ref" else "port",
+            "sample": (f"{apps} applications over the full {mesh.num_cells}-cell mesh in {dt:.1f} s; "
+                       "oracle cell loop (restated PETSc DMPlexComputeResidual) calling "
+                       + ("the reference's compiled pointwise kernels (oracle/_ref)" if source == "ref"
+                          else "the restated pointwise kernels")
+                       + "; J v counted as one more pass of the same loop")}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from pylith_b200 import materials as MAT
+
+    mesh = load_mesh(TARGET_CELLS, 0)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    base = cpu_baseline(mesh, mat, "ref", budget_s=max(5.0, 0.6 * args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 2 * mesh.num_dof / (base["value"] * 1e9) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "elasticity P1 tet residual+Jv",
+                                            "cells": mesh.num_cells, "dof": mesh.num_dof},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="pylith_b200")
+    ap.add_argument("--cells", type=int, default=TARGET_CELLS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import materials as MAT
+
+    mesh = load_mesh(args.cells, seed=rank)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=rank)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    ctx = FA.Context(local_rank)
+    dmesh = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dmesh)
+    n = dmesh.num_dof
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    u = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+    v = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+    r = torch.empty_like(u)
+    jv = torch.empty_like(u)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def app_residual():
+        ig.compute_lhs_residual(0.0, 0.0, u, r)
+
+    def app_jv():
+        ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, u, v, jv)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        app_residual()
+        flush.zero_()
+        app_jv()
+    ctx.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(2 * args.steps)]
+    launches0 = _lib.lib().pl_kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[2 * k][0].record(stream)
+            app_residual()
+            ev[2 * k][1].record(stream)
+            flush.zero_()
+            ev[2 * k + 1][0].record(stream)
+            app_jv()
+            ev[2 * k + 1][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = _lib.lib().pl_kernel_launches() - launches0
+    ctx.synchronize()
+    t_res = sum(ev[2 * k][0].elapsed_time(ev[2 * k][1]) for k in range(args.steps)) / 1e3
+    t_jv = sum(ev[2 * k + 1][0].elapsed_time(ev[2 * k + 1][1]) for k in range(args.steps)) / 1e3
+    t_total = t_res + t_jv
+    if dist:
+        tt = torch.tensor([t_total, t_res, t_jv], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total, t_res, t_jv = tt.tolist()
+    value = world * 2 * n * args.steps / t_total / 1e9
+
+    # End to end through the public API with host buffers: H2D of u and v from pinned memory,
+    # residual and J v, D2H of both results, every step.
+    hu = torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(u.cpu())
+    hv = torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(v.cpu())
+    hr = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    hjv = torch.empty(n, dtype=torch.float64, pin_memory=True)
+
+    def e2e_step():
+        u.copy_(hu, non_blocking=True)
+        v.copy_(hv, non_blocking=True)
+        app_residual()
+        app_jv()
+        hr.copy_(r, non_blocking=True)
+        hjv.copy_(jv, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = e0.elapsed_time(e1) / 1e3
+    if dist:
+        tt = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = tt.item()
+    e2e_value = world * 2 * n * args.steps / t_e2e / 1e9
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        alg = algorithmic_bytes(mesh)
+        achieved = alg / (t_res / args.steps) / 1e9
+        traffic = profiled_traffic(mesh)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_total / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "elasticity P1 tet residual+Jv", "cells": mesh.num_cells,
+                       "nodes": mesh.num_nodes, "dof": n, "l2": "flushed before every application (256 MiB write)",
+                       "ms_residual": t_res / args.steps * 1e3, "ms_jv": t_jv / args.steps * 1e3},
+            "roofline": {"bound": "hbm", "kernel": "residual (P1 tet, FP64)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "algorithmic_bytes": alg, "traffic": traffic},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 8,
+                    "d2h_bytes_per_step": 2 * n * 8},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(mesh, mat, "oracle")
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

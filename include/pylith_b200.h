@@ -1,0 +1,270 @@
+/*
+ * pylith_b200 — C ABI of the B200 (sm_100a) finite-element residual/Jacobian engine.
+ *
+ * This is the drop-in boundary for PyLith's per-cell residual and Jacobian loop. In the
+ * reference that loop is PETSc's DMPlexComputeResidualByKey / DMPlexComputeJacobianByKey /
+ * DMPlexCompute{Residual,Jacobian}HybridByKey / DMProjectFieldLocal, driven by
+ * IntegratorDomain and IntegratorInterface. Each entry point below names the reference
+ * interface it replaces (paths relative to the PyLith source tree).
+ *
+ * Conventions
+ *   - Every function returns PL_OK (0) or a negative PL_ERR_* code; nothing throws across
+ *     the ABI. pl_last_error() returns a message for the calling thread's last failure.
+ *   - Pointers named *_dev are device pointers (cudaMalloc'd or torch-owned); *_host are
+ *     host pointers. The library never frees caller memory.
+ *   - Local vectors follow the reference's local-vector semantics
+ *     (docs/developer/implementation/petsc-fem.md:60-75): 3 displacement DOFs per mesh node
+ *     (constrained DOFs included, holding their boundary values), followed, for meshes with
+ *     a fault, by 3 Lagrange-multiplier DOFs per fault node.
+ *   - Work is enqueued on the context's stream; results are ready after that stream
+ *     synchronises. A context is used by one host thread at a time.
+ *   - Pointwise kernels are identified by the address of the host function with PETSc's
+ *     pointwise signature (the same function pointers PyLith hands to PetscWeakForm). The
+ *     library maps each known address to its device implementation; an unknown address is
+ *     rejected with PL_ERR_UNKNOWN_KERNEL (there is no CPU fallback).
+ */
+#ifndef PYLITH_B200_H
+#define PYLITH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PL_OK 0
+#define PL_ERR_INVALID_ARG (-1)
+#define PL_ERR_UNKNOWN_KERNEL (-2)
+#define PL_ERR_CUDA (-3)
+#define PL_ERR_OUT_OF_MEMORY (-4)
+#define PL_ERR_NOT_CONVERGED (-5)
+#define PL_ERR_DEVICE_CHECK (-6)
+#define PL_ERR_UNSUPPORTED (-7)
+#define PL_ERR_NOT_READY (-8)
+
+/* Scalar types of the reference (libsrc/pylith/utils/types.hh:14-16 with PETSc real
+ * double, 32-bit indices). */
+typedef int PylithInt;
+typedef double PylithReal;
+typedef double PylithScalar;
+
+/* PETSc pointwise-function signatures (docs/developer/implementation/petsc-fem.md:438-600;
+ * libsrc/pylith/fekernels/Elasticity.hh:125-142, FaultCohesiveKin.hh:74-92,298-317). */
+typedef void (*PetscPointFn)(PylithInt dim, PylithInt numS, PylithInt numA, const PylithInt sOff[],
+                             const PylithInt sOff_x[], const PylithScalar s[],
+                             const PylithScalar s_t[], const PylithScalar s_x[],
+                             const PylithInt aOff[], const PylithInt aOff_x[],
+                             const PylithScalar a[], const PylithScalar a_t[],
+                             const PylithScalar a_x[], PylithReal t, const PylithScalar x[],
+                             PylithInt numConstants, const PylithScalar constants[],
+                             PylithScalar f[]);
+typedef void (*PetscPointJacFn)(PylithInt dim, PylithInt numS, PylithInt numA,
+                                const PylithInt sOff[], const PylithInt sOff_x[],
+                                const PylithScalar s[], const PylithScalar s_t[],
+                                const PylithScalar s_x[], const PylithInt aOff[],
+                                const PylithInt aOff_x[], const PylithScalar a[],
+                                const PylithScalar a_t[], const PylithScalar a_x[], PylithReal t,
+                                PylithReal s_tshift, const PylithScalar x[],
+                                PylithInt numConstants, const PylithScalar constants[],
+                                PylithScalar g[]);
+typedef void (*PetscBdPointFn)(PylithInt dim, PylithInt numS, PylithInt numA,
+                               const PylithInt sOff[], const PylithInt sOff_x[],
+                               const PylithScalar s[], const PylithScalar s_t[],
+                               const PylithScalar s_x[], const PylithInt aOff[],
+                               const PylithInt aOff_x[], const PylithScalar a[],
+                               const PylithScalar a_t[], const PylithScalar a_x[], PylithReal t,
+                               const PylithScalar x[], const PylithReal n[],
+                               PylithInt numConstants, const PylithScalar constants[],
+                               PylithScalar f[]);
+typedef void (*PetscBdPointJacFn)(PylithInt dim, PylithInt numS, PylithInt numA,
+                                  const PylithInt sOff[], const PylithInt sOff_x[],
+                                  const PylithScalar s[], const PylithScalar s_t[],
+                                  const PylithScalar s_x[], const PylithInt aOff[],
+                                  const PylithInt aOff_x[], const PylithScalar a[],
+                                  const PylithScalar a_t[], const PylithScalar a_x[],
+                                  PylithReal t, PylithReal s_tshift, const PylithScalar x[],
+                                  const PylithReal n[], PylithInt numConstants,
+                                  const PylithScalar constants[], PylithScalar g[]);
+
+/* Equation parts (libsrc/pylith/feassemble/Integrator.hh:26-31). */
+enum { PL_LHS = 0, PL_RHS = 1, PL_LHS_LUMPED_INV = 2, PL_LHS_WEIGHTED = 3 };
+
+/* Cell types. Node order: see pylith_b200/meshing.py. */
+enum { PL_CELL_TET4 = 0, PL_CELL_HEX8 = 1, PL_CELL_HEX27 = 2 };
+
+/* Aux subfield storage: one value set per cell (basis order 0) or per quadrature point
+ * ("point" finite-element space, pylith/topology/Subfield.py:28-30). Host layouts are
+ * [ncells][ncomp] and [ncells][nquad][ncomp]. */
+enum { PL_AUX_PER_CELL = 0, PL_AUX_PER_QUADPT = 1, PL_AUX_PER_FAULT_NODE = 2 };
+
+/* Output modes of the compute calls: overwrite the whole output vector with this
+ * integrator's contribution, or add into it (ADD_VALUES). */
+enum { PL_INSERT = 0, PL_ADD = 1 };
+
+/* Scatter (assembly) strategies of the domain kernels. */
+enum {
+    PL_SCATTER_AUTO = 0,      /* library choice (cell-block gather when available) */
+    PL_SCATTER_ATOMIC = 1,    /* one thread per cell, FP64 atomics into the output */
+    PL_SCATTER_BLOCKED = 2    /* cell blocks in shared memory, deterministic gather */
+};
+
+typedef struct pl_context_s* pl_context;
+typedef struct pl_mesh_s* pl_mesh;
+typedef struct pl_integrator_s* pl_integrator;
+typedef struct pl_matrix_s* pl_matrix;
+
+/* Registration records (libsrc/pylith/feassemble/IntegratorDomain.hh:25-86,
+ * IntegratorInterface.hh:31-120). Unused kernels are NULL. */
+typedef struct {
+    const char* subfield;
+    int part;
+    PetscPointFn r0;
+    PetscPointFn r1;
+} pl_residual_kernels;
+
+typedef struct {
+    const char* subfield_trial;
+    const char* subfield_basis;
+    int part;
+    PetscPointJacFn j0, j1, j2, j3;
+} pl_jacobian_kernels;
+
+typedef struct {
+    const char* subfield;
+    PetscPointFn f;
+} pl_project_kernels;
+
+/* Interface faces (IntegratorInterface::FaceEnum): negative side, positive side, fault. */
+enum { PL_FACE_NEGATIVE = 0, PL_FACE_POSITIVE = 1, PL_FACE_FAULT = 2 };
+
+typedef struct {
+    const char* subfield;
+    int part;
+    int face;
+    PetscBdPointFn r0;
+    PetscBdPointFn r1;
+} pl_interface_residual_kernels;
+
+typedef struct {
+    const char* subfield_trial;
+    const char* subfield_basis;
+    int part;
+    int face;
+    PetscBdPointJacFn j0, j1, j2, j3;
+} pl_interface_jacobian_kernels;
+
+/* ---- errors, kernels ------------------------------------------------------------------ */
+const char* pl_error_string(int code);
+const char* pl_last_error(void);
+/* Number of device kernels this library has launched in the process (all contexts). */
+int64_t pl_kernel_launches(void);
+/* Address of a pointwise kernel by its PyLith name, e.g.
+ * "IsotropicLinearElasticity3D::f1v_infinitesimalStrain"; NULL if unknown. The addresses are
+ * those of the pylith::fekernels declarations in include/pylith_b200/fekernels.hh. */
+void* pl_fekernel_lookup(const char* name);
+
+/* ---- context -------------------------------------------------------------------------- */
+int pl_context_create(int device, pl_context* out);
+int pl_context_destroy(pl_context ctx);
+/* Enqueue all work on a caller-owned cudaStream_t; NULL is CUDA's legacy default stream
+ * (torch's default stream). A new context starts on its own non-blocking stream. */
+int pl_context_set_stream(pl_context ctx, void* stream);
+int pl_context_use_own_stream(pl_context ctx);
+void* pl_context_get_stream(pl_context ctx);
+int pl_context_synchronize(pl_context ctx);
+
+/* ---- mesh ----------------------------------------------------------------------------- */
+/* Uploads cells [num_cells][nodes_per_cell] (int32) and coordinates [num_nodes][3] (FP64).
+ * Replaces the mesh/closure data PETSc keeps in the DMPlex (topology/Field.cc:276-440,
+ * CoordsVisitor.icc:145-157). */
+int pl_mesh_create(pl_context ctx, int cell_type, int64_t num_cells, const int32_t* cells_host,
+                   int64_t num_nodes, const double* coords_host, pl_mesh* out);
+/* Adds cohesive cells [num_cohesive][12] (4 negative, 4 positive, 4 Lagrange nodes) and the
+ * number of Lagrange nodes (fault vertices). */
+int pl_mesh_set_cohesive(pl_mesh mesh, int64_t num_cohesive, const int32_t* cohesive_host,
+                         int64_t num_lagrange);
+int pl_mesh_destroy(pl_mesh mesh);
+int64_t pl_mesh_num_dof(pl_mesh mesh);
+
+/* ---- domain integrator (libsrc/pylith/feassemble/IntegratorDomain.cc) ------------------ */
+/* Integrates over cells [cell_ids] of the mesh (NULL = all cells). */
+int pl_integrator_domain_create(pl_mesh mesh, int64_t num_ids, const int32_t* cell_ids_host,
+                                pl_integrator* out);
+/* IntegratorDomain::setKernelsResidual (IntegratorDomain.cc:135-167). */
+int pl_integrator_set_kernels_residual(pl_integrator integ, const pl_residual_kernels* kernels,
+                                       int num);
+/* IntegratorDomain::setKernelsJacobian (IntegratorDomain.cc:172-205). */
+int pl_integrator_set_kernels_jacobian(pl_integrator integ, const pl_jacobian_kernels* kernels,
+                                       int num);
+/* IntegratorDomain::setKernelsUpdateStateVars (IntegratorDomain.cc:221-228). */
+int pl_integrator_set_kernels_update_state_vars(pl_integrator integ,
+                                                const pl_project_kernels* kernels, int num);
+/* Auxiliary subfields in the reference's order (the registered kernels index them from the
+ * back, e.g. IsotropicLinearElasticity.hh:95-127). Names: density, body_force,
+ * shear_modulus, bulk_modulus, maxwell_time, shear_modulus_ratio, viscous_strain,
+ * total_strain (domain); slip (interface). Values are copied to the device. */
+int pl_integrator_set_aux(pl_integrator integ, const char* name, int storage, int ncomp,
+                          const double* values_host);
+/* Copies an aux subfield back in the host layout of pl_integrator_set_aux. */
+int pl_integrator_get_aux(pl_integrator integ, const char* name, double* values_host);
+/* Integrator::_setKernelConstants (Integrator.cc:264-290). */
+int pl_integrator_set_constants(pl_integrator integ, int num, const double* constants);
+int pl_integrator_set_scatter(pl_integrator integ, int scatter);
+int pl_integrator_destroy(pl_integrator integ);
+
+/* ---- interface integrator (libsrc/pylith/feassemble/IntegratorInterface.cc) ------------ */
+int pl_integrator_interface_create(pl_mesh mesh, pl_integrator* out);
+/* IntegratorInterface::setKernels (IntegratorInterface.cc:243-310). */
+int pl_integrator_interface_set_kernels_residual(pl_integrator integ,
+                                                 const pl_interface_residual_kernels* kernels,
+                                                 int num);
+int pl_integrator_interface_set_kernels_jacobian(pl_integrator integ,
+                                                 const pl_interface_jacobian_kernels* kernels,
+                                                 int num);
+
+/* ---- compute (Integrator.hh:164-200) --------------------------------------------------- */
+/* computeLHSResidual: DMPlexComputeResidualByKey (IntegratorDomain.cc:448) or
+ * DMPlexComputeResidualHybridByKey (IntegratorInterface.cc:653). u_t may be NULL for
+ * quasi-static problems. */
+int pl_compute_lhs_residual(pl_integrator integ, double t, double dt, const double* u_dev,
+                            const double* u_t_dev, double* r_dev, int mode);
+/* Matrix-free Jacobian action Jv with the registered Jacobian kernels
+ * (DMPlexComputeJacobianActionByKey, IntegratorDomain.cc:540). */
+int pl_compute_lhs_jacobian_action(pl_integrator integ, double t, double dt, double s_tshift,
+                                   const double* u_dev, const double* v_dev, double* jv_dev,
+                                   int mode);
+/* FP32 variant of the Jacobian action (FP32 operands, FP32 accumulation, FP64 geometry);
+ * used inside the mixed-precision Krylov iterations. */
+int pl_compute_lhs_jacobian_action_f32(pl_integrator integ, double t, double dt,
+                                       const float* v_dev, float* jv_dev, int mode);
+/* Host-buffer convenience: copies u to the device, computes the residual and copies it
+ * back (the end-to-end path a CPU caller takes). */
+int pl_compute_lhs_residual_host(pl_integrator integ, double t, double dt, const double* u_host,
+                                 double* r_host);
+/* DMProjectFieldLocal with the registered update-state kernels (IntegratorDomain.cc:555-590):
+ * replaces the per-quadrature-point state subfields in place. */
+int pl_update_state_vars(pl_integrator integ, double t, double dt, const double* u_dev);
+
+/* ---- assembled Jacobian (DMPlexComputeJacobianByKey, IntegratorDomain.cc:489) ---------- */
+/* Block-CSR matrix with 3x3 blocks over the mesh's node graph (plus Lagrange nodes). */
+int pl_matrix_create(pl_mesh mesh, pl_matrix* out);
+int pl_matrix_zero(pl_matrix mat);
+int pl_compute_lhs_jacobian(pl_integrator integ, double t, double dt, double s_tshift,
+                            const double* u_dev, pl_matrix mat);
+/* Sizes and device arrays: row_ptr [nrows+1] int32, col_idx [nnzb] int32, values
+ * [nnzb][3][3] FP64 (row-major blocks). */
+int pl_matrix_info(pl_matrix mat, int64_t* nrows_blocks, int64_t* nnz_blocks,
+                   const int32_t** row_ptr_dev, const int32_t** col_idx_dev,
+                   double** values_dev);
+/* Copies the matrix to host arrays sized by pl_matrix_info (synchronises the stream). */
+int pl_matrix_copy_to_host(pl_matrix mat, int32_t* row_ptr_host, int32_t* col_idx_host,
+                           double* values_host);
+int pl_matrix_spmv(pl_matrix mat, const double* x_dev, double* y_dev);
+int pl_matrix_destroy(pl_matrix mat);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYLITH_B200_H */

@@ -1,0 +1,129 @@
+// Internal host-side structures shared by the pylith_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pylith_b200.h"
+
+namespace plb {
+
+// Device implementations of the pointwise kernels the registry knows about.
+enum KernelId {
+    K_NONE = 0,
+    K_G0V_BODYFORCE,
+    K_ILE_F1V,
+    K_ILE_JF3VU,
+    K_GM_F1V,
+    K_GM_JF3VU,
+    K_GM_VISCOUS_STRAIN,
+    K_EL_STRAIN_VECTOR,
+    K_FCK_F0U_NEG,
+    K_FCK_F0U_POS,
+    K_FCK_F0L_SLIP,
+    K_FCK_JF0UL_NEG,
+    K_FCK_JF0UL_POS,
+    K_FCK_JF0LU,
+};
+
+KernelId lookup_kernel(const void* fn);
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define PLB_CUDA(call)                                             \
+    do {                                                           \
+        cudaError_t _e = (call);                                   \
+        if (_e != cudaSuccess) return ::plb::cuda_fail(_e, #call); \
+    } while (0)
+
+// Cell-block layout of a tetrahedral mesh for the shared-memory kernels (built once per mesh).
+struct BlockedLayout {
+    int cells_per_block = 0;
+    int64_t num_blocks = 0;
+    int max_local_nodes = 0;
+    int32_t* d_block_node_begin = nullptr;  // [num_blocks + 1] into node_ids
+    int32_t* d_node_ids = nullptr;          // global node of each block-local slot (sorted per block)
+    uint16_t* d_local_cells = nullptr;      // [ncells][4] block-local slot of each cell corner
+    uint8_t* d_slot_shared = nullptr;       // per slot: 1 if other blocks also touch the node
+    int64_t num_shared_nodes = 0;
+    int32_t* d_shared_node = nullptr;       // nodes touched by more than one block
+    int64_t num_untouched = 0;
+    int32_t* d_untouched = nullptr;         // nodes no cell touches
+    size_t device_bytes = 0;
+};
+
+}  // namespace plb
+
+struct pl_context_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    unsigned int* d_err = nullptr;
+    // staging buffers for the host-buffer entry points
+    double* h_pinned = nullptr;
+    size_t h_pinned_bytes = 0;
+    double* d_stage = nullptr;
+    size_t d_stage_bytes = 0;
+};
+
+struct pl_mesh_s {
+    pl_context ctx = nullptr;
+    int cell_type = 0;
+    int nen = 0;
+    int nq = 0;
+    int64_t ncells = 0;
+    int64_t nnodes = 0;
+    int32_t* d_cells = nullptr;
+    double* d_coords = nullptr;
+    std::vector<int32_t> h_cells;
+    std::vector<double> h_coords;
+    int64_t ncoh = 0;
+    int64_t nlag = 0;
+    int32_t* d_coh = nullptr;
+    std::vector<int32_t> h_coh;
+    plb::BlockedLayout* blocked = nullptr;
+};
+
+namespace plb {
+struct AuxField {
+    std::string name;
+    int storage = PL_AUX_PER_CELL;
+    int ncomp = 0;
+    double* d = nullptr;  // device SoA: [ncomp][(nq)][ncells]
+};
+}  // namespace plb
+
+struct pl_integrator_s {
+    pl_mesh mesh = nullptr;
+    bool is_interface = false;
+    int64_t ncells = 0;                 // cells integrated over
+    int32_t* d_cell_ids = nullptr;      // NULL: all cells of the mesh, in order
+    std::vector<int32_t> h_cell_ids;
+    // domain kernels
+    plb::KernelId r0 = plb::K_NONE, r1 = plb::K_NONE;
+    plb::KernelId j0 = plb::K_NONE, j3 = plb::K_NONE;
+    std::vector<plb::KernelId> project;
+    std::vector<std::string> project_subfields;
+    // interface kernels: residual per face and Jacobian per face
+    plb::KernelId if_r[3] = {plb::K_NONE, plb::K_NONE, plb::K_NONE};
+    plb::KernelId if_j[3] = {plb::K_NONE, plb::K_NONE, plb::K_NONE};
+    std::vector<plb::AuxField> aux;
+    std::vector<double> constants;
+    int scatter = PL_SCATTER_AUTO;
+};
+
+struct pl_matrix_s {
+    pl_mesh mesh = nullptr;
+    int64_t nrows = 0;  // block rows: nodes + Lagrange nodes
+    int64_t nnzb = 0;
+    int32_t* d_row_ptr = nullptr;
+    int32_t* d_col = nullptr;
+    double* d_val = nullptr;
+    int32_t* d_cell_pos = nullptr;  // [ncells][nen][nen] block index of each element block
+    int32_t* d_coh_pos = nullptr;   // [ncoh][4 (blocks)][4][4]
+};

@@ -1,0 +1,61 @@
+// Kernel launchers shared between translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+struct pl_mesh_s;
+
+struct pl_integrator_s;
+
+namespace plb {
+
+struct DomainParams;
+struct BlockedLayout;
+
+// Counts kernel launches made by this library (reported by pl_kernel_launches).
+void count_launch(int n = 1);
+
+void launch_domain_apply_atomic(const DomainParams& p, int cell, int rheo, bool bf, int op,
+                                cudaStream_t s);
+void launch_domain_jv_f32_atomic(const DomainParams& p, int cell, int rheo, cudaStream_t s);
+void launch_domain_jacobian(const DomainParams& p, int cell, int rheo, const int32_t* pos,
+                            double* vals, cudaStream_t s);
+// Aux binding of a domain integrator for its registered Jacobian kernels.
+int bind_domain_jacobian(pl_integrator_s* ig, DomainParams* p);
+void launch_domain_update_state(const DomainParams& p, int cell, cudaStream_t s);
+// Builds (once per mesh) the cell-block layout used by the blocked scatter.
+int ensure_blocked_layout(pl_mesh_s* m);
+void free_blocked_layout(BlockedLayout* b);
+// Cell-block (shared-memory, deterministic) residual / Jacobian action; returns false when the
+// layout does not support the configuration.
+bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell,
+                                 int rheo, bool bf, int op, bool insert, int64_t nnodes,
+                                 cudaStream_t s);
+
+struct CohesiveParams {
+    const int32_t* coh;      // [ncoh][12]
+    int64_t ncoh;
+    const double* coords;
+    const double* u;         // full local vector
+    const double* v;         // Jacobian-action direction
+    double* out;
+    const float* v32;
+    float* out32;
+    const double* slip;      // [nlag][3]
+    int64_t lag_offset;      // 3 * nnodes
+    double t, s_tshift;
+    int num_constants;
+    double constants[8];
+    int kr[3];               // residual kernel per face (KernelId)
+    int kj[3];               // Jacobian kernel per face
+};
+
+void launch_cohesive_residual(const CohesiveParams& p, cudaStream_t s);
+void launch_cohesive_jv(const CohesiveParams& p, cudaStream_t s);
+void launch_cohesive_jv_f32(const CohesiveParams& p, cudaStream_t s);
+void launch_cohesive_jacobian(const CohesiveParams& p, const int32_t* pos, double* vals,
+                              cudaStream_t s);
+
+}  // namespace plb

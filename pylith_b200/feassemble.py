@@ -1,0 +1,301 @@
+"""Python mirror of PyLith's integrator registration API over the C ABI.
+
+Same names, argument meaning and error behaviour as
+libsrc/pylith/feassemble/IntegratorDomain.hh:25-86 and IntegratorInterface.hh:31-120:
+kernels are registered as (subfield, part, pointwise functions) records; an unknown
+pointwise function raises (PL_ERR_UNKNOWN_KERNEL) instead of falling back to the CPU.
+Device buffers are torch CUDA tensors (float64, or float32 for the mixed-precision action).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as C
+from ._lib import check
+
+LHS, RHS, LHS_LUMPED_INV, LHS_WEIGHTED = C.PL_LHS, C.PL_RHS, C.PL_LHS_LUMPED_INV, C.PL_LHS_WEIGHTED
+PER_CELL, PER_QUADPT, PER_FAULT_NODE = C.PL_AUX_PER_CELL, C.PL_AUX_PER_QUADPT, C.PL_AUX_PER_FAULT_NODE
+INSERT, ADD = C.PL_INSERT, C.PL_ADD
+FACE_NEGATIVE, FACE_POSITIVE, FACE_FAULT = C.PL_FACE_NEGATIVE, C.PL_FACE_POSITIVE, C.PL_FACE_FAULT
+
+
+class _Kernels:
+    """Addresses of the registered pointwise kernels, by PyLith class and function name."""
+
+    def __getattr__(self, cls):
+        return _KernelClass(cls)
+
+
+class _KernelClass:
+    def __init__(self, cls):
+        self.cls = cls
+
+    def __getattr__(self, fn):
+        addr = C.lib().pl_fekernel_lookup(f"{self.cls}::{fn}".encode())
+        if not addr:
+            raise AttributeError(f"no pointwise kernel {self.cls}::{fn}")
+        return addr
+
+
+fekernels = _Kernels()
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return 0
+    return t.data_ptr()
+
+
+@dataclass
+class ResidualKernels:
+    subfield: str
+    part: int
+    r0: Optional[int]
+    r1: Optional[int]
+
+
+@dataclass
+class JacobianKernels:
+    subfield_trial: str
+    subfield_basis: str
+    part: int
+    j0: Optional[int]
+    j1: Optional[int]
+    j2: Optional[int]
+    j3: Optional[int]
+
+
+@dataclass
+class ProjectKernels:
+    subfield: str
+    f: int
+
+
+@dataclass
+class InterfaceResidualKernels:
+    subfield: str
+    part: int
+    face: int
+    r0: Optional[int]
+    r1: Optional[int] = None
+
+
+@dataclass
+class InterfaceJacobianKernels:
+    subfield_trial: str
+    subfield_basis: str
+    part: int
+    face: int
+    j0: Optional[int]
+    j1: Optional[int] = None
+    j2: Optional[int] = None
+    j3: Optional[int] = None
+
+
+class Context:
+    """One CUDA device and the stream all work is enqueued on (torch's current stream)."""
+
+    def __init__(self, device: int = 0, use_torch_stream: bool = True):
+        self.handle = ctypes.c_void_p()
+        check(C.lib().pl_context_create(device, ctypes.byref(self.handle)))
+        self.device = device
+        if use_torch_stream:
+            import torch
+
+            self.set_stream(torch.cuda.current_stream(device).cuda_stream)
+
+    def set_stream(self, stream_handle: int) -> None:
+        check(C.lib().pl_context_set_stream(self.handle, stream_handle))
+
+    def synchronize(self) -> None:
+        check(C.lib().pl_context_synchronize(self.handle))
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_context_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceMesh:
+    """A mesh resident on the device (pylith_b200.meshing.Mesh uploaded once)."""
+
+    def __init__(self, ctx: Context, mesh):
+        self.ctx = ctx
+        self.mesh = mesh
+        self.handle = ctypes.c_void_p()
+        cells = np.ascontiguousarray(mesh.cells, dtype=np.int32)
+        coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+        check(C.lib().pl_mesh_create(ctx.handle, mesh.cell_type, mesh.num_cells,
+                                     cells.ctypes.data, mesh.num_nodes, coords.ctypes.data,
+                                     ctypes.byref(self.handle)))
+        if mesh.cohesive is not None and len(mesh.cohesive):
+            coh = np.ascontiguousarray(mesh.cohesive, dtype=np.int32)
+            check(C.lib().pl_mesh_set_cohesive(self.handle, len(coh), coh.ctypes.data,
+                                               mesh.num_lagrange))
+
+    @property
+    def num_dof(self) -> int:
+        return int(C.lib().pl_mesh_num_dof(self.handle))
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_mesh_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Integrator:
+    def __init__(self, mesh: DeviceMesh):
+        self.dmesh = mesh
+        self.handle = ctypes.c_void_p()
+
+    def set_aux(self, name: str, storage: int, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        ncomp = v.shape[-1]
+        check(C.lib().pl_integrator_set_aux(self.handle, name.encode(), storage, ncomp, v.ctypes.data))
+
+    def get_aux(self, name: str, shape) -> np.ndarray:
+        out = np.zeros(shape, dtype=np.float64)
+        check(C.lib().pl_integrator_get_aux(self.handle, name.encode(), out.ctypes.data))
+        return out
+
+    def set_constants(self, constants: Sequence[float]) -> None:
+        c = np.ascontiguousarray(constants, dtype=np.float64)
+        check(C.lib().pl_integrator_set_constants(self.handle, len(c), c.ctypes.data if len(c) else None))
+
+    def set_scatter(self, scatter: int) -> None:
+        check(C.lib().pl_integrator_set_scatter(self.handle, scatter))
+
+    def compute_lhs_residual(self, t, dt, u, r, u_t=None, mode=INSERT) -> None:
+        check(C.lib().pl_compute_lhs_residual(self.handle, t, dt, _ptr(u), _ptr(u_t), _ptr(r), mode))
+
+    def compute_lhs_jacobian_action(self, t, dt, s_tshift, u, v, jv, mode=INSERT) -> None:
+        check(C.lib().pl_compute_lhs_jacobian_action(self.handle, t, dt, s_tshift, _ptr(u), _ptr(v),
+                                                     _ptr(jv), mode))
+
+    def compute_lhs_jacobian_action_f32(self, t, dt, v, jv, mode=INSERT) -> None:
+        check(C.lib().pl_compute_lhs_jacobian_action_f32(self.handle, t, dt, _ptr(v), _ptr(jv), mode))
+
+    def compute_lhs_residual_host(self, t, dt, u: np.ndarray, r: np.ndarray) -> None:
+        assert u.dtype == np.float64 and r.dtype == np.float64
+        check(C.lib().pl_compute_lhs_residual_host(self.handle, t, dt, u.ctypes.data, r.ctypes.data))
+
+    def compute_lhs_jacobian(self, t, dt, s_tshift, u, matrix: "Matrix") -> None:
+        check(C.lib().pl_compute_lhs_jacobian(self.handle, t, dt, s_tshift, _ptr(u), matrix.handle))
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_integrator_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class IntegratorDomain(Integrator):
+    """IntegratorDomain (libsrc/pylith/feassemble/IntegratorDomain.cc) over all or some cells."""
+
+    def __init__(self, mesh: DeviceMesh, cell_ids: Optional[np.ndarray] = None):
+        super().__init__(mesh)
+        ids = None if cell_ids is None else np.ascontiguousarray(cell_ids, dtype=np.int32)
+        check(C.lib().pl_integrator_domain_create(mesh.handle, 0 if ids is None else len(ids),
+                                                  None if ids is None else ids.ctypes.data,
+                                                  ctypes.byref(self.handle)))
+
+    def set_kernels_residual(self, kernels: Sequence[ResidualKernels]) -> None:
+        arr = (C.ResidualKernelsC * len(kernels))(
+            *[C.ResidualKernelsC(k.subfield.encode(), k.part, k.r0, k.r1) for k in kernels])
+        check(C.lib().pl_integrator_set_kernels_residual(self.handle, arr, len(kernels)))
+
+    def set_kernels_jacobian(self, kernels: Sequence[JacobianKernels]) -> None:
+        arr = (C.JacobianKernelsC * len(kernels))(
+            *[C.JacobianKernelsC(k.subfield_trial.encode(), k.subfield_basis.encode(), k.part,
+                                 k.j0, k.j1, k.j2, k.j3) for k in kernels])
+        check(C.lib().pl_integrator_set_kernels_jacobian(self.handle, arr, len(kernels)))
+
+    def set_kernels_update_state_vars(self, kernels: Sequence[ProjectKernels]) -> None:
+        arr = (C.ProjectKernelsC * len(kernels))(
+            *[C.ProjectKernelsC(k.subfield.encode(), k.f) for k in kernels])
+        check(C.lib().pl_integrator_set_kernels_update_state_vars(self.handle, arr, len(kernels)))
+
+    def update_state_vars(self, t, dt, u) -> None:
+        check(C.lib().pl_update_state_vars(self.handle, t, dt, _ptr(u)))
+
+
+class IntegratorInterface(Integrator):
+    """IntegratorInterface (libsrc/pylith/feassemble/IntegratorInterface.cc) over the mesh's
+    cohesive cells."""
+
+    def __init__(self, mesh: DeviceMesh):
+        super().__init__(mesh)
+        check(C.lib().pl_integrator_interface_create(mesh.handle, ctypes.byref(self.handle)))
+
+    def set_kernels_residual(self, kernels: Sequence[InterfaceResidualKernels]) -> None:
+        arr = (C.InterfaceResidualKernelsC * len(kernels))(
+            *[C.InterfaceResidualKernelsC(k.subfield.encode(), k.part, k.face, k.r0, k.r1)
+              for k in kernels])
+        check(C.lib().pl_integrator_interface_set_kernels_residual(self.handle, arr, len(kernels)))
+
+    def set_kernels_jacobian(self, kernels: Sequence[InterfaceJacobianKernels]) -> None:
+        arr = (C.InterfaceJacobianKernelsC * len(kernels))(
+            *[C.InterfaceJacobianKernelsC(k.subfield_trial.encode(), k.subfield_basis.encode(),
+                                          k.part, k.face, k.j0, k.j1, k.j2, k.j3) for k in kernels])
+        check(C.lib().pl_integrator_interface_set_kernels_jacobian(self.handle, arr, len(kernels)))
+
+
+class Matrix:
+    """Assembled Jacobian in 3x3-block CSR form on the device."""
+
+    def __init__(self, mesh: DeviceMesh):
+        self.dmesh = mesh
+        self.handle = ctypes.c_void_p()
+        check(C.lib().pl_matrix_create(mesh.handle, ctypes.byref(self.handle)))
+
+    def zero(self):
+        check(C.lib().pl_matrix_zero(self.handle))
+
+    def spmv(self, x, y):
+        check(C.lib().pl_matrix_spmv(self.handle, _ptr(x), _ptr(y)))
+
+    def to_scipy(self):
+        """Copy to a host scipy.sparse BSR matrix (synchronises)."""
+        import scipy.sparse as sp
+
+        nr, nb = ctypes.c_int64(), ctypes.c_int64()
+        check(C.lib().pl_matrix_info(self.handle, ctypes.byref(nr), ctypes.byref(nb), None, None, None))
+        nr, nb = nr.value, nb.value
+        h_rp = np.zeros(nr + 1, dtype=np.int32)
+        h_ci = np.zeros(nb, dtype=np.int32)
+        h_val = np.zeros((nb, 3, 3), dtype=np.float64)
+        check(C.lib().pl_matrix_copy_to_host(self.handle, h_rp.ctypes.data, h_ci.ctypes.data,
+                                             h_val.ctypes.data))
+        return sp.bsr_matrix((h_val, h_ci, h_rp), shape=(3 * nr, 3 * nr))
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_matrix_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,324 @@
+"""GPU parity: the CUDA cell loop (called through the C ABI) against the oracle on the same
+seeded meshes, fields and parameters. FP64 tolerance: relative L2 <= 1e-12 (the north-star
+bar); FP32 Jacobian action: relative L2 <= 1e-5."""
+import numpy as np
+import pytest
+
+import known_answers as KA
+from pylith_b200 import materials as MAT
+from pylith_b200 import meshing as M
+
+pytestmark = pytest.mark.gpu
+
+F1_ILE = "IsotropicLinearElasticity3D::f1v_infinitesimalStrain"
+JF3_ILE = "IsotropicLinearElasticity3D::Jf3vu_infinitesimalStrain"
+F1_GM = "IsotropicLinearGenMaxwell3D::f1v_infinitesimalStrain"
+JF3_GM = "IsotropicLinearGenMaxwell3D::Jf3vu_infinitesimalStrain"
+TOL64 = 1e-12
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ctx(torch_cuda):
+    from pylith_b200 import feassemble as FA
+
+    return FA.Context(0)
+
+
+def dev(torch, a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda()
+
+
+MESHES = {
+    "tet4": lambda: M.box_tet_delaunay(6000, seed=5),
+    "hex8": lambda: M.box_hex(6, 5, 4),
+    "hex27": lambda: M.box_hex27(3, 3, 2),
+    "tet4_unsorted": lambda: M.box_tet_delaunay(3000, seed=9, reorder=False),
+}
+
+
+def elastic_setup(mesh, seed=0, body_force=False):
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=seed)
+    bf = np.random.default_rng(seed + 1).standard_normal((mesh.num_cells, 3)) * 1e3 if body_force else None
+    return MAT.IsotropicLinearElasticity(rho, mu, K, bf)
+
+
+def oracle_aux(O, mat):
+    fields = [(mat.density[:, None], "cell")]
+    if mat.body_force is not None:
+        fields.append((mat.body_force, "cell"))
+    fields += [(mat.shear_modulus[:, None], "cell"), (mat.bulk_modulus[:, None], "cell")]
+    return O.AuxFields(fields)
+
+
+@pytest.mark.parametrize("kind", list(MESHES))
+@pytest.mark.parametrize("scatter", [0, 1])
+def test_elastic_residual_matches_oracle(oracle_lib, torch_cuda, ctx, kind, scatter):
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES[kind]()
+    mat = elastic_setup(mesh)
+    u = np.random.default_rng(2).standard_normal(mesh.num_nodes * 3)
+    r_ref = O.residual(mesh, u, oracle_aux(O, mat), f1=F1_ILE)
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm)
+    ig.set_scatter(scatter)
+    du = dev(torch, u)
+    dr = torch.full_like(du, np.nan)
+    ig.compute_lhs_residual(0.0, 0.0, du, dr)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), r_ref) <= TOL64
+    # ADD mode accumulates on top of the existing values
+    ig.compute_lhs_residual(0.0, 0.0, du, dr, mode=FA.ADD)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), 2 * r_ref) <= TOL64
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+def test_body_force_residual(oracle_lib, torch_cuda, ctx, kind):
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES[kind]()
+    mat = elastic_setup(mesh, body_force=True)
+    u = np.random.default_rng(3).standard_normal(mesh.num_nodes * 3) * 1e-3
+    r_ref = O.residual(mesh, u, oracle_aux(O, mat), f0="Elasticity::g0v_bodyforce", f1=F1_ILE)
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm)
+    du = dev(torch, u)
+    dr = torch.zeros_like(du)
+    ig.compute_lhs_residual(0.0, 0.0, du, dr)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), r_ref) <= TOL64
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8", "hex27"])
+def test_jacobian_action_and_assembly_match_oracle(oracle_lib, torch_cuda, ctx, kind):
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES[kind]()
+    mat = elastic_setup(mesh, seed=4)
+    aux = oracle_aux(O, mat)
+    J = O.assemble(mesh, O.jacobian_elements(mesh, aux, g3=JF3_ILE))
+    v = np.random.default_rng(5).standard_normal(mesh.num_nodes * 3)
+    jv_ref = J @ v
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm)
+    dv = dev(torch, v)
+    djv = torch.zeros_like(dv)
+    ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, None, dv, djv)
+    ctx.synchronize()
+    assert rel_l2(djv.cpu().numpy(), jv_ref) <= TOL64
+    # FP32 action (FP32 operands and accumulation, FP64 geometry)
+    dv32 = dv.float()
+    djv32 = torch.zeros_like(dv32)
+    ig.compute_lhs_jacobian_action_f32(0.0, 0.0, dv32, djv32)
+    ctx.synchronize()
+    assert rel_l2(djv32.double().cpu().numpy(), jv_ref) <= 1e-5
+    # assembled block-CSR Jacobian
+    A = FA.Matrix(dm)
+    ig.compute_lhs_jacobian(0.0, 0.0, 0.0, None, A)
+    Jg = A.to_scipy().tocsr()
+    assert abs(Jg - J).max() <= TOL64 * abs(J).max()
+    dy = torch.zeros_like(dv)
+    A.spmv(dv, dy)
+    ctx.synchronize()
+    assert rel_l2(dy.cpu().numpy(), jv_ref) <= TOL64
+
+
+def genmaxwell_setup(mesh, seed=0):
+    rng = np.random.default_rng(seed)
+    nc = mesh.num_cells
+    nq = M.QUAD_POINTS[mesh.cell_type]
+    rho, mu, K = MAT.lognormal_elastic(nc, seed=seed)
+    tau = MAT.genmaxwell_times(rho, np.sqrt(mu / rho), [1e18, 1e19, 1e20], [0.3, 0.3, 0.3])
+    ratio = np.tile([0.3, 0.3, 0.3], (nc, 1))
+    visc = rng.standard_normal((nc, nq, 18)) * 1e-5
+    total = rng.standard_normal((nc, nq, 6)) * 1e-5
+    return MAT.IsotropicLinearGenMaxwell(rho, mu, K, tau, ratio, visc, total)
+
+
+def genmaxwell_oracle_aux(O, g):
+    return O.AuxFields([(g.density[:, None], "cell"), (g.shear_modulus[:, None], "cell"),
+                        (g.bulk_modulus[:, None], "cell"), (g.maxwell_time, "cell"),
+                        (g.shear_modulus_ratio, "cell"), (g.viscous_strain, "qp"), (g.total_strain, "qp")])
+
+
+@pytest.mark.parametrize("kind", ["hex8", "tet4"])
+def test_genmaxwell_residual_jacobian_and_state_update(oracle_lib, torch_cuda, ctx, kind):
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES[kind]()
+    g = genmaxwell_setup(mesh)
+    dt = 1.0 * MAT.YEAR
+    aux = genmaxwell_oracle_aux(O, g)
+    u = np.random.default_rng(7).standard_normal(mesh.num_nodes * 3) * 1e-2
+    r_ref = O.residual(mesh, u, aux, f1=F1_GM, constants=[dt])
+    J = O.assemble(mesh, O.jacobian_elements(mesh, aux, g3=JF3_GM, constants=[dt]))
+    v = np.random.default_rng(8).standard_normal(mesh.num_nodes * 3)
+    visc_ref, total_ref = O.project_qp(
+        mesh, u, aux, ["IsotropicLinearGenMaxwell3D::viscousStrain_infinitesimalStrain_asVector",
+                       "Elasticity3D::infinitesimalStrain_asVector"], [18, 6], constants=[dt])
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = g.create_integrator(dm, dt)
+    du, dv = dev(torch, u), dev(torch, v)
+    dr, djv = torch.zeros_like(du), torch.zeros_like(du)
+    ig.compute_lhs_residual(0.0, dt, du, dr)
+    ig.compute_lhs_jacobian_action(0.0, dt, 0.0, du, dv, djv)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), r_ref) <= TOL64
+    assert rel_l2(djv.cpu().numpy(), J @ v) <= TOL64
+    ig.update_state_vars(0.0, dt, du)
+    ctx.synchronize()
+    nq = M.QUAD_POINTS[mesh.cell_type]
+    visc = ig.get_aux("viscous_strain", (mesh.num_cells, nq, 18))
+    total = ig.get_aux("total_strain", (mesh.num_cells, nq, 6))
+    assert rel_l2(visc, visc_ref) <= TOL64
+    assert rel_l2(total, total_ref) <= TOL64
+
+
+def test_genmaxwell_relaxation_known_answer_on_gpu(torch_cuda, ctx):
+    """The analytic relaxation of axialstrain_genmaxwell_soln.py, stepped on the GPU."""
+    from pylith_b200 import feassemble as FA
+
+    torch = torch_cuda
+    mesh = M.box_hex(2, 2, 2, lo=(-4000.0, -4000.0, -8000.0), hi=(4000.0, 4000.0, 0.0))
+    mu, K, lam, tau = KA.genmaxwell_params()
+    nc, nq, e0 = mesh.num_cells, 8, KA.GM_E0
+    g = MAT.IsotropicLinearGenMaxwell(
+        np.full(nc, KA.GM_DENSITY), np.full(nc, mu), np.full(nc, K), np.tile(tau, (nc, 1)),
+        np.tile(KA.GM_RATIO, (nc, 1)), np.tile([-e0 / 3, -e0 / 3, 2 * e0 / 3, 0, 0, 0] * 3, (nc, nq, 1)),
+        np.tile([0, 0, e0, 0, 0, 0.0], (nc, nq, 1)))
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = g.create_integrator(dm, KA.GM_DT)
+    X = mesh.coords
+    u = np.stack([0 * X[:, 0], 0 * X[:, 1], e0 * (X[:, 2] + 8000.0)], axis=1).ravel()
+    du = dev(torch, u)
+    dr = torch.zeros_like(du)
+    for step in range(1, KA.GM_STEPS + 1):
+        ig.compute_lhs_residual(step * KA.GM_DT, KA.GM_DT, du, dr)
+        ig.update_state_vars(step * KA.GM_DT, KA.GM_DT, du)
+        ctx.synchronize()
+        sigma = KA.stress_from_residual(X, dr.cpu().numpy(), 8000.0**3)
+        np.testing.assert_allclose(np.diag(sigma), KA.genmaxwell_stress(step * KA.GM_DT), rtol=1e-10)
+
+
+def fault_setup(nx=4, ny=3, nz=3):
+    mesh = M.insert_fault_x(M.box_hex(nx, ny, nz))
+    rng = np.random.default_rng(11)
+    slip = rng.standard_normal((mesh.num_lagrange, 3))
+    fault = MAT.FaultCohesiveKin(slip, ref_dir_1=(0, 0, 1), ref_dir_2=(0.5, 0, 0.5))
+    return mesh, fault
+
+
+def test_cohesive_residual_jacobian_action_and_assembly(oracle_lib, torch_cuda, ctx):
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh, fault = fault_setup()
+    u = np.random.default_rng(12).standard_normal(mesh.num_dof)
+    r_ref = O.cohesive_residual(mesh, u, fault.slip, fault.constants)
+    Jc = O.cohesive_jacobian(mesh, fault.constants)
+    v = np.random.default_rng(13).standard_normal(mesh.num_dof)
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = fault.create_integrator(dm)
+    du, dv = dev(torch, u), dev(torch, v)
+    dr, djv = torch.zeros_like(du), torch.zeros_like(du)
+    ig.compute_lhs_residual(0.0, 0.0, du, dr)
+    ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, du, dv, djv)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), r_ref) <= TOL64
+    assert rel_l2(djv.cpu().numpy(), Jc @ v) <= TOL64
+    A = FA.Matrix(dm)
+    ig.compute_lhs_jacobian(0.0, 0.0, 0.0, None, A)
+    Jg = A.to_scipy().tocsr()
+    assert abs(Jg - Jc).max() <= 1e-12 * abs(Jc).max()
+
+
+def test_full_fault_problem_residual(oracle_lib, torch_cuda, ctx):
+    """Domain + interface integrators summed into one local vector (TimeDependent's loop over
+    integrators, TimeDependent.cc:659-662)."""
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh, fault = fault_setup(6, 4, 3)
+    mat = elastic_setup(mesh, seed=21)
+    u = np.random.default_rng(14).standard_normal(mesh.num_dof)
+    r_ref = np.zeros(mesh.num_dof)
+    r_ref[:3 * mesh.num_nodes] = O.residual(mesh, u[:3 * mesh.num_nodes], oracle_aux(O, mat), f1=F1_ILE)
+    O.cohesive_residual(mesh, u, fault.slip, fault.constants, r=r_ref)
+    dm = FA.DeviceMesh(ctx, mesh)
+    igs = [mat.create_integrator(dm), fault.create_integrator(dm)]
+    du = dev(torch, u)
+    dr = torch.zeros_like(du)
+    for i, ig in enumerate(igs):
+        ig.compute_lhs_residual(0.0, 0.0, du, dr, mode=FA.INSERT if i == 0 else FA.ADD)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), r_ref) <= TOL64
+
+
+def test_host_buffer_entry_point(oracle_lib, torch_cuda, ctx):
+    from pylith_b200 import feassemble as FA
+
+    O = oracle_lib
+    mesh = MESHES["tet4"]()
+    mat = elastic_setup(mesh)
+    u = np.random.default_rng(2).standard_normal(mesh.num_nodes * 3)
+    r_ref = O.residual(mesh, u, oracle_aux(O, mat), f1=F1_ILE)
+    ig = mat.create_integrator(FA.DeviceMesh(ctx, mesh))
+    r = np.zeros_like(u)
+    ig.compute_lhs_residual_host(0.0, 0.0, u, r)
+    assert rel_l2(r, r_ref) <= TOL64
+
+
+def test_unknown_kernel_is_rejected(torch_cuda, ctx):
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+    import oracle as O
+
+    mesh = MESHES["hex8"]()
+    ig = FA.IntegratorDomain(FA.DeviceMesh(ctx, mesh))
+    # the oracle's restated kernel has the right signature but is not a registered kernel
+    foreign = O.kernel(F1_ILE, "oracle")
+    with pytest.raises(_lib.PylithB200Error) as e:
+        ig.set_kernels_residual([FA.ResidualKernels("displacement", FA.LHS, None, foreign)])
+    assert e.value.code == -2
+    with pytest.raises(_lib.PylithB200Error) as e:
+        ig.compute_lhs_residual(0.0, 0.0, None, None)
+    assert e.value.code == -1
+
+
+def test_inverted_cell_is_reported(torch_cuda, ctx):
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+
+    torch = torch_cuda
+    mesh = M.box_hex(2, 2, 2)
+    mesh.cells[0] = mesh.cells[0][[1, 0, 3, 2, 5, 4, 7, 6]]  # mirror cell 0 -> negative |J|
+    mat = elastic_setup(mesh)
+    ig = mat.create_integrator(FA.DeviceMesh(ctx, mesh))
+    du = torch.zeros(mesh.num_nodes * 3, dtype=torch.float64, device="cuda")
+    dr = torch.zeros_like(du)
+    ig.compute_lhs_residual(0.0, 0.0, du, dr)
+    with pytest.raises(_lib.PylithB200Error) as e:
+        ctx.synchronize()
+    assert e.value.code == -6
+    ctx.synchronize()  # the flag is cleared after it is reported
