@@ -106,7 +106,8 @@ enum { PL_INSERT = 0, PL_ADD = 1 };
 enum {
     PL_SCATTER_AUTO = 0,      /* library choice (cell-block gather when available) */
     PL_SCATTER_ATOMIC = 1,    /* one thread per cell, FP64 atomics into the output */
-    PL_SCATTER_BLOCKED = 2    /* cell blocks in shared memory, deterministic gather */
+    PL_SCATTER_BLOCKED = 2    /* cell blocks staged in shared memory, per-node gather, one FP64
+                                 reduction per node shared between blocks (P1 tetrahedra) */
 };
 
 typedef struct pl_context_s* pl_context;
@@ -166,6 +167,8 @@ void* pl_fekernel_lookup(const char* name);
 
 /* ---- context -------------------------------------------------------------------------- */
 int pl_context_create(int device, pl_context* out);
+/* Destroy calls may come in any order: an object still referenced by a dependent one (a mesh by
+ * an integrator, a context by a mesh) is released when its last dependent is destroyed. */
 int pl_context_destroy(pl_context ctx);
 /* Enqueue all work on a caller-owned cudaStream_t; NULL is CUDA's legacy default stream
  * (torch's default stream). A new context starts on its own non-blocking stream. */
@@ -262,6 +265,33 @@ int pl_matrix_copy_to_host(pl_matrix mat, int32_t* row_ptr_host, int32_t* col_id
                            double* values_host);
 int pl_matrix_spmv(pl_matrix mat, const double* x_dev, double* y_dev);
 int pl_matrix_destroy(pl_matrix mat);
+
+/* ---- device Krylov solver (replaces the PETSc KSP of the quasi-static step;
+ *      libsrc/pylith/materials/Elasticity.cc:298-330, petsc/Options.cc:320-331) ------------ */
+/* Solves A x = b with A = -(sum of the added domain integrators' Jacobians), on the DOFs whose
+ * constrained flag is 0 (Dirichlet DOFs of x are returned as 0). Preconditioned conjugate
+ * gradients with point-block Jacobi. PL_SOLVER_FP32_REFINED runs the inner iterations in FP32
+ * (FP64 dot products) inside FP64 iterative refinement.
+ * Meshes with cohesive cells are solved in the reduced space of the slip constraint
+ * u+ = u- + d: the positive-side DOFs of fault nodes follow the negative side and the two sides'
+ * equations are summed, where the Lagrange-multiplier terms of f0u_neg/f0u_pos cancel; this
+ * reduced operator is SPD. Vectors span the whole local vector (nodes, then Lagrange nodes);
+ * the Lagrange-multiplier entries of x are returned as 0. */
+enum { PL_SOLVER_FP64 = 0, PL_SOLVER_FP32_REFINED = 1 };
+typedef struct pl_solver_s* pl_solver;
+int pl_solver_create(pl_mesh mesh, const uint8_t* constrained_host, pl_solver* out);
+int pl_solver_add_integrator(pl_solver solver, pl_integrator integ);
+int pl_solver_set_tolerances(pl_solver solver, double rtol, double atol, int max_iter);
+int pl_solver_set_precision(pl_solver solver, int precision, double inner_rtol);
+/* Builds the preconditioner at (t, dt). */
+int pl_solver_setup(pl_solver solver, double t, double dt);
+int pl_solver_solve(pl_solver solver, const double* b_dev, double* x_dev);
+/* Sets the positive side of every fault node to u+ = u- + d from the interface integrator's
+ * slip and reference directions (planar faults: one normal per fault node). */
+int pl_solver_apply_fault_slip(pl_solver solver, pl_integrator iface, double* u_dev);
+int pl_solver_get_stats(pl_solver solver, int* iterations, int* inner_iterations,
+                        int* outer_iterations, double* rel_residual);
+int pl_solver_destroy(pl_solver solver);
 
 #ifdef __cplusplus
 }

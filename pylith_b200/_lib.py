@@ -101,7 +101,18 @@ SIGNATURES = {
     "pl_matrix_copy_to_host": (_I, [_P, _P, _P, _P]),
     "pl_matrix_spmv": (_I, [_P, _P, _P]),
     "pl_matrix_destroy": (_I, [_P]),
+    "pl_solver_create": (_I, [_P, _P, ctypes.POINTER(_P)]),
+    "pl_solver_add_integrator": (_I, [_P, _P]),
+    "pl_solver_set_tolerances": (_I, [_P, _D, _D, _I]),
+    "pl_solver_set_precision": (_I, [_P, _I, _D]),
+    "pl_solver_setup": (_I, [_P, _D, _D]),
+    "pl_solver_solve": (_I, [_P, _P, _P]),
+    "pl_solver_get_stats": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                 ctypes.POINTER(_D)]),
+    "pl_solver_apply_fault_slip": (_I, [_P, _P, _P]),
+    "pl_solver_destroy": (_I, [_P]),
 }
+PL_SOLVER_FP64, PL_SOLVER_FP32_REFINED = 0, 1
 
 _lib = None
 

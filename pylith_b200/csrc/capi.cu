@@ -179,8 +179,7 @@ int pl_context_create(int device, pl_context* out) {
     return PL_OK;
 }
 
-int pl_context_destroy(pl_context c) {
-    if (!c) return PL_OK;
+static void context_free(pl_context c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     if (c->d_err) cudaFree(c->d_err);
@@ -188,6 +187,15 @@ int pl_context_destroy(pl_context c) {
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
+}
+
+int pl_context_destroy(pl_context c) {
+    if (!c) return PL_OK;
+    if (c->refs > 0) {
+        c->destroy_requested = true;
+        return PL_OK;
+    }
+    context_free(c);
     return PL_OK;
 }
 
@@ -238,6 +246,7 @@ int pl_mesh_create(pl_context c, int cell_type, int64_t num_cells, const int32_t
     PLB_CUDA(cudaSetDevice(c->device));
     pl_mesh m = new pl_mesh_s();
     m->ctx = c;
+    c->refs++;
     m->cell_type = cell_type;
     m->nen = nen;
     m->nq = quad_points(cell_type);
@@ -277,8 +286,8 @@ int pl_mesh_set_cohesive(pl_mesh m, int64_t ncoh, const int32_t* coh, int64_t nl
 }
 
 
-int pl_mesh_destroy(pl_mesh m) {
-    if (!m) return PL_OK;
+static void mesh_free(pl_mesh m) {
+    pl_context c = m->ctx;
     cudaSetDevice(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
     if (m->d_cells) cudaFree(m->d_cells);
@@ -286,7 +295,26 @@ int pl_mesh_destroy(pl_mesh m) {
     if (m->d_coh) cudaFree(m->d_coh);
     if (m->blocked) free_blocked_layout(m->blocked);
     delete m;
+    if (--c->refs == 0 && c->destroy_requested) context_free(c);
+}
+
+int pl_mesh_destroy(pl_mesh m) {
+    if (!m) return PL_OK;
+    if (m->refs > 0) {
+        m->destroy_requested = true;
+        return PL_OK;
+    }
+    mesh_free(m);
     return PL_OK;
+}
+
+extern "C++" {
+namespace plb {
+void mesh_retain(pl_mesh_s* m) { m->refs++; }
+void mesh_release(pl_mesh_s* m) {
+    if (--m->refs == 0 && m->destroy_requested) mesh_free(m);
+}
+}  // namespace plb
 }
 
 int64_t pl_mesh_num_dof(pl_mesh m) { return m ? 3 * (m->nnodes + m->nlag) : 0; }
@@ -297,10 +325,12 @@ int pl_integrator_domain_create(pl_mesh m, int64_t num_ids, const int32_t* ids, 
     *out = nullptr;
     pl_integrator ig = new pl_integrator_s();
     ig->mesh = m;
+    mesh_retain(m);
     if (ids && num_ids > 0) {
         for (int64_t i = 0; i < num_ids; ++i)
             if (ids[i] < 0 || ids[i] >= m->ncells) {
                 delete ig;
+                mesh_release(m);
                 return fail(PL_ERR_INVALID_ARG, "cell id out of range");
             }
         ig->ncells = num_ids;
@@ -309,6 +339,7 @@ int pl_integrator_domain_create(pl_mesh m, int64_t num_ids, const int32_t* ids, 
         int rc = upload(&ig->d_cell_ids, ids, num_ids, m->ctx->stream);
         if (rc) {
             delete ig;
+            mesh_release(m);
             return rc;
         }
     } else {
@@ -323,6 +354,7 @@ int pl_integrator_interface_create(pl_mesh m, pl_integrator* out) {
     if (m->ncoh == 0) return fail(PL_ERR_INVALID_ARG, "mesh has no cohesive cells");
     pl_integrator ig = new pl_integrator_s();
     ig->mesh = m;
+    mesh_retain(m);
     ig->is_interface = true;
     ig->ncells = m->ncoh;
     *out = ig;
@@ -506,7 +538,9 @@ int pl_integrator_destroy(pl_integrator ig) {
     for (AuxField& f : ig->aux)
         if (f.d) cudaFree(f.d);
     if (ig->d_cell_ids) cudaFree(ig->d_cell_ids);
+    pl_mesh m = ig->mesh;
     delete ig;
+    mesh_release(m);
     return PL_OK;
 }
 

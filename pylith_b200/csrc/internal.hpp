@@ -50,16 +50,24 @@ struct BlockedLayout {
     int32_t* d_node_ids = nullptr;          // global node of each block-local slot (sorted per block)
     uint16_t* d_local_cells = nullptr;      // [ncells][4] block-local slot of each cell corner
     uint8_t* d_slot_shared = nullptr;       // per slot: 1 if other blocks also touch the node
+    uint16_t* d_inc_off = nullptr;          // per block: ns+1 offsets into the block's incidence list
+    uint16_t* d_inc = nullptr;              // [num_blocks][4 * cells_per_block] (cell * 4 + corner)
     int64_t num_shared_nodes = 0;
-    int32_t* d_shared_node = nullptr;       // nodes touched by more than one block
     int64_t num_untouched = 0;
-    int32_t* d_untouched = nullptr;         // nodes no cell touches
     size_t device_bytes = 0;
 };
 
+void mesh_retain(pl_mesh_s* m);
+void mesh_release(pl_mesh_s* m);
+
 }  // namespace plb
 
+// Object lifetimes: meshes hold a reference on their context, integrators, matrices and solvers
+// on their mesh; a destroy request on an object that is still referenced is deferred until the
+// last dependent object is destroyed, so any destroy order is safe.
 struct pl_context_s {
+    int refs = 0;
+    bool destroy_requested = false;
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
@@ -72,6 +80,8 @@ struct pl_context_s {
 };
 
 struct pl_mesh_s {
+    int refs = 0;
+    bool destroy_requested = false;
     pl_context ctx = nullptr;
     int cell_type = 0;
     int nen = 0;

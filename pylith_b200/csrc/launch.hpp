@@ -12,6 +12,7 @@ struct pl_integrator_s;
 namespace plb {
 
 struct DomainParams;
+void launch_domain_diag_blocks(const DomainParams& p, int cell, int rheo, double* diag, cudaStream_t s);
 struct BlockedLayout;
 
 // Counts kernel launches made by this library (reported by pl_kernel_launches).

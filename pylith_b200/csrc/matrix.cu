@@ -113,6 +113,7 @@ int pl_matrix_create(pl_mesh m, pl_matrix* out) {
     PLB_CUDA(cudaSetDevice(m->ctx->device));
     pl_matrix A = new pl_matrix_s();
     A->mesh = m;
+    mesh_retain(m);
     A->nrows = nrows;
     A->nnzb = (int64_t)ci.size();
     cudaStream_t s = m->ctx->stream;
@@ -220,7 +221,9 @@ int pl_matrix_destroy(pl_matrix A) {
     if (A->d_val) cudaFree(A->d_val);
     if (A->d_cell_pos) cudaFree(A->d_cell_pos);
     if (A->d_coh_pos) cudaFree(A->d_coh_pos);
+    pl_mesh m = A->mesh;
     delete A;
+    mesh_release(m);
     return PL_OK;
 }
 

@@ -1,0 +1,689 @@
+// Device Krylov solver for the quasi-static step: preconditioned conjugate gradients on
+// A = -J (J = sum of the registered integrators' Jacobian actions, negative definite for the
+// elasticity kernels, f1 = -sigma and Jf3 = -C), restricted to the unconstrained DOFs.
+//
+// Replaces the PETSc KSP the reference configures for these problems (defaults in
+// libsrc/pylith/materials/Elasticity.cc:298-330, tolerances in
+// libsrc/pylith/petsc/Options.cc:320-331). Preconditioner: point-block Jacobi (inverse 3x3
+// node blocks of A, the "vpbjacobi" idea the reference uses on faults), optionally wrapped in
+// a Chebyshev polynomial. Two precisions:
+//   * FP64: every vector and reduction in FP64;
+//   * FP32 refined: inner PCG in FP32 vectors and FP32 operator application with FP64 dot
+//     products, inside FP64 iterative refinement (outer residual b - A x in FP64).
+// Reductions are two-pass and deterministic (per-CTA partials, then one CTA in fixed order).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "domain_kernels.cuh"
+#include "internal.hpp"
+#include "launch.hpp"
+
+namespace plb {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 296;  // 2 per SM
+
+enum Scalar { S_RZ = 0, S_RZ_OLD, S_PQ, S_RR, S_ALPHA, S_BETA, S_BB, S_COUNT };
+
+template <typename T>
+PL_D double to_d(T v) { return (double)v; }
+
+// Block-level sum of up to 2 values; thread 0 of each block writes partials[blk*2 + k].
+PL_D void block_sum2(double a, double b, double* partials) {
+    __shared__ double sa[kRedThreads / 32], sb[kRedThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sa[w] = a;
+        sb[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = l < (int)(blockDim.x >> 5) ? sa[l] : 0.0;
+        b = l < (int)(blockDim.x >> 5) ? sb[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (l == 0) {
+            partials[2 * blockIdx.x] = a;
+            partials[2 * blockIdx.x + 1] = b;
+        }
+    }
+}
+
+// Sum the partials of the previous pass in a fixed order into scal[i0], scal[i1].
+__global__ void k_finish2(const double* __restrict__ partials, int nblk, double* scal, int i0, int i1) {
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+        a += partials[2 * i];
+        b += partials[2 * i + 1];
+    }
+    __shared__ double sa[32], sb[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sa[w] = a;
+        sb[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = l < (int)(blockDim.x >> 5) ? sa[l] : 0.0;
+        b = l < (int)(blockDim.x >> 5) ? sb[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (l == 0) {
+            if (i0 >= 0) scal[i0] = a;
+            if (i1 >= 0) scal[i1] = b;
+        }
+    }
+}
+
+// dots (a.b, c.d) over unconstrained DOFs.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dot2(const T* a, const T* b, const T* c, const T* d,
+                                                      const uint8_t* mask, int64_t n, double* partials) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (mask[i]) continue;
+        s0 += to_d(a[i]) * to_d(b[i]);
+        if (c) s1 += to_d(c[i]) * to_d(d[i]);
+    }
+    block_sum2(s0, s1, partials);
+}
+
+// z = P^{-1} r with point blocks; constrained entries of r are zero and P^{-1} is the identity
+// on them, so z stays zero there.
+template <typename T>
+PL_D void apply_pinv(const T* pinv, const T* r, int64_t node, T out[3]) {
+    const T* B = pinv + 9 * node;
+    const T r0 = r[3 * node], r1 = r[3 * node + 1], r2 = r[3 * node + 2];
+    out[0] = B[0] * r0 + B[1] * r1 + B[2] * r2;
+    out[1] = B[3] * r0 + B[4] * r1 + B[5] * r2;
+    out[2] = B[6] * r0 + B[7] * r1 + B[8] * r2;
+}
+
+// r := b (masked), z := P^{-1} r, p := z; partial (r.z, r.r).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_cg_init(const T* b, const uint8_t* mask, const T* pinv, int64_t nnodes,
+                                                         T* r, T* z, T* p, double* partials) {
+    double rz = 0.0, rr = 0.0;
+    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) r[3 * nd + k] = mask[3 * nd + k] ? T(0) : b[3 * nd + k];
+        T zz[3];
+        apply_pinv(pinv, r, nd, zz);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            z[3 * nd + k] = zz[k];
+            p[3 * nd + k] = zz[k];
+            rz += to_d(r[3 * nd + k]) * to_d(zz[k]);
+            rr += to_d(r[3 * nd + k]) * to_d(r[3 * nd + k]);
+        }
+    }
+    block_sum2(rz, rr, partials);
+}
+
+// q holds J p (not yet negated). A p = -q on free DOFs. Partial of p.(A p).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_cg_pq(const T* p, const T* q, const uint8_t* mask, int64_t n,
+                                                       double* partials) {
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (!mask[i]) s -= to_d(p[i]) * to_d(q[i]);
+    block_sum2(s, 0.0, partials);
+}
+
+// alpha = rz / pq; x += alpha p; r -= alpha A p (= r + alpha q); z = P^{-1} r; partial (r.z, r.r).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_cg_update(T* x, T* r, const T* p, const T* q, T* z, const uint8_t* mask,
+                                                           const T* pinv, int64_t nnodes, const double* scal,
+                                                           double* partials) {
+    const double pq = scal[S_PQ];
+    const T alpha = (T)(pq != 0.0 ? scal[S_RZ] / pq : 0.0);
+    double rz = 0.0, rr = 0.0;
+    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = 3 * nd + k;
+            if (!mask[i]) {
+                x[i] += alpha * p[i];
+                r[i] += alpha * q[i];
+            }
+        }
+        T zz[3];
+        apply_pinv(pinv, r, nd, zz);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            z[3 * nd + k] = zz[k];
+            rz += to_d(r[3 * nd + k]) * to_d(zz[k]);
+            rr += to_d(r[3 * nd + k]) * to_d(r[3 * nd + k]);
+        }
+    }
+    block_sum2(rz, rr, partials);
+}
+
+// beta = rz / rz_old; p = z + beta p.
+template <typename T>
+__global__ void k_cg_pupdate(T* p, const T* z, int64_t n, double* scal) {
+    const double beta = scal[S_RZ_OLD] != 0.0 ? scal[S_RZ] / scal[S_RZ_OLD] : 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + (T)beta * p[i];
+}
+
+__global__ void k_copy_scalar(double* scal, int from, int to) { scal[to] = scal[from]; }
+
+// Point-block Jacobi: invert each node's 3x3 block of A = -J with constrained rows/columns
+// replaced by the identity.
+__global__ void k_invert_blocks(const double* __restrict__ diagJ, const uint8_t* __restrict__ mask, int64_t nnodes,
+                                double* pinv, float* pinv32) {
+    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
+        double A[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const bool ci = mask[3 * nd + i], cj = mask[3 * nd + j];
+                A[i][j] = (ci || cj) ? (i == j ? 1.0 : 0.0) : -diagJ[9 * nd + 3 * i + j];
+            }
+        double inv[3][3];
+        const double det = invert3(A, inv);
+        const bool ok = det != 0.0 && isfinite(det);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const double v = ok ? inv[i][j] : (i == j ? 1.0 : 0.0);
+                pinv[9 * nd + 3 * i + j] = v;
+                pinv32[9 * nd + 3 * i + j] = (float)v;
+            }
+    }
+}
+
+template <typename T>
+__global__ void k_masked_copy(const double* src, const uint8_t* mask, int64_t n, T* dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = mask[i] ? T(0) : (T)src[i];
+}
+
+// r64 = b - A x = b + J x on free DOFs (q holds J x).
+__global__ void k_outer_residual(const double* b, const double* Jx, const uint8_t* mask, int64_t n, double* r,
+                                 float* r32, double* partials) {
+    double rr = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = mask[i] ? 0.0 : b[i] + Jx[i];
+        r[i] = v;
+        r32[i] = (float)v;
+        rr += v * v;
+    }
+    block_sum2(rr, 0.0, partials);
+}
+
+__global__ void k_add_correction(double* x, const float* d, const uint8_t* mask, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (!mask[i]) x[i] += (double)d[i];
+}
+
+// Diagonal 3x3 blocks of J from the registered Jf3 (thread per cell, reductions per node).
+template <int CELL, int RHEO>
+__global__ void __launch_bounds__(128) k_domain_diag_blocks(DomainParams p, double* diag) {
+    using E = Elem<CELL>;
+    using L = AuxLayout<RHEO, false>;
+    const AuxOffsets<RHEO, false> aoff;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < p.ncells; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t mc = p.cell_ids ? p.cell_ids[c] : c;
+        const int32_t* cn = p.cells + mc * E::nen;
+        double X[E::ngeom][3];
+#pragma unroll
+        for (int k = 0; k < E::ngeom; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)cn[E::corner(k)] + i];
+        double a[L::size];
+        L::load_cell(p, c, a);
+#pragma unroll 1
+        for (int q = 0; q < E::nq; ++q) {
+            Geom g;
+            E::geom(X, q, &g);
+            L::load_qp(p, c, q, E::nq, a);
+            double x[3] = {0, 0, 0};
+            double Jf3[81];
+#pragma unroll
+            for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
+            call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
+#pragma unroll 1
+            for (int n = 0; n < E::nen; ++n) {
+                double gr[3];
+                E::grad(g, q, n, gr);
+                double* blk = diag + 9 * (int64_t)cn[n];
+#pragma unroll
+                for (int f = 0; f < 3; ++f)
+#pragma unroll
+                    for (int gg = 0; gg < 3; ++gg) {
+                        double v = 0.0;
+#pragma unroll
+                        for (int df = 0; df < 3; ++df)
+#pragma unroll
+                            for (int dg = 0; dg < 3; ++dg) v += gr[df] * Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * gr[dg];
+                        red_add(&blk[f * 3 + gg], g.wdetJ * v);
+                    }
+            }
+        }
+    }
+}
+
+void launch_domain_diag_blocks(const DomainParams& p, int cell, int rheo, double* diag, cudaStream_t s) {
+    if (p.ncells == 0) return;
+    const int64_t b = (p.ncells + 127) / 128;
+    const int gr = (int)std::min<int64_t>(b, 148 * 64);
+#define PLB_DIAG(C, R) k_domain_diag_blocks<C, R><<<gr, 128, 0, s>>>(p, diag)
+    if (cell == TET4) { if (rheo == RHEO_ILE) PLB_DIAG(TET4, RHEO_ILE); else PLB_DIAG(TET4, RHEO_GENMAXWELL); }
+    else if (cell == HEX8) { if (rheo == RHEO_ILE) PLB_DIAG(HEX8, RHEO_ILE); else PLB_DIAG(HEX8, RHEO_GENMAXWELL); }
+    else { if (rheo == RHEO_ILE) PLB_DIAG(HEX27, RHEO_ILE); else PLB_DIAG(HEX27, RHEO_GENMAXWELL); }
+#undef PLB_DIAG
+    count_launch();
+}
+
+static int vec_grid(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 8); }
+
+// Faults are solved in the reduced space of the slip constraint u+ = u- + d: the positive-side
+// DOFs of every fault node follow the negative side ("unfold"), and the equations of both sides
+// are summed onto the negative side ("fold"), where the Lagrange-multiplier terms cancel
+// (f0u_neg = -lambda, f0u_pos = +lambda). The reduced operator P^T (-J) P is SPD.
+template <typename T>
+__global__ void k_fault_unfold(T* v, const int32_t* __restrict__ neg, const int32_t* __restrict__ pos, int64_t npairs) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * npairs; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = i / 3, c = i % 3;
+        v[3 * (int64_t)pos[k] + c] = v[3 * (int64_t)neg[k] + c];
+    }
+}
+
+template <typename T>
+__global__ void k_fault_fold(T* v, const int32_t* __restrict__ neg, const int32_t* __restrict__ pos, int64_t npairs) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * npairs; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = i / 3, c = i % 3;
+        v[3 * (int64_t)neg[k] + c] += v[3 * (int64_t)pos[k] + c];
+    }
+}
+
+__global__ void k_fault_fold_blocks(double* diag, const int32_t* __restrict__ neg, const int32_t* __restrict__ pos,
+                                    int64_t npairs) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 9 * npairs; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = i / 9, c = i % 9;
+        diag[9 * (int64_t)neg[k] + c] += diag[9 * (int64_t)pos[k] + c];
+    }
+}
+
+// u+ = u- + d, d = n slip[0] + t1 slip[1] + t2 slip[2] with the fault's tangential directions
+// (BoundaryDirections::tangential_directions, the same construction f0l_slip uses).
+__global__ void k_fault_apply_slip(double* u, const int32_t* __restrict__ neg, const int32_t* __restrict__ pos,
+                                   const double* __restrict__ normal, const double* __restrict__ slip, int64_t npairs,
+                                   double r10, double r11, double r12, double r20, double r21, double r22) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < npairs; k += (int64_t)gridDim.x * blockDim.x) {
+        const double n[3] = {normal[3 * k], normal[3 * k + 1], normal[3 * k + 2]};
+        const double ref1[3] = {r10, r11, r12}, ref2[3] = {r20, r21, r22};
+        double t1[3], t2[3];
+        pw::tangential_directions(t1, t2, ref1, ref2, n);
+        for (int c = 0; c < 3; ++c) {
+            const double d = n[c] * slip[3 * k] + t1[c] * slip[3 * k + 1] + t2[c] * slip[3 * k + 2];
+            u[3 * (int64_t)pos[k] + c] = u[3 * (int64_t)neg[k] + c] + d;
+        }
+    }
+}
+
+}  // namespace plb
+
+using namespace plb;
+
+struct pl_solver_s {
+    pl_mesh mesh = nullptr;
+    std::vector<pl_integrator> ops;
+    int64_t n = 0;       // DOFs (3 per node)
+    int64_t nnodes = 0;  // node rows
+    uint8_t* d_mask = nullptr;
+    double* d_diag = nullptr;
+    double* d_pinv = nullptr;
+    float* d_pinv32 = nullptr;
+    double *d_r = nullptr, *d_p = nullptr, *d_q = nullptr, *d_z = nullptr, *d_x = nullptr;
+    float *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_z = nullptr, *f_x = nullptr;
+    double* d_scal = nullptr;
+    double* d_partials = nullptr;
+    int64_t npairs = 0;               // fault nodes (Lagrange nodes)
+    int32_t* d_pair_neg = nullptr;    // negative-side node of each fault node
+    int32_t* d_pair_pos = nullptr;    // positive-side node
+    double* d_pair_normal = nullptr;  // fault normal at each fault node
+    double rtol = 1e-12, atol = 0.0, inner_rtol = 1e-5;
+    int max_iter = 10000, precision = 0, check_every = 10;
+    double t = 0.0, dt = 0.0;
+    int iterations = 0, inner_iterations = 0, outer_iterations = 0;
+    double rel_residual = 0.0;
+    bool ready = false;
+};
+
+namespace {
+
+template <typename T>
+void fault_unfold(pl_solver S, T* v) {
+    if (S->npairs == 0) return;
+    k_fault_unfold<T><<<vec_grid(3 * S->npairs), 256, 0, S->mesh->ctx->stream>>>(v, S->d_pair_neg, S->d_pair_pos, S->npairs);
+    count_launch();
+}
+
+template <typename T>
+void fault_fold(pl_solver S, T* v) {
+    if (S->npairs == 0) return;
+    k_fault_fold<T><<<vec_grid(3 * S->npairs), 256, 0, S->mesh->ctx->stream>>>(v, S->d_pair_neg, S->d_pair_pos, S->npairs);
+    count_launch();
+}
+
+// out = P^T J P v (the unfold writes the positive-side entries of v in place).
+int apply_J(pl_solver S, const double* v, double* out) {
+    fault_unfold(S, const_cast<double*>(v));
+    for (size_t i = 0; i < S->ops.size(); ++i) {
+        int rc = pl_compute_lhs_jacobian_action(S->ops[i], S->t, S->dt, 0.0, nullptr, v, out, i == 0 ? PL_INSERT : PL_ADD);
+        if (rc) return rc;
+    }
+    fault_fold(S, out);
+    return PL_OK;
+}
+
+int apply_J32(pl_solver S, const float* v, float* out) {
+    fault_unfold(S, const_cast<float*>(v));
+    for (size_t i = 0; i < S->ops.size(); ++i) {
+        int rc = pl_compute_lhs_jacobian_action_f32(S->ops[i], S->t, S->dt, v, out, i == 0 ? PL_INSERT : PL_ADD);
+        if (rc) return rc;
+    }
+    fault_fold(S, out);
+    return PL_OK;
+}
+
+template <typename T>
+int pcg(pl_solver S, const T* b, T* x, double rtol, double atol, int max_iter, const T* pinv, T* r, T* p, T* q, T* z,
+        int* iters, double* rel) {
+    cudaStream_t s = S->mesh->ctx->stream;
+    const int64_t n = S->n, nn = S->nnodes;
+    double* part = S->d_partials;
+    double* scal = S->d_scal;
+    PLB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
+    k_cg_init<T><<<kRedBlocks, kRedThreads, 0, s>>>(b, S->d_mask, pinv, nn, r, z, p, part);
+    k_finish2<<<1, 1024, 0, s>>>(part, kRedBlocks, scal, S_RZ, S_RR);
+    count_launch(2);
+    double h[S_COUNT];
+    PLB_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PLB_CUDA(cudaStreamSynchronize(s));
+    const double r0 = std::sqrt(h[S_RR]);
+    const double stop = std::max(rtol * r0, atol);
+    *iters = 0;
+    *rel = r0 > 0.0 ? 1.0 : 0.0;
+    if (r0 == 0.0 || r0 <= stop) return PL_OK;
+    for (int it = 1; it <= max_iter; ++it) {
+        int rc;
+        if constexpr (sizeof(T) == 8) rc = apply_J(S, (const double*)p, (double*)q);
+        else rc = apply_J32(S, (const float*)p, (float*)q);
+        if (rc) return rc;
+        k_cg_pq<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, q, S->d_mask, n, part);
+        k_finish2<<<1, 1024, 0, s>>>(part, kRedBlocks, scal, S_PQ, -1);
+        k_copy_scalar<<<1, 1, 0, s>>>(scal, S_RZ, S_RZ_OLD);
+        k_cg_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, q, z, S->d_mask, pinv, nn, scal, part);
+        k_finish2<<<1, 1024, 0, s>>>(part, kRedBlocks, scal, S_RZ, S_RR);
+        k_cg_pupdate<T><<<vec_grid(n), 256, 0, s>>>(p, z, n, scal);
+        count_launch(6);
+        *iters = it;
+        if (it % S->check_every == 0 || it == max_iter) {
+            PLB_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+            PLB_CUDA(cudaStreamSynchronize(s));
+            const double rn = std::sqrt(h[S_RR]);
+            *rel = rn / r0;
+            if (!(rn == rn)) return fail(PL_ERR_NOT_CONVERGED, "PCG diverged (NaN residual)");
+            if (rn <= stop) return PL_OK;
+        }
+    }
+    return fail(PL_ERR_NOT_CONVERGED, "PCG reached the iteration limit");
+}
+
+}  // namespace
+
+extern "C" {
+
+int pl_solver_create(pl_mesh m, const uint8_t* constrained, pl_solver* out) {
+    if (!m || !out) return fail(PL_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    // Fault nodes: (negative node, positive node, normal) per Lagrange node, from the cohesive cells.
+    std::vector<int32_t> pneg(m->nlag, -1), ppos(m->nlag, -1);
+    std::vector<double> pnrm(3 * m->nlag, 0.0);
+    for (int64_t c = 0; c < m->ncoh; ++c) {
+        const int32_t* cc = &m->h_coh[12 * c];
+        double X[4][3];
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) X[a][d] = m->h_coords[3 * (int64_t)cc[a] + d];
+        double dxi[3], deta[3];
+        for (int d = 0; d < 3; ++d) {
+            dxi[d] = X[1][d] + X[2][d] - X[0][d] - X[3][d];
+            deta[d] = X[2][d] + X[3][d] - X[0][d] - X[1][d];
+        }
+        double nrm[3] = {dxi[1] * deta[2] - dxi[2] * deta[1], dxi[2] * deta[0] - dxi[0] * deta[2],
+                         dxi[0] * deta[1] - dxi[1] * deta[0]};
+        const double mag = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        for (int a = 0; a < 4; ++a) {
+            const int32_t l = cc[8 + a];
+            if (pneg[l] >= 0 && (pneg[l] != cc[a] || ppos[l] != cc[4 + a]))
+                return fail(PL_ERR_INVALID_ARG, "inconsistent cohesive cells: a fault node maps to two node pairs");
+            pneg[l] = cc[a];
+            ppos[l] = cc[4 + a];
+            for (int d = 0; d < 3; ++d) pnrm[3 * l + d] = nrm[d] / mag;
+        }
+    }
+    for (int64_t l = 0; l < m->nlag; ++l)
+        if (pneg[l] < 0) return fail(PL_ERR_INVALID_ARG, "fault node without a cohesive cell");
+    pl_solver S = new pl_solver_s();
+    S->mesh = m;
+    mesh_retain(m);
+    S->nnodes = m->nnodes + m->nlag;
+    S->n = 3 * S->nnodes;
+    S->npairs = m->nlag;
+    PLB_CUDA(cudaSetDevice(m->ctx->device));
+    const int64_t n = S->n;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](auto** p, size_t cnt) {
+        if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(**p));
+    };
+    A(&S->d_mask, n);
+    A(&S->d_diag, 9 * S->nnodes);
+    A(&S->d_pinv, 9 * S->nnodes);
+    A(&S->d_pinv32, 9 * S->nnodes);
+    A(&S->d_r, n); A(&S->d_p, n); A(&S->d_q, n); A(&S->d_z, n); A(&S->d_x, n);
+    A(&S->f_r, n); A(&S->f_p, n); A(&S->f_q, n); A(&S->f_z, n); A(&S->f_x, n);
+    A(&S->d_scal, S_COUNT);
+    A(&S->d_partials, 2 * kRedBlocks);
+    if (S->npairs > 0) {
+        A(&S->d_pair_neg, S->npairs);
+        A(&S->d_pair_pos, S->npairs);
+        A(&S->d_pair_normal, 3 * S->npairs);
+    }
+    cudaStream_t s = m->ctx->stream;
+    // Unknowns: DOFs not constrained by the caller, minus the positive side of fault nodes and
+    // the Lagrange-multiplier DOFs (eliminated by the reduced formulation).
+    std::vector<uint8_t> mask(n, 0);
+    if (constrained) std::memcpy(mask.data(), constrained, n);
+    for (int64_t l = 0; l < S->npairs; ++l)
+        for (int d = 0; d < 3; ++d) {
+            mask[3 * (int64_t)ppos[l] + d] = 1;
+            mask[3 * (m->nnodes + l) + d] = 1;
+        }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S->d_mask, mask.data(), n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && S->npairs > 0) {
+        e = cudaMemcpyAsync(S->d_pair_neg, pneg.data(), pneg.size() * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S->d_pair_pos, ppos.data(), ppos.size() * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S->d_pair_normal, pnrm.data(), pnrm.size() * 8, cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->d_scal, 0, S_COUNT * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        pl_solver_destroy(S);
+        return cuda_fail(e, "pl_solver_create");
+    }
+    *out = S;
+    return PL_OK;
+}
+
+int pl_solver_add_integrator(pl_solver S, pl_integrator ig) {
+    if (!S || !ig || ig->mesh != S->mesh) return fail(PL_ERR_INVALID_ARG, "bad arguments");
+    if (ig->is_interface)
+        return fail(PL_ERR_INVALID_ARG, "interface integrators are not part of the reduced operator; "
+                                        "pass them to pl_solver_apply_fault_slip");
+    if (ig->j3 == K_NONE) return fail(PL_ERR_NOT_READY, "integrator has no Jacobian kernels");
+    S->ops.push_back(ig);
+    S->ready = false;
+    return PL_OK;
+}
+
+int pl_solver_set_tolerances(pl_solver S, double rtol, double atol, int max_iter) {
+    if (!S || rtol < 0 || atol < 0 || max_iter <= 0) return fail(PL_ERR_INVALID_ARG, "bad tolerances");
+    S->rtol = rtol;
+    S->atol = atol;
+    S->max_iter = max_iter;
+    return PL_OK;
+}
+
+int pl_solver_set_precision(pl_solver S, int precision, double inner_rtol) {
+    if (!S || (precision != PL_SOLVER_FP64 && precision != PL_SOLVER_FP32_REFINED) || !(inner_rtol > 0 && inner_rtol < 1))
+        return fail(PL_ERR_INVALID_ARG, "bad precision settings");
+    S->precision = precision;
+    S->inner_rtol = inner_rtol;
+    return PL_OK;
+}
+
+int pl_solver_setup(pl_solver S, double t, double dt) {
+    if (!S || S->ops.empty()) return fail(PL_ERR_NOT_READY, "no integrators");
+    pl_mesh m = S->mesh;
+    cudaStream_t s = m->ctx->stream;
+    PLB_CUDA(cudaSetDevice(m->ctx->device));
+    S->t = t;
+    S->dt = dt;
+    PLB_CUDA(cudaMemsetAsync(S->d_diag, 0, 9 * S->nnodes * sizeof(double), s));
+    for (pl_integrator ig : S->ops) {
+        DomainParams p;
+        int rc = bind_domain_jacobian(ig, &p);
+        if (rc) return rc;
+        p.t = t;
+        p.dt = dt;
+        launch_domain_diag_blocks(p, m->cell_type, ig->j3 == K_ILE_JF3VU ? RHEO_ILE : RHEO_GENMAXWELL, S->d_diag, s);
+    }
+    if (S->npairs > 0) {
+        k_fault_fold_blocks<<<vec_grid(9 * S->npairs), 256, 0, s>>>(S->d_diag, S->d_pair_neg, S->d_pair_pos, S->npairs);
+        count_launch();
+    }
+    k_invert_blocks<<<vec_grid(S->nnodes), 256, 0, s>>>(S->d_diag, S->d_mask, S->nnodes, S->d_pinv, S->d_pinv32);
+    count_launch();
+    PLB_CUDA(cudaGetLastError());
+    S->ready = true;
+    return PL_OK;
+}
+
+int pl_solver_solve(pl_solver S, const double* b, double* x) {
+    if (!S || !b || !x) return fail(PL_ERR_INVALID_ARG, "bad arguments");
+    if (!S->ready) return fail(PL_ERR_NOT_READY, "call pl_solver_setup first");
+    pl_mesh m = S->mesh;
+    cudaStream_t s = m->ctx->stream;
+    PLB_CUDA(cudaSetDevice(m->ctx->device));
+    S->iterations = S->inner_iterations = S->outer_iterations = 0;
+    const int64_t n = S->n;
+    if (S->npairs > 0) {  // right-hand side of the reduced system: P^T b
+        PLB_CUDA(cudaMemcpyAsync(S->d_x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        fault_fold(S, S->d_x);
+        b = S->d_x;
+    }
+    if (S->precision == PL_SOLVER_FP64) {
+        int it = 0;
+        double rel = 0.0;
+        int rc = pcg<double>(S, b, x, S->rtol, S->atol, S->max_iter, S->d_pinv, S->d_r, S->d_p, S->d_q, S->d_z, &it, &rel);
+        fault_unfold(S, x);
+        S->iterations = it;
+        S->rel_residual = rel;
+        return rc;
+    }
+    // FP64 iterative refinement around FP32 PCG (apply_J unfolds x on every outer pass).
+    PLB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    double h[S_COUNT];
+    double b0 = -1.0;
+    for (int outer = 0; outer < 50; ++outer) {
+        int rc = apply_J(S, x, S->d_q);
+        if (rc) return rc;
+        k_outer_residual<<<kRedBlocks, kRedThreads, 0, s>>>(b, S->d_q, S->d_mask, n, S->d_r, S->f_r, S->d_partials);
+        k_finish2<<<1, 1024, 0, s>>>(S->d_partials, kRedBlocks, S->d_scal, S_BB, -1);
+        count_launch(2);
+        PLB_CUDA(cudaMemcpyAsync(h, S->d_scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+        PLB_CUDA(cudaStreamSynchronize(s));
+        const double rn = std::sqrt(h[S_BB]);
+        if (b0 < 0.0) b0 = rn;
+        S->rel_residual = b0 > 0.0 ? rn / b0 : 0.0;
+        S->outer_iterations = outer;
+        if (rn <= std::max(S->rtol * b0, S->atol) || b0 == 0.0) return PL_OK;
+        int it = 0;
+        double rel = 0.0;
+        // Inner solve A d = r in FP32 (d in f_x).
+        // The right-hand side f_r doubles as the inner residual vector (read before written).
+        rc = pcg<float>(S, S->f_r, S->f_x, S->inner_rtol, 0.0, S->max_iter, S->d_pinv32, S->f_r, S->f_p, S->f_q, S->f_z,
+                        &it, &rel);
+        if (rc && rc != PL_ERR_NOT_CONVERGED) return rc;
+        S->inner_iterations += it;
+        k_add_correction<<<vec_grid(n), 256, 0, s>>>(x, S->f_x, S->d_mask, n);
+        count_launch();
+    }
+    fault_unfold(S, x);
+    return fail(PL_ERR_NOT_CONVERGED, "iterative refinement did not converge");
+}
+
+int pl_solver_apply_fault_slip(pl_solver S, pl_integrator iface, double* u) {
+    if (!S || !iface || !u || !iface->is_interface || iface->mesh != S->mesh)
+        return fail(PL_ERR_INVALID_ARG, "bad arguments");
+    if (S->npairs == 0) return PL_OK;
+    const AuxField* slip = nullptr;
+    for (const AuxField& f : iface->aux)
+        if (f.name == "slip") slip = &f;
+    if (!slip || slip->ncomp != 3 || slip->storage != PL_AUX_PER_FAULT_NODE)
+        return fail(PL_ERR_INVALID_ARG, "interface integrator needs the slip(3) aux subfield per fault node");
+    if (iface->constants.size() < 6) return fail(PL_ERR_INVALID_ARG, "interface integrator needs constants refDir1, refDir2");
+    const std::vector<double>& c = iface->constants;
+    PLB_CUDA(cudaSetDevice(S->mesh->ctx->device));
+    k_fault_apply_slip<<<vec_grid(S->npairs), 256, 0, S->mesh->ctx->stream>>>(
+        u, S->d_pair_neg, S->d_pair_pos, S->d_pair_normal, slip->d, S->npairs, c[0], c[1], c[2], c[3], c[4], c[5]);
+    count_launch();
+    PLB_CUDA(cudaGetLastError());
+    return PL_OK;
+}
+
+int pl_solver_get_stats(pl_solver S, int* iterations, int* inner_iterations, int* outer_iterations, double* rel_residual) {
+    if (!S) return fail(PL_ERR_INVALID_ARG, "null solver");
+    if (iterations) *iterations = S->iterations;
+    if (inner_iterations) *inner_iterations = S->inner_iterations;
+    if (outer_iterations) *outer_iterations = S->outer_iterations;
+    if (rel_residual) *rel_residual = S->rel_residual;
+    return PL_OK;
+}
+
+int pl_solver_destroy(pl_solver S) {
+    if (!S) return PL_OK;
+    cudaSetDevice(S->mesh->ctx->device);
+    cudaStreamSynchronize(S->mesh->ctx->stream);
+    void* ptrs[] = {S->d_mask, S->d_diag, S->d_pinv, S->d_pinv32, S->d_r, S->d_p, S->d_q, S->d_z, S->d_x,
+                    S->f_r, S->f_p, S->f_q, S->f_z, S->f_x, S->d_scal, S->d_partials,
+                    S->d_pair_neg, S->d_pair_pos, S->d_pair_normal};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    pl_mesh m = S->mesh;
+    delete S;
+    mesh_release(m);
+    return PL_OK;
+}
+
+}  // extern "C"

@@ -299,3 +299,52 @@ class Matrix:
             self.close()
         except Exception:
             pass
+
+
+class Solver:
+    """Device PCG for A x = b, A = -(sum of the integrators' Jacobians), on the unconstrained DOFs
+    (include/pylith_b200.h, pl_solver_*)."""
+
+    FP64 = C.PL_SOLVER_FP64
+    FP32_REFINED = C.PL_SOLVER_FP32_REFINED
+
+    def __init__(self, mesh: DeviceMesh, constrained: Optional[np.ndarray], integrators,
+                 rtol=1e-12, atol=0.0, max_iter=20000, precision=C.PL_SOLVER_FP64, inner_rtol=1e-5):
+        self.dmesh = mesh
+        self.integrators = list(integrators)
+        self.handle = ctypes.c_void_p()
+        mask = None if constrained is None else np.ascontiguousarray(constrained, dtype=np.uint8)
+        self._mask = mask
+        check(C.lib().pl_solver_create(mesh.handle, None if mask is None else mask.ctypes.data,
+                                       ctypes.byref(self.handle)))
+        for ig in self.integrators:
+            check(C.lib().pl_solver_add_integrator(self.handle, ig.handle))
+        check(C.lib().pl_solver_set_tolerances(self.handle, rtol, atol, max_iter))
+        check(C.lib().pl_solver_set_precision(self.handle, precision, inner_rtol))
+
+    def setup(self, t=0.0, dt=0.0):
+        check(C.lib().pl_solver_setup(self.handle, t, dt))
+
+    def solve(self, b, x):
+        check(C.lib().pl_solver_solve(self.handle, _ptr(b), _ptr(x)))
+
+    def apply_fault_slip(self, iface: "IntegratorInterface", u) -> None:
+        check(C.lib().pl_solver_apply_fault_slip(self.handle, iface.handle, _ptr(u)))
+
+    def stats(self):
+        it, inner, outer, rel = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(C.lib().pl_solver_get_stats(self.handle, ctypes.byref(it), ctypes.byref(inner),
+                                          ctypes.byref(outer), ctypes.byref(rel)))
+        return {"iterations": it.value, "inner_iterations": inner.value,
+                "outer_iterations": outer.value, "rel_residual": rel.value}
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_solver_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -322,3 +322,21 @@ def test_inverted_cell_is_reported(torch_cuda, ctx):
         ctx.synchronize()
     assert e.value.code == -6
     ctx.synchronize()  # the flag is cleared after it is reported
+
+
+def test_destroy_in_any_order(torch_cuda):
+    """Context, mesh and integrator handles may be released in any order (the C layer defers a
+    destroy until no dependent object is left)."""
+    from pylith_b200 import feassemble as FA
+
+    c = FA.Context(0)
+    mesh = M.box_hex(2, 2, 2)
+    dm = FA.DeviceMesh(c, mesh)
+    ig = elastic_setup(mesh).create_integrator(dm)
+    A = FA.Matrix(dm)
+    c.close()
+    dm.close()
+    du = torch_cuda.zeros(mesh.num_nodes * 3, dtype=torch_cuda.float64, device="cuda")
+    ig.compute_lhs_residual(0.0, 0.0, du, du.clone())
+    A.close()
+    ig.close()
