@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libpylith_b200.so")
+# PYLITH_B200_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("PYLITH_B200_LIB", os.path.join(HERE, "libpylith_b200.so"))
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int

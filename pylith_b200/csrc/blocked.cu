@@ -1,18 +1,23 @@
 // Cell-block kernels for P1 tetrahedra: the hot path of the residual and Jacobian action.
 //
 // Cells are processed in blocks of kTetBlockCells consecutive cells (meshes are ordered along
-// a Morton curve, so a block is a compact patch). One CTA per block:
-//   1. gathers the block's nodes (coordinates and the input field) into shared memory once,
-//      instead of once per incident cell;
-//   2. one thread per cell forms the affine geometry, the solution gradient, calls the
-//      pointwise kernel and stages its 12-entry element vector in shared memory;
-//   3. one thread per node sums the staged entries of its incident corners in a fixed order
-//      (a precomputed block-local incidence list) and writes the node's value: a plain store
-//      for nodes whose cells all lie in the block, one FP64 reduction into global memory for
-//      nodes shared with other blocks.
+// a Morton curve, so a block is a compact patch). Persistent CTAs walk every gridDim.x-th block.
+// For each block the CTA
+//   1. has the block's nodes (coordinates and input field), node ids and incidence list in
+//      shared memory: they were copied asynchronously (cp.async) into a second buffer while the
+//      previous block computed, so a node is read from global memory once per block instead of
+//      once per incident cell;
+//   2. forms, one thread per cell, the affine geometry and the solution gradient, calls the
+//      pointwise kernel and stages the 12-entry element vector in shared memory;
+//   3. sums, one thread per node, the staged entries of the node's incident corners in a fixed
+//      order (the precomputed block-local incidence list) and writes the node: a plain store for
+//      nodes whose cells all lie in the block, one FP64 reduction into global memory for nodes
+//      shared with other blocks.
 // Geometry in cofactor form: with C = det(J) J^{-1}, grad(u) = (G C) / det(J) for the edge
 // differences G, and the element vector of corner a (a = 1..3) is f1 C_{a-1}^T / 6, so the
-// Jacobian determinant only enters through one reciprocal.
+// Jacobian determinant enters through one reciprocal.
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 #include <vector>
 
@@ -23,9 +28,10 @@
 namespace plb {
 
 constexpr int kTetBlockCells = 256;
+constexpr int kMaxSlotsPerThread = 2;  // blocks touching more than 2 * 256 nodes use the atomic kernel
+constexpr uint32_t kSharedBit = 0x80000000u;
 
-// Cofactor matrix C = adj(J)^T with J = [X1-X0, X2-X0, X3-X0] (columns), so that
-// J^{-1} = C^T / det ... stored here directly as cof[i][j] = (J^{-1})[i][j] * det.
+// cof[i][j] = det(J) (J^{-1})[i][j] with J = [X1-X0, X2-X0, X3-X0] (columns); returns det(J).
 PL_D double tet_cofactors(const double X[4][3], double cof[3][3]) {
     double J[3][3];
 #pragma unroll
@@ -46,57 +52,158 @@ PL_D double tet_cofactors(const double X[4][3], double cof[3][3]) {
     return J[0][0] * cof[0][0] + J[0][1] * cof[1][0] + J[0][2] * cof[2][0];
 }
 
-template <int RHEO, bool BF, int OP, bool INSERT>
-__global__ void __launch_bounds__(kTetBlockCells, 4)
-    k_tet_blocked(DomainParams p, const int32_t* __restrict__ slot_begin, const int32_t* __restrict__ slot_node,
-                  const uint8_t* __restrict__ slot_shared, const ushort4* __restrict__ lconn,
-                  const uint16_t* __restrict__ inc_off, const uint16_t* __restrict__ inc, int64_t nblocks) {
-    using L = AuxLayout<RHEO, BF>;
-    extern __shared__ double smem[];
-    const AuxOffsets<RHEO, BF> aoff;
-    const double* __restrict__ field = OP == OP_RESIDUAL ? p.u : p.v;
-    double* sE = smem;                          // [12][kTetBlockCells] staged element vectors
-    double* sN = smem + 12 * kTetBlockCells;    // [ns][6]: coordinates, field
-    for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
-        const int s0 = slot_begin[b];
-        const int ns = slot_begin[b + 1] - s0;
-        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-            const int64_t nd = slot_node[s0 + i];
+struct BlockArrays {
+    const int32_t* slot_begin;  // [nblocks + 1]
+    const uint32_t* slot_node;  // node id | kSharedBit if other blocks touch the node
+    const ushort4* lconn;       // [ncells] block-local slots of the 4 corners
+    const uint32_t* inc_off;    // per block ns+1 offsets (block b starts at slot_begin[b] + b)
+    const uint16_t* inc;        // [nblocks][4 * kTetBlockCells] cell * 4 + corner
+    int64_t nblocks;
+    int max_local_nodes;
+};
+
+// Shared-memory buffer of one block: node data [maxloc][8] doubles (x, y, z, u0, u1, u2, -, -:
+// three 16-byte loads per node), node ids [maxloc],
+// incidence offsets [maxloc + 1], incidence list [4 * kTetBlockCells].
+struct SmemBuf {
+    double* node;
+    uint32_t* id;
+    uint32_t* off;
+    uint16_t* inc;
+};
+
+PL_HD size_t round16(size_t x) { return (x + 15) & ~size_t(15); }
+
+PL_HD size_t buf_bytes(int maxloc) {
+    return round16(64 * (size_t)maxloc) + round16(4 * (size_t)maxloc) + round16(4 * ((size_t)maxloc + 1)) +
+           round16(2 * 4 * (size_t)kTetBlockCells);
+}
+
+PL_D SmemBuf make_buf(char* base, int maxloc) {
+    SmemBuf s;
+    s.node = reinterpret_cast<double*>(base);
+    base += round16(64 * (size_t)maxloc);
+    s.id = reinterpret_cast<uint32_t*>(base);
+    base += round16(4 * (size_t)maxloc);
+    s.off = reinterpret_cast<uint32_t*>(base);
+    base += round16(4 * ((size_t)maxloc + 1));
+    s.inc = reinterpret_cast<uint16_t*>(base);
+    return s;
+}
+
+// Asynchronous copies of block b into buffer s; nd[k] holds slot_node of slots tid + k*blockDim
+// (read one block earlier, so no global latency is exposed here).
+PL_D void prefetch_block(const DomainParams& p, const double* __restrict__ field, const BlockArrays& A, int64_t b,
+                         const uint32_t nd[kMaxSlotsPerThread], const SmemBuf& s) {
+    const int s0 = A.slot_begin[b];
+    const int ns = A.slot_begin[b + 1] - s0;
+#pragma unroll
+    for (int k = 0; k < kMaxSlotsPerThread; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        if (i < ns) {
+            const int64_t node = nd[k] & ~kSharedBit;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                sN[6 * i + d] = p.coords[3 * nd + d];
-                sN[6 * i + 3 + d] = field[3 * nd + d];
+                __pipeline_memcpy_async(&s.node[8 * i + d], &p.coords[3 * node + d], sizeof(double));
+                __pipeline_memcpy_async(&s.node[8 * i + 3 + d], &field[3 * node + d], sizeof(double));
             }
+            s.id[i] = nd[k];
         }
-        __syncthreads();
+    }
+    for (int i = threadIdx.x; i <= ns; i += blockDim.x)
+        __pipeline_memcpy_async(&s.off[i], &A.inc_off[s0 + b + i], sizeof(uint32_t));
+    // 4 * kTetBlockCells uint16 = 128 chunks of 16 bytes
+    for (int i = threadIdx.x; i < kTetBlockCells / 2; i += blockDim.x)
+        __pipeline_memcpy_async(&s.inc[8 * i], &A.inc[b * 4 * kTetBlockCells + 8 * i], 16);
+}
+
+PL_D void load_slot_ids(const BlockArrays& A, int64_t b, uint32_t nd[kMaxSlotsPerThread]) {
+    if (b >= A.nblocks) return;
+    const int s0 = A.slot_begin[b];
+    const int ns = A.slot_begin[b + 1] - s0;
+#pragma unroll
+    for (int k = 0; k < kMaxSlotsPerThread; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        nd[k] = i < ns ? A.slot_node[s0 + i] : 0u;
+    }
+}
+
+#ifndef PLB_TET_MIN_BLOCKS
+#define PLB_TET_MIN_BLOCKS 4
+#endif
+
+template <int RHEO, bool BF, int OP, bool INSERT>
+__global__ void __launch_bounds__(kTetBlockCells, PLB_TET_MIN_BLOCKS) k_tet_blocked(DomainParams p, BlockArrays A) {
+    using L = AuxLayout<RHEO, BF>;
+    extern __shared__ __align__(16) char smem_raw[];
+    const AuxOffsets<RHEO, BF> aoff;
+    const double* __restrict__ field = OP == OP_RESIDUAL ? p.u : p.v;
+    double* sE = reinterpret_cast<double*>(smem_raw);  // [12][kTetBlockCells]
+    char* bufbase = smem_raw + 12 * kTetBlockCells * sizeof(double);
+    const size_t bb = buf_bytes(A.max_local_nodes);
+    const int64_t G = gridDim.x;
+    int64_t b = blockIdx.x;
+    uint32_t nd_next[kMaxSlotsPerThread] = {0u, 0u};
+    {
+        uint32_t nd0[kMaxSlotsPerThread] = {0u, 0u};
+        load_slot_ids(A, b, nd0);
+        if (b < A.nblocks) prefetch_block(p, field, A, b, nd0, make_buf(bufbase, A.max_local_nodes));
+        __pipeline_commit();
+        load_slot_ids(A, b + G, nd_next);
+    }
+    int cur = 0;
+    for (; b < A.nblocks; b += G) {
+        const int s0 = A.slot_begin[b];
+        const int ns = A.slot_begin[b + 1] - s0;
         const int tc = threadIdx.x;
         const int64_t c = b * kTetBlockCells + tc;
+        // per-cell inputs and the slot ids two blocks ahead: issued before the wait
+        ushort4 lc = make_ushort4(0, 0, 0, 0);
+        double a[L::size];
         if (c < p.ncells) {
-            const ushort4 lc = lconn[c];
+            lc = A.lconn[c];
+            L::load_cell(p, c, a);
+        }
+        uint32_t nd_after[kMaxSlotsPerThread] = {0u, 0u};
+        load_slot_ids(A, b + 2 * G, nd_after);
+        __pipeline_wait_prior(0);
+        __syncthreads();
+        if (b + G < A.nblocks)
+            prefetch_block(p, field, A, b + G, nd_next, make_buf(bufbase + (cur ^ 1) * bb, A.max_local_nodes));
+        __pipeline_commit();
+#pragma unroll
+        for (int k = 0; k < kMaxSlotsPerThread; ++k) nd_next[k] = nd_after[k];
+        const SmemBuf S = make_buf(bufbase + cur * bb, A.max_local_nodes);
+        if (c < p.ncells) {
             const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
-            double X[4][3];
+            double X[4][3], U[4][3];
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) X[k][d] = sN[6 * ln[k] + d];
+            for (int k = 0; k < 4; ++k) {
+                const double2* nd2 = reinterpret_cast<const double2*>(S.node + 8 * ln[k]);
+                const double2 a01 = nd2[0], a23 = nd2[1], a45 = nd2[2];
+                X[k][0] = a01.x;
+                X[k][1] = a01.y;
+                X[k][2] = a23.x;
+                U[k][0] = a23.y;
+                U[k][1] = a45.x;
+                U[k][2] = a45.y;
+            }
             double cof[3][3];
             const double det = tet_cofactors(X, cof);
             if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
             const double rdet = 1.0 / det;
             // G[c][k] = u_{k+1}[c] - u_0[c]; s_x = G cof / det
-            double G[3][3];
+            double Gm[3][3];
 #pragma unroll
             for (int k = 0; k < 3; ++k)
 #pragma unroll
-                for (int cc = 0; cc < 3; ++cc) G[cc][k] = sN[6 * ln[k + 1] + 3 + cc] - sN[6 * ln[0] + 3 + cc];
+                for (int cc = 0; cc < 3; ++cc) Gm[cc][k] = U[k + 1][cc] - U[0][cc];
             double s_x[9];
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc)
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    s_x[cc * 3 + d] = (G[cc][0] * cof[0][d] + G[cc][1] * cof[1][d] + G[cc][2] * cof[2][d]) * rdet;
-            double a[L::size];
-            L::load_cell(p, c, a);
+                    s_x[cc * 3 + d] = (Gm[cc][0] * cof[0][d] + Gm[cc][1] * cof[1][d] + Gm[cc][2] * cof[2][d]) * rdet;
             double x[3] = {0, 0, 0}, s[3] = {0, 0, 0};
             double f0[3] = {0, 0, 0}, f1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             if (OP == OP_RESIDUAL) {
@@ -143,19 +250,18 @@ __global__ void __launch_bounds__(kTetBlockCells, 4)
         }
         __syncthreads();
         for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-            const int j0 = inc_off[s0 + b + i], j1 = inc_off[s0 + b + i + 1];
-            const uint16_t* lst = inc + b * 4 * kTetBlockCells;
+            const int j0 = S.off[i], j1 = S.off[i + 1];
             double r0 = 0.0, r1 = 0.0, r2 = 0.0;
             for (int j = j0; j < j1; ++j) {
-                const int e = lst[j];
+                const int e = S.inc[j];
                 const int cell = e >> 2, corner = e & 3;
                 r0 += sE[(corner * 3 + 0) * kTetBlockCells + cell];
                 r1 += sE[(corner * 3 + 1) * kTetBlockCells + cell];
                 r2 += sE[(corner * 3 + 2) * kTetBlockCells + cell];
             }
-            const int64_t nd = slot_node[s0 + i];
-            double* o = p.out + 3 * nd;
-            if (slot_shared[s0 + i]) {
+            const uint32_t id = S.id[i];
+            double* o = p.out + 3 * (int64_t)(id & ~kSharedBit);
+            if (id & kSharedBit) {
                 red_add(o, r0);
                 red_add(o + 1, r1);
                 red_add(o + 2, r2);
@@ -170,24 +276,169 @@ __global__ void __launch_bounds__(kTetBlockCells, 4)
             }
         }
         __syncthreads();
+        cur ^= 1;
     }
+    __pipeline_wait_prior(0);
+}
+
+// FP32 Jacobian action of isotropic linear elasticity on the cell blocks: geometry (cofactors,
+// 1/det) and the elastic tangent in FP64 per cell, the field, gradient, flux and element vectors
+// in FP32. Used by the inner iterations of the mixed-precision solver.
+__global__ void __launch_bounds__(kTetBlockCells, 4) k_tet_blocked_jv32(DomainParams p, BlockArrays A) {
+    using L = AuxLayout<RHEO_ILE, false>;
+    extern __shared__ __align__(16) char smem_raw[];
+    const AuxOffsets<RHEO_ILE, false> aoff;
+    float* sE = reinterpret_cast<float*>(smem_raw);                                          // [12][kTetBlockCells]
+    double* sX = reinterpret_cast<double*>(smem_raw + 12 * kTetBlockCells * sizeof(float));  // [ns][3]
+    for (int64_t b = blockIdx.x; b < A.nblocks; b += gridDim.x) {
+        const int s0 = A.slot_begin[b];
+        const int ns = A.slot_begin[b + 1] - s0;
+        float* sV = reinterpret_cast<float*>(sX + 3 * ns);  // [ns][3] field
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+            const int64_t nd = A.slot_node[s0 + i] & ~kSharedBit;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                sX[3 * i + d] = p.coords[3 * nd + d];
+                sV[3 * i + d] = p.v32[3 * nd + d];
+            }
+        }
+        __syncthreads();
+        const int tc = threadIdx.x;
+        const int64_t c = b * kTetBlockCells + tc;
+        if (c < p.ncells) {
+            const ushort4 lc = A.lconn[c];
+            const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
+            double X[4][3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) X[k][d] = sX[3 * ln[k] + d];
+            double cof[3][3];
+            const double det = tet_cofactors(X, cof);
+            if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+            const double rdet = 1.0 / det;
+            float inv[3][3], cf[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    inv[i][j] = (float)(cof[i][j] * rdet);
+                    cf[i][j] = (float)(cof[i][j] * (1.0 / 6.0));
+                }
+            double a[L::size];
+            L::load_cell(p, c, a);
+            double x[3] = {0, 0, 0};
+            double Jf3d[81];
+#pragma unroll
+            for (int i = 0; i < 81; ++i) Jf3d[i] = 0.0;
+            call_jf3<RHEO_ILE>(L::numA, aoff.v, a, p, x, Jf3d);
+            float s_x[9];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                const float g0 = sV[3 * ln[1] + cc] - sV[3 * ln[0] + cc];
+                const float g1 = sV[3 * ln[2] + cc] - sV[3 * ln[0] + cc];
+                const float g2 = sV[3 * ln[3] + cc] - sV[3 * ln[0] + cc];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) s_x[cc * 3 + d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
+            }
+            float f1[9];
+#pragma unroll
+            for (int f = 0; f < 3; ++f)
+#pragma unroll
+                for (int df = 0; df < 3; ++df) {
+                    float acc1 = 0.0f;
+#pragma unroll
+                    for (int gg = 0; gg < 3; ++gg)
+#pragma unroll
+                        for (int dg = 0; dg < 3; ++dg)
+                            acc1 += (float)Jf3d[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
+                    f1[f * 3 + df] = acc1;
+                }
+            float e0[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    const float v = f1[cc * 3 + 0] * cf[k][0] + f1[cc * 3 + 1] * cf[k][1] + f1[cc * 3 + 2] * cf[k][2];
+                    e0[cc] -= v;
+                    sE[((k + 1) * 3 + cc) * kTetBlockCells + tc] = v;
+                }
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + tc] = e0[cc];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+            const int j0 = A.inc_off[s0 + b + i], j1 = A.inc_off[s0 + b + i + 1];
+            const uint16_t* lst = A.inc + b * 4 * kTetBlockCells;
+            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+            for (int j = j0; j < j1; ++j) {
+                const int e = lst[j];
+                const int cell = e >> 2, corner = e & 3;
+                r0 += sE[(corner * 3 + 0) * kTetBlockCells + cell];
+                r1 += sE[(corner * 3 + 1) * kTetBlockCells + cell];
+                r2 += sE[(corner * 3 + 2) * kTetBlockCells + cell];
+            }
+            const uint32_t id = A.slot_node[s0 + i];
+            float* o = p.out32 + 3 * (int64_t)(id & ~kSharedBit);
+            if (id & kSharedBit) {
+                red_add(o, r0);
+                red_add(o + 1, r1);
+                red_add(o + 2, r2);
+            } else {
+                o[0] += r0;
+                o[1] += r1;
+                o[2] += r2;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+static BlockArrays arrays_of(const BlockedLayout& b) {
+    BlockArrays A;
+    A.slot_begin = b.d_block_node_begin;
+    A.slot_node = b.d_slot_node;
+    A.lconn = (const ushort4*)b.d_local_cells;
+    A.inc_off = b.d_inc_off;
+    A.inc = b.d_inc;
+    A.nblocks = b.num_blocks;
+    A.max_local_nodes = b.max_local_nodes;
+    return A;
+}
+
+static size_t blocked_smem(const BlockedLayout& b) {
+    return (size_t)12 * kTetBlockCells * sizeof(double) + 2 * buf_bytes(b.max_local_nodes);
+}
+
+static int persistent_grid(int64_t nblocks) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return (int)std::min<int64_t>(nblocks, (int64_t)nsm * PLB_TET_MIN_BLOCKS);
 }
 
 template <int RHEO, bool BF, int OP>
 static void launch_t(const DomainParams& p, const BlockedLayout& b, bool insert, cudaStream_t s) {
-    const size_t smem = (size_t)(12 * kTetBlockCells + 6 * b.max_local_nodes) * sizeof(double);
-    const int grid = (int)b.num_blocks;
-#define PLB_ARGS p, b.d_block_node_begin, b.d_node_ids, b.d_slot_shared, (const ushort4*)b.d_local_cells, b.d_inc_off, b.d_inc, b.num_blocks
-    if (insert) k_tet_blocked<RHEO, BF, OP, true><<<grid, kTetBlockCells, smem, s>>>(PLB_ARGS);
-    else k_tet_blocked<RHEO, BF, OP, false><<<grid, kTetBlockCells, smem, s>>>(PLB_ARGS);
-#undef PLB_ARGS
+    const size_t smem = blocked_smem(b);
+    const int grid = persistent_grid(b.num_blocks);
+    if (smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_tet_blocked<RHEO, BF, OP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_tet_blocked<RHEO, BF, OP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    const BlockArrays A = arrays_of(b);
+    if (insert) k_tet_blocked<RHEO, BF, OP, true><<<grid, kTetBlockCells, smem, s>>>(p, A);
+    else k_tet_blocked<RHEO, BF, OP, false><<<grid, kTetBlockCells, smem, s>>>(p, A);
     count_launch();
+}
+
+static bool blocked_usable(const BlockedLayout& b) {
+    return b.num_blocks > 0 && b.max_local_nodes <= kMaxSlotsPerThread * kTetBlockCells &&
+           blocked_smem(b) <= 200 * 1024;
 }
 
 bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, bool bf,
                                  int op, bool insert, int64_t nnodes, cudaStream_t s) {
-    if (cell != TET4 || rheo != RHEO_ILE || b.num_blocks == 0) return false;
-    if ((size_t)(12 * kTetBlockCells + 6 * b.max_local_nodes) * sizeof(double) > 200 * 1024) return false;
+    if (cell != TET4 || rheo != RHEO_ILE || !blocked_usable(b)) return false;
     // INSERT: shared nodes receive reductions from several blocks, untouched nodes none, so the
     // output starts from zero; nodes owned by one block are then stored directly.
     if (insert && (b.num_shared_nodes > 0 || b.num_untouched > 0))
@@ -201,21 +452,34 @@ bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, 
     return true;
 }
 
+bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,
+                                cudaStream_t s) {
+    if (cell != TET4 || rheo != RHEO_ILE || !blocked_usable(b)) return false;
+    const size_t smem = (size_t)12 * kTetBlockCells * sizeof(float) +
+                        (size_t)b.max_local_nodes * (3 * sizeof(double) + 3 * sizeof(float));
+    if (smem > 200 * 1024) return false;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_tet_blocked_jv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the output was zeroed by the caller (INSERT) or holds the partial sum (ADD)
+    k_tet_blocked_jv32<<<persistent_grid(b.num_blocks), kTetBlockCells, smem, s>>>(p, arrays_of(b));
+    count_launch();
+    return true;
+}
+
 // Host: block layout from the cell connectivity (cells should be in a locality-preserving order).
 int ensure_blocked_layout(pl_mesh_s* m) {
     if (m->blocked) return PL_OK;
-    if (m->cell_type != PL_CELL_TET4) {
-        m->blocked = new BlockedLayout();  // empty: not supported for this cell type
+    if (m->cell_type != PL_CELL_TET4 || m->nnodes >= (int64_t)kSharedBit) {
+        m->blocked = new BlockedLayout();  // empty: not supported for this mesh
         return PL_OK;
     }
     const int B = kTetBlockCells;
     const int64_t nc = m->ncells;
     const int64_t nb = (nc + B - 1) / B;
     std::vector<int32_t> begin(nb + 1, 0);
-    std::vector<int32_t> node_ids;
+    std::vector<uint32_t> node_ids;
     std::vector<uint16_t> lconn((size_t)nc * 4);
     std::vector<uint16_t> inc((size_t)nb * 4 * B, 0);
-    std::vector<uint16_t> inc_off;
+    std::vector<uint32_t> inc_off;
     std::vector<int32_t> nblocks_of(m->nnodes, 0);
     node_ids.reserve((size_t)nc);
     inc_off.reserve((size_t)nc + nb);
@@ -230,7 +494,7 @@ int ensure_blocked_layout(pl_mesh_s* m) {
         maxloc = std::max<int>(maxloc, (int)loc.size());
         begin[b] = (int32_t)node_ids.size();
         for (int32_t nd : loc) {
-            node_ids.push_back(nd);
+            node_ids.push_back((uint32_t)nd);
             nblocks_of[nd]++;
         }
         count.assign(loc.size() + 1, 0);
@@ -242,8 +506,8 @@ int ensure_blocked_layout(pl_mesh_s* m) {
                 count[l + 1]++;
             }
         for (size_t i = 0; i < loc.size(); ++i) count[i + 1] += count[i];
-        for (size_t i = 0; i <= loc.size(); ++i) inc_off.push_back((uint16_t)count[i]);
-        // incidence entries in (cell, corner) order for every node: fixed summation order
+        for (size_t i = 0; i <= loc.size(); ++i) inc_off.push_back((uint32_t)count[i]);
+        // incidence entries in (cell, corner) order for every node: a fixed summation order
         std::vector<int> fill(count.begin(), count.end() - 1);
         for (int64_t c = c0; c < c1; ++c)
             for (int k = 0; k < 4; ++k) {
@@ -252,8 +516,8 @@ int ensure_blocked_layout(pl_mesh_s* m) {
             }
     }
     begin[nb] = (int32_t)node_ids.size();
-    std::vector<uint8_t> shared(node_ids.size());
-    for (size_t i = 0; i < node_ids.size(); ++i) shared[i] = nblocks_of[node_ids[i]] > 1 ? 1 : 0;
+    for (uint32_t& id : node_ids)
+        if (nblocks_of[id] > 1) id |= kSharedBit;
     int64_t nshared = 0, nuntouched = 0;
     for (int64_t nd = 0; nd < m->nnodes; ++nd) {
         nshared += nblocks_of[nd] > 1;
@@ -275,9 +539,8 @@ int ensure_blocked_layout(pl_mesh_s* m) {
         L->device_bytes += bytes;
     };
     up(&L->d_block_node_begin, begin);
-    up(&L->d_node_ids, node_ids);
+    up(&L->d_slot_node, node_ids);
     up(&L->d_local_cells, lconn);
-    up(&L->d_slot_shared, shared);
     up(&L->d_inc_off, inc_off);
     up(&L->d_inc, inc);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -292,9 +555,8 @@ int ensure_blocked_layout(pl_mesh_s* m) {
 void free_blocked_layout(BlockedLayout* b) {
     if (!b) return;
     cudaFree(b->d_block_node_begin);
-    cudaFree(b->d_node_ids);
+    cudaFree(b->d_slot_node);
     cudaFree(b->d_local_cells);
-    cudaFree(b->d_slot_shared);
     cudaFree(b->d_inc_off);
     cudaFree(b->d_inc);
     delete b;

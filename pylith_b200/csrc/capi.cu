@@ -670,6 +670,12 @@ int pl_compute_lhs_jacobian_action_f32(pl_integrator ig, double t, double dt, co
     p.out32 = jv;
     p.t = t;
     p.dt = dt;
+    if (use_blocked(ig) && (rc = ensure_blocked_layout(m)) == PL_OK &&
+        launch_domain_jv32_blocked(p, *m->blocked, m->cell_type, rheo, m->nnodes, s)) {
+        PLB_CUDA(cudaGetLastError());
+        return PL_OK;
+    }
+    if (rc) return rc;
     launch_domain_jv_f32_atomic(p, m->cell_type, rheo, s);
     PLB_CUDA(cudaGetLastError());
     return PL_OK;

@@ -46,11 +46,11 @@ struct BlockedLayout {
     int cells_per_block = 0;
     int64_t num_blocks = 0;
     int max_local_nodes = 0;
-    int32_t* d_block_node_begin = nullptr;  // [num_blocks + 1] into node_ids
-    int32_t* d_node_ids = nullptr;          // global node of each block-local slot (sorted per block)
+    int32_t* d_block_node_begin = nullptr;  // [num_blocks + 1] into slot_node
+    uint32_t* d_slot_node = nullptr;        // global node of each block-local slot (sorted per block),
+                                            // high bit set if other blocks also touch the node
     uint16_t* d_local_cells = nullptr;      // [ncells][4] block-local slot of each cell corner
-    uint8_t* d_slot_shared = nullptr;       // per slot: 1 if other blocks also touch the node
-    uint16_t* d_inc_off = nullptr;          // per block: ns+1 offsets into the block's incidence list
+    uint32_t* d_inc_off = nullptr;          // per block: ns+1 offsets into the block's incidence list
     uint16_t* d_inc = nullptr;              // [num_blocks][4 * cells_per_block] (cell * 4 + corner)
     int64_t num_shared_nodes = 0;
     int64_t num_untouched = 0;

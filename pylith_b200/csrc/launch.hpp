@@ -35,6 +35,10 @@ bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, 
                                  int rheo, bool bf, int op, bool insert, int64_t nnodes,
                                  cudaStream_t s);
 
+// FP32 Jacobian action on the cell blocks (the output must be zeroed or hold the sum to add to).
+bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,
+                                cudaStream_t s);
+
 struct CohesiveParams {
     const int32_t* coh;      // [ncoh][12]
     int64_t ncoh;
