@@ -293,6 +293,21 @@ int pl_solver_get_stats(pl_solver solver, int* iterations, int* inner_iterations
                         int* outer_iterations, double* rel_residual);
 int pl_solver_destroy(pl_solver solver);
 
+/* ---- batched right-hand sides (Green's functions; replaces the one-impulse-at-a-time
+ *      SNES loop of libsrc/pylith/problems/GreensFns.cc:291-337) ------------------------------ */
+/* Solves A x_i = b_i for many right-hand sides with the operator, constraints, preconditioner and
+ * tolerances of `base` (after pl_solver_setup). Tiles of `tile` (1, 2, 4 or 8) right-hand sides
+ * share every launch of an FP32 PCG (FP64 dot products, CUDA-graph replay between convergence
+ * checks) inside FP64 iterative refinement per right-hand side. b_dev/x_dev are arrays of nrhs
+ * device pointers to full local vectors. P1 tetrahedra with isotropic linear elasticity. */
+typedef struct pl_batch_solver_s* pl_batch_solver;
+int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out);
+int pl_batch_solver_solve(pl_batch_solver solver, int nrhs, const double* const* b_dev,
+                          double* const* x_dev);
+int pl_batch_solver_get_stats(pl_batch_solver solver, int64_t* solves, int64_t* inner_iterations,
+                              int64_t* outer_iterations, double* max_rel_residual);
+int pl_batch_solver_destroy(pl_batch_solver solver);
+
 #ifdef __cplusplus
 }
 #endif

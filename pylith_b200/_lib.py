@@ -112,6 +112,11 @@ SIGNATURES = {
                                  ctypes.POINTER(_D)]),
     "pl_solver_apply_fault_slip": (_I, [_P, _P, _P]),
     "pl_solver_destroy": (_I, [_P]),
+    "pl_batch_solver_create": (_I, [_P, _I, ctypes.POINTER(_P)]),
+    "pl_batch_solver_solve": (_I, [_P, _I, _P, _P]),
+    "pl_batch_solver_get_stats": (_I, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                                       ctypes.POINTER(_D)]),
+    "pl_batch_solver_destroy": (_I, [_P]),
 }
 PL_SOLVER_FP64, PL_SOLVER_FP32_REFINED = 0, 1
 

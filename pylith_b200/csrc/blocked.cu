@@ -62,8 +62,8 @@ struct BlockArrays {
     int max_local_nodes;
 };
 
-// Shared-memory buffer of one block: node data [maxloc][8] doubles (x, y, z, u0, u1, u2, -, -:
-// three 16-byte loads per node), node ids [maxloc],
+// Shared-memory buffer of one block: node data [maxloc][6] doubles (x, y, z, u0, u1, u2),
+// node ids [maxloc],
 // incidence offsets [maxloc + 1], incidence list [4 * kTetBlockCells].
 struct SmemBuf {
     double* node;
@@ -75,14 +75,14 @@ struct SmemBuf {
 PL_HD size_t round16(size_t x) { return (x + 15) & ~size_t(15); }
 
 PL_HD size_t buf_bytes(int maxloc) {
-    return round16(64 * (size_t)maxloc) + round16(4 * (size_t)maxloc) + round16(4 * ((size_t)maxloc + 1)) +
+    return round16(48 * (size_t)maxloc) + round16(4 * (size_t)maxloc) + round16(4 * ((size_t)maxloc + 1)) +
            round16(2 * 4 * (size_t)kTetBlockCells);
 }
 
 PL_D SmemBuf make_buf(char* base, int maxloc) {
     SmemBuf s;
     s.node = reinterpret_cast<double*>(base);
-    base += round16(64 * (size_t)maxloc);
+    base += round16(48 * (size_t)maxloc);
     s.id = reinterpret_cast<uint32_t*>(base);
     base += round16(4 * (size_t)maxloc);
     s.off = reinterpret_cast<uint32_t*>(base);
@@ -104,8 +104,8 @@ PL_D void prefetch_block(const DomainParams& p, const double* __restrict__ field
             const int64_t node = nd[k] & ~kSharedBit;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                __pipeline_memcpy_async(&s.node[8 * i + d], &p.coords[3 * node + d], sizeof(double));
-                __pipeline_memcpy_async(&s.node[8 * i + 3 + d], &field[3 * node + d], sizeof(double));
+                __pipeline_memcpy_async(&s.node[6 * i + d], &p.coords[3 * node + d], sizeof(double));
+                __pipeline_memcpy_async(&s.node[6 * i + 3 + d], &field[3 * node + d], sizeof(double));
             }
             s.id[i] = nd[k];
         }
@@ -178,16 +178,12 @@ __global__ void __launch_bounds__(kTetBlockCells, PLB_TET_MIN_BLOCKS) k_tet_bloc
             const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
             double X[4][3], U[4][3];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const double2* nd2 = reinterpret_cast<const double2*>(S.node + 8 * ln[k]);
-                const double2 a01 = nd2[0], a23 = nd2[1], a45 = nd2[2];
-                X[k][0] = a01.x;
-                X[k][1] = a01.y;
-                X[k][2] = a23.x;
-                U[k][0] = a23.y;
-                U[k][1] = a45.x;
-                U[k][2] = a45.y;
-            }
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    X[k][d] = S.node[6 * ln[k] + d];
+                    U[k][d] = S.node[6 * ln[k] + 3 + d];
+                }
             double cof[3][3];
             const double det = tet_cofactors(X, cof);
             if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);

@@ -137,3 +137,30 @@ struct pl_matrix_s {
     int32_t* d_cell_pos = nullptr;  // [ncells][nen][nen] block index of each element block
     int32_t* d_coh_pos = nullptr;   // [ncoh][4 (blocks)][4][4]
 };
+
+// Device Krylov solver state (csrc/solver.cu); the batched solver (csrc/multirhs.cu) reuses its
+// operator, mask, preconditioner and fault pairs.
+struct pl_solver_s {
+    pl_mesh mesh = nullptr;
+    std::vector<pl_integrator> ops;
+    int64_t n = 0;       // DOFs (3 per node)
+    int64_t nnodes = 0;  // node rows
+    uint8_t* d_mask = nullptr;
+    double* d_diag = nullptr;
+    double* d_pinv = nullptr;
+    float* d_pinv32 = nullptr;
+    double *d_r = nullptr, *d_p = nullptr, *d_q = nullptr, *d_z = nullptr, *d_x = nullptr;
+    float *f_r = nullptr, *f_p = nullptr, *f_q = nullptr, *f_z = nullptr, *f_x = nullptr;
+    double* d_scal = nullptr;
+    double* d_partials = nullptr;
+    int64_t npairs = 0;               // fault nodes (Lagrange nodes)
+    int32_t* d_pair_neg = nullptr;    // negative-side node of each fault node
+    int32_t* d_pair_pos = nullptr;    // positive-side node
+    double* d_pair_normal = nullptr;  // fault normal at each fault node
+    double rtol = 1e-12, atol = 0.0, inner_rtol = 1e-5;
+    int max_iter = 10000, precision = 0, check_every = 10;
+    double t = 0.0, dt = 0.0;
+    int iterations = 0, inner_iterations = 0, outer_iterations = 0;
+    double rel_residual = 0.0;
+    bool ready = false;
+};

@@ -348,3 +348,37 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+class BatchSolver:
+    """Many right-hand sides with the operator and preconditioner of a set-up `Solver`
+    (pl_batch_solver_*): tiles of `tile` RHS share each FP32 PCG launch, FP64 refinement per RHS."""
+
+    def __init__(self, solver: Solver, tile: int = 8):
+        self.solver = solver
+        self.handle = ctypes.c_void_p()
+        check(C.lib().pl_batch_solver_create(solver.handle, tile, ctypes.byref(self.handle)))
+
+    def solve(self, bs, xs) -> None:
+        n = len(bs)
+        pb = (ctypes.c_void_p * max(n, 1))(*[_ptr(b) for b in bs])
+        px = (ctypes.c_void_p * max(n, 1))(*[_ptr(x) for x in xs])
+        check(C.lib().pl_batch_solver_solve(self.handle, n, pb, px))
+
+    def stats(self):
+        s, i, o, r = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+        check(C.lib().pl_batch_solver_get_stats(self.handle, ctypes.byref(s), ctypes.byref(i), ctypes.byref(o),
+                                                ctypes.byref(r)))
+        return {"solves": s.value, "inner_iterations": i.value, "outer_iterations": o.value,
+                "max_rel_residual": r.value}
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_batch_solver_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

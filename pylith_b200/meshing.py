@@ -260,3 +260,48 @@ def insert_fault_x(mesh: Mesh, x0: float = 0.0, tol: float = 1e-6) -> Mesh:
     coh = np.concatenate([neg, pos, lag], axis=1).astype(np.int32)
     return Mesh(CELL_HEX8, np.ascontiguousarray(new_coords), cells.astype(np.int32), coh,
                 len(plane_nodes))
+
+
+# Kuhn split of a hexahedron (corner order above) into 6 tetrahedra around the 0-6 diagonal;
+# every hexahedron uses the same diagonal direction, so the split is conforming across faces.
+_KUHN = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6], [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]])
+
+
+def box_tet_kuhn(nx: int, ny: int, nz: int, lo=BOX_LO, hi=BOX_HI, fault_x: float | None = None,
+                 jitter: float = 0.1, seed: int = 0, reorder: bool = True) -> Mesh:
+    """P1 tetrahedra from a Kuhn split of a hex grid, nodes jittered by up to `jitter` times the
+    spacing (boundary nodes stay on their faces, fault nodes on the fault plane).
+
+    With `fault_x`, a planar vertical fault of cohesive cells is inserted at x = fault_x first
+    (`insert_fault_x`); the cohesive cells stay the quadrilateral hex faces on the plane, whose
+    two triangles are faces of the adjacent tetrahedra. This is how the Green's-function mesh
+    gets a fault that is a union of cell faces, which a Delaunay triangulation of random points
+    does not provide.
+    """
+    hexes = box_hex(nx, ny, nz, lo, hi)
+    if fault_x is not None:
+        hexes = insert_fault_x(hexes, fault_x)
+    coords = hexes.coords.copy()
+    lo_a, hi_a = np.asarray(lo, float), np.asarray(hi, float)
+    h = (hi_a - lo_a) / np.array([nx, ny, nz])
+    rng = np.random.default_rng(seed)
+    delta = rng.uniform(-jitter, jitter, coords.shape) * h
+    for d in range(3):
+        on = np.isclose(coords[:, d], lo_a[d]) | np.isclose(coords[:, d], hi_a[d])
+        delta[on, d] = 0.0
+    if fault_x is not None:
+        delta[np.isclose(coords[:, 0], fault_x), 0] = 0.0
+        # both sides of a split node move together
+        nn0 = (nx + 1) * (ny + 1) * (nz + 1)
+        plane = np.nonzero(np.isclose(hexes.coords[:nn0, 0], fault_x))[0]
+        delta[nn0:nn0 + len(plane)] = delta[plane]
+    coords = coords + delta
+    tets = hexes.cells[:, _KUHN].reshape(-1, 4).astype(np.int64)
+    vol = _tet_volumes(coords, tets)
+    neg = vol < 0
+    tets[neg, 2], tets[neg, 3] = tets[neg, 3].copy(), tets[neg, 2].copy()
+    if np.any(np.abs(vol) < 1e-12 * np.abs(vol).mean()):
+        raise RuntimeError("degenerate tetrahedron after jitter; lower the jitter")
+    mesh = Mesh(CELL_TET4, np.ascontiguousarray(coords), tets.astype(np.int32), hexes.cohesive,
+                hexes.num_lagrange)
+    return reorder_for_locality(mesh) if reorder else mesh
