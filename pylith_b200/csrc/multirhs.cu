@@ -350,6 +350,10 @@ struct pl_batch_solver_s {
     double* jx64 = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
+    // The solve runs on a private stream (graph capture is not possible on the legacy default
+    // stream a caller may use), fenced against the caller's stream with events.
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int64_t solves = 0, inner_iterations = 0, outer_iterations = 0;
     double max_rel_residual = 0.0;
 };
@@ -589,6 +593,17 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     A(&B->part_b, (size_t)kBBlocks * 8);
     A(&B->r64, B->n);
     A(&B->jx64, B->n);
+    // the cell-block layout is built here, outside any stream capture
+    if (e == cudaSuccess) {
+        const int rc = ensure_blocked_layout(base->mesh);
+        if (rc) {
+            pl_batch_solver_destroy(B);
+            return rc;
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ev_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ev_out, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         pl_batch_solver_destroy(B);
         return cuda_fail(e, "pl_batch_solver_create");
@@ -601,22 +616,29 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
     if (!B || nrhs < 0 || (nrhs > 0 && (!b_dev || !x_dev))) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     pl_solver S = B->base;
     if (!S->ready) return fail(PL_ERR_NOT_READY, "call pl_solver_setup on the base solver first");
-    PLB_CUDA(cudaSetDevice(S->mesh->ctx->device));
+    pl_context c = S->mesh->ctx;
+    PLB_CUDA(cudaSetDevice(c->device));
     B->solves = B->inner_iterations = B->outer_iterations = 0;
     B->max_rel_residual = 0.0;
-    for (int r0 = 0; r0 < nrhs; r0 += B->K) {
+    cudaStream_t user = c->stream;
+    PLB_CUDA(cudaEventRecord(B->ev_in, user));
+    PLB_CUDA(cudaStreamWaitEvent(B->stream, B->ev_in, 0));
+    c->stream = B->stream;
+    int rc = PL_OK;
+    for (int r0 = 0; r0 < nrhs && rc == PL_OK; r0 += B->K) {
         const int nact = std::min(B->K, nrhs - r0);
-        int rc = PL_OK;
         switch (B->K) {
             case 1: rc = solve_tile<1>(B, nact, b_dev + r0, x_dev + r0); break;
             case 2: rc = solve_tile<2>(B, nact, b_dev + r0, x_dev + r0); break;
             case 4: rc = solve_tile<4>(B, nact, b_dev + r0, x_dev + r0); break;
             default: rc = solve_tile<8>(B, nact, b_dev + r0, x_dev + r0); break;
         }
-        if (rc) return rc;
-        B->solves += nact;
+        if (rc == PL_OK) B->solves += nact;
     }
-    return PL_OK;
+    c->stream = user;
+    cudaEventRecord(B->ev_out, B->stream);
+    cudaStreamWaitEvent(user, B->ev_out, 0);
+    return rc;
 }
 
 int pl_batch_solver_get_stats(pl_batch_solver B, int64_t* solves, int64_t* inner_iterations, int64_t* outer_iterations,
@@ -635,6 +657,10 @@ int pl_batch_solver_destroy(pl_batch_solver B) {
     cudaSetDevice(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
     if (B->graph) cudaGraphExecDestroy(B->graph);
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    if (B->ev_in) cudaEventDestroy(B->ev_in);
+    if (B->ev_out) cudaEventDestroy(B->ev_out);
+    if (B->stream) cudaStreamDestroy(B->stream);
     void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64};
     for (void* p : ptrs)
         if (p) cudaFree(p);
