@@ -10,6 +10,7 @@ The L2 cache (126 MB) is flushed (256 MiB write) before every application, becau
 application's working set (~53 MB) would otherwise stay cached between applications.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pylith_b200|reference]
+  python bench.py --config c0|c1q2|c2|c3|c4     (the other configurations, one JSON line each)
 
 Under torchrun (N > 1) every rank runs the same workload on its own GPU (weak scaling, its own
 seeded mesh); the slowest rank's device time defines the step time.
@@ -194,8 +195,13 @@ def main():
     ap.add_argument("--impl", default="pylith_b200")
     ap.add_argument("--cells", type=int, default=TARGET_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1q2", "c2", "c3", "c4"])
+    ap.add_argument("--scale", type=float, default=1.0, help="size factor for the --config runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.config != "c1":
+        print(json.dumps(CONFIGS[args.config](args)), flush=True)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -339,6 +345,245 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# The other configurations (one JSON line each). They are measurements recorded beside the
+# headline, not driver bench lines.
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # CPU baseline leg only
+
+    return O
+
+
+def _ev_time(fn, reps=1):
+    import torch
+
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def config_c0(args):
+    """16^3 Q1 hex, uniform material, ux = -/+1 on the x faces, uy = 0 on the y faces (the
+    reference test's y-face constraint, without which uy is a nullspace), uz = 0 at the bottom:
+    residual, assembled Jacobian and the linear solve against the closed-form uniaxial answer."""
+    import scipy.sparse.linalg as spla
+    import torch
+
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import materials as MAT
+    from pylith_b200 import meshing as M
+
+    O = _oracle()
+    mesh = M.box_hex(16, 16, 16)
+    rho, mu, K = MAT.uniform_elastic(mesh.num_cells, 2500.0, 3000.0, 5291.503)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    bc = np.zeros((mesh.num_nodes, 3))
+    for sd, val in (("neg", -1.0), ("pos", 1.0)):
+        m = M.boundary_mask(mesh, 0, sd)
+        cons[m, 0] = True
+        bc[m, 0] = val
+        cons[M.boundary_mask(mesh, 1, sd), 1] = True
+    cons[M.boundary_mask(mesh, 2, "neg"), 2] = True
+    cons, bc = cons.ravel(), bc.ravel()
+    ctx = FA.Context(0)
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm)
+    u = torch.from_numpy(np.where(cons, bc, 0.0)).cuda()
+    F = torch.zeros_like(u)
+    t_res = _ev_time(lambda: ig.compute_lhs_residual(0.0, 0.0, u, F), reps=20)
+    A = FA.Matrix(dm)
+    t_jac = _ev_time(lambda: (A.zero(), ig.compute_lhs_jacobian(0.0, 0.0, 0.0, u, A)), reps=5)
+    S = FA.Solver(dm, cons, [ig], rtol=1e-12)
+    S.setup()
+    du = torch.zeros_like(u)
+    ig.compute_lhs_residual(0.0, 0.0, u, F)
+    t_solve = _ev_time(lambda: S.solve(F, du))
+    sol = (u + du).cpu().numpy().reshape(-1, 3)
+    # closed form: exx = 2/12000, eyy = 0, szz = 0 -> ezz = -lam exx / (lam + 2 mu)
+    lam = K[0] - 2.0 / 3.0 * mu[0]
+    exx = 2.0 / 12000.0
+    ezz = -lam * exx / (lam + 2.0 * mu[0])
+    X = mesh.coords
+    exact = np.stack([exx * X[:, 0], 0 * X[:, 1], ezz * (X[:, 2] + 9000.0)], axis=1)
+    err = np.abs(sol - exact).max() / np.abs(exact).max()
+    # CPU: oracle residual, element Jacobians + assembly, scipy direct solve
+    aux = O.AuxFields([(rho[:, None], "cell"), (mu[:, None], "cell"), (K[:, None], "cell")])
+    un = np.where(cons, bc, 0.0)
+    t0 = time.perf_counter()
+    r = O.residual(mesh, un, aux, f1="IsotropicLinearElasticity3D::f1v_infinitesimalStrain")
+    c_res = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J = O.assemble(mesh, O.jacobian_elements(mesh, aux, g3="IsotropicLinearElasticity3D::Jf3vu_infinitesimalStrain"))
+    c_jac = time.perf_counter() - t0
+    free = ~cons
+    t0 = time.perf_counter()
+    spla.spsolve(J[free][:, free].tocsc(), -r[free])
+    c_solve = time.perf_counter() - t0
+    return {"config": "c0", "cells": mesh.num_cells, "dof": mesh.num_dof,
+            "gpu_ms": {"residual": t_res * 1e3, "jacobian_assembly": t_jac * 1e3, "solve": t_solve * 1e3},
+            "solve": S.stats(), "max_rel_error_vs_closed_form": float(err),
+            "cpu_ms": {"residual": c_res * 1e3, "jacobian_assembly": c_jac * 1e3, "direct_solve": c_solve * 1e3,
+                       "cores": os.cpu_count(), "what": "oracle cell loop + scipy spsolve"}}
+
+
+def config_c1q2(args):
+    """64^3 Q2 hexahedra (27 nodes, 3x3x3 Gauss), log-normal material: FP64 residual and Jacobian
+    action GDOF/s; bound: FP64 arithmetic."""
+    import torch
+
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import materials as MAT
+    from pylith_b200 import meshing as M
+
+    n = max(4, int(round(64 * args.scale)))
+    mesh = M.box_hex27(n, n, n)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    ctx = FA.Context(0)
+    ig = mat.create_integrator(FA.DeviceMesh(ctx, mesh))
+    ndof = mesh.num_dof
+    u = torch.randn(ndof, dtype=torch.float64, device="cuda")
+    r = torch.empty_like(u)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        ig.compute_lhs_residual(0.0, 0.0, u, r)
+        ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, u, u, r)
+    times = {"residual": [], "jv": []}
+    for _ in range(max(args.steps, 3)):
+        flush.zero_()
+        times["residual"].append(_ev_time(lambda: ig.compute_lhs_residual(0.0, 0.0, u, r)))
+        flush.zero_()
+        times["jv"].append(_ev_time(lambda: ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, u, u, r)))
+    tr, tj = np.mean(times["residual"]), np.mean(times["jv"])
+    flop_per_cell = 27 * (2 * 27 * 9 + 2 * 27 * 9 + 2 * 8 * 9 + 120)  # gradient, contraction, geometry, pointwise
+    return {"config": "c1q2", "cells": mesh.num_cells, "dof": ndof,
+            "gdof_s_residual_plus_jv": 2 * ndof / (tr + tj) / 1e9,
+            "ms_residual": tr * 1e3, "ms_jv": tj * 1e3,
+            "fp64_tflops_residual": mesh.num_cells * flop_per_cell / tr / 1e12,
+            "flop_per_cell_counted": flop_per_cell}
+
+
+def config_c2(args):
+    """96x96x72 Q1 hex, generalized Maxwell (3 elements, 1e18/1e19/1e20 Pa s, ratios 0.3), planar
+    vertical fault at x = 0 with 2 m left-lateral slip (step at t = 0), state per quadrature point,
+    steps of 1 yr: FP64 vs FP32-refined solver, time per step and displacement difference."""
+    import torch
+
+    from pylith_b200 import materials as MAT
+    from pylith_b200 import meshing as M
+    from pylith_b200 import problems as P
+
+    nx, ny, nz = (max(4, int(round(v * args.scale))) for v in (96, 96, 72))
+    nx += nx % 2
+    steps = max(1, int(round(50 * min(1.0, args.scale))))
+    mesh = M.insert_fault_x(M.box_hex(nx, ny, nz))
+    nc, nq = mesh.num_cells, 8
+    rho, mu, K = MAT.lognormal_elastic(nc, seed=0)
+    tau = MAT.genmaxwell_times(rho, np.sqrt(mu / rho), [1e18, 1e19, 1e20], [0.3, 0.3, 0.3])
+    ratio = np.tile([0.3, 0.3, 0.3], (nc, 1))
+    z = np.zeros((nc, nq, 18)), np.zeros((nc, nq, 6))
+    slip = np.tile([0.0, 2.0, 0.0], (mesh.num_lagrange, 1))
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg")] = True
+    cons[M.boundary_mask(mesh, 0, "pos")] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    bc = np.zeros(mesh.num_dof)
+    dt = MAT.YEAR
+    out = {"config": "c2", "cells": nc, "dof": mesh.num_dof, "steps": steps}
+    from pylith_b200 import feassemble as FA
+
+    ctx = FA.Context(0)
+    sols = {}
+    for name, prec in (("fp64", FA.Solver.FP64), ("fp32_refined", FA.Solver.FP32_REFINED)):
+        g = MAT.IsotropicLinearGenMaxwell(rho, mu, K, tau, ratio, z[0], z[1])
+        prob = P.QuasistaticProblem(ctx, mesh, [(g, None)], cons, bc, faults=[MAT.FaultCohesiveKin(slip)],
+                                    dt=dt, precision=prec, rtol=1e-10, inner_rtol=1e-4)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        its = 0
+        for k in range(1, steps + 1):
+            st = prob.step(k * dt)
+            its += st.iterations + st.inner_iterations
+        ctx.synchronize()
+        el = time.perf_counter() - t0
+        sols[name] = prob.u.cpu().numpy()
+        out[name] = {"s_per_step": el / steps, "iterations_per_step": its / steps}
+    nd = 3 * mesh.num_nodes
+    out["rel_displacement_diff_fp32_vs_fp64"] = float(
+        np.linalg.norm(sols["fp32_refined"][:nd] - sols["fp64"][:nd]) / np.linalg.norm(sols["fp64"][:nd]))
+    out["speedup_fp32_refined"] = out["fp64"]["s_per_step"] / out["fp32_refined"]["s_per_step"]
+    return out
+
+
+def config_c3(args):
+    """Green's functions: tetrahedral mesh (Kuhn split of a jittered 64x80x48 hex grid, 1.47 M
+    tets) of [-12,12]x[-15,15]x[-20,0] km with a vertical fault at x = 0; 40x25 unit-slip patches
+    over y in [-12,12] km, z in [-15,0] km, left-lateral then reverse. Batched FP32-refined
+    solves vs one-at-a-time FP64 solves on samples of the 2000 impulses."""
+    import torch
+
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import greensfns as GF
+    from pylith_b200 import materials as MAT
+    from pylith_b200 import meshing as M
+
+    dims = [max(4, int(round(v * args.scale))) for v in (64, 80, 48)]
+    dims[0] += dims[0] % 2
+    lo, hi = (-12000.0, -15000.0, -20000.0), (12000.0, 15000.0, 0.0)
+    mesh = M.box_tet_kuhn(*dims, lo=lo, hi=hi, fault_x=0.0, seed=0)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    for sd in ("neg", "pos"):
+        cons[M.boundary_mask(mesh, 0, sd, lo, hi)] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    patches = GF.fault_patches(mesh, (-12000.0, 12000.0), (-15000.0, 0.0), 40, 25)
+    ctx = FA.Context(0)
+    g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-10, inner_rtol=1e-4, tile=8)
+    nb = max(8, int(args.steps) * 8)
+    ns = max(2, int(args.steps) // 2)
+    step = max(1, len(g.impulses) // nb)
+    sample_b = g.impulses[::step][:nb]
+    sol_b, t_b = g.solve(sample_b, batched=True)
+    sample_s = sample_b[:ns]
+    sol_s, t_s = g.solve(sample_s, batched=False)
+    err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(sol_b[:ns], sol_s))
+    return {"config": "c3", "cells": mesh.num_cells, "dof": mesh.num_dof, "impulses_total": len(g.impulses),
+            "batched": {"sample": len(sample_b), "solves_per_s": len(sample_b) / t_b, **g.batch.stats()},
+            "fp64_one_at_a_time": {"sample": len(sample_s), "solves_per_s": len(sample_s) / t_s,
+                                   "iterations_last": g.solver64.stats()["iterations"]},
+            "speedup": (len(sample_b) / t_b) / (len(sample_s) / t_s),
+            "max_rel_displacement_error_vs_fp64": err}
+
+
+def config_c4(args):
+    """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
+    material, random rectangular left-lateral slip patch of 0.1-3 m. Server (FP32-refined, 8 slots,
+    HBM-budget admission) vs the FP64 one-at-a-time path on the same stream."""
+    from pylith_b200 import serving as SV
+
+    count = max(8, int(40 * args.scale))
+    reqs = SV.poisson_requests(count, rate=200.0, seed=0, n_min=8, n_max=max(8, int(96 * min(1.0, args.scale))))
+    served = SV.Server(slots=8).run(reqs)
+    seq = SV.serve_sequential(reqs)
+    a, b = SV.summarize(served), SV.summarize(seq)
+    return {"config": "c4", "requests": count, "server": a, "fp64_one_at_a_time": b,
+            "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"]}
+
+
+CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c4": config_c4}
 
 
 if __name__ == "__main__":

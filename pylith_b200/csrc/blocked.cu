@@ -27,8 +27,11 @@
 
 namespace plb {
 
-constexpr int kTetBlockCells = 256;
-constexpr int kMaxSlotsPerThread = 2;  // blocks touching more than 2 * 256 nodes use the atomic kernel
+#ifndef PLB_TET_BLOCK
+#define PLB_TET_BLOCK 256
+#endif
+constexpr int kTetBlockCells = PLB_TET_BLOCK;
+constexpr int kMaxSlotsPerThread = 512 / PLB_TET_BLOCK;  // blocks touching more than 512 nodes use the atomic kernel
 constexpr uint32_t kSharedBit = 0x80000000u;
 
 // cof[i][j] = det(J) (J^{-1})[i][j] with J = [X1-X0, X2-X0, X3-X0] (columns); returns det(J).
@@ -112,7 +115,7 @@ PL_D void prefetch_block(const DomainParams& p, const double* __restrict__ field
     }
     for (int i = threadIdx.x; i <= ns; i += blockDim.x)
         __pipeline_memcpy_async(&s.off[i], &A.inc_off[s0 + b + i], sizeof(uint32_t));
-    // 4 * kTetBlockCells uint16 = 128 chunks of 16 bytes
+    // 4 * kTetBlockCells uint16 = kTetBlockCells / 2 chunks of 16 bytes
     for (int i = threadIdx.x; i < kTetBlockCells / 2; i += blockDim.x)
         __pipeline_memcpy_async(&s.inc[8 * i], &A.inc[b * 4 * kTetBlockCells + 8 * i], 16);
 }
@@ -143,9 +146,9 @@ __global__ void __launch_bounds__(kTetBlockCells, PLB_TET_MIN_BLOCKS) k_tet_bloc
     const size_t bb = buf_bytes(A.max_local_nodes);
     const int64_t G = gridDim.x;
     int64_t b = blockIdx.x;
-    uint32_t nd_next[kMaxSlotsPerThread] = {0u, 0u};
+    uint32_t nd_next[kMaxSlotsPerThread] = {};
     {
-        uint32_t nd0[kMaxSlotsPerThread] = {0u, 0u};
+        uint32_t nd0[kMaxSlotsPerThread] = {};
         load_slot_ids(A, b, nd0);
         if (b < A.nblocks) prefetch_block(p, field, A, b, nd0, make_buf(bufbase, A.max_local_nodes));
         __pipeline_commit();
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(kTetBlockCells, PLB_TET_MIN_BLOCKS) k_tet_bloc
             lc = A.lconn[c];
             L::load_cell(p, c, a);
         }
-        uint32_t nd_after[kMaxSlotsPerThread] = {0u, 0u};
+        uint32_t nd_after[kMaxSlotsPerThread] = {};
         load_slot_ids(A, b + 2 * G, nd_after);
         __pipeline_wait_prior(0);
         __syncthreads();

@@ -26,7 +26,10 @@
 
 namespace plb {
 
-constexpr int kMultiBlockCells = 256;  // must match the cell-block layout
+#ifndef PLB_TET_BLOCK
+#define PLB_TET_BLOCK 256
+#endif
+constexpr int kMultiBlockCells = PLB_TET_BLOCK;  // the cell-block layout's cells per block
 constexpr uint32_t kSharedBitM = 0x80000000u;
 
 PL_D double tet_cof_m(const double X[4][3], double cof[3][3]) {
