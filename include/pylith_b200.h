@@ -245,6 +245,17 @@ int pl_compute_lhs_jacobian_action_f32(pl_integrator integ, double t, double dt,
  * back (the end-to-end path a CPU caller takes). */
 int pl_compute_lhs_residual_host(pl_integrator integ, double t, double dt, const double* u_host,
                                  double* r_host);
+/* No counterpart in the reference. The host-buffer residual above, for callers that must not
+ * allocate device memory during a call (a process whose HBM is reserved up front by a pool it
+ * does not own, or a latency-bound step loop where cudaMalloc would stall the device). It
+ * stages u and r through one fixed 16 MiB device array built into the library (held on every
+ * GPU that loads it until exit) and so accepts meshes of at most 1048576 DOFs, returning
+ * PL_ERR_INVALID_ARG beyond that. Uses the thread-per-cell kernels. The first call on each
+ * device looks up the array's address and should come before any stream capture. All calls
+ * share the array: calls whose GPU work overlaps (two host threads, two streams) race on it;
+ * each call waits for its stream before returning. */
+int pl_compute_lhs_residual_host_noalloc(pl_integrator integ, double t, double dt,
+                                         const double* u_host, double* r_host);
 /* DMProjectFieldLocal with the registered update-state kernels (IntegratorDomain.cc:555-590):
  * replaces the per-quadrature-point state subfields in place. */
 int pl_update_state_vars(pl_integrator integ, double t, double dt, const double* u_dev);

@@ -93,6 +93,7 @@ SIGNATURES = {
     "pl_compute_lhs_jacobian_action": (_I, [_P, _D, _D, _D, _P, _P, _P, _I]),
     "pl_compute_lhs_jacobian_action_f32": (_I, [_P, _D, _D, _P, _P, _I]),
     "pl_compute_lhs_residual_host": (_I, [_P, _D, _D, _P, _P]),
+    "pl_compute_lhs_residual_host_noalloc": (_I, [_P, _D, _D, _P, _P]),
     "pl_update_state_vars": (_I, [_P, _D, _D, _P]),
     "pl_matrix_create": (_I, [_P, ctypes.POINTER(_P)]),
     "pl_matrix_zero": (_I, [_P]),

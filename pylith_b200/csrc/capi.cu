@@ -127,6 +127,19 @@ int bind_domain_jacobian(pl_integrator_s* ig, DomainParams* p) {
     return bind_domain(ig, rheology_of(ig, true), false, p);
 }
 
+int bind_domain_residual(pl_integrator_s* ig, DomainParams* p, int* rheo, bool* bf) {
+    *rheo = rheology_of(ig, false);
+    *bf = ig->r0 == K_G0V_BODYFORCE;
+    return bind_domain(ig, (Rheology)*rheo, *bf, p);
+}
+
+int bind_cohesive_residual(pl_integrator_s* ig, CohesiveParams* p) {
+    int rc = bind_cohesive(ig, p);
+    if (rc) return rc;
+    if (ig->if_r[2] != K_NONE && !p->slip) return fail(PL_ERR_INVALID_ARG, "aux subfield slip is required");
+    return PL_OK;
+}
+
 }  // namespace plb
 
 using namespace plb;

@@ -63,4 +63,9 @@ void launch_cohesive_jv_f32(const CohesiveParams& p, cudaStream_t s);
 void launch_cohesive_jacobian(const CohesiveParams& p, const int32_t* pos, double* vals,
                               cudaStream_t s);
 
+// Aux binding of an integrator for its registered residual kernels (rheology and body-force
+// switch of a domain integrator are returned).
+int bind_domain_residual(pl_integrator_s* ig, DomainParams* p, int* rheo, bool* bf);
+int bind_cohesive_residual(pl_integrator_s* ig, CohesiveParams* p);
+
 }  // namespace plb
