@@ -136,7 +136,7 @@ def profiled_traffic(mesh):
     return float(d["dram_bytes_per_cell"]) * mesh.num_cells
 
 
-def cpu_baseline(mesh, mat, source: str, budget_s: float = 12.0):
+def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
     """Oracle cell loop on every host core: residual F(u) plus a second pass of the same loop
     standing in for J v (linear elasticity: F(u) = J u), repeated within a time budget."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -155,10 +155,17 @@ def cpu_baseline(mesh, mat, source: str, budget_s: float = 12.0):
     while True:
         O.residual(mesh, u, aux, f1=f1, source=source, nthreads=cores)
         apps += 1
-        if time.perf_counter() - t0 > budget_s or apps >= 40:
+        if time.perf_counter() - t0 > budget_s or apps >= 5000:
             break
     dt = time.perf_counter() - t0
+    apps1 = 0
+    t1 = time.perf_counter()
+    while apps1 < 3 and (apps1 == 0 or time.perf_counter() - t1 < 0.25 * budget_s):
+        O.residual(mesh, u, aux, f1=f1, source=source, nthreads=1)
+        apps1 += 1
+    dt1 = time.perf_counter() - t1
     return {"value": mesh.num_dof * apps / dt / 1e9, "unit": UNIT, "cores": cores,
+            "one_core_value": mesh.num_dof * apps1 / dt1 / 1e9,
             "kind": "reference" if source == "ref" else "port",
             "sample": (f"{apps} applications over the full {mesh.num_cells}-cell mesh in {dt:.1f} s; "
                        "oracle cell loop (restated PETSc DMPlexComputeResidual) calling "
@@ -284,31 +291,61 @@ def main():
         t_total, t_res, t_jv = tt.tolist()
     value = world * 2 * n * args.steps / t_total / 1e9
 
-    # End to end through the public API with host buffers: H2D of u and v from pinned memory,
-    # residual and J v, D2H of both results, every step.
-    hu = torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(u.cpu())
-    hv = torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(v.cpu())
-    hr = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    hjv = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    # End to end through the public API with host buffers: every step copies its u and v from
+    # pinned host memory, computes the residual and J v, and copies both results back. Copies in
+    # and out run on their own streams and the device buffers alternate between steps, so one
+    # step's transfers overlap the neighbouring steps' work (PCIe is full duplex).
+    hu = [torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(u.cpu()) for _ in range(2)]
+    hv = [torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(v.cpu()) for _ in range(2)]
+    hr = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    hjv = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    du = [u, torch.empty_like(u)]
+    dv = [v, torch.empty_like(v)]
+    dr = [r, torch.empty_like(r)]
+    djv = [jv, torch.empty_like(jv)]
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_res = [torch.cuda.Event() for _ in range(2)]
+    ev_done = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
+    for i in range(2):  # every buffer starts free
+        ev_done[i].record(stream)
+        ev_out[i].record(stream)
 
-    def e2e_step():
-        u.copy_(hu, non_blocking=True)
-        v.copy_(hv, non_blocking=True)
-        app_residual()
-        app_jv()
-        hr.copy_(r, non_blocking=True)
-        hjv.copy_(jv, non_blocking=True)
+    def e2e_step(k):
+        i = k % 2
+        s_in.wait_event(ev_done[i])  # inputs of step k - 2 consumed
+        with torch.cuda.stream(s_in):
+            du[i].copy_(hu[i], non_blocking=True)
+            dv[i].copy_(hv[i], non_blocking=True)
+            ev_in[i].record(s_in)
+        stream.wait_event(ev_in[i])
+        stream.wait_event(ev_out[i])  # results of step k - 2 copied out
+        ig.compute_lhs_residual(0.0, 0.0, du[i], dr[i])
+        ev_res[i].record(stream)
+        ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, du[i], dv[i], djv[i])
+        ev_done[i].record(stream)
+        s_out.wait_event(ev_res[i])
+        with torch.cuda.stream(s_out):
+            hr[i].copy_(dr[i], non_blocking=True)
+            s_out.wait_event(ev_done[i])
+            hjv[i].copy_(djv[i], non_blocking=True)
+            ev_out[i].record(s_out)
 
-    for _ in range(args.warmup):
-        e2e_step()
+    for k in range(args.warmup):
+        e2e_step(k)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
+    s_in.wait_event(e0)
+    s_out.wait_event(e0)
+    for k in range(args.steps):
+        e2e_step(k)
+    for i in range(2):
+        stream.wait_event(ev_out[i])
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = e0.elapsed_time(e1) / 1e3
@@ -554,8 +591,11 @@ def config_c3(args):
     g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-10, inner_rtol=1e-4, tile=8)
     nb = max(8, int(args.steps) * 8)
     ns = max(2, int(args.steps) // 2)
-    step = max(1, len(g.impulses) // nb)
-    sample_b = g.impulses[::step][:nb]
+    usable = [imp for imp in g.impulses if len(patches[imp.patch]) > 0]  # coarse meshes leave some patches empty
+    step = max(1, len(usable) // nb)
+    sample_b = usable[::step][:nb]
+    g.solve(sample_b[:8], batched=True)  # warm-up: captures the batched solver's CUDA graph
+    g.solve(sample_b[:1], batched=False)
     sol_b, t_b = g.solve(sample_b, batched=True)
     sample_s = sample_b[:ns]
     sol_s, t_s = g.solve(sample_s, batched=False)

@@ -260,6 +260,19 @@ int pl_compute_lhs_residual_host_noalloc(pl_integrator integ, double t, double d
  * replaces the per-quadrature-point state subfields in place. */
 int pl_update_state_vars(pl_integrator integ, double t, double dt, const double* u_dev);
 
+/* Derived (output) fields of basis order 0, the default for cauchy_stress and cauchy_strain
+ * (IntegratorDomain::setKernelsDerivedField, IntegratorDomain.cc:233-240; Elasticity.cc:629-651
+ * registers them). Supported project kernels: Elasticity3D::infinitesimalStrain_asVector and the
+ * cauchyStress_infinitesimalStrain_asVector of the integrator's material; at most 4. */
+int pl_integrator_set_kernels_derived_field(pl_integrator integ, const pl_project_kernels* kernels,
+                                            int num_kernels);
+/* IntegratorDomain::_computeDerivedField (IntegratorDomain.cc:596-630): every registered
+ * kernel evaluated at each cell's centroid (PETSc's order-0 dual basis), written to
+ * out_dev[cell][6 * k + i] (Voigt order xx, yy, zz, xy, yz, xz) for the integrator's cells in
+ * order. The generalized Maxwell stress is available on P1 tetrahedra. */
+int pl_compute_derived_field(pl_integrator integ, double t, double dt, const double* u_dev,
+                             double* out_dev);
+
 /* ---- assembled Jacobian (DMPlexComputeJacobianByKey, IntegratorDomain.cc:489) ---------- */
 /* Block-CSR matrix with 3x3 blocks over the mesh's node graph (plus Lagrange nodes). */
 int pl_matrix_create(pl_mesh mesh, pl_matrix* out);

@@ -43,17 +43,19 @@ struct Elasticity3D {
     PYLITH_B200_POINTFN(infinitesimalStrain_asVector);
 };
 
-// IsotropicLinearElasticity.hh:804-838, 891-1035
+// IsotropicLinearElasticity.hh:804-838, 891-1035, 1243-1273
 struct IsotropicLinearElasticity3D {
     PYLITH_B200_POINTFN(f1v_infinitesimalStrain);
     PYLITH_B200_JACFN(Jf3vu_infinitesimalStrain);
+    PYLITH_B200_POINTFN(cauchyStress_infinitesimalStrain_asVector);
 };
 
-// IsotropicLinearGenMaxwell.hh:1054-1087, 1143-1300, 1507-1549
+// IsotropicLinearGenMaxwell.hh:1054-1087, 1143-1300, 1507-1549, 1556-1589
 struct IsotropicLinearGenMaxwell3D {
     PYLITH_B200_POINTFN(f1v_infinitesimalStrain);
     PYLITH_B200_JACFN(Jf3vu_infinitesimalStrain);
     PYLITH_B200_POINTFN(viscousStrain_infinitesimalStrain_asVector);
+    PYLITH_B200_POINTFN(cauchyStress_infinitesimalStrain_asVector);
 };
 
 // FaultCohesiveKin.hh:74-225, 298-412

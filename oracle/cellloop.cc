@@ -56,7 +56,9 @@ void lagrange1d(int order, double x, double* v, double* d) {
 }
 
 void gauss1d(int n, double* x, double* w) {
-    if (n == 2) {
+    if (n == 1) {
+        x[0] = 0.0; w[0] = 2.0;
+    } else if (n == 2) {
         const double a = 1.0 / std::sqrt(3.0);
         x[0] = -a; x[1] = a; w[0] = w[1] = 1.0;
     } else {
@@ -70,7 +72,9 @@ void gauss1d(int n, double* x, double* w) {
 const int kHexCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
                               {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
 
-Element make_element(int type) {
+// centre: a single evaluation point at the cell centroid (the order-0 dual basis of derived
+// fields) instead of the quadrature rule.
+Element make_element(int type, bool centre = false) {
     Element e;
     if (type == TET4) {
         // Reference tetrahedron (0,0,0),(1,0,0),(0,1,0),(0,0,1); one point at the centroid.
@@ -84,7 +88,7 @@ Element make_element(int type) {
     }
     const int order = (type == HEX8) ? 1 : 2;
     const int np1 = order + 1;          // nodes per direction
-    const int nqd = (type == HEX8) ? 2 : 3;
+    const int nqd = centre ? 1 : ((type == HEX8) ? 2 : 3);
     e.nen = np1 * np1 * np1;
     e.nq = nqd * nqd * nqd;
     e.ngeom = 8;
@@ -424,6 +428,48 @@ int64_t oracle_project_qp(int cell_type, int64_t ncells, const int* cells, const
     return bad;
 }
 
+// Derived fields of basis order 0 (IntegratorDomain::_computeDerivedField,
+// IntegratorDomain.cc:596-630): each function evaluated once per cell at the centroid,
+// out_k[cell][ncomp_k]. Aux subfields per quadrature point are read at point 0.
+int64_t oracle_project_centroid(int cell_type, int64_t ncells, const int* cells, const double* coords,
+                                const double* u, int numA, const int* aux_kind, const int* aux_ncomp,
+                                const double* const* aux_data, double t, int numConstants,
+                                const double* constants, int nfn, const PointFn* fns,
+                                const int* out_ncomp, double* const* outs, int nthreads) {
+    const Element e = make_element(cell_type, true);
+    const Element eq = make_element(cell_type);
+    const Aux aux(numA, aux_kind, aux_ncomp, aux_data);
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    int64_t bad = 0;
+#pragma omp parallel num_threads(nthreads)
+    {
+        std::vector<double> a(aux.total > 0 ? aux.total : 1);
+        QPoint p;
+        const int sOff[1] = {0}, sOff_x[1] = {0};
+        double s[3], s_t[3] = {0, 0, 0}, s_x[9];
+        std::vector<double> o(64);
+#pragma omp for schedule(static)
+        for (int64_t cell = 0; cell < ncells; ++cell) {
+            const int* cn = &cells[cell * e.nen];
+            if (!eval_geometry(e, 0, cn, coords, &p)) {
+#pragma omp critical
+                { if (!bad) bad = -(cell + 1); }
+                continue;
+            }
+            eval_field(e, 0, p, cn, u, s, s_x);
+            aux.eval(eq, cell, 0, cn, a.data());
+            for (int k = 0; k < nfn; ++k) {
+                const int nc = out_ncomp[k];
+                std::fill(o.begin(), o.begin() + nc, 0.0);
+                fns[k](3, 1, numA, sOff, sOff_x, s, s_t, s_x, aux.off.data(), nullptr, a.data(), nullptr,
+                       nullptr, t, p.x, numConstants, constants, o.data());
+                for (int c = 0; c < nc; ++c) outs[k][cell * nc + c] = o[c];
+            }
+        }
+    }
+    return bad;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Cohesive cells (DMPlexCompute{Residual,Jacobian}HybridByKey, IntegratorInterface.cc:603-720).
 // Each cohesive cell is a quadrilateral fault face: coh[c*12 + 0..3] negative-side vertices,
@@ -603,6 +649,8 @@ ORACLE_EXPORT_POINT(oracle_gm3d_f1v, gm3d_f1v)
 ORACLE_EXPORT_JAC(oracle_gm3d_Jf3vu, gm3d_Jf3vu)
 ORACLE_EXPORT_POINT(oracle_gm3d_viscous_strain, gm3d_viscous_strain)
 ORACLE_EXPORT_POINT(oracle_el3d_strain_vector, el3d_strain_vector)
+ORACLE_EXPORT_POINT(oracle_ile3d_stress_vector, ile3d_stress_vector)
+ORACLE_EXPORT_POINT(oracle_gm3d_stress_vector, gm3d_stress_vector)
 ORACLE_EXPORT_BD(oracle_fck_f0u_neg, fck_f0u_neg)
 ORACLE_EXPORT_BD(oracle_fck_f0u_pos, fck_f0u_pos)
 ORACLE_EXPORT_BD(oracle_fck_f0l_slip, fck_f0l_slip)

@@ -50,6 +50,7 @@ def lib():
         _lib.oracle_residual.restype = _I64
         _lib.oracle_jacobian_elements.restype = _I64
         _lib.oracle_project_qp.restype = _I64
+        _lib.oracle_project_centroid.restype = _I64
     return _lib
 
 
@@ -81,6 +82,12 @@ KERNELS = {
         "ref_IsotropicLinearGenMaxwell3D_viscousStrain_infinitesimalStrain_asVector", "point"),
     "Elasticity3D::infinitesimalStrain_asVector": (
         "oracle_el3d_strain_vector", "ref_Elasticity3D_infinitesimalStrain_asVector", "point"),
+    "IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector": (
+        "oracle_ile3d_stress_vector", "ref_IsotropicLinearElasticity3D_cauchyStress_infinitesimalStrain_asVector",
+        "point"),
+    "IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector": (
+        "oracle_gm3d_stress_vector", "ref_IsotropicLinearGenMaxwell3D_cauchyStress_infinitesimalStrain_asVector",
+        "point"),
     "FaultCohesiveKin::f0u_neg": ("oracle_fck_f0u_neg", "ref_FaultCohesiveKin_f0u_neg", "bd"),
     "FaultCohesiveKin::f0u_pos": ("oracle_fck_f0u_pos", "ref_FaultCohesiveKin_f0u_pos", "bd"),
     "FaultCohesiveKin::f0l_slip": ("oracle_fck_f0l_slip", "ref_FaultCohesiveKin_f0l_slip", "bd"),
@@ -188,6 +195,27 @@ def project_qp(mesh, u, aux: AuxFields, fns, out_ncomp, t=0.0, constants=None, n
                               _p(np.ascontiguousarray(u, dtype=np.float64)), _I(aux.num),
                               _p(aux.kinds), _p(aux.ncomp), aux.ptrs, _D(t), _I(nc), _p(c),
                               _I(len(fns)), fptrs, _p(oc), optrs, _I(nthreads))
+    if bad:
+        raise ValueError(f"non-positive Jacobian determinant in cell {-bad - 1}")
+    return outs
+
+
+def project_centroid(mesh, u, aux: AuxFields, fns, out_ncomp, t=0.0, constants=None, nthreads=0,
+                     source="oracle"):
+    """Derived fields of basis order 0: each kernel at every cell centroid -> [ncells][ncomp]."""
+    L = lib()
+    outs = [np.zeros((mesh.num_cells, n)) for n in out_ncomp]
+    cells = np.ascontiguousarray(mesh.cells, dtype=np.int32)
+    coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+    c = np.ascontiguousarray(constants if constants is not None else [0.0], dtype=np.float64)
+    nc = 0 if constants is None else len(constants)
+    fptrs = (_P * len(fns))(*[kernel(f, source) for f in fns])
+    optrs = (_P * len(outs))(*[o.ctypes.data for o in outs])
+    oc = np.array(out_ncomp, dtype=np.int32)
+    bad = L.oracle_project_centroid(_I(mesh.cell_type), _I64(mesh.num_cells), _p(cells), _p(coords),
+                                    _p(np.ascontiguousarray(u, dtype=np.float64)), _I(aux.num),
+                                    _p(aux.kinds), _p(aux.ncomp), aux.ptrs, _D(t), _I(nc), _p(c),
+                                    _I(len(fns)), fptrs, _p(oc), optrs, _I(nthreads))
     if bad:
         raise ValueError(f"non-positive Jacobian determinant in cell {-bad - 1}")
     return outs

@@ -242,6 +242,54 @@ static inline void el3d_strain_vector(ORACLE_POINT_ARGS, const Real x[], Int num
     out[0] = e.xx; out[1] = e.yy; out[2] = e.zz; out[3] = e.xy; out[4] = e.yz; out[5] = e.xz;
 }
 
+// Stress tensor as a vector, xx, yy, zz, xy, yz, xz (Elasticity::stress_asVector,
+// Elasticity.hh:441-456).
+static inline void stress_to_vector(const Sym& s, Real out[]) {
+    out[0] = s.xx; out[1] = s.yy; out[2] = s.zz; out[3] = s.xy; out[4] = s.yz; out[5] = s.xz;
+}
+
+// IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector
+// (IsotropicLinearElasticity.hh:1243-1273): IsotropicLinearElasticity::cauchyStress
+// (:183-193) = meanStress then deviatoricStress.
+static inline void ile3d_stress_vector(ORACLE_POINT_ARGS, const Real x[], Int numConstants,
+                                       const Real constants[], Real out[]) {
+    const Real mu = a[aOff[numA - 2]];
+    const Real K = a[aOff[numA - 1]];
+    const Sym e = strain_from_grad(&s_x[sOff_x[0]]);
+    Sym sig;
+    add_mean_stress(K, e, &sig);
+    add_dev_stress(mu, e, &sig);
+    stress_to_vector(sig, out);
+}
+
+// IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector
+// (IsotropicLinearGenMaxwell.hh:1556-1589) with cauchyStress_stateVars (:340-357): the stored
+// viscous strains, not updated.
+static inline void gm3d_stress_vector(ORACLE_POINT_ARGS, const Real x[], Int numConstants,
+                                      const Real constants[], Real out[]) {
+    const GenMaxwellCtx c = genmaxwell_ctx(numA, aOff, a, constants);
+    const Sym e = strain_from_grad(&s_x[sOff_x[0]]);
+    Sym sig;
+    add_mean_stress(c.K, e, &sig);
+    const Sym de = deviatoric(e);
+    Real ratio = 1.0;
+    for (int i = 0; i < 3; ++i) ratio -= c.ratio[i];
+    const Real mu_el = c.mu * ratio;
+    sig.xx += 2.0 * mu_el * de.xx;
+    for (int i = 0; i < 3; ++i) sig.xx += 2.0 * c.mu * c.ratio[i] * c.visc[i].xx;
+    sig.yy += 2.0 * mu_el * de.yy;
+    for (int i = 0; i < 3; ++i) sig.yy += 2.0 * c.mu * c.ratio[i] * c.visc[i].yy;
+    sig.zz += 2.0 * mu_el * de.zz;
+    for (int i = 0; i < 3; ++i) sig.zz += 2.0 * c.mu * c.ratio[i] * c.visc[i].zz;
+    sig.xy += 2.0 * mu_el * de.xy;
+    for (int i = 0; i < 3; ++i) sig.xy += 2.0 * c.mu * c.ratio[i] * c.visc[i].xy;
+    sig.yz += 2.0 * mu_el * de.yz;
+    for (int i = 0; i < 3; ++i) sig.yz += 2.0 * c.mu * c.ratio[i] * c.visc[i].yz;
+    sig.xz += 2.0 * mu_el * de.xz;
+    for (int i = 0; i < 3; ++i) sig.xz += 2.0 * c.mu * c.ratio[i] * c.visc[i].xz;
+    stress_to_vector(sig, out);
+}
+
 // BoundaryDirections::_unitCrossProduct (BoundaryDirections.hh:248-270).
 static inline void unit_cross(Real r[3], const Real a[3], const Real b[3]) {
     r[0] = +a[1] * b[2] - a[2] * b[1];

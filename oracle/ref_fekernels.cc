@@ -60,6 +60,10 @@ REF_POINT(ref_IsotropicLinearGenMaxwell3D_viscousStrain_infinitesimalStrain_asVe
           fk::IsotropicLinearGenMaxwell3D::viscousStrain_infinitesimalStrain_asVector)
 REF_POINT(ref_Elasticity3D_infinitesimalStrain_asVector,
           fk::Elasticity3D::infinitesimalStrain_asVector)
+REF_POINT(ref_IsotropicLinearElasticity3D_cauchyStress_infinitesimalStrain_asVector,
+          fk::IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector)
+REF_POINT(ref_IsotropicLinearGenMaxwell3D_cauchyStress_infinitesimalStrain_asVector,
+          fk::IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector)
 REF_BD_POINT(ref_FaultCohesiveKin_f0u_neg, fk::FaultCohesiveKin::f0u_neg)
 REF_BD_POINT(ref_FaultCohesiveKin_f0u_pos, fk::FaultCohesiveKin::f0u_pos)
 REF_BD_POINT(ref_FaultCohesiveKin_f0l_slip, fk::FaultCohesiveKin::f0l_slip)

@@ -95,6 +95,8 @@ SIGNATURES = {
     "pl_compute_lhs_residual_host": (_I, [_P, _D, _D, _P, _P]),
     "pl_compute_lhs_residual_host_noalloc": (_I, [_P, _D, _D, _P, _P]),
     "pl_update_state_vars": (_I, [_P, _D, _D, _P]),
+    "pl_integrator_set_kernels_derived_field": (_I, [_P, ctypes.POINTER(ProjectKernelsC), _I]),
+    "pl_compute_derived_field": (_I, [_P, _D, _D, _P, _P]),
     "pl_matrix_create": (_I, [_P, ctypes.POINTER(_P)]),
     "pl_matrix_zero": (_I, [_P]),
     "pl_compute_lhs_jacobian": (_I, [_P, _D, _D, _D, _P, _P]),

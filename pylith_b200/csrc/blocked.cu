@@ -30,8 +30,15 @@ namespace plb {
 #ifndef PLB_TET_BLOCK
 #define PLB_TET_BLOCK 256
 #endif
+#ifndef PLB_TET_CPT
+#define PLB_TET_CPT 1
+#endif
 constexpr int kTetBlockCells = PLB_TET_BLOCK;
-constexpr int kMaxSlotsPerThread = 512 / PLB_TET_BLOCK;  // blocks touching more than 512 nodes use the atomic kernel
+// cells per thread of the FP64 cell-block kernel (two independent cells per thread give the
+// scheduler more independent instructions per warp)
+constexpr int kTetCellsPerThread = PLB_TET_CPT;
+constexpr int kTetThreads = kTetBlockCells / kTetCellsPerThread;
+constexpr int kMaxSlotsPerThread = 512 / kTetThreads;  // blocks touching more than 512 nodes use the atomic kernel
 constexpr uint32_t kSharedBit = 0x80000000u;
 
 // cof[i][j] = det(J) (J^{-1})[i][j] with J = [X1-X0, X2-X0, X3-X0] (columns); returns det(J).
@@ -65,15 +72,21 @@ struct BlockArrays {
     int max_local_nodes;
 };
 
-// Shared-memory buffer of one block: node data [maxloc][6] doubles (x, y, z, u0, u1, u2),
-// node ids [maxloc],
-// incidence offsets [maxloc + 1], incidence list [4 * kTetBlockCells].
+// Shared-memory buffer of one block: node data, 6 doubles per node (x, y, z, u0, u1, u2; see
+// node_index), node ids [maxloc], incidence offsets [maxloc + 1], incidence list
+// [4 * kTetBlockCells].
 struct SmemBuf {
     double* node;
     uint32_t* id;
     uint32_t* off;
     uint16_t* inc;
+    int ld;  // leading dimension of the node arrays
 };
+
+// Word index of component d (0-2 coordinates, 3-5 field) of block-local node i. Component-major
+// storage makes consecutive nodes fall in consecutive bank pairs, so the random node reads of a
+// warp spread over all 16 bank pairs (a 6-double record per node reaches only 8 of them).
+PL_D int node_index(const SmemBuf& s, int i, int d) { return d * s.ld + i; }
 
 PL_HD size_t round16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -84,6 +97,7 @@ PL_HD size_t buf_bytes(int maxloc) {
 
 PL_D SmemBuf make_buf(char* base, int maxloc) {
     SmemBuf s;
+    s.ld = maxloc;
     s.node = reinterpret_cast<double*>(base);
     base += round16(48 * (size_t)maxloc);
     s.id = reinterpret_cast<uint32_t*>(base);
@@ -107,8 +121,8 @@ PL_D void prefetch_block(const DomainParams& p, const double* __restrict__ field
             const int64_t node = nd[k] & ~kSharedBit;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                __pipeline_memcpy_async(&s.node[6 * i + d], &p.coords[3 * node + d], sizeof(double));
-                __pipeline_memcpy_async(&s.node[6 * i + 3 + d], &field[3 * node + d], sizeof(double));
+                __pipeline_memcpy_async(&s.node[node_index(s, i, d)], &p.coords[3 * node + d], sizeof(double));
+                __pipeline_memcpy_async(&s.node[node_index(s, i, 3 + d)], &field[3 * node + d], sizeof(double));
             }
             s.id[i] = nd[k];
         }
@@ -131,12 +145,91 @@ PL_D void load_slot_ids(const BlockArrays& A, int64_t b, uint32_t nd[kMaxSlotsPe
     }
 }
 
+#ifndef PLB_PREFETCH_CELLS
+#define PLB_PREFETCH_CELLS 1
+#endif
+
+PL_D void prefetch_l2(const void* ptr) { asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr)); }
+
 #ifndef PLB_TET_MIN_BLOCKS
 #define PLB_TET_MIN_BLOCKS 4
 #endif
 
+// Element vector of one cell (block slot `slot`) into the staging array sE.
+template <int RHEO, bool BF, int OP>
+PL_D void tet_cell_element(const DomainParams& p, const int* aoff, const double* a, ushort4 lc, const SmemBuf& S,
+                           double* sE, int slot) {
+    using L = AuxLayout<RHEO, BF>;
+    const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
+    double X[4][3], U[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            X[k][d] = S.node[node_index(S, ln[k], d)];
+            U[k][d] = S.node[node_index(S, ln[k], 3 + d)];
+        }
+    double cof[3][3];
+    const double det = tet_cofactors(X, cof);
+    if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+    const double rdet = 1.0 / det;
+    // G[c][k] = u_{k+1}[c] - u_0[c]; s_x = G cof / det
+    double Gm[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) Gm[cc][k] = U[k + 1][cc] - U[0][cc];
+    double s_x[9];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            s_x[cc * 3 + d] = (Gm[cc][0] * cof[0][d] + Gm[cc][1] * cof[1][d] + Gm[cc][2] * cof[2][d]) * rdet;
+    double x[3] = {0, 0, 0}, s[3] = {0, 0, 0};
+    double f0[3] = {0, 0, 0}, f1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (OP == OP_RESIDUAL) {
+        if (BF) {
+            const int sOff[1] = {0}, sOff_x[1] = {0};
+            pw::g0v_bodyforce<double>(3, 1, L::numA, sOff, sOff_x, s, nullptr, s_x, aoff, nullptr, a, nullptr,
+                                      nullptr, p.t, x, p.num_constants, p.constants, f0);
+        }
+        call_f1<RHEO>(L::numA, aoff, a, s, s_x, p, x, f1);
+    } else {
+        double Jf3[81];
+#pragma unroll
+        for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
+        call_jf3<RHEO>(L::numA, aoff, a, p, x, Jf3);
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+#pragma unroll
+            for (int df = 0; df < 3; ++df) {
+                double acc1 = 0.0;
+#pragma unroll
+                for (int gg = 0; gg < 3; ++gg)
+#pragma unroll
+                    for (int dg = 0; dg < 3; ++dg) acc1 += Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
+                f1[f * 3 + df] = acc1;
+            }
+    }
+    // corners 1..3: |J|/6 * f1 . grad(phi_a) = f1 . cof_{a-1} / 6; corner 0: minus their sum,
+    // plus the body-force term |J|/6 * f0 / 4 at every corner.
+    const double sixth = 1.0 / 6.0;
+    const double bfw = BF && OP == OP_RESIDUAL ? det * sixth * 0.25 : 0.0;
+    double e0[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+            const double v = (f1[cc * 3 + 0] * cof[k][0] + f1[cc * 3 + 1] * cof[k][1] + f1[cc * 3 + 2] * cof[k][2]) * sixth;
+            e0[cc] -= v;
+            sE[((k + 1) * 3 + cc) * kTetBlockCells + slot] = v + bfw * f0[cc];
+        }
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + slot] = e0[cc] + bfw * f0[cc];
+}
+
 template <int RHEO, bool BF, int OP, bool INSERT>
-__global__ void __launch_bounds__(kTetBlockCells, PLB_TET_MIN_BLOCKS) k_tet_blocked(DomainParams p, BlockArrays A) {
+__global__ void __launch_bounds__(kTetThreads, PLB_TET_MIN_BLOCKS) k_tet_blocked(DomainParams p, BlockArrays A) {
     using L = AuxLayout<RHEO, BF>;
     extern __shared__ __align__(16) char smem_raw[];
     const AuxOffsets<RHEO, BF> aoff;
@@ -159,98 +252,53 @@ __global__ void __launch_bounds__(kTetBlockCells, PLB_TET_MIN_BLOCKS) k_tet_bloc
         const int s0 = A.slot_begin[b];
         const int ns = A.slot_begin[b + 1] - s0;
         const int tc = threadIdx.x;
-        const int64_t c = b * kTetBlockCells + tc;
         // per-cell inputs and the slot ids two blocks ahead: issued before the wait
-        ushort4 lc = make_ushort4(0, 0, 0, 0);
-        double a[L::size];
-        if (c < p.ncells) {
-            lc = A.lconn[c];
-            L::load_cell(p, c, a);
+        ushort4 lc[kTetCellsPerThread];
+        double a[kTetCellsPerThread][L::size];
+#pragma unroll
+        for (int j = 0; j < kTetCellsPerThread; ++j) {
+            const int64_t c = b * kTetBlockCells + tc + j * kTetThreads;
+            lc[j] = make_ushort4(0, 0, 0, 0);
+            if (c < p.ncells) {
+                lc[j] = A.lconn[c];
+                L::load_cell(p, c, a[j]);
+            }
         }
         uint32_t nd_after[kMaxSlotsPerThread] = {};
         load_slot_ids(A, b + 2 * G, nd_after);
         __pipeline_wait_prior(0);
         __syncthreads();
-        if (b + G < A.nblocks)
+        if (b + G < A.nblocks) {
             prefetch_block(p, field, A, b + G, nd_next, make_buf(bufbase + (cur ^ 1) * bb, A.max_local_nodes));
+#if PLB_PREFETCH_CELLS
+            // the next block's per-cell inputs, streamed once: start their trip to L2 now
+#pragma unroll
+            for (int j = 0; j < kTetCellsPerThread; ++j) {
+                const int64_t cn = (b + G) * kTetBlockCells + tc + j * kTetThreads;
+                if (cn < p.ncells) {
+                    prefetch_l2(&A.lconn[cn]);
+                    prefetch_l2(&p.mu[cn]);
+                    prefetch_l2(&p.K[cn]);
+                    if (BF)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) prefetch_l2(&p.body_force[d * p.ncells + cn]);
+                }
+            }
+#endif
+        }
         __pipeline_commit();
 #pragma unroll
         for (int k = 0; k < kMaxSlotsPerThread; ++k) nd_next[k] = nd_after[k];
         const SmemBuf S = make_buf(bufbase + cur * bb, A.max_local_nodes);
-        if (c < p.ncells) {
-            const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
-            double X[4][3], U[4][3];
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    X[k][d] = S.node[6 * ln[k] + d];
-                    U[k][d] = S.node[6 * ln[k] + 3 + d];
-                }
-            double cof[3][3];
-            const double det = tet_cofactors(X, cof);
-            if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
-            const double rdet = 1.0 / det;
-            // G[c][k] = u_{k+1}[c] - u_0[c]; s_x = G cof / det
-            double Gm[3][3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) Gm[cc][k] = U[k + 1][cc] - U[0][cc];
-            double s_x[9];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc)
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    s_x[cc * 3 + d] = (Gm[cc][0] * cof[0][d] + Gm[cc][1] * cof[1][d] + Gm[cc][2] * cof[2][d]) * rdet;
-            double x[3] = {0, 0, 0}, s[3] = {0, 0, 0};
-            double f0[3] = {0, 0, 0}, f1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            if (OP == OP_RESIDUAL) {
-                if (BF) {
-                    const int sOff[1] = {0}, sOff_x[1] = {0};
-                    pw::g0v_bodyforce<double>(3, 1, L::numA, sOff, sOff_x, s, nullptr, s_x, aoff.v, nullptr, a,
-                                              nullptr, nullptr, p.t, x, p.num_constants, p.constants, f0);
-                }
-                call_f1<RHEO>(L::numA, aoff.v, a, s, s_x, p, x, f1);
-            } else {
-                double Jf3[81];
-#pragma unroll
-                for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
-                call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
-#pragma unroll
-                for (int f = 0; f < 3; ++f)
-#pragma unroll
-                    for (int df = 0; df < 3; ++df) {
-                        double acc1 = 0.0;
-#pragma unroll
-                        for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                            for (int dg = 0; dg < 3; ++dg)
-                                acc1 += Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                        f1[f * 3 + df] = acc1;
-                    }
-            }
-            // corners 1..3: |J|/6 * f1 . grad(phi_a) = f1 . cof_{a-1} / 6; corner 0: minus their sum,
-            // plus the body-force term |J|/6 * f0 / 4 at every corner.
-            const double sixth = 1.0 / 6.0;
-            const double bfw = BF && OP == OP_RESIDUAL ? det * sixth * 0.25 : 0.0;
-            double e0[3] = {0, 0, 0};
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    const double v =
-                        (f1[cc * 3 + 0] * cof[k][0] + f1[cc * 3 + 1] * cof[k][1] + f1[cc * 3 + 2] * cof[k][2]) * sixth;
-                    e0[cc] -= v;
-                    sE[((k + 1) * 3 + cc) * kTetBlockCells + tc] = v + bfw * f0[cc];
-                }
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + tc] = e0[cc] + bfw * f0[cc];
-        }
+        for (int j = 0; j < kTetCellsPerThread; ++j)
+            if (b * kTetBlockCells + tc + j * kTetThreads < p.ncells)
+                tet_cell_element<RHEO, BF, OP>(p, aoff.v, a[j], lc[j], S, sE, tc + j * kTetThreads);
         __syncthreads();
         for (int i = threadIdx.x; i < ns; i += blockDim.x) {
             const int j0 = S.off[i], j1 = S.off[i + 1];
             double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+#pragma unroll 4
             for (int j = j0; j < j1; ++j) {
                 const int e = S.inc[j];
                 const int cell = e >> 2, corner = e & 3;
@@ -425,13 +473,13 @@ static void launch_t(const DomainParams& p, const BlockedLayout& b, bool insert,
         cudaFuncSetAttribute(k_tet_blocked<RHEO, BF, OP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     const BlockArrays A = arrays_of(b);
-    if (insert) k_tet_blocked<RHEO, BF, OP, true><<<grid, kTetBlockCells, smem, s>>>(p, A);
-    else k_tet_blocked<RHEO, BF, OP, false><<<grid, kTetBlockCells, smem, s>>>(p, A);
+    if (insert) k_tet_blocked<RHEO, BF, OP, true><<<grid, kTetThreads, smem, s>>>(p, A);
+    else k_tet_blocked<RHEO, BF, OP, false><<<grid, kTetThreads, smem, s>>>(p, A);
     count_launch();
 }
 
 static bool blocked_usable(const BlockedLayout& b) {
-    return b.num_blocks > 0 && b.max_local_nodes <= kMaxSlotsPerThread * kTetBlockCells &&
+    return b.num_blocks > 0 && b.max_local_nodes <= kMaxSlotsPerThread * kTetThreads &&
            blocked_smem(b) <= 200 * 1024;
 }
 

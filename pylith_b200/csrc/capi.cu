@@ -427,6 +427,23 @@ int pl_integrator_set_kernels_update_state_vars(pl_integrator ig, const pl_proje
     return PL_OK;
 }
 
+int pl_integrator_set_kernels_derived_field(pl_integrator ig, const pl_project_kernels* k, int num) {
+    if (!ig || ig->is_interface || num < 0 || num > 4 || (num > 0 && !k))
+        return fail(PL_ERR_INVALID_ARG, "bad arguments (at most 4 derived-field kernels)");
+    std::vector<KernelId> ids;
+    std::vector<std::string> names;
+    for (int i = 0; i < num; ++i) {
+        const KernelId c = lookup_kernel((const void*)k[i].f);
+        if (c != K_EL_STRAIN_VECTOR && c != K_ILE_STRESS_VECTOR && c != K_GM_STRESS_VECTOR)
+            return fail(PL_ERR_UNKNOWN_KERNEL, "unsupported derived-field kernel");
+        ids.push_back(c);
+        names.push_back(k[i].subfield ? k[i].subfield : "");
+    }
+    ig->derived = ids;
+    ig->derived_subfields = names;
+    return PL_OK;
+}
+
 int pl_integrator_interface_set_kernels_residual(pl_integrator ig, const pl_interface_residual_kernels* k, int num) {
     if (!ig || !ig->is_interface || (num > 0 && !k)) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     KernelId r[3] = {K_NONE, K_NONE, K_NONE};
@@ -736,6 +753,39 @@ int pl_update_state_vars(pl_integrator ig, double t, double dt, const double* u)
     p.t = t;
     p.dt = dt;
     launch_domain_update_state(p, m->cell_type, m->ctx->stream);
+    PLB_CUDA(cudaGetLastError());
+    return PL_OK;
+}
+
+int pl_compute_derived_field(pl_integrator ig, double t, double dt, const double* u, double* out) {
+    if (!ig || !u || !out || ig->is_interface) return fail(PL_ERR_INVALID_ARG, "bad arguments");
+    if (ig->derived.empty()) return fail(PL_ERR_NOT_READY, "no derived-field kernels registered");
+    pl_mesh m = ig->mesh;
+    const Rheology rheo = rheology_of(ig, false) != RHEO_NONE ? rheology_of(ig, false) : rheology_of(ig, true);
+    DerivedSpec spec;
+    spec.n = (int)ig->derived.size();
+    for (int i = 0; i < spec.n; ++i) {
+        const KernelId k = ig->derived[i];
+        if (k == K_ILE_STRESS_VECTOR && rheo != RHEO_ILE)
+            return fail(PL_ERR_INVALID_ARG, "the isotropic linear elastic stress needs an isotropic linear elastic material");
+        if (k == K_GM_STRESS_VECTOR && rheo != RHEO_GENMAXWELL)
+            return fail(PL_ERR_INVALID_ARG, "the generalized Maxwell stress needs a generalized Maxwell material");
+        if (k == K_GM_STRESS_VECTOR && m->cell_type != PL_CELL_TET4)
+            return fail(PL_ERR_UNSUPPORTED,
+                        "the generalized Maxwell stress of basis order 0 needs the state at the centroid "
+                        "(P1 tetrahedra, whose single quadrature point is the centroid)");
+        spec.kind[i] = (int)k;
+    }
+    if (rheo == RHEO_NONE) return fail(PL_ERR_NOT_READY, "register the material's residual or Jacobian kernels first");
+    PLB_CUDA(cudaSetDevice(m->ctx->device));
+    DomainParams p;
+    int rc = bind_domain(ig, rheo, false, &p);
+    if (rc) return rc;
+    p.u = u;
+    p.out = out;
+    p.t = t;
+    p.dt = dt;
+    launch_domain_derived(p, m->cell_type, rheo, spec, m->ctx->stream);
     PLB_CUDA(cudaGetLastError());
     return PL_OK;
 }

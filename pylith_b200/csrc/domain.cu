@@ -288,6 +288,63 @@ __global__ void __launch_bounds__(128) k_domain_update_state(DomainParams p) {
     }
 }
 
+// Derived fields of basis order 0 (IntegratorDomain::_computeDerivedField,
+// IntegratorDomain.cc:596-630, with PyLith's default basis order 0 for cauchy_stress and
+// cauchy_strain, DerivedSubfieldsElasticity.py:42-44): each registered project kernel evaluated
+// at the cell centroid, out[c][6 * k + i] for kernel k. A generalized-Maxwell stress reads the
+// state of the cell's single quadrature point (P1 tetrahedra only).
+template <int CELL, int RHEO>
+__global__ void __launch_bounds__(128) k_domain_derived(DomainParams p, DerivedSpec spec) {
+    using E = Elem<CELL>;
+    using L = AuxLayout<RHEO, false>;
+    const AuxOffsets<RHEO, false> aoff;
+    const int nout = 6 * spec.n;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < p.ncells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t mc = p.cell_ids ? p.cell_ids[c] : c;
+        const int32_t* cn = p.cells + mc * E::nen;
+        double X[E::ngeom][3];
+#pragma unroll
+        for (int k = 0; k < E::ngeom; ++k)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)cn[E::corner(k)] + i];
+        Geom g;
+        E::centre_geom(X, &g);
+        if (!(g.detJ > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+        double s_x[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int n = 0; n < E::nen; ++n) {
+            double gr[3];
+            E::centre_grad(g, n, gr);
+            const double* un = p.u + 3 * (int64_t)cn[n];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s_x[0 + d] += un[0] * gr[d];
+                s_x[3 + d] += un[1] * gr[d];
+                s_x[6 + d] += un[2] * gr[d];
+            }
+        }
+        double a[L::size];
+        L::load_cell(p, c, a);
+        L::load_qp(p, c, 0, E::nq, a);
+        const int sOff[1] = {0}, sOff_x[1] = {0};
+        double x[3] = {0, 0, 0};
+        for (int k = 0; k < spec.n; ++k) {
+            double o[6] = {0, 0, 0, 0, 0, 0};
+            if (spec.kind[k] == K_EL_STRAIN_VECTOR)
+                pw::el3d_strain_vector<double>(3, 1, L::numA, sOff, sOff_x, nullptr, nullptr, s_x, aoff.v, nullptr, a,
+                                               nullptr, nullptr, p.t, x, p.num_constants, p.constants, o);
+            else if (RHEO == RHEO_ILE && spec.kind[k] == K_ILE_STRESS_VECTOR)
+                pw::ile3d_stress_vector<double>(3, 1, L::numA, sOff, sOff_x, nullptr, nullptr, s_x, aoff.v, nullptr, a,
+                                                nullptr, nullptr, p.t, x, p.num_constants, p.constants, o);
+            else if (RHEO == RHEO_GENMAXWELL && spec.kind[k] == K_GM_STRESS_VECTOR)
+                pw::gm3d_stress_vector<double>(3, 1, L::numA, sOff, sOff_x, nullptr, nullptr, s_x, aoff.v, nullptr, a,
+                                               nullptr, nullptr, p.t, x, p.num_constants, p.constants, o);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) p.out[c * nout + 6 * k + i] = o[i];
+        }
+    }
+}
+
 static int grid_for(int64_t n, int threads) {
     const int64_t blocks = (n + threads - 1) / threads;
     return (int)(blocks < 148 * 64 ? (blocks > 0 ? blocks : 1) : 148 * 64);
@@ -354,6 +411,22 @@ void launch_domain_update_state(const DomainParams& p, int cell, cudaStream_t s)
     if (cell == TET4) k_domain_update_state<TET4><<<gr, th, 0, s>>>(p);
     else if (cell == HEX8) k_domain_update_state<HEX8><<<gr, th, 0, s>>>(p);
     else k_domain_update_state<HEX27><<<gr, th, 0, s>>>(p);
+    count_launch();
+}
+
+void launch_domain_derived(const DomainParams& p, int cell, int rheo, const DerivedSpec& spec, cudaStream_t s) {
+    if (p.ncells == 0) return;
+    const int th = 128;
+    const int gr = grid_for(p.ncells, th);
+    if (rheo == RHEO_GENMAXWELL) {
+        if (cell == TET4) k_domain_derived<TET4, RHEO_GENMAXWELL><<<gr, th, 0, s>>>(p, spec);
+        else if (cell == HEX8) k_domain_derived<HEX8, RHEO_GENMAXWELL><<<gr, th, 0, s>>>(p, spec);
+        else k_domain_derived<HEX27, RHEO_GENMAXWELL><<<gr, th, 0, s>>>(p, spec);
+    } else {
+        if (cell == TET4) k_domain_derived<TET4, RHEO_ILE><<<gr, th, 0, s>>>(p, spec);
+        else if (cell == HEX8) k_domain_derived<HEX8, RHEO_ILE><<<gr, th, 0, s>>>(p, spec);
+        else k_domain_derived<HEX27, RHEO_ILE><<<gr, th, 0, s>>>(p, spec);
+    }
     count_launch();
 }
 

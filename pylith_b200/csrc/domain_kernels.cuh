@@ -51,6 +51,8 @@ struct Elem<TET4> {
     PL_D static void geom(const double X[][3], int q, Geom* g) { tet_geometry(X, g); }
     PL_D static void grad(const Geom& g, int q, int n, double out[3]) { tet_grad(g, n, out); }
     PL_D static double phi(int q, int n) { return 0.25; }
+    PL_D static void centre_geom(const double X[][3], Geom* g) { tet_geometry(X, g); }
+    PL_D static void centre_grad(const Geom& g, int n, double out[3]) { tet_grad(g, n, out); }
 };
 
 template <>
@@ -68,6 +70,12 @@ struct Elem<HEX8> {
     }
     PL_D static double phi(int q, int n) {
         return hex_corner_N(n, gauss2_x(q & 1), gauss2_x((q >> 1) & 1), gauss2_x(q >> 2));
+    }
+    PL_D static void centre_geom(const double X[][3], Geom* g) { hex_geometry_centre(X, g); }
+    PL_D static void centre_grad(const Geom& g, int n, double out[3]) {
+        const double d[3] = {lin_d(hex_cx(n)) * 0.25, lin_d(hex_cy(n)) * 0.25, lin_d(hex_cz(n)) * 0.25};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) out[j] = d[0] * g.inv[0][j] + d[1] * g.inv[1][j] + d[2] * g.inv[2][j];
     }
 };
 
@@ -91,6 +99,15 @@ struct Elem<HEX27> {
     PL_D static double phi(int q, int n) {
         const double x = gauss3_x(q % 3), y = gauss3_x((q / 3) % 3), z = gauss3_x(q / 9);
         return quad_v(n % 3, x) * quad_v((n / 3) % 3, y) * quad_v(n / 9, z);
+    }
+    PL_D static void centre_geom(const double X[][3], Geom* g) { hex_geometry_centre(X, g); }
+    PL_D static void centre_grad(const Geom& g, int n, double out[3]) {
+        const int a = n % 3, b = (n / 3) % 3, c = n / 9;
+        const double d[3] = {quad_d(a, 0.0) * quad_v(b, 0.0) * quad_v(c, 0.0),
+                             quad_v(a, 0.0) * quad_d(b, 0.0) * quad_v(c, 0.0),
+                             quad_v(a, 0.0) * quad_v(b, 0.0) * quad_d(c, 0.0)};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) out[j] = d[0] * g.inv[0][j] + d[1] * g.inv[1][j] + d[2] * g.inv[2][j];
     }
 };
 

@@ -113,6 +113,22 @@ PL_HD void hex_geometry(const double X[8][3], int qi, int qj, int qk, double w, 
     g->wdetJ = w * g->detJ;
 }
 
+// Trilinear geometry at the cell centre (reference point (0,0,0)): where basis-order-0 derived
+// fields are evaluated (PETSc's order-0 Lagrange dual basis is the value at the centroid).
+PL_HD void hex_geometry_centre(const double X[8][3], Geom* g) {
+    double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const double d[3] = {lin_d(hex_cx(c)) * 0.25, lin_d(hex_cy(c)) * 0.25, lin_d(hex_cz(c)) * 0.25};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) J[i][j] += X[c][i] * d[j];
+    }
+    g->detJ = invert3(J, g->inv);
+    g->wdetJ = 8.0 * g->detJ;
+}
+
 // Affine tetrahedron geometry: reference vertices (0,0,0),(1,0,0),(0,1,0),(0,0,1).
 PL_HD void tet_geometry(const double X[4][3], Geom* g) {
     double J[3][3];

@@ -50,6 +50,16 @@ void fk::IsotropicLinearGenMaxwell3D::viscousStrain_infinitesimalStrain_asVector
     const PylithScalar constants[], PylithScalar f[]) {
     plb::pw::gm3d_viscous_strain<double>(ARGS, x, numConstants, constants, f);
 }
+void fk::IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector(
+    PYLITH_B200_POINT_ARGS, const PylithScalar x[], const PylithInt numConstants,
+    const PylithScalar constants[], PylithScalar f[]) {
+    plb::pw::ile3d_stress_vector<double>(ARGS, x, numConstants, constants, f);
+}
+void fk::IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector(
+    PYLITH_B200_POINT_ARGS, const PylithScalar x[], const PylithInt numConstants,
+    const PylithScalar constants[], PylithScalar f[]) {
+    plb::pw::gm3d_stress_vector<double>(ARGS, x, numConstants, constants, f);
+}
 void fk::FaultCohesiveKin::f0u_neg(PYLITH_B200_POINT_ARGS, const PylithScalar x[],
                                    const PylithReal n[], const PylithInt numConstants,
                                    const PylithScalar constants[], PylithScalar f[]) {
@@ -106,6 +116,10 @@ const Entry kRegistry[] = {
      plb::K_GM_VISCOUS_STRAIN},
     {"Elasticity3D::infinitesimalStrain_asVector",
      (const void*)&fk::Elasticity3D::infinitesimalStrain_asVector, plb::K_EL_STRAIN_VECTOR},
+    {"IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector",
+     (const void*)&fk::IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector, plb::K_ILE_STRESS_VECTOR},
+    {"IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector",
+     (const void*)&fk::IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector, plb::K_GM_STRESS_VECTOR},
     {"FaultCohesiveKin::f0u_neg", (const void*)&fk::FaultCohesiveKin::f0u_neg, plb::K_FCK_F0U_NEG},
     {"FaultCohesiveKin::f0u_pos", (const void*)&fk::FaultCohesiveKin::f0u_pos, plb::K_FCK_F0U_POS},
     {"FaultCohesiveKin::f0l_slip", (const void*)&fk::FaultCohesiveKin::f0l_slip, plb::K_FCK_F0L_SLIP},

@@ -21,6 +21,8 @@ enum KernelId {
     K_GM_JF3VU,
     K_GM_VISCOUS_STRAIN,
     K_EL_STRAIN_VECTOR,
+    K_ILE_STRESS_VECTOR,
+    K_GM_STRESS_VECTOR,
     K_FCK_F0U_NEG,
     K_FCK_F0U_POS,
     K_FCK_F0L_SLIP,
@@ -119,6 +121,8 @@ struct pl_integrator_s {
     plb::KernelId j0 = plb::K_NONE, j3 = plb::K_NONE;
     std::vector<plb::KernelId> project;
     std::vector<std::string> project_subfields;
+    std::vector<plb::KernelId> derived;  // derived-field (output) project kernels
+    std::vector<std::string> derived_subfields;
     // interface kernels: residual per face and Jacobian per face
     plb::KernelId if_r[3] = {plb::K_NONE, plb::K_NONE, plb::K_NONE};
     plb::KernelId if_j[3] = {plb::K_NONE, plb::K_NONE, plb::K_NONE};

@@ -26,6 +26,12 @@ void launch_domain_jacobian(const DomainParams& p, int cell, int rheo, const int
 // Aux binding of a domain integrator for its registered Jacobian kernels.
 int bind_domain_jacobian(pl_integrator_s* ig, DomainParams* p);
 void launch_domain_update_state(const DomainParams& p, int cell, cudaStream_t s);
+// Derived fields of basis order 0: up to 4 registered project kernels, 6 values each per cell.
+struct DerivedSpec {
+    int n;
+    int kind[4];
+};
+void launch_domain_derived(const DomainParams& p, int cell, int rheo, const DerivedSpec& spec, cudaStream_t s);
 // Builds (once per mesh) the cell-block layout used by the blocked scatter.
 int ensure_blocked_layout(pl_mesh_s* m);
 void free_blocked_layout(BlockedLayout* b);

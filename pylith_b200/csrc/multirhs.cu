@@ -7,8 +7,8 @@
 //   * k_tet_blocked_jv32_multi<K>: the FP32 Jacobian action of K vectors per cell block; the
 //     geometry (cofactors, 1/det in FP64), the tangent and the block metadata are read and formed
 //     once and applied to all K vectors, which are interleaved per DOF ([ndof][K]) so one node's
-//     K values are contiguous; element contributions are summed in shared memory (native FP32
-//     shared atomics) and written once per node;
+//     K values are contiguous; element vectors are staged in shared memory a few right-hand
+//     sides at a time and summed per node over the block-local incidence list in a fixed order;
 //   * a batched PCG whose vector kernels update all K vectors with per-RHS step lengths and FP64
 //     dot products, captured in a CUDA graph and replayed between convergence checks;
 //   * FP64 iterative refinement per RHS around the FP32 tile solve (outer residual b - A x in
@@ -52,45 +52,76 @@ PL_D double tet_cof_m(const double X[4][3], double cof[3][3]) {
     return J[0][0] * cof[0][0] + J[0][1] * cof[1][0] + J[0][2] * cof[2][0];
 }
 
+// Chunk of right-hand sides whose element vectors are staged in shared memory at once.
+#ifndef PLB_MULTI_KC
+#define PLB_MULTI_KC 2
+#endif
+template <int K>
+struct MultiChunk {
+    static constexpr int value = K < PLB_MULTI_KC ? K : PLB_MULTI_KC;
+};
+
 // v, out: [ndof][K] FP32 (ndof = 3 * nodes, node-major); out must be zeroed or hold the sum to add to.
+// Per cell block: the block's node coordinates (FP64) and K field vectors (FP32) are staged in
+// shared memory component-major ([3][ld], [3K][ld]); one thread per cell forms the geometry and
+// the isotropic tangent once and then, KC right-hand sides at a time, the element vectors, which
+// are staged ([12][KC][cells]) and summed per node over the block-local incidence list in a fixed
+// order (nodes shared with other blocks get FP32 reductions into global memory).
 template <int K>
 __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     DomainParams p, const int32_t* __restrict__ slot_begin, const uint32_t* __restrict__ slot_node,
-    const ushort4* __restrict__ lconn, int64_t nblocks, const float* __restrict__ v, float* out) {
+    const ushort4* __restrict__ lconn, const uint32_t* __restrict__ inc_off, const uint16_t* __restrict__ inc,
+    int64_t nblocks, int ld, const float* __restrict__ v, float* out) {
+    constexpr int KC = MultiChunk<K>::value;
     using L = AuxLayout<RHEO_ILE, false>;
     extern __shared__ __align__(16) char smem_raw[];
     const AuxOffsets<RHEO_ILE, false> aoff;
+    float* sE = reinterpret_cast<float*>(smem_raw);                                              // [12][KC][cells]
+    double* sX = reinterpret_cast<double*>(smem_raw + 12 * KC * kMultiBlockCells * sizeof(float));  // [3][ld]
+    float* sV = reinterpret_cast<float*>(sX + 3 * ld);                                           // [3K][ld]
+    const int tc = threadIdx.x;
     for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int s0 = slot_begin[b];
         const int ns = slot_begin[b + 1] - s0;
-        double* sX = reinterpret_cast<double*>(smem_raw);       // [ns][3]
-        float* sV = reinterpret_cast<float*>(sX + 3 * ns);        // [ns][3][K]
-        float* sR = sV + 3 * K * ns;                              // [ns][3][K]
-        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+        for (int i = tc; i < ns; i += blockDim.x) {
             const int64_t nd = slot_node[s0 + i] & ~kSharedBitM;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) sX[3 * i + d] = p.coords[3 * nd + d];
+            for (int d = 0; d < 3; ++d) sX[d * ld + i] = p.coords[3 * nd + d];
+            const float* vr = v + 3 * K * nd;
+            if (K % 4 == 0) {
 #pragma unroll
-            for (int j = 0; j < 3 * K; ++j) {
-                sV[3 * K * i + j] = v[3 * K * nd + j];
-                sR[3 * K * i + j] = 0.0f;
+                for (int j = 0; j < 3 * K; j += 4) {
+                    const float4 q = *reinterpret_cast<const float4*>(vr + j);
+                    sV[(j + 0) * ld + i] = q.x;
+                    sV[(j + 1) * ld + i] = q.y;
+                    sV[(j + 2) * ld + i] = q.z;
+                    sV[(j + 3) * ld + i] = q.w;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 3 * K; ++j) sV[j * ld + i] = vr[j];
             }
         }
         __syncthreads();
-        const int64_t c = b * kMultiBlockCells + threadIdx.x;
-        if (c < p.ncells) {
+        const int64_t c = b * kMultiBlockCells + tc;
+        const bool live = c < p.ncells;
+        int ln[4] = {0, 0, 0, 0};
+        float inv[3][3], cf[3][3], lam = 0.f, mu = 0.f;
+        if (live) {
             const ushort4 lc = lconn[c];
-            const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
+            ln[0] = lc.x;
+            ln[1] = lc.y;
+            ln[2] = lc.z;
+            ln[3] = lc.w;
             double X[4][3];
 #pragma unroll
             for (int k = 0; k < 4; ++k)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) X[k][d] = sX[3 * ln[k] + d];
+                for (int d = 0; d < 3; ++d) X[k][d] = sX[d * ld + ln[k]];
             double cof[3][3];
             const double det = tet_cof_m(X, cof);
             if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
             const double rdet = 1.0 / det;
-            float inv[3][3], cf[3][3];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -98,6 +129,9 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                     inv[i][j] = (float)(cof[i][j] * rdet);
                     cf[i][j] = (float)(cof[i][j] * (1.0 / 6.0));
                 }
+            // The registered tangent (Jf3vu_infinitesimalStrain) is isotropic: Jf3 = -C with
+            // C = lambda d_ij d_kl + mu (d_ik d_jl + d_il d_jk); its (f,g,df,dg) = (0,1,0,1) and
+            // (0,1,1,0) entries are -lambda and -mu.
             double a[L::size];
             L::load_cell(p, c, a);
             double x[3] = {0, 0, 0};
@@ -105,65 +139,108 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 #pragma unroll
             for (int i = 0; i < 81; ++i) Jf3d[i] = 0.0;
             call_jf3<RHEO_ILE>(L::numA, aoff.v, a, p, x, Jf3d);
+            lam = (float)(-Jf3d[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
+            mu = (float)(-Jf3d[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
+        }
+        const uint16_t* lst = inc + b * 4 * kMultiBlockCells;
 #pragma unroll 1
-            for (int r = 0; r < K; ++r) {
-                float s_x[9];
+        for (int r0 = 0; r0 < K; r0 += KC) {
+            if (live) {
 #pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    const float u0 = sV[(3 * ln[0] + cc) * K + r];
-                    const float g0 = sV[(3 * ln[1] + cc) * K + r] - u0;
-                    const float g1 = sV[(3 * ln[2] + cc) * K + r] - u0;
-                    const float g2 = sV[(3 * ln[3] + cc) * K + r] - u0;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) s_x[cc * 3 + d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
-                }
-                float f1[9];
-#pragma unroll
-                for (int f = 0; f < 3; ++f)
-#pragma unroll
-                    for (int df = 0; df < 3; ++df) {
-                        float acc1 = 0.0f;
-#pragma unroll
-                        for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                            for (int dg = 0; dg < 3; ++dg)
-                                acc1 += (float)Jf3d[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                        f1[f * 3 + df] = acc1;
-                    }
-                float e0[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
+                for (int rr = 0; rr < KC; ++rr) {
+                    const int r = r0 + rr;
+                    float s_x[3][3];
 #pragma unroll
                     for (int cc = 0; cc < 3; ++cc) {
-                        const float val = f1[cc * 3 + 0] * cf[k][0] + f1[cc * 3 + 1] * cf[k][1] + f1[cc * 3 + 2] * cf[k][2];
-                        e0[cc] -= val;
-                        atomicAdd(&sR[(3 * ln[k + 1] + cc) * K + r], val);
+                        const float* vc = sV + (cc * K + r) * ld;
+                        const float u0 = vc[ln[0]];
+                        const float g0 = vc[ln[1]] - u0, g1 = vc[ln[2]] - u0, g2 = vc[ln[3]] - u0;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) s_x[cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
                     }
+                    const float ltr = lam * (s_x[0][0] + s_x[1][1] + s_x[2][2]);
+                    float f1[3][3];
 #pragma unroll
-                for (int cc = 0; cc < 3; ++cc) atomicAdd(&sR[(3 * ln[0] + cc) * K + r], e0[cc]);
+                    for (int f = 0; f < 3; ++f)
+#pragma unroll
+                        for (int df = 0; df < 3; ++df)
+                            f1[f][df] = -(mu * (s_x[f][df] + s_x[df][f]) + (f == df ? ltr : 0.0f));
+                    float e0[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) {
+                            const float val = f1[cc][0] * cf[k][0] + f1[cc][1] * cf[k][1] + f1[cc][2] * cf[k][2];
+                            e0[cc] -= val;
+                            sE[(((k + 1) * 3 + cc) * KC + rr) * kMultiBlockCells + tc] = val;
+                        }
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) sE[(cc * KC + rr) * kMultiBlockCells + tc] = e0[cc];
+                }
             }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-            const uint32_t id = slot_node[s0 + i];
-            float* o = out + 3 * K * (int64_t)(id & ~kSharedBitM);
-            if (id & kSharedBitM) {
-#pragma unroll
-                for (int j = 0; j < 3 * K; ++j) red_add(o + j, sR[3 * K * i + j]);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 3 * K; ++j) o[j] += sR[3 * K * i + j];
+            __syncthreads();
+            // one work item per (node, right-hand side of the chunk): consecutive threads take
+            // consecutive nodes of the same right-hand side
+            for (int w = tc; w < ns * KC; w += blockDim.x) {
+                const int rr = w / ns, i = w - rr * ns;
+                const int j0 = inc_off[s0 + b + i], j1 = inc_off[s0 + b + i + 1];
+                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll 4
+                for (int j = j0; j < j1; ++j) {
+                    const int e = lst[j];
+                    const int cell = e >> 2, corner = e & 3;
+                    const float* se = sE + (corner * 3 * KC + rr) * kMultiBlockCells + cell;
+                    a0 += se[0];
+                    a1 += se[KC * kMultiBlockCells];
+                    a2 += se[2 * KC * kMultiBlockCells];
+                }
+                const uint32_t id = slot_node[s0 + i];
+                float* o = out + 3 * K * (int64_t)(id & ~kSharedBitM) + r0 + rr;
+                if (id & kSharedBitM) {
+                    red_add(o, a0);
+                    red_add(o + K, a1);
+                    red_add(o + 2 * K, a2);
+                } else {
+                    o[0] += a0;
+                    o[K] += a1;
+                    o[2 * K] += a2;
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
-// ---- batched vector kernels, layout [n][K] -------------------------------------------------
-constexpr int kBThreads = 256;
-constexpr int kBBlocks = 296;
+template <int K>
+size_t multi_smem(int ld) {
+    return (size_t)12 * MultiChunk<K>::value * kMultiBlockCells * sizeof(float) + (size_t)ld * 3 * sizeof(double) +
+           (size_t)ld * 3 * K * sizeof(float);
+}
 
-// Per-block sums of K values -> partials[blk][K].
+// ---- batched vector kernels, layout [n][K] -------------------------------------------------
+// Element e of an [n][K] array is DOF e / K of right-hand side e % K; every kernel below maps
+// consecutive threads to consecutive elements (thread index % K == right-hand side).
+constexpr int kBThreads = 256;
+constexpr int kBBlocks = 1184;
+
+// Per-block sums of one value per thread, by right-hand side (thread index % K), in a fixed
+// order -> partials[blk][K].
+template <int K>
+PL_D void block_sum_by_rhs(double a, double* partials) {
+    __shared__ double sh[kBThreads / 32][K];
+#pragma unroll
+    for (int o = K; o < 32; o <<= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l < K) sh[w][l] = a;
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sh[i][threadIdx.x];
+        partials[blockIdx.x * K + threadIdx.x] = s;
+    }
+}
+
+// Per-block sums of K values per thread (used by the single-RHS outer residual).
 template <int K>
 PL_D void block_sumK(double (&acc)[K], double* partials) {
     __shared__ double sh[K][kBThreads / 32];
@@ -183,128 +260,119 @@ PL_D void block_sumK(double (&acc)[K], double* partials) {
     }
 }
 
-// Fixed-order final sums: out[k] = sum_blk partials[blk][k].
+// Fixed-order final sums, one block per right-hand side (launch with K blocks of kBThreads):
+// out[k] = sum_blk partials[blk][k]; with `prev`, the value out held before is copied there first.
 template <int K>
-__global__ void k_b_finish(const double* __restrict__ partials, int nblk, double* out) {
-    const int k = threadIdx.x;
-    if (k >= K) return;
+__global__ void __launch_bounds__(kBThreads) k_b_finish(const double* __restrict__ partials, int nblk, double* out,
+                                                       double* prev) {
+    __shared__ double sh[kBThreads / 32];
+    const int k = blockIdx.x;
     double s = 0.0;
-    for (int i = 0; i < nblk; ++i) s += partials[i * K + k];
-    out[k] = s;
-}
-
-template <int K>
-PL_D void pinv_apply_K(const float* __restrict__ P, const float* r, int64_t node, float z[3][K]) {
-    const float* B = P + 9 * node;
+#pragma unroll 8
+    for (int i = threadIdx.x; i < nblk; i += kBThreads) s += partials[i * K + k];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const float r0 = r[(3 * node + 0) * K + k], r1 = r[(3 * node + 1) * K + k], r2 = r[(3 * node + 2) * K + k];
-        z[0][k] = B[0] * r0 + B[1] * r1 + B[2] * r2;
-        z[1][k] = B[3] * r0 + B[4] * r1 + B[5] * r2;
-        z[2][k] = B[6] * r0 + B[7] * r1 + B[8] * r2;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < kBThreads / 32; ++i) t += sh[i];
+        if (prev) prev[k] = out[k];
+        out[k] = t;
     }
 }
 
-// r = b (masked); z = P r; p = z; partial (r.z)[K], (r.r)[K]
+template <int K>
+PL_D void pinv_apply(const float* __restrict__ P, const float* r, int64_t node, int k, float z[3]) {
+    const float* B = P + 9 * node;
+    const float r0 = r[(3 * node + 0) * K + k], r1 = r[(3 * node + 1) * K + k], r2 = r[(3 * node + 2) * K + k];
+    z[0] = B[0] * r0 + B[1] * r1 + B[2] * r2;
+    z[1] = B[3] * r0 + B[4] * r1 + B[5] * r2;
+    z[2] = B[6] * r0 + B[7] * r1 + B[8] * r2;
+}
+
+// r = b (masked); z = P r; p = z; partial (r.z)[K], (r.r)[K]. One thread per (node, rhs).
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_b_init(float* r, float* z, float* p, const uint8_t* mask, const float* P,
                                                       int64_t nnodes, double* part_rz, double* part_rr) {
-    double rz[K], rr[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) rz[k] = rr[k] = 0.0;
-    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-            if (mask[3 * nd + c])
-#pragma unroll
-                for (int k = 0; k < K; ++k) r[(3 * nd + c) * K + k] = 0.0f;
-        float zz[3][K];
-        pinv_apply_K<K>(P, r, nd, zz);
+    double rz = 0.0, rr = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        const int k = (int)(t % K);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
+            if (mask[3 * nd + c]) r[(3 * nd + c) * K + k] = 0.0f;
+        float zz[3];
+        pinv_apply<K>(P, r, nd, k, zz);
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const int64_t i = (3 * nd + c) * K + k;
-                z[i] = zz[c][k];
-                p[i] = zz[c][k];
-                rz[k] += (double)r[i] * zz[c][k];
-                rr[k] += (double)r[i] * r[i];
-            }
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const float ri = r[i];
+            z[i] = zz[c];
+            p[i] = zz[c];
+            rz += (double)ri * zz[c];
+            rr += (double)ri * ri;
+        }
     }
-    block_sumK<K>(rz, part_rz);
+    block_sum_by_rhs<K>(rz, part_rz);
     __syncthreads();
-    block_sumK<K>(rr, part_rr);
+    block_sum_by_rhs<K>(rr, part_rr);
 }
 
 // partial p.(A p) with q = J p: -p.q over free DOFs
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_b_pq(const float* p, const float* q, const uint8_t* mask, int64_t n,
                                                     double* part) {
-    double s[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) s[k] = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (mask[i]) continue;
-#pragma unroll
-        for (int k = 0; k < K; ++k) s[k] -= (double)p[i * K + k] * q[i * K + k];
-    }
-    block_sumK<K>(s, part);
+    double s = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
+        if (!mask[e / K]) s -= (double)p[e] * q[e];
+    block_sum_by_rhs<K>(s, part);
 }
 
-// alpha_k = active_k ? rz_k / pq_k : 0; x += alpha p; r += alpha q; z = P r; partial rz, rr
+// alpha_k = active_k ? rz_k / pq_k : 0; x += alpha p; r += alpha q; z = P r; partial rz, rr.
+// One thread per (node, rhs).
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_b_update(float* x, float* r, const float* p, const float* q, float* z,
                                                         const uint8_t* mask, const float* P, int64_t nnodes,
                                                         const double* rz, const double* pq, const int* active,
                                                         double* part_rz, double* part_rr) {
-    float alpha[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) alpha[k] = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
-    double srz[K], srr[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) srz[k] = srr[k] = 0.0;
-    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
+    const int k = threadIdx.x % K;  // blockDim and the grid stride are multiples of K
+    const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
+    double srz = 0.0, srr = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (mask[3 * nd + c]) continue;
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const int64_t i = (3 * nd + c) * K + k;
-                x[i] += alpha[k] * p[i];
-                r[i] += alpha[k] * q[i];
-            }
+            const int64_t i = (3 * nd + c) * K + k;
+            x[i] += alpha * p[i];
+            r[i] += alpha * q[i];
         }
-        float zz[3][K];
-        pinv_apply_K<K>(P, r, nd, zz);
+        float zz[3];
+        pinv_apply<K>(P, r, nd, k, zz);
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const int64_t i = (3 * nd + c) * K + k;
-                z[i] = zz[c][k];
-                srz[k] += (double)r[i] * zz[c][k];
-                srr[k] += (double)r[i] * r[i];
-            }
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const float ri = r[i];
+            z[i] = zz[c];
+            srz += (double)ri * zz[c];
+            srr += (double)ri * ri;
+        }
     }
-    block_sumK<K>(srz, part_rz);
+    block_sum_by_rhs<K>(srz, part_rz);
     __syncthreads();
-    block_sumK<K>(srr, part_rr);
+    block_sum_by_rhs<K>(srr, part_rr);
 }
 
-// beta_k = rz_k / rz_old_k; p = z + beta p; then rz_old = rz
+// beta_k = rz_k / rz_old_k; p = z + beta p
 template <int K>
 __global__ void k_b_pupdate(float* p, const float* z, int64_t n, const double* rz, const double* rz_old, const int* active) {
-    float beta[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) beta[k] = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-#pragma unroll
-        for (int k = 0; k < K; ++k) p[i * K + k] = z[i * K + k] + beta[k] * p[i * K + k];
-}
-
-template <int K>
-__global__ void k_b_copyK(const double* src, double* dst) {
-    if (threadIdx.x < K) dst[threadIdx.x] = src[threadIdx.x];
+    const int k = threadIdx.x % K;
+    const float beta = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
+        p[e] = z[e] + beta * p[e];
 }
 
 // fault unfold / fold on [n][K]
@@ -385,16 +453,20 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
         if (rc) return rc;
         const BlockedLayout& L = *m->blocked;
         if (L.num_blocks == 0) return fail(PL_ERR_UNSUPPORTED, "no cell-block layout for this mesh");
-        const size_t smem = (size_t)L.max_local_nodes * (3 * sizeof(double) + 2 * 3 * K * sizeof(float));
+        if (L.max_local_nodes > 2 * kMultiBlockCells)
+            return fail(PL_ERR_UNSUPPORTED, "cell blocks too large for the batched kernel");
+        const size_t smem = multi_smem<K>(L.max_local_nodes);
         if (smem > 200 * 1024) return fail(PL_ERR_UNSUPPORTED, "cell blocks too large for the batched kernel");
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(k_tet_blocked_jv32_multi<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int dev = 0, nsm = 148;
+        int dev = 0, nsm = 148, per_sm = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const int grid = (int)std::min<int64_t>(L.num_blocks, (int64_t)nsm * 8);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tet_blocked_jv32_multi<K>, kMultiBlockCells, smem);
+        const int grid = (int)std::min<int64_t>(L.num_blocks, (int64_t)nsm * std::max(per_sm, 1));
         k_tet_blocked_jv32_multi<K><<<grid, kMultiBlockCells, smem, s>>>(
-            pp, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.num_blocks, v, out);
+            pp, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
+            L.num_blocks, L.max_local_nodes, v, out);
         count_launch();
     }
     if (S->npairs > 0) {
@@ -416,14 +488,13 @@ int pcg_iteration(pl_batch_solver B) {
     int rc = jv32_multi<K>(B, B->p, B->q);
     if (rc) return rc;
     k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a);
-    k_b_finish<K><<<1, 32, 0, s>>>(B->part_a, kBBlocks, pq);
-    k_b_copyK<K><<<1, 32, 0, s>>>(rz, rz_old);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, pq, nullptr);
     k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes, rz, pq,
                                                  B->active, B->part_a, B->part_b);
-    k_b_finish<K><<<1, 32, 0, s>>>(B->part_a, kBBlocks, rz);
-    k_b_finish<K><<<1, 32, 0, s>>>(B->part_b, kBBlocks, rr);
-    k_b_pupdate<K><<<bgrid(B->n), 256, 0, s>>>(B->p, B->z, B->n, rz, rz_old, B->active);
-    count_launch(7);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, rz, rz_old);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, rr, nullptr);
+    k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->z, B->n, rz, rz_old, B->active);
+    count_launch(6);
     return PL_OK;
 }
 
@@ -434,8 +505,8 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     cudaStream_t s = S->mesh->ctx->stream;
     PLB_CUDA(cudaMemsetAsync(B->x, 0, B->n * K * sizeof(float), s));
     k_b_init<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, B->p, S->d_mask, S->d_pinv32, B->nnodes, B->part_a, B->part_b);
-    k_b_finish<K><<<1, 32, 0, s>>>(B->part_a, kBBlocks, B->scal);
-    k_b_finish<K><<<1, 32, 0, s>>>(B->part_b, kBBlocks, B->scal + 3 * K);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, B->scal + 3 * K, nullptr);
     count_launch(3);
     double h[4 * 8];
     int act[8];
@@ -537,7 +608,7 @@ int solve_tile(pl_batch_solver B, int nact, const double* const* bs, double* con
                 count_launch(2);
             }
             k_outer64<<<kBBlocks, kBThreads, 0, s>>>(B->r64, B->jx64, S->d_mask, n, B->r64, B->part_a);
-            k_b_finish<1><<<1, 32, 0, s>>>(B->part_a, kBBlocks, B->scal);
+            k_b_finish<1><<<1, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
             k_b_pack<<<bgrid(n), 256, 0, s>>>(B->r64, n, K, k, B->r);
             count_launch(3);
             double h;

@@ -237,6 +237,61 @@ PL_HD void el3d_strain_vector(PLB_POINT_ARGS(R), const R* x, int numConstants,
     out[0] = e.xx; out[1] = e.yy; out[2] = e.zz; out[3] = e.xy; out[4] = e.yz; out[5] = e.xz;
 }
 
+// Cauchy stress as a vector (xx, yy, zz, xy, yz, xz) for output, basis order 0 derived field
+// (Elasticity::stress_asVector, Elasticity.hh:441-456).
+template <typename R>
+PL_HD void sym_to_vector(const Sym<R>& t, R* out) {
+    out[0] = t.xx; out[1] = t.yy; out[2] = t.zz; out[3] = t.xy; out[4] = t.yz; out[5] = t.xz;
+}
+
+// IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector
+// (IsotropicLinearElasticity.hh:1243-1273): mean stress, then deviatoric stress.
+template <typename R>
+PL_HD void ile3d_stress_vector(PLB_POINT_ARGS(R), const R* x, int numConstants, const R* constants,
+                               R* out) {
+    const R mu = a[aOff[numA - 2]];
+    const R K = a[aOff[numA - 1]];
+    const Sym<R> e = strain(&s_x[sOff_x[0]]);
+    Sym<R> sig = sym_zero<R>();
+    add_mean_stress(K, e, &sig);
+    add_dev_stress(mu, e, &sig);
+    sym_to_vector(sig, out);
+}
+
+// IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector
+// (IsotropicLinearGenMaxwell.hh:1556-1589) through cauchyStress_stateVars (:340-357): the
+// stored viscous strains enter as they are (no update with dt).
+template <typename R>
+PL_HD void gm3d_stress_vector(PLB_POINT_ARGS(R), const R* x, int numConstants, const R* constants,
+                              R* out) {
+    const R mu = a[aOff[numA - 6]];
+    const R K = a[aOff[numA - 5]];
+    const R* ratio = &a[aOff[numA - 3]];
+    const R* visc = &a[aOff[numA - 2]];
+    const Sym<R> e = strain(&s_x[sOff_x[0]]);
+    Sym<R> sig = sym_zero<R>();
+    add_mean_stress(K, e, &sig);
+    Sym<R> v[3];
+    for (int i = 0; i < 3; ++i) v[i] = sym_from_vector(&visc[6 * i]);
+    const Sym<R> de = deviatoric(e);
+    R r = R(1.0);
+    for (int i = 0; i < 3; ++i) r -= ratio[i];
+    const R mu_el = mu * r;
+    sig.xx += R(2.0) * mu_el * de.xx;
+    for (int i = 0; i < 3; ++i) sig.xx += R(2.0) * mu * ratio[i] * v[i].xx;
+    sig.yy += R(2.0) * mu_el * de.yy;
+    for (int i = 0; i < 3; ++i) sig.yy += R(2.0) * mu * ratio[i] * v[i].yy;
+    sig.zz += R(2.0) * mu_el * de.zz;
+    for (int i = 0; i < 3; ++i) sig.zz += R(2.0) * mu * ratio[i] * v[i].zz;
+    sig.xy += R(2.0) * mu_el * de.xy;
+    for (int i = 0; i < 3; ++i) sig.xy += R(2.0) * mu * ratio[i] * v[i].xy;
+    sig.yz += R(2.0) * mu_el * de.yz;
+    for (int i = 0; i < 3; ++i) sig.yz += R(2.0) * mu * ratio[i] * v[i].yz;
+    sig.xz += R(2.0) * mu_el * de.xz;
+    for (int i = 0; i < 3; ++i) sig.xz += R(2.0) * mu * ratio[i] * v[i].xz;
+    sym_to_vector(sig, out);
+}
+
 // BoundaryDirections::tangential_directions and _unitCrossProduct
 // (BoundaryDirections.hh:35-67, 248-270). The sign test on the second tangent repeats
 // refDir2[1]*n[1], as the reference does.

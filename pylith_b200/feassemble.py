@@ -239,6 +239,18 @@ class IntegratorDomain(Integrator):
     def update_state_vars(self, t, dt, u) -> None:
         check(C.lib().pl_update_state_vars(self.handle, t, dt, _ptr(u)))
 
+    def set_kernels_derived_field(self, kernels: Sequence[ProjectKernels]) -> None:
+        """IntegratorDomain::setKernelsDerivedField (IntegratorDomain.cc:233-240)."""
+        arr = (C.ProjectKernelsC * len(kernels))(
+            *[C.ProjectKernelsC(k.subfield.encode(), k.f) for k in kernels])
+        check(C.lib().pl_integrator_set_kernels_derived_field(self.handle, arr, len(kernels)))
+        self.derived_subfields = [k.subfield for k in kernels]
+
+    def compute_derived_field(self, t, dt, u, out) -> None:
+        """Basis-order-0 derived fields at the cell centroids into out [ncells, 6 * nkernels]
+        (IntegratorDomain::_computeDerivedField, IntegratorDomain.cc:596-630)."""
+        check(C.lib().pl_compute_derived_field(self.handle, t, dt, _ptr(u), _ptr(out)))
+
 
 class IntegratorInterface(Integrator):
     """IntegratorInterface (libsrc/pylith/feassemble/IntegratorInterface.cc) over the mesh's

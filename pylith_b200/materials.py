@@ -79,6 +79,10 @@ class IsotropicLinearElasticity:
         ig.set_kernels_jacobian([FA.JacobianKernels(
             "displacement", "displacement", FA.LHS, None, None, None,
             k.IsotropicLinearElasticity3D.Jf3vu_infinitesimalStrain)])
+        # Elasticity::_setKernelsDerivedField (Elasticity.cc:629-651)
+        ig.set_kernels_derived_field([
+            FA.ProjectKernels("cauchy_stress", k.IsotropicLinearElasticity3D.cauchyStress_infinitesimalStrain_asVector),
+            FA.ProjectKernels("cauchy_strain", k.Elasticity3D.infinitesimalStrain_asVector)])
         return ig
 
 
@@ -119,6 +123,10 @@ class IsotropicLinearGenMaxwell:
             FA.ProjectKernels("viscous_strain",
                               k.IsotropicLinearGenMaxwell3D.viscousStrain_infinitesimalStrain_asVector),
             FA.ProjectKernels("total_strain", k.Elasticity3D.infinitesimalStrain_asVector)])
+        # Elasticity::_setKernelsDerivedField (Elasticity.cc:629-651)
+        ig.set_kernels_derived_field([
+            FA.ProjectKernels("cauchy_stress", k.IsotropicLinearGenMaxwell3D.cauchyStress_infinitesimalStrain_asVector),
+            FA.ProjectKernels("cauchy_strain", k.Elasticity3D.infinitesimalStrain_asVector)])
         return ig
 
 

@@ -340,3 +340,56 @@ def test_destroy_in_any_order(torch_cuda):
     ig.compute_lhs_residual(0.0, 0.0, du, du.clone())
     A.close()
     ig.close()
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8", "hex27"])
+def test_derived_fields_match_oracle(oracle_lib, torch_cuda, ctx, kind):
+    """pl_compute_derived_field (cauchy_stress, cauchy_strain of basis order 0 at the cell
+    centroids, IntegratorDomain.cc:596-630) against the oracle's centroid projection."""
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES[kind]()
+    mat = elastic_setup(mesh, seed=31)
+    u = np.random.default_rng(32).standard_normal(mesh.num_dof)
+    ref_s, ref_e = O.project_centroid(
+        mesh, u, oracle_aux(O, mat),
+        ["IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector",
+         "Elasticity3D::infinitesimalStrain_asVector"], [6, 6])
+    ig = mat.create_integrator(FA.DeviceMesh(ctx, mesh))
+    out = torch.zeros((mesh.num_cells, 12), dtype=torch.float64, device="cuda")
+    ig.compute_derived_field(0.0, 0.0, dev(torch, u), out)
+    ctx.synchronize()
+    got = out.cpu().numpy()
+    assert rel_l2(got[:, :6], ref_s) <= TOL64
+    assert rel_l2(got[:, 6:], ref_e) <= TOL64
+
+
+def test_derived_genmaxwell_stress(oracle_lib, torch_cuda, ctx):
+    """Generalized-Maxwell stress from the stored state (cauchyStress_stateVars) on P1 tets,
+    whose single quadrature point is the centroid; hexahedra are rejected (-7)."""
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES["tet4"]()
+    g = genmaxwell_setup(mesh, seed=33)
+    dt = 0.1 * MAT.YEAR
+    u = np.random.default_rng(34).standard_normal(mesh.num_dof) * 1e-2
+    ref_s, ref_e = O.project_centroid(
+        mesh, u, genmaxwell_oracle_aux(O, g),
+        ["IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector",
+         "Elasticity3D::infinitesimalStrain_asVector"], [6, 6], constants=[dt])
+    ig = g.create_integrator(FA.DeviceMesh(ctx, mesh), dt)
+    out = torch.zeros((mesh.num_cells, 12), dtype=torch.float64, device="cuda")
+    ig.compute_derived_field(0.0, dt, dev(torch, u), out)
+    ctx.synchronize()
+    got = out.cpu().numpy()
+    assert rel_l2(got[:, :6], ref_s) <= TOL64
+    assert rel_l2(got[:, 6:], ref_e) <= TOL64
+    hexm = MESHES["hex8"]()
+    ih = genmaxwell_setup(hexm, seed=35).create_integrator(FA.DeviceMesh(ctx, hexm), dt)
+    with pytest.raises(_lib.PylithB200Error) as e:
+        ih.compute_derived_field(0.0, dt, dev(torch, np.zeros(hexm.num_dof)),
+                                 torch.zeros((hexm.num_cells, 12), dtype=torch.float64, device="cuda"))
+    assert e.value.code == -7

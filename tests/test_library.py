@@ -20,6 +20,8 @@ KERNEL_NAMES = [
     "IsotropicLinearGenMaxwell3D::Jf3vu_infinitesimalStrain",
     "IsotropicLinearGenMaxwell3D::viscousStrain_infinitesimalStrain_asVector",
     "Elasticity3D::infinitesimalStrain_asVector",
+    "IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector",
+    "IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector",
     "FaultCohesiveKin::f0u_neg", "FaultCohesiveKin::f0u_pos", "FaultCohesiveKin::f0l_slip",
     "FaultCohesiveKin::Jf0ul_neg", "FaultCohesiveKin::Jf0ul_pos", "FaultCohesiveKin::Jf0lu",
 ]

@@ -32,6 +32,8 @@ def elastic_aux(O, rho, mu, K):
     "IsotropicLinearGenMaxwell3D::Jf3vu_infinitesimalStrain",
     "IsotropicLinearGenMaxwell3D::viscousStrain_infinitesimalStrain_asVector",
     "Elasticity3D::infinitesimalStrain_asVector",
+    "IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector",
+    "IsotropicLinearGenMaxwell3D::cauchyStress_infinitesimalStrain_asVector",
     "FaultCohesiveKin::f0u_neg", "FaultCohesiveKin::f0u_pos", "FaultCohesiveKin::f0l_slip",
     "FaultCohesiveKin::Jf0ul_neg", "FaultCohesiveKin::Jf0ul_pos", "FaultCohesiveKin::Jf0lu",
 ])
@@ -198,3 +200,32 @@ def test_rigid_two_block_slip_known_answer(oracle_lib):
     np.testing.assert_allclose(u[:nd], uex_full[:nd], atol=1e-9)
     # lambda is a traction (Pa); zero to rounding relative to mu
     np.testing.assert_allclose(u[nd:], 0.0, atol=1e-12 * mu.max())
+
+
+@pytest.mark.parametrize("make", [lambda: M.box_hex(3, 3, 2), lambda: M.box_tet_delaunay(1500, seed=4),
+                                  lambda: M.box_hex27(2, 2, 2)], ids=["hex8", "tet4", "hex27"])
+def test_derived_fields_known_answer(oracle_lib, make):
+    """Basis-order-0 derived fields (Elasticity::_setKernelsDerivedField, Elasticity.cc:629-651):
+    for a linear displacement the centroid strain is the imposed strain and the stress is
+    K tr(e) I + 2 mu dev(e) in every cell; the restatement and the reference kernels agree bit for
+    bit through the same projection."""
+    O = oracle_lib
+    mesh = make()
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=2)
+    aux = elastic_aux(O, rho, mu, K)
+    G = np.array([[1e-4, 2e-5, -3e-5], [3e-5, -1e-4, 4e-5], [-2e-5, 1e-5, 5e-5]])
+    u = (mesh.coords @ G.T).ravel()
+    fns = ["IsotropicLinearElasticity3D::cauchyStress_infinitesimalStrain_asVector",
+           "Elasticity3D::infinitesimalStrain_asVector"]
+    stress, strain = O.project_centroid(mesh, u, aux, fns, [6, 6])
+    e = 0.5 * (G + G.T)
+    ev = np.array([e[0, 0], e[1, 1], e[2, 2], e[0, 1], e[1, 2], e[0, 2]])
+    np.testing.assert_allclose(strain, np.tile(ev, (mesh.num_cells, 1)), rtol=0, atol=1e-13 * np.abs(ev).max())
+    tr = np.trace(e)
+    dev = ev - np.array([tr / 3, tr / 3, tr / 3, 0, 0, 0])
+    sig = K[:, None] * np.array([tr, tr, tr, 0, 0, 0]) + 2 * mu[:, None] * dev
+    np.testing.assert_allclose(stress, sig, rtol=1e-12, atol=1e-12 * np.abs(sig).max())
+    if O.ref_available():
+        s_ref, e_ref = O.project_centroid(mesh, u, aux, fns, [6, 6], source="ref")
+        np.testing.assert_array_equal(stress, s_ref)
+        np.testing.assert_array_equal(strain, e_ref)
