@@ -191,7 +191,8 @@ int pl_mesh_destroy(pl_mesh mesh);
 int64_t pl_mesh_num_dof(pl_mesh mesh);
 
 /* ---- domain integrator (libsrc/pylith/feassemble/IntegratorDomain.cc) ------------------ */
-/* Integrates over cells [cell_ids] of the mesh (NULL = all cells). */
+/* Integrates over cells [cell_ids] of the mesh (NULL = all cells; a non-NULL list with
+ * num_ids = 0 is an empty integrator, as for a material label that matches no cells). */
 int pl_integrator_domain_create(pl_mesh mesh, int64_t num_ids, const int32_t* cell_ids_host,
                                 pl_integrator* out);
 /* IntegratorDomain::setKernelsResidual (IntegratorDomain.cc:135-167). */

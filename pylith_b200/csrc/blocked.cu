@@ -322,7 +322,9 @@ __global__ void __launch_bounds__(kTetThreads, PLB_TET_MIN_BLOCKS) k_tet_blocked
                 o[2] += r2;
             }
         }
-        __syncthreads();
+        // No barrier here: the next iteration writes shared memory (sE, and the prefetch into
+        // this block's buffer) only after its own barrier, which every thread reaches after
+        // finishing this gather.
         cur ^= 1;
     }
     __pipeline_wait_prior(0);

@@ -334,11 +334,12 @@ int64_t pl_mesh_num_dof(pl_mesh m) { return m ? 3 * (m->nnodes + m->nlag) : 0; }
 
 // ---- integrators --------------------------------------------------------------------------
 int pl_integrator_domain_create(pl_mesh m, int64_t num_ids, const int32_t* ids, pl_integrator* out) {
-    if (!m || !out) return fail(PL_ERR_INVALID_ARG, "null argument");
+    if (!m || !out || num_ids < 0) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     *out = nullptr;
     pl_integrator ig = new pl_integrator_s();
     ig->mesh = m;
     mesh_retain(m);
+    ig->subset = ids != nullptr;  // a label that matches no cells gives an empty integrator
     if (ids && num_ids > 0) {
         for (int64_t i = 0; i < num_ids; ++i)
             if (ids[i] < 0 || ids[i] >= m->ncells) {
@@ -356,7 +357,7 @@ int pl_integrator_domain_create(pl_mesh m, int64_t num_ids, const int32_t* ids, 
             return rc;
         }
     } else {
-        ig->ncells = m->ncells;
+        ig->ncells = ids ? 0 : m->ncells;
     }
     *out = ig;
     return PL_OK;
@@ -580,7 +581,7 @@ int pl_integrator_destroy(pl_integrator ig) {
 static bool use_blocked(pl_integrator ig) {
     pl_mesh m = ig->mesh;
     if (ig->scatter == PL_SCATTER_ATOMIC) return false;
-    if (ig->d_cell_ids) return false;  // the blocked layout covers whole meshes
+    if (ig->subset) return false;  // the blocked layout covers whole meshes
     return m->cell_type == PL_CELL_TET4 || ig->scatter == PL_SCATTER_BLOCKED;
 }
 

@@ -114,7 +114,8 @@ struct pl_integrator_s {
     pl_mesh mesh = nullptr;
     bool is_interface = false;
     int64_t ncells = 0;                 // cells integrated over
-    int32_t* d_cell_ids = nullptr;      // NULL: all cells of the mesh, in order
+    bool subset = false;                // created with a cell list (possibly empty)
+    int32_t* d_cell_ids = nullptr;      // NULL: all cells of the mesh, in order (or none, for an empty subset)
     std::vector<int32_t> h_cell_ids;
     // domain kernels
     plb::KernelId r0 = plb::K_NONE, r1 = plb::K_NONE;

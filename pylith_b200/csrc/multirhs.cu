@@ -447,7 +447,7 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
         if (rc) return rc;
         pp.t = S->t;
         pp.dt = S->dt;
-        if (m->cell_type != PL_CELL_TET4 || ig->j3 != K_ILE_JF3VU || ig->d_cell_ids)
+        if (m->cell_type != PL_CELL_TET4 || ig->j3 != K_ILE_JF3VU || ig->subset)
             return fail(PL_ERR_UNSUPPORTED, "batched solves support P1 tetrahedra with isotropic linear elasticity");
         rc = ensure_blocked_layout(m);
         if (rc) return rc;

@@ -393,3 +393,46 @@ def test_derived_genmaxwell_stress(oracle_lib, torch_cuda, ctx):
         ih.compute_derived_field(0.0, dt, dev(torch, np.zeros(hexm.num_dof)),
                                  torch.zeros((hexm.num_cells, 12), dtype=torch.float64, device="cuda"))
     assert e.value.code == -7
+
+
+@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+def test_two_materials_on_cell_subsets(oracle_lib, torch_cuda, ctx, kind):
+    """Two materials on complementary cell subsets (one IntegratorDomain per material label,
+    IntegratorDomain.cc:422-453) summed into one residual and one Jacobian action; an integrator
+    over an empty subset contributes nothing."""
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    mesh = MESHES[kind]()
+    rng = np.random.default_rng(41)
+    ids = [np.flatnonzero(mesh.coords[mesh.cells].mean(axis=1)[:, 0] < 0.0),
+           np.flatnonzero(mesh.coords[mesh.cells].mean(axis=1)[:, 0] >= 0.0)]
+    mats = [elastic_setup(M.Mesh(mesh.cell_type, mesh.coords, mesh.cells[i]), seed=42 + k) for k, i in enumerate(ids)]
+    u = rng.standard_normal(mesh.num_dof)
+    v = rng.standard_normal(mesh.num_dof)
+    r_ref = np.zeros(mesh.num_dof)
+    jv_ref = np.zeros(mesh.num_dof)
+    for i, mat in zip(ids, mats):
+        sub = M.Mesh(mesh.cell_type, mesh.coords, mesh.cells[i])
+        aux = oracle_aux(O, mat)
+        r_ref += O.residual(sub, u, aux, f1=F1_ILE)
+        J = O.assemble(sub, O.jacobian_elements(sub, aux, g3=JF3_ILE))
+        jv_ref += J @ v
+    dm = FA.DeviceMesh(ctx, mesh)
+    igs = [mat.create_integrator(dm, i) for i, mat in zip(ids, mats)]
+    empty = elastic_setup(M.Mesh(mesh.cell_type, mesh.coords, mesh.cells[:0]), seed=9).create_integrator(
+        dm, np.zeros(0, dtype=np.int32))
+    du, dv = dev(torch, u), dev(torch, v)
+    dr = torch.full_like(du, 7.0)
+    djv = torch.full_like(du, 7.0)
+    for k, ig in enumerate(igs + [empty]):
+        mode = FA.INSERT if k == 0 else FA.ADD
+        ig.compute_lhs_residual(0.0, 0.0, du, dr, mode=mode)
+        ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, du, dv, djv, mode=mode)
+    ctx.synchronize()
+    assert rel_l2(dr.cpu().numpy(), r_ref) <= TOL64
+    assert rel_l2(djv.cpu().numpy(), jv_ref) <= TOL64
+    # the empty integrator alone in INSERT mode writes zeros
+    empty.compute_lhs_residual(0.0, 0.0, du, dr, mode=FA.INSERT)
+    ctx.synchronize()
+    assert float(dr.abs().max()) == 0.0
