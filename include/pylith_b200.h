@@ -104,7 +104,8 @@ enum { PL_INSERT = 0, PL_ADD = 1 };
 
 /* Scatter (assembly) strategies of the domain kernels. */
 enum {
-    PL_SCATTER_AUTO = 0,      /* library choice (cell-block gather when available) */
+    PL_SCATTER_AUTO = 0,      /* library choice: cell-block gather for P1 tetrahedra, a group of
+                                 lanes per cell with FP64 reductions for hexahedra */
     PL_SCATTER_ATOMIC = 1,    /* one thread per cell, FP64 atomics into the output */
     PL_SCATTER_BLOCKED = 2    /* cell blocks staged in shared memory, per-node gather, one FP64
                                  reduction per node shared between blocks (P1 tetrahedra) */

@@ -624,7 +624,9 @@ int pl_compute_lhs_residual(pl_integrator ig, double t, double dt, const double*
     }
     if (rc) return rc;
     if (mode == PL_INSERT) PLB_CUDA(cudaMemsetAsync(r, 0, pl_mesh_num_dof(m) * sizeof(double), s));
-    launch_domain_apply_atomic(p, m->cell_type, rheo, bf, OP_RESIDUAL, s);
+    if (ig->scatter == PL_SCATTER_ATOMIC ||
+        !launch_domain_apply_hexgroup(p, m->cell_type, rheo, bf, OP_RESIDUAL, s))
+        launch_domain_apply_atomic(p, m->cell_type, rheo, bf, OP_RESIDUAL, s);
     PLB_CUDA(cudaGetLastError());
     return PL_OK;
 }
@@ -670,7 +672,9 @@ int pl_compute_lhs_jacobian_action(pl_integrator ig, double t, double dt, double
     }
     if (rc) return rc;
     if (mode == PL_INSERT) PLB_CUDA(cudaMemsetAsync(jv, 0, pl_mesh_num_dof(m) * sizeof(double), s));
-    launch_domain_apply_atomic(p, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, s);
+    if (ig->scatter == PL_SCATTER_ATOMIC ||
+        !launch_domain_apply_hexgroup(p, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, s))
+        launch_domain_apply_atomic(p, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, s);
     PLB_CUDA(cudaGetLastError());
     return PL_OK;
 }
