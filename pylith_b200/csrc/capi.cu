@@ -16,6 +16,10 @@ namespace plb {
 
 static thread_local std::string g_last_error;
 static std::atomic<long long> g_launches{0};
+static std::atomic<unsigned long long> g_epoch{1};
+
+void bump_state_epoch() { ++g_epoch; }
+unsigned long long state_epoch() { return g_epoch.load(); }
 
 void count_launch(int n) { g_launches += n; }
 
@@ -376,6 +380,7 @@ int pl_integrator_interface_create(pl_mesh m, pl_integrator* out) {
 }
 
 int pl_integrator_set_kernels_residual(pl_integrator ig, const pl_residual_kernels* k, int num) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || ig->is_interface || (num > 0 && !k)) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     KernelId r0 = K_NONE, r1 = K_NONE;
     for (int i = 0; i < num; ++i) {
@@ -398,6 +403,7 @@ int pl_integrator_set_kernels_residual(pl_integrator ig, const pl_residual_kerne
 }
 
 int pl_integrator_set_kernels_jacobian(pl_integrator ig, const pl_jacobian_kernels* k, int num) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || ig->is_interface || (num > 0 && !k)) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     KernelId j3 = K_NONE;
     for (int i = 0; i < num; ++i) {
@@ -413,6 +419,7 @@ int pl_integrator_set_kernels_jacobian(pl_integrator ig, const pl_jacobian_kerne
 }
 
 int pl_integrator_set_kernels_update_state_vars(pl_integrator ig, const pl_project_kernels* k, int num) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || ig->is_interface || (num > 0 && !k)) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     std::vector<KernelId> ids;
     std::vector<std::string> names;
@@ -429,6 +436,7 @@ int pl_integrator_set_kernels_update_state_vars(pl_integrator ig, const pl_proje
 }
 
 int pl_integrator_set_kernels_derived_field(pl_integrator ig, const pl_project_kernels* k, int num) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || ig->is_interface || num < 0 || num > 4 || (num > 0 && !k))
         return fail(PL_ERR_INVALID_ARG, "bad arguments (at most 4 derived-field kernels)");
     std::vector<KernelId> ids;
@@ -446,6 +454,7 @@ int pl_integrator_set_kernels_derived_field(pl_integrator ig, const pl_project_k
 }
 
 int pl_integrator_interface_set_kernels_residual(pl_integrator ig, const pl_interface_residual_kernels* k, int num) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || !ig->is_interface || (num > 0 && !k)) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     KernelId r[3] = {K_NONE, K_NONE, K_NONE};
     for (int i = 0; i < num; ++i) {
@@ -463,6 +472,7 @@ int pl_integrator_interface_set_kernels_residual(pl_integrator ig, const pl_inte
 }
 
 int pl_integrator_interface_set_kernels_jacobian(pl_integrator ig, const pl_interface_jacobian_kernels* k, int num) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || !ig->is_interface || (num > 0 && !k)) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     KernelId r[3] = {K_NONE, K_NONE, K_NONE};
     for (int i = 0; i < num; ++i) {
@@ -480,6 +490,7 @@ int pl_integrator_interface_set_kernels_jacobian(pl_integrator ig, const pl_inte
 }
 
 int pl_integrator_set_aux(pl_integrator ig, const char* name, int storage, int ncomp, const double* values) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || !name || !values || ncomp <= 0 || ncomp > 64) return fail(PL_ERR_INVALID_ARG, "bad aux arguments");
     pl_mesh m = ig->mesh;
     int64_t nc = ig->ncells;
@@ -551,18 +562,21 @@ int pl_integrator_get_aux(pl_integrator ig, const char* name, double* values) {
 }
 
 int pl_integrator_set_constants(pl_integrator ig, int num, const double* constants) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || num < 0 || num > 8 || (num > 0 && !constants)) return fail(PL_ERR_INVALID_ARG, "bad constants (at most 8)");
     ig->constants.assign(constants, constants + num);
     return PL_OK;
 }
 
 int pl_integrator_set_scatter(pl_integrator ig, int scatter) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || scatter < PL_SCATTER_AUTO || scatter > PL_SCATTER_BLOCKED) return fail(PL_ERR_INVALID_ARG, "bad scatter");
     ig->scatter = scatter;
     return PL_OK;
 }
 
 int pl_integrator_destroy(pl_integrator ig) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig) return PL_OK;
     cudaSetDevice(ig->mesh->ctx->device);
     cudaStreamSynchronize(ig->mesh->ctx->stream);
@@ -711,7 +725,8 @@ int pl_compute_lhs_jacobian_action_f32(pl_integrator ig, double t, double dt, co
         return PL_OK;
     }
     if (rc) return rc;
-    launch_domain_jv_f32_atomic(p, m->cell_type, rheo, s);
+    if (ig->scatter == PL_SCATTER_ATOMIC || !launch_domain_jv32_hexgroup(p, m->cell_type, rheo, s))
+        launch_domain_jv_f32_atomic(p, m->cell_type, rheo, s);
     PLB_CUDA(cudaGetLastError());
     return PL_OK;
 }

@@ -33,6 +33,11 @@ enum KernelId {
 
 KernelId lookup_kernel(const void* fn);
 
+// Incremented whenever an integrator's kernels, aux fields, constants or scatter change (or it is
+// destroyed): solvers re-capture their CUDA graphs when the value differs from their capture's.
+void bump_state_epoch();
+unsigned long long state_epoch();
+
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
@@ -168,4 +173,12 @@ struct pl_solver_s {
     int iterations = 0, inner_iterations = 0, outer_iterations = 0;
     double rel_residual = 0.0;
     bool ready = false;
+    // PCG iterations run as a CUDA graph of check_every iterations (index 0: FP64, 1: FP32) on a
+    // private stream fenced against the context's stream with events.
+    double* d_xs = nullptr;  // FP64 PCG solution (the graph's fixed output buffer)
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_iters[2] = {0, 0};
+    unsigned long long graph_epoch[2] = {0, 0};
 };

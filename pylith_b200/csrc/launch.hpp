@@ -24,6 +24,8 @@ void launch_domain_jv_f32_atomic(const DomainParams& p, int cell, int rheo, cuda
 // Hexahedra (Q1, Q2) with a group of lanes per cell (FP64 residual / Jacobian action, FP64
 // reductions into the output); returns false for other cell types.
 bool launch_domain_apply_hexgroup(const DomainParams& p, int cell, int rheo, bool bf, int op, cudaStream_t s);
+// FP32 Jacobian action of hexahedra with a group of lanes per cell (FP64 geometry and tangent).
+bool launch_domain_jv32_hexgroup(const DomainParams& p, int cell, int rheo, cudaStream_t s);
 void launch_domain_jacobian(const DomainParams& p, int cell, int rheo, const int32_t* pos,
                             double* vals, cudaStream_t s);
 // Aux binding of a domain integrator for its registered Jacobian kernels.

@@ -421,6 +421,7 @@ struct pl_batch_solver_s {
     double* jx64 = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
+    unsigned long long graph_epoch = 0;
     // The solve runs on a private stream (graph capture is not possible on the legacy default
     // stream a caller may use), fenced against the caller's stream with events.
     cudaStream_t stream = nullptr;
@@ -520,7 +521,7 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
     const int chunk = S->check_every;
     // capture `chunk` iterations once per tile size, replay between checks
-    if (!B->graph || B->graph_iters != chunk) {
+    if (!B->graph || B->graph_iters != chunk || B->graph_epoch != state_epoch()) {
         if (B->graph) cudaGraphExecDestroy(B->graph);
         B->graph = nullptr;
         cudaGraph_t g;
@@ -534,6 +535,7 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
         B->graph_iters = chunk;
+        B->graph_epoch = state_epoch();
     }
     *iters = 0;
     for (int it = 0; it < max_iter; it += chunk) {

@@ -402,30 +402,71 @@ int pcg(pl_solver S, const T* b, T* x, double rtol, double atol, int max_iter, c
     *iters = 0;
     *rel = r0 > 0.0 ? 1.0 : 0.0;
     if (r0 == 0.0 || r0 <= stop) return PL_OK;
-    for (int it = 1; it <= max_iter; ++it) {
+    // The iterations run on the solver's private stream (capture is impossible on the legacy
+    // default stream a caller may use), as a CUDA graph of check_every iterations replayed
+    // between convergence checks; the graph is captured again when the integrators changed.
+    pl_context c = S->mesh->ctx;
+    const int gi = sizeof(T) == 8 ? 0 : 1;
+    const int chunk = std::max(1, S->check_every);
+    if (S->mesh->cell_type == PL_CELL_TET4) {
+        int rcl = ensure_blocked_layout(S->mesh);  // allocates: outside any capture
+        if (rcl) return rcl;
+    }
+    PLB_CUDA(cudaEventRecord(S->ev_in, s));
+    PLB_CUDA(cudaStreamWaitEvent(S->cstream, S->ev_in, 0));
+    c->stream = S->cstream;
+    auto iteration = [&]() -> int {
         int rc;
         if constexpr (sizeof(T) == 8) rc = apply_J(S, (const double*)p, (double*)q);
         else rc = apply_J32(S, (const float*)p, (float*)q);
         if (rc) return rc;
-        k_cg_pq<T><<<kRedBlocks, kRedThreads, 0, s>>>(p, q, S->d_mask, n, part);
-        k_finish2<<<1, 1024, 0, s>>>(part, kRedBlocks, scal, S_PQ, -1);
-        k_copy_scalar<<<1, 1, 0, s>>>(scal, S_RZ, S_RZ_OLD);
-        k_cg_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, q, z, S->d_mask, pinv, nn, scal, part);
-        k_finish2<<<1, 1024, 0, s>>>(part, kRedBlocks, scal, S_RZ, S_RR);
-        k_cg_pupdate<T><<<vec_grid(n), 256, 0, s>>>(p, z, n, scal);
+        k_cg_pq<T><<<kRedBlocks, kRedThreads, 0, S->cstream>>>(p, q, S->d_mask, n, part);
+        k_finish2<<<1, 1024, 0, S->cstream>>>(part, kRedBlocks, scal, S_PQ, -1);
+        k_copy_scalar<<<1, 1, 0, S->cstream>>>(scal, S_RZ, S_RZ_OLD);
+        k_cg_update<T><<<kRedBlocks, kRedThreads, 0, S->cstream>>>(x, r, p, q, z, S->d_mask, pinv, nn, scal, part);
+        k_finish2<<<1, 1024, 0, S->cstream>>>(part, kRedBlocks, scal, S_RZ, S_RR);
+        k_cg_pupdate<T><<<vec_grid(n), 256, 0, S->cstream>>>(p, z, n, scal);
         count_launch(6);
-        *iters = it;
-        if (it % S->check_every == 0 || it == max_iter) {
-            PLB_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, s));
-            PLB_CUDA(cudaStreamSynchronize(s));
-            const double rn = std::sqrt(h[S_RR]);
-            *rel = rn / r0;
-            if (!(rn == rn)) return fail(PL_ERR_NOT_CONVERGED, "PCG diverged (NaN residual)");
-            if (rn <= stop) return PL_OK;
-        }
+        return PL_OK;
+    };
+    int rc = PL_OK;
+    if (!S->graph[gi] || S->graph_iters[gi] != chunk || S->graph_epoch[gi] != state_epoch()) {
+        if (S->graph[gi]) cudaGraphExecDestroy(S->graph[gi]);
+        S->graph[gi] = nullptr;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(S->cstream, cudaStreamCaptureModeRelaxed);
+        for (int i = 0; i < chunk && rc == PL_OK && e == cudaSuccess; ++i) rc = iteration();
+        if (e == cudaSuccess) e = cudaStreamEndCapture(S->cstream, &g);
+        if (e == cudaSuccess && rc == PL_OK) e = cudaGraphInstantiate(&S->graph[gi], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (rc == PL_OK && e != cudaSuccess) rc = cuda_fail(e, "PCG graph capture");
+        S->graph_iters[gi] = chunk;
+        S->graph_epoch[gi] = state_epoch();
     }
-    return fail(PL_ERR_NOT_CONVERGED, "PCG reached the iteration limit");
+    for (int it = 0; rc == PL_OK && it < max_iter; it += chunk) {
+        cudaError_t e = cudaGraphLaunch(S->graph[gi], S->cstream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, S->cstream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->cstream);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "PCG iterations");
+            break;
+        }
+        *iters = it + chunk;
+        const double rn = std::sqrt(h[S_RR]);
+        *rel = rn / r0;
+        if (!(rn == rn)) {
+            rc = fail(PL_ERR_NOT_CONVERGED, "PCG diverged (NaN residual)");
+            break;
+        }
+        if (rn <= stop) break;
+        if (it + chunk >= max_iter) rc = fail(PL_ERR_NOT_CONVERGED, "PCG reached the iteration limit");
+    }
+    c->stream = s;
+    cudaEventRecord(S->ev_out, S->cstream);
+    cudaStreamWaitEvent(s, S->ev_out, 0);
+    return rc;
 }
+
 
 }  // namespace
 
@@ -477,7 +518,7 @@ int pl_solver_create(pl_mesh m, const uint8_t* constrained, pl_solver* out) {
     A(&S->d_diag, 9 * S->nnodes);
     A(&S->d_pinv, 9 * S->nnodes);
     A(&S->d_pinv32, 9 * S->nnodes);
-    A(&S->d_r, n); A(&S->d_p, n); A(&S->d_q, n); A(&S->d_z, n); A(&S->d_x, n);
+    A(&S->d_r, n); A(&S->d_p, n); A(&S->d_q, n); A(&S->d_z, n); A(&S->d_x, n); A(&S->d_xs, n);
     A(&S->f_r, n); A(&S->f_p, n); A(&S->f_q, n); A(&S->f_z, n); A(&S->f_x, n);
     A(&S->d_scal, S_COUNT);
     A(&S->d_partials, 2 * kRedBlocks);
@@ -504,6 +545,9 @@ int pl_solver_create(pl_mesh m, const uint8_t* constrained, pl_solver* out) {
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(S->d_scal, 0, S_COUNT * sizeof(double), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->cstream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->ev_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S->ev_out, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         pl_solver_destroy(S);
         return cuda_fail(e, "pl_solver_create");
@@ -546,6 +590,7 @@ int pl_solver_setup(pl_solver S, double t, double dt) {
     PLB_CUDA(cudaSetDevice(m->ctx->device));
     S->t = t;
     S->dt = dt;
+    bump_state_epoch();  // t and dt are arguments of captured kernels: re-capture
     PLB_CUDA(cudaMemsetAsync(S->d_diag, 0, 9 * S->nnodes * sizeof(double), s));
     for (pl_integrator ig : S->ops) {
         DomainParams p;
@@ -582,7 +627,9 @@ int pl_solver_solve(pl_solver S, const double* b, double* x) {
     if (S->precision == PL_SOLVER_FP64) {
         int it = 0;
         double rel = 0.0;
-        int rc = pcg<double>(S, b, x, S->rtol, S->atol, S->max_iter, S->d_pinv, S->d_r, S->d_p, S->d_q, S->d_z, &it, &rel);
+        int rc = pcg<double>(S, b, S->d_xs, S->rtol, S->atol, S->max_iter, S->d_pinv, S->d_r, S->d_p, S->d_q, S->d_z,
+                             &it, &rel);
+        PLB_CUDA(cudaMemcpyAsync(x, S->d_xs, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         fault_unfold(S, x);
         S->iterations = it;
         S->rel_residual = rel;
@@ -652,8 +699,14 @@ int pl_solver_destroy(pl_solver S) {
     if (!S) return PL_OK;
     cudaSetDevice(S->mesh->ctx->device);
     cudaStreamSynchronize(S->mesh->ctx->stream);
+    for (cudaGraphExec_t g : S->graph)
+        if (g) cudaGraphExecDestroy(g);
+    if (S->cstream) cudaStreamSynchronize(S->cstream);
+    if (S->ev_in) cudaEventDestroy(S->ev_in);
+    if (S->ev_out) cudaEventDestroy(S->ev_out);
+    if (S->cstream) cudaStreamDestroy(S->cstream);
     void* ptrs[] = {S->d_mask, S->d_diag, S->d_pinv, S->d_pinv32, S->d_r, S->d_p, S->d_q, S->d_z, S->d_x,
-                    S->f_r, S->f_p, S->f_q, S->f_z, S->f_x, S->d_scal, S->d_partials,
+                    S->d_xs, S->f_r, S->f_p, S->f_q, S->f_z, S->f_x, S->d_scal, S->d_partials,
                     S->d_pair_neg, S->d_pair_pos, S->d_pair_normal};
     for (void* p : ptrs)
         if (p) cudaFree(p);
