@@ -188,7 +188,8 @@ def run_reference(args, rank, world):
             "ms_per_step": 2 * mesh.num_dof / (base["value"] * 1e9) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": "elasticity P1 tet residual+Jv",
-                                            "cells": mesh.num_cells, "dof": mesh.num_dof},
+                                            "cells": mesh.num_cells, "nodes": mesh.num_nodes,
+                                            "dof": mesh.num_dof},
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

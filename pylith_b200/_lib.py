@@ -27,7 +27,7 @@ ERRORS = {
 PL_LHS, PL_RHS, PL_LHS_LUMPED_INV, PL_LHS_WEIGHTED = 0, 1, 2, 3
 PL_AUX_PER_CELL, PL_AUX_PER_QUADPT, PL_AUX_PER_FAULT_NODE = 0, 1, 2
 PL_INSERT, PL_ADD = 0, 1
-PL_SCATTER_AUTO, PL_SCATTER_ATOMIC, PL_SCATTER_BLOCKED = 0, 1, 2
+PL_SCATTER_AUTO, PL_SCATTER_ATOMIC, PL_SCATTER_BLOCKED, PL_SCATTER_DETERMINISTIC = 0, 1, 2, 3
 PL_FACE_NEGATIVE, PL_FACE_POSITIVE, PL_FACE_FAULT = 0, 1, 2
 
 

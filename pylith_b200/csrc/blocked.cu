@@ -68,6 +68,7 @@ struct BlockArrays {
     const ushort4* lconn;       // [ncells] block-local slots of the 4 corners
     const uint32_t* inc_off;    // per block ns+1 offsets (block b starts at slot_begin[b] + b)
     const uint16_t* inc;        // [nblocks][4 * kTetBlockCells] cell * 4 + corner
+    double* partial;            // [slots][3] sums of shared nodes, per block (FP64 kernels)
     int64_t nblocks;
     int max_local_nodes;
 };
@@ -228,7 +229,10 @@ PL_D void tet_cell_element(const DomainParams& p, const int* aoff, const double*
     for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + slot] = e0[cc] + bfw * f0[cc];
 }
 
-template <int RHEO, bool BF, int OP, bool INSERT>
+// DET: a shared node's block sum goes to the partial-sum buffer for the fixup pass (bit-identical
+// results run to run); otherwise it is added into the output with an FP64 reduction (the output
+// was zeroed first for INSERT).
+template <int RHEO, bool BF, int OP, bool INSERT, bool DET>
 __global__ void __launch_bounds__(kTetThreads, PLB_TET_MIN_BLOCKS) k_tet_blocked(DomainParams p, BlockArrays A) {
     using L = AuxLayout<RHEO, BF>;
     extern __shared__ __align__(16) char smem_raw[];
@@ -308,7 +312,13 @@ __global__ void __launch_bounds__(kTetThreads, PLB_TET_MIN_BLOCKS) k_tet_blocked
             }
             const uint32_t id = S.id[i];
             double* o = p.out + 3 * (int64_t)(id & ~kSharedBit);
-            if (id & kSharedBit) {
+            if ((id & kSharedBit) && DET) {
+                // this block's part of a shared node: summed over blocks by the fixup pass
+                double* pp = A.partial + 3 * (int64_t)(s0 + i);
+                pp[0] = r0;
+                pp[1] = r1;
+                pp[2] = r2;
+            } else if (id & kSharedBit) {
                 red_add(o, r0);
                 red_add(o + 1, r1);
                 red_add(o + 2, r2);
@@ -443,8 +453,36 @@ __global__ void __launch_bounds__(kTetBlockCells, 4) k_tet_blocked_jv32(DomainPa
     }
 }
 
-static BlockArrays arrays_of(const BlockedLayout& b) {
+// Second pass of the FP64 cell-block kernels: every node that is not owned by exactly one block
+// gets the sum of its blocks' partial sums, in block order (nodes in no cell get zero).
+template <bool INSERT>
+__global__ void k_blocked_fixup(double* __restrict__ out, const double* __restrict__ partial,
+                                const int32_t* __restrict__ fix_node, const int32_t* __restrict__ fix_off,
+                                const int32_t* __restrict__ fix_slot, int64_t nfix) {
+    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nfix; f += (int64_t)gridDim.x * blockDim.x) {
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+        for (int j = fix_off[f]; j < fix_off[f + 1]; ++j) {
+            const double* pp = partial + 3 * (int64_t)fix_slot[j];
+            r0 += pp[0];
+            r1 += pp[1];
+            r2 += pp[2];
+        }
+        double* o = out + 3 * (int64_t)fix_node[f];
+        if (INSERT) {
+            o[0] = r0;
+            o[1] = r1;
+            o[2] = r2;
+        } else {
+            o[0] += r0;
+            o[1] += r1;
+            o[2] += r2;
+        }
+    }
+}
+
+static BlockArrays arrays_of(const BlockedLayout& b, double* partial = nullptr) {
     BlockArrays A;
+    A.partial = partial;
     A.slot_begin = b.d_block_node_begin;
     A.slot_node = b.d_slot_node;
     A.lconn = (const ushort4*)b.d_local_cells;
@@ -466,18 +504,30 @@ static int persistent_grid(int64_t nblocks) {
     return (int)std::min<int64_t>(nblocks, (int64_t)nsm * PLB_TET_MIN_BLOCKS);
 }
 
+template <int RHEO, bool BF, int OP, bool INSERT, bool DET>
+static void launch_one(const DomainParams& p, const BlockArrays& A, size_t smem, int grid, cudaStream_t s) {
+    auto kern = k_tet_blocked<RHEO, BF, OP, INSERT, DET>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, kTetThreads, smem, s>>>(p, A);
+    count_launch();
+}
+
 template <int RHEO, bool BF, int OP>
-static void launch_t(const DomainParams& p, const BlockedLayout& b, bool insert, cudaStream_t s) {
+static void launch_t(const DomainParams& p, const BlockedLayout& b, bool insert, double* partial, cudaStream_t s) {
     const size_t smem = blocked_smem(b);
     const int grid = persistent_grid(b.num_blocks);
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_tet_blocked<RHEO, BF, OP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_tet_blocked<RHEO, BF, OP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const BlockArrays A = arrays_of(b, partial);
+    const bool det = partial != nullptr;
+    if (insert && det) launch_one<RHEO, BF, OP, true, true>(p, A, smem, grid, s);
+    else if (insert) launch_one<RHEO, BF, OP, true, false>(p, A, smem, grid, s);
+    else if (det) launch_one<RHEO, BF, OP, false, true>(p, A, smem, grid, s);
+    else launch_one<RHEO, BF, OP, false, false>(p, A, smem, grid, s);
+    if (det && b.num_fix > 0) {
+        const int fg = (int)std::min<int64_t>((b.num_fix + 255) / 256, 148 * 8);
+        if (insert) k_blocked_fixup<true><<<fg, 256, 0, s>>>(p.out, partial, b.d_fix_node, b.d_fix_off, b.d_fix_slot, b.num_fix);
+        else k_blocked_fixup<false><<<fg, 256, 0, s>>>(p.out, partial, b.d_fix_node, b.d_fix_off, b.d_fix_slot, b.num_fix);
+        count_launch();
     }
-    const BlockArrays A = arrays_of(b);
-    if (insert) k_tet_blocked<RHEO, BF, OP, true><<<grid, kTetThreads, smem, s>>>(p, A);
-    else k_tet_blocked<RHEO, BF, OP, false><<<grid, kTetThreads, smem, s>>>(p, A);
-    count_launch();
 }
 
 static bool blocked_usable(const BlockedLayout& b) {
@@ -486,17 +536,19 @@ static bool blocked_usable(const BlockedLayout& b) {
 }
 
 bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, bool bf,
-                                 int op, bool insert, int64_t nnodes, cudaStream_t s) {
+                                 int op, bool insert, int64_t nnodes, double* partial, cudaStream_t s) {
     if (cell != TET4 || rheo != RHEO_ILE || !blocked_usable(b)) return false;
-    // INSERT: shared nodes receive reductions from several blocks, untouched nodes none, so the
-    // output starts from zero; nodes owned by one block are then stored directly.
-    if (insert && (b.num_shared_nodes > 0 || b.num_untouched > 0))
+    // Nodes owned by one block are stored (INSERT) or added (ADD) by their block. With a
+    // partial-sum buffer (deterministic mode) the fixup pass then writes or adds every other
+    // node, so no output zeroing and no atomics are needed and the sums are the same every run.
+    // Without one, shared nodes get FP64 reductions, and for INSERT the output starts from zero.
+    if (!partial && insert && (b.num_shared_nodes > 0 || b.num_untouched > 0))
         if (cudaMemsetAsync(p.out, 0, 3 * nnodes * sizeof(double), s) != cudaSuccess) return false;
     if (op == OP_RESIDUAL) {
-        if (bf) launch_t<RHEO_ILE, true, OP_RESIDUAL>(p, b, insert, s);
-        else launch_t<RHEO_ILE, false, OP_RESIDUAL>(p, b, insert, s);
+        if (bf) launch_t<RHEO_ILE, true, OP_RESIDUAL>(p, b, insert, partial, s);
+        else launch_t<RHEO_ILE, false, OP_RESIDUAL>(p, b, insert, partial, s);
     } else {
-        launch_t<RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, insert, s);
+        launch_t<RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, insert, partial, s);
     }
     return true;
 }
@@ -572,7 +624,31 @@ int ensure_blocked_layout(pl_mesh_s* m) {
         nshared += nblocks_of[nd] > 1;
         nuntouched += nblocks_of[nd] == 0;
     }
+    // fixup lists: nodes not owned by exactly one block, with their slots in block order
+    std::vector<int32_t> fix_node, fix_off(1, 0), fix_slot;
+    {
+        std::vector<int32_t> first(m->nnodes + 1, 0);
+        for (size_t gs = 0; gs < node_ids.size(); ++gs) {
+            const uint32_t nd = node_ids[gs] & ~kSharedBit;
+            if (nblocks_of[nd] > 1) first[nd + 1]++;
+        }
+        for (int64_t nd = 0; nd < m->nnodes; ++nd) first[nd + 1] += first[nd];
+        std::vector<int32_t> slots(first[m->nnodes]);
+        std::vector<int32_t> pos(first.begin(), first.end() - 1);
+        for (size_t gs = 0; gs < node_ids.size(); ++gs) {
+            const uint32_t nd = node_ids[gs] & ~kSharedBit;
+            if (nblocks_of[nd] > 1) slots[pos[nd]++] = (int32_t)gs;
+        }
+        for (int64_t nd = 0; nd < m->nnodes; ++nd) {
+            if (nblocks_of[nd] == 1) continue;
+            fix_node.push_back((int32_t)nd);
+            for (int32_t j = first[nd]; j < first[nd + 1]; ++j) fix_slot.push_back(slots[j]);
+            fix_off.push_back((int32_t)fix_slot.size());
+        }
+    }
     BlockedLayout* L = new BlockedLayout();
+    L->num_slots = (int64_t)node_ids.size();
+    L->num_fix = (int64_t)fix_node.size();
     L->cells_per_block = B;
     L->num_blocks = nb;
     L->max_local_nodes = maxloc;
@@ -592,6 +668,9 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     up(&L->d_local_cells, lconn);
     up(&L->d_inc_off, inc_off);
     up(&L->d_inc, inc);
+    up(&L->d_fix_node, fix_node);
+    up(&L->d_fix_off, fix_off);
+    up(&L->d_fix_slot, fix_slot);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         free_blocked_layout(L);
@@ -608,6 +687,9 @@ void free_blocked_layout(BlockedLayout* b) {
     cudaFree(b->d_local_cells);
     cudaFree(b->d_inc_off);
     cudaFree(b->d_inc);
+    cudaFree(b->d_fix_node);
+    cudaFree(b->d_fix_off);
+    cudaFree(b->d_fix_slot);
     delete b;
 }
 

@@ -570,7 +570,7 @@ int pl_integrator_set_constants(pl_integrator ig, int num, const double* constan
 
 int pl_integrator_set_scatter(pl_integrator ig, int scatter) {
     bump_state_epoch();  // captured solver graphs hold kernel arguments
-    if (!ig || scatter < PL_SCATTER_AUTO || scatter > PL_SCATTER_BLOCKED) return fail(PL_ERR_INVALID_ARG, "bad scatter");
+    if (!ig || scatter < PL_SCATTER_AUTO || scatter > PL_SCATTER_DETERMINISTIC) return fail(PL_ERR_INVALID_ARG, "bad scatter");
     ig->scatter = scatter;
     return PL_OK;
 }
@@ -583,6 +583,7 @@ int pl_integrator_destroy(pl_integrator ig) {
     for (AuxField& f : ig->aux)
         if (f.d) cudaFree(f.d);
     if (ig->d_cell_ids) cudaFree(ig->d_cell_ids);
+    if (ig->d_block_partial) cudaFree(ig->d_block_partial);
     pl_mesh m = ig->mesh;
     delete ig;
     mesh_release(m);
@@ -592,11 +593,24 @@ int pl_integrator_destroy(pl_integrator ig) {
 // ---- compute ----------------------------------------------------------------------------
 
 
+extern "C++" {
+namespace plb {
+int prepare_blocked(pl_integrator_s* ig) {
+    pl_mesh m = ig->mesh;
+    int rc = ensure_blocked_layout(m);
+    if (rc) return rc;
+    if (ig->scatter == PL_SCATTER_DETERMINISTIC && !ig->d_block_partial && m->blocked->num_slots > 0)
+        PLB_CUDA(cudaMalloc((void**)&ig->d_block_partial, 3 * m->blocked->num_slots * sizeof(double)));
+    return PL_OK;
+}
+}  // namespace plb
+}
+
 static bool use_blocked(pl_integrator ig) {
     pl_mesh m = ig->mesh;
     if (ig->scatter == PL_SCATTER_ATOMIC) return false;
     if (ig->subset) return false;  // the blocked layout covers whole meshes
-    return m->cell_type == PL_CELL_TET4 || ig->scatter == PL_SCATTER_BLOCKED;
+    return m->cell_type == PL_CELL_TET4 || ig->scatter == PL_SCATTER_BLOCKED || ig->scatter == PL_SCATTER_DETERMINISTIC;
 }
 
 int pl_compute_lhs_residual(pl_integrator ig, double t, double dt, const double* u, const double* u_t,
@@ -628,9 +642,10 @@ int pl_compute_lhs_residual(pl_integrator ig, double t, double dt, const double*
     p.out = r;
     p.t = t;
     p.dt = dt;
-    if (use_blocked(ig) && (rc = ensure_blocked_layout(m)) == PL_OK &&
-        launch_domain_apply_blocked(p, *m->blocked, m->cell_type, rheo, bf, OP_RESIDUAL,
-                                    mode == PL_INSERT, m->nnodes, s)) {
+    if (use_blocked(ig) && (rc = prepare_blocked(ig)) == PL_OK &&
+        launch_domain_apply_blocked(p, *m->blocked, m->cell_type, rheo, bf, OP_RESIDUAL, mode == PL_INSERT,
+                                    m->nnodes, ig->scatter == PL_SCATTER_DETERMINISTIC ? ig->d_block_partial : nullptr,
+                                    s)) {
         if (mode == PL_INSERT && m->nlag > 0)
             PLB_CUDA(cudaMemsetAsync(r + 3 * m->nnodes, 0, 3 * m->nlag * sizeof(double), s));
         PLB_CUDA(cudaGetLastError());
@@ -676,9 +691,10 @@ int pl_compute_lhs_jacobian_action(pl_integrator ig, double t, double dt, double
     p.t = t;
     p.dt = dt;
     p.s_tshift = s_tshift;
-    if (use_blocked(ig) && (rc = ensure_blocked_layout(m)) == PL_OK &&
-        launch_domain_apply_blocked(p, *m->blocked, m->cell_type, rheo, false, OP_JACOBIAN_ACTION,
-                                    mode == PL_INSERT, m->nnodes, s)) {
+    if (use_blocked(ig) && (rc = prepare_blocked(ig)) == PL_OK &&
+        launch_domain_apply_blocked(p, *m->blocked, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, mode == PL_INSERT,
+                                    m->nnodes, ig->scatter == PL_SCATTER_DETERMINISTIC ? ig->d_block_partial : nullptr,
+                                    s)) {
         if (mode == PL_INSERT && m->nlag > 0)
             PLB_CUDA(cudaMemsetAsync(jv + 3 * m->nnodes, 0, 3 * m->nlag * sizeof(double), s));
         PLB_CUDA(cudaGetLastError());

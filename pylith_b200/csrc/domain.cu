@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(128) k_domain_apply(DomainParams p) {
 #pragma unroll
             for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)nodes[E::corner(k)] + i];
         const double* field = OP == OP_RESIDUAL ? p.u : p.v;
-        double a[L::size];
+        double a[L::size] = {};
         L::load_cell(p, c, a);
         double acc[E::nen * 3];
 #pragma unroll
@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(128) k_domain_apply(DomainParams p) {
                     s_x[6 + d] += u2 * gr[d];
                 }
             }
-            L::load_qp(p, c, q, E::nq, a);
+            if (OP == OP_RESIDUAL) L::load_qp(p, c, q, E::nq, a);  // the tangents read no state
             double x[3] = {0, 0, 0};
             double f0[3] = {0, 0, 0}, f1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             if (OP == OP_RESIDUAL) {
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(128) k_domain_jv_f32(DomainParams p) {
         for (int k = 0; k < E::ngeom; ++k)
 #pragma unroll
             for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)nodes[E::corner(k)] + i];
-        double a[L::size];
+        double a[L::size] = {};
         L::load_cell(p, c, a);
         float acc[E::nen * 3];
 #pragma unroll
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(128) k_domain_jv_f32(DomainParams p) {
                     s_x[6 + d] += vn[2] * gr[d];
                 }
             }
-            L::load_qp(p, c, q, E::nq, a);
+            // the tangents (Jf3vu of both rheologies) read no per-point state
             double x[3] = {0, 0, 0};
             double Jf3d[81];
 #pragma unroll
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(128) k_domain_jacobian(DomainParams p, const i
         for (int k = 0; k < E::ngeom; ++k)
 #pragma unroll
             for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)cn[E::corner(k)] + i];
-        double a[L::size];
+        double a[L::size] = {};
         L::load_cell(p, c, a);
         const int32_t* cpos = pos + mc * E::nen * E::nen;
 #pragma unroll 1
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(128) k_domain_jacobian(DomainParams p, const i
             Geom g;
             E::geom(X, q, &g);
             if (!(g.detJ > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
-            L::load_qp(p, c, q, E::nq, a);
+            // the tangents (Jf3vu of both rheologies) read no per-point state
             double x[3] = {0, 0, 0};
             double Jf3[81];
 #pragma unroll
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(128) k_domain_update_state(DomainParams p) {
         for (int k = 0; k < E::ngeom; ++k)
 #pragma unroll
             for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)nodes[E::corner(k)] + i];
-        double a[L::size];
+        double a[L::size] = {};
         L::load_cell(p, c, a);
 #pragma unroll 1
         for (int q = 0; q < E::nq; ++q) {
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(128) k_domain_derived(DomainParams p, DerivedS
                 s_x[6 + d] += un[2] * gr[d];
             }
         }
-        double a[L::size];
+        double a[L::size] = {};
         L::load_cell(p, c, a);
         L::load_qp(p, c, 0, E::nq, a);
         const int sOff[1] = {0}, sOff_x[1] = {0};

@@ -161,9 +161,9 @@ __global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(Dom
 #pragma unroll
                 for (int e = 0; e < 3; ++e)
                     s_x[cc * 3 + e] = Gr[cc][0] * inv[0][e] + Gr[cc][1] * inv[1][e] + Gr[cc][2] * inv[2][e];
-            double a[L::size];
+            double a[L::size] = {};
             L::load_cell(p, c, a);
-            L::load_qp(p, c, q, H::NQ, a);
+            if (OP == OP_RESIDUAL) L::load_qp(p, c, q, H::NQ, a);  // the tangents read no state
             double x[3] = {0, 0, 0}, s[3] = {0, 0, 0};
             double f0[3] = {0, 0, 0};
             T f1[9];

@@ -61,6 +61,13 @@ struct BlockedLayout {
     uint16_t* d_inc = nullptr;              // [num_blocks][4 * cells_per_block] (cell * 4 + corner)
     int64_t num_shared_nodes = 0;
     int64_t num_untouched = 0;
+    int64_t num_slots = 0;                  // block-local node slots over all blocks
+    // Nodes not owned by exactly one block (shared between blocks, or in no cell): the FP64
+    // kernels leave them to a second pass that sums the blocks' partial sums in block order.
+    int64_t num_fix = 0;
+    int32_t* d_fix_node = nullptr;          // [num_fix] node ids
+    int32_t* d_fix_off = nullptr;           // [num_fix + 1] offsets into d_fix_slot
+    int32_t* d_fix_slot = nullptr;          // global slot ids of each node, in block order
     size_t device_bytes = 0;
 };
 
@@ -121,6 +128,7 @@ struct pl_integrator_s {
     int64_t ncells = 0;                 // cells integrated over
     bool subset = false;                // created with a cell list (possibly empty)
     int32_t* d_cell_ids = nullptr;      // NULL: all cells of the mesh, in order (or none, for an empty subset)
+    double* d_block_partial = nullptr;  // [num_slots][3] partial sums of shared nodes (cell-block kernels)
     std::vector<int32_t> h_cell_ids;
     // domain kernels
     plb::KernelId r0 = plb::K_NONE, r1 = plb::K_NONE;

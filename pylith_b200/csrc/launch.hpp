@@ -43,8 +43,11 @@ void free_blocked_layout(BlockedLayout* b);
 // Cell-block (shared-memory, deterministic) residual / Jacobian action; returns false when the
 // layout does not support the configuration.
 bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell,
-                                 int rheo, bool bf, int op, bool insert, int64_t nnodes,
+                                 int rheo, bool bf, int op, bool insert, int64_t nnodes, double* partial,
                                  cudaStream_t s);
+// The cell-block layout of the integrator's mesh and the integrator's partial-sum buffer
+// (allocations: call outside stream capture).
+int prepare_blocked(pl_integrator_s* ig);
 
 // FP32 Jacobian action on the cell blocks (the output must be zeroed or hold the sum to add to).
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,

@@ -248,13 +248,13 @@ __global__ void __launch_bounds__(128) k_domain_diag_blocks(DomainParams p, doub
         for (int k = 0; k < E::ngeom; ++k)
 #pragma unroll
             for (int i = 0; i < 3; ++i) X[k][i] = p.coords[3 * (int64_t)cn[E::corner(k)] + i];
-        double a[L::size];
+        double a[L::size] = {};
         L::load_cell(p, c, a);
 #pragma unroll 1
         for (int q = 0; q < E::nq; ++q) {
             Geom g;
             E::geom(X, q, &g);
-            L::load_qp(p, c, q, E::nq, a);
+            // the tangents (Jf3vu of both rheologies) read no per-point state
             double x[3] = {0, 0, 0};
             double Jf3[81];
 #pragma unroll
@@ -408,10 +408,11 @@ int pcg(pl_solver S, const T* b, T* x, double rtol, double atol, int max_iter, c
     pl_context c = S->mesh->ctx;
     const int gi = sizeof(T) == 8 ? 0 : 1;
     const int chunk = std::max(1, S->check_every);
-    if (S->mesh->cell_type == PL_CELL_TET4) {
-        int rcl = ensure_blocked_layout(S->mesh);  // allocates: outside any capture
-        if (rcl) return rcl;
-    }
+    if (S->mesh->cell_type == PL_CELL_TET4)
+        for (pl_integrator ig : S->ops) {
+            int rcl = prepare_blocked(ig);  // allocates: outside any capture
+            if (rcl) return rcl;
+        }
     PLB_CUDA(cudaEventRecord(S->ev_in, s));
     PLB_CUDA(cudaStreamWaitEvent(S->cstream, S->ev_in, 0));
     c->stream = S->cstream;

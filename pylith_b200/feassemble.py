@@ -20,7 +20,8 @@ from ._lib import check
 LHS, RHS, LHS_LUMPED_INV, LHS_WEIGHTED = C.PL_LHS, C.PL_RHS, C.PL_LHS_LUMPED_INV, C.PL_LHS_WEIGHTED
 PER_CELL, PER_QUADPT, PER_FAULT_NODE = C.PL_AUX_PER_CELL, C.PL_AUX_PER_QUADPT, C.PL_AUX_PER_FAULT_NODE
 INSERT, ADD = C.PL_INSERT, C.PL_ADD
-SCATTER_AUTO, SCATTER_ATOMIC, SCATTER_BLOCKED = C.PL_SCATTER_AUTO, C.PL_SCATTER_ATOMIC, C.PL_SCATTER_BLOCKED
+SCATTER_AUTO, SCATTER_ATOMIC, SCATTER_BLOCKED, SCATTER_DETERMINISTIC = (
+    C.PL_SCATTER_AUTO, C.PL_SCATTER_ATOMIC, C.PL_SCATTER_BLOCKED, C.PL_SCATTER_DETERMINISTIC)
 FACE_NEGATIVE, FACE_POSITIVE, FACE_FAULT = C.PL_FACE_NEGATIVE, C.PL_FACE_POSITIVE, C.PL_FACE_FAULT
 
 

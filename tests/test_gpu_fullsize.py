@@ -3,9 +3,10 @@ linear elasticity, where the oracle would take too long:
   * rigid-body motions (translation, infinitesimal rotation) give a zero residual;
   * F(u) = J u (the residual of isotropic linear elasticity is linear in u, F(u) = -K u);
   * linearity: F(a u + b w) = a F(u) + b F(w);
-  * the cell-block kernel reproduces itself to rounding (nodes shared between cell blocks get
-    FP64 reductions whose order varies between runs) and agrees with the thread-per-cell
-    atomic kernel.
+  * the deterministic cell-block scatter gives bit-identical reruns (shared nodes are summed
+    over their blocks in block order by a second pass); the default scatter (FP64 reductions for
+    shared nodes) reproduces itself to rounding; both agree with the thread-per-cell atomic
+    kernel.
 Relative tolerances are FP64 rounding levels (1e-12 of the residual scale)."""
 import numpy as np
 import pytest
@@ -73,12 +74,23 @@ def test_residual_equals_jacobian_action_and_is_linear(setup):
     assert float((rab - (a * ru + b * rw)).norm() / rab.norm()) <= TOL64
 
 
-def test_blocked_kernel_reruns_and_matches_atomic(setup):
+def test_blocked_kernel_is_deterministic_and_matches_atomic(setup):
     torch, FA, ctx, dm, mesh, mat, ig = setup
     g = torch.Generator(device="cuda").manual_seed(7)
     u = torch.randn(mesh.num_dof, dtype=torch.float64, device="cuda", generator=g)
-    r1, r2 = _res(torch, ctx, ig, u), _res(torch, ctx, ig, u)
-    assert float((r1 - r2).norm() / r1.norm()) <= 1e-14
+    idet = mat.create_integrator(dm)
+    idet.set_scatter(FA.SCATTER_DETERMINISTIC)
+    r1, r2 = _res(torch, ctx, idet, u), _res(torch, ctx, idet, u)
+    assert torch.equal(r1, r2)
+    jv1, jv2 = torch.empty_like(u), torch.empty_like(u)
+    idet.compute_lhs_jacobian_action(0.0, 0.0, 0.0, u, u, jv1)
+    idet.compute_lhs_jacobian_action(0.0, 0.0, 0.0, u, u, jv2)
+    ctx.synchronize()
+    assert torch.equal(jv1, jv2)
+    # the default cell-block scatter reproduces itself to rounding
+    rb1, rb2 = _res(torch, ctx, ig, u), _res(torch, ctx, ig, u)
+    assert float((rb1 - r1).norm() / r1.norm()) <= TOL64
+    assert float((rb1 - rb2).norm() / rb1.norm()) <= 1e-14
     ia = mat.create_integrator(dm)
     ia.set_scatter(FA.SCATTER_ATOMIC)
     ra = _res(torch, ctx, ia, u)

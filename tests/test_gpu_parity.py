@@ -67,7 +67,7 @@ def oracle_aux(O, mat):
 
 
 @pytest.mark.parametrize("kind", list(MESHES))
-@pytest.mark.parametrize("scatter", [0, 1])
+@pytest.mark.parametrize("scatter", [0, 1, 3])
 def test_elastic_residual_matches_oracle(oracle_lib, torch_cuda, ctx, kind, scatter):
     from pylith_b200 import feassemble as FA
 
