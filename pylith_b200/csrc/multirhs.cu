@@ -52,21 +52,54 @@ PL_D double tet_cof_m(const double X[4][3], double cof[3][3]) {
     return J[0][0] * cof[0][0] + J[0][1] * cof[1][0] + J[0][2] * cof[2][0];
 }
 
-// Chunk of right-hand sides whose element vectors are staged in shared memory at once.
-#ifndef PLB_MULTI_KC
-#define PLB_MULTI_KC 2
-#endif
+// Right-hand sides handled together: their values travel as one vector (float, float2, float4)
+// through shared memory and into the output.
 template <int K>
 struct MultiChunk {
-    static constexpr int value = K < PLB_MULTI_KC ? K : PLB_MULTI_KC;
+    static constexpr int value = K < 4 ? K : 4;
 };
 
+template <int W>
+PL_D void ld_vec(const float* p, float (&v)[W]) {
+    if (W == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        v[0] = q.x; v[1] = q.y; v[2 % W] = q.z; v[3 % W] = q.w;
+    } else if (W == 2) {
+        const float2 q = *reinterpret_cast<const float2*>(p);
+        v[0] = q.x; v[1 % W] = q.y;
+    } else {
+        v[0] = p[0];
+    }
+}
+
+template <int W>
+PL_D void st_vec(float* p, const float (&v)[W]) {
+    if (W == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1 % W], v[2 % W], v[3 % W]);
+    else if (W == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1 % W]);
+    else p[0] = v[0];
+}
+
+// out[0..W) += v, as one vector FP32 reduction (the address is W*4-byte aligned).
+template <int W>
+PL_D void red_vec(float* p, const float (&v)[W]) {
+    if (W == 4)
+        asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v[0]), "f"(v[1 % W]), "f"(v[2 % W]),
+                     "f"(v[3 % W])
+                     : "memory");
+    else if (W == 2)
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v[0]), "f"(v[1 % W]) : "memory");
+    else
+        red_add(p, v[0]);
+}
+
 // v, out: [ndof][K] FP32 (ndof = 3 * nodes, node-major); out must be zeroed or hold the sum to add to.
-// Per cell block: the block's node coordinates (FP64) and K field vectors (FP32) are staged in
-// shared memory component-major ([3][ld], [3K][ld]); one thread per cell forms the geometry and
-// the isotropic tangent once and then, KC right-hand sides at a time, the element vectors, which
-// are staged ([12][KC][cells]) and summed per node over the block-local incidence list in a fixed
-// order (nodes shared with other blocks get FP32 reductions into global memory).
+// Per cell block: the block's node coordinates (FP64, [3][ld]) and K field vectors (FP32, one row
+// of 3K values per node, as in global memory) are staged in shared memory. One thread per cell
+// forms the geometry and the isotropic tangent once and then, KC right-hand sides at a time (one
+// vector load per node and component), the element vectors, staged as [12][cells][KC]; then one
+// work item per (node, component) sums its incident corners over the block-local incidence list
+// in a fixed order, KC right-hand sides per vector, and adds the node into the output (one vector
+// reduction when the node is shared with other blocks).
 template <int K>
 __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     DomainParams p, const int32_t* __restrict__ slot_begin, const uint32_t* __restrict__ slot_node,
@@ -76,9 +109,10 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     using L = AuxLayout<RHEO_ILE, false>;
     extern __shared__ __align__(16) char smem_raw[];
     const AuxOffsets<RHEO_ILE, false> aoff;
-    float* sE = reinterpret_cast<float*>(smem_raw);                                              // [12][KC][cells]
-    double* sX = reinterpret_cast<double*>(smem_raw + 12 * KC * kMultiBlockCells * sizeof(float));  // [3][ld]
-    float* sV = reinterpret_cast<float*>(sX + 3 * ld);                                           // [3K][ld]
+    float* sE = reinterpret_cast<float*>(smem_raw);                                              // [12][cells][KC]
+    float* sV = sE + 12 * kMultiBlockCells * KC;                                                 // [ld][3K]
+    // [3][ld], at a 16-byte boundary after sV
+    double* sX = reinterpret_cast<double*>(reinterpret_cast<char*>(sV) + ((size_t)ld * 3 * K * sizeof(float) + 15) / 16 * 16);
     const int tc = threadIdx.x;
     for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int s0 = slot_begin[b];
@@ -88,18 +122,12 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 #pragma unroll
             for (int d = 0; d < 3; ++d) sX[d * ld + i] = p.coords[3 * nd + d];
             const float* vr = v + 3 * K * nd;
-            if (K % 4 == 0) {
+            float* sr = sV + 3 * K * i;
 #pragma unroll
-                for (int j = 0; j < 3 * K; j += 4) {
-                    const float4 q = *reinterpret_cast<const float4*>(vr + j);
-                    sV[(j + 0) * ld + i] = q.x;
-                    sV[(j + 1) * ld + i] = q.y;
-                    sV[(j + 2) * ld + i] = q.z;
-                    sV[(j + 3) * ld + i] = q.w;
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < 3 * K; ++j) sV[j * ld + i] = vr[j];
+            for (int j = 0; j < 3 * K; j += KC) {
+                float t[KC];
+                ld_vec<KC>(vr + j, t);
+                st_vec<KC>(sr + j, t);
             }
         }
         __syncthreads();
@@ -146,64 +174,81 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 #pragma unroll 1
         for (int r0 = 0; r0 < K; r0 += KC) {
             if (live) {
+                // gradient of the KC fields: G[cc][k] = v_{k+1} - v_0 per component, then s_x = G inv
+                float s_x[KC][3][3];
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    float u0[KC], u1[KC], u2[KC], u3[KC];
+                    ld_vec<KC>(sV + 3 * K * ln[0] + cc * K + r0, u0);
+                    ld_vec<KC>(sV + 3 * K * ln[1] + cc * K + r0, u1);
+                    ld_vec<KC>(sV + 3 * K * ln[2] + cc * K + r0, u2);
+                    ld_vec<KC>(sV + 3 * K * ln[3] + cc * K + r0, u3);
+#pragma unroll
+                    for (int rr = 0; rr < KC; ++rr) {
+                        const float g0 = u1[rr] - u0[rr], g1 = u2[rr] - u0[rr], g2 = u3[rr] - u0[rr];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) s_x[rr][cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
+                    }
+                }
+                // flux f1 = -(lambda tr(e) I + 2 mu e), in place of s_x
 #pragma unroll
                 for (int rr = 0; rr < KC; ++rr) {
-                    const int r = r0 + rr;
-                    float s_x[3][3];
+                    const float ltr = lam * (s_x[rr][0][0] + s_x[rr][1][1] + s_x[rr][2][2]);
+                    const float xy = -mu * (s_x[rr][0][1] + s_x[rr][1][0]);
+                    const float yz = -mu * (s_x[rr][1][2] + s_x[rr][2][1]);
+                    const float xz = -mu * (s_x[rr][0][2] + s_x[rr][2][0]);
+                    s_x[rr][0][0] = -(2.0f * mu * s_x[rr][0][0] + ltr);
+                    s_x[rr][1][1] = -(2.0f * mu * s_x[rr][1][1] + ltr);
+                    s_x[rr][2][2] = -(2.0f * mu * s_x[rr][2][2] + ltr);
+                    s_x[rr][0][1] = s_x[rr][1][0] = xy;
+                    s_x[rr][1][2] = s_x[rr][2][1] = yz;
+                    s_x[rr][0][2] = s_x[rr][2][0] = xz;
+                }
 #pragma unroll
-                    for (int cc = 0; cc < 3; ++cc) {
-                        const float* vc = sV + (cc * K + r) * ld;
-                        const float u0 = vc[ln[0]];
-                        const float g0 = vc[ln[1]] - u0, g1 = vc[ln[2]] - u0, g2 = vc[ln[3]] - u0;
+                for (int cc = 0; cc < 3; ++cc) {
+                    float e0[KC];
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) s_x[cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
-                    }
-                    const float ltr = lam * (s_x[0][0] + s_x[1][1] + s_x[2][2]);
-                    float f1[3][3];
+                    for (int rr = 0; rr < KC; ++rr) e0[rr] = 0.f;
 #pragma unroll
-                    for (int f = 0; f < 3; ++f)
+                    for (int k = 0; k < 3; ++k) {
+                        float val[KC];
 #pragma unroll
-                        for (int df = 0; df < 3; ++df)
-                            f1[f][df] = -(mu * (s_x[f][df] + s_x[df][f]) + (f == df ? ltr : 0.0f));
-                    float e0[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                    for (int k = 0; k < 3; ++k)
-#pragma unroll
-                        for (int cc = 0; cc < 3; ++cc) {
-                            const float val = f1[cc][0] * cf[k][0] + f1[cc][1] * cf[k][1] + f1[cc][2] * cf[k][2];
-                            e0[cc] -= val;
-                            sE[(((k + 1) * 3 + cc) * KC + rr) * kMultiBlockCells + tc] = val;
+                        for (int rr = 0; rr < KC; ++rr) {
+                            val[rr] = s_x[rr][cc][0] * cf[k][0] + s_x[rr][cc][1] * cf[k][1] + s_x[rr][cc][2] * cf[k][2];
+                            e0[rr] -= val[rr];
                         }
-#pragma unroll
-                    for (int cc = 0; cc < 3; ++cc) sE[(cc * KC + rr) * kMultiBlockCells + tc] = e0[cc];
+                        st_vec<KC>(sE + (((k + 1) * 3 + cc) * kMultiBlockCells + tc) * KC, val);
+                    }
+                    st_vec<KC>(sE + ((cc)*kMultiBlockCells + tc) * KC, e0);
                 }
             }
             __syncthreads();
-            // one work item per (node, right-hand side of the chunk): consecutive threads take
-            // consecutive nodes of the same right-hand side
-            for (int w = tc; w < ns * KC; w += blockDim.x) {
-                const int rr = w / ns, i = w - rr * ns;
+            // one work item per (node, component): consecutive threads take consecutive nodes
+            for (int w = tc; w < ns * 3; w += blockDim.x) {
+                const int cc = w / ns, i = w - cc * ns;
                 const int j0 = inc_off[s0 + b + i], j1 = inc_off[s0 + b + i + 1];
-                float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+                float acc[KC];
+#pragma unroll
+                for (int rr = 0; rr < KC; ++rr) acc[rr] = 0.f;
 #pragma unroll 4
                 for (int j = j0; j < j1; ++j) {
                     const int e = lst[j];
                     const int cell = e >> 2, corner = e & 3;
-                    const float* se = sE + (corner * 3 * KC + rr) * kMultiBlockCells + cell;
-                    a0 += se[0];
-                    a1 += se[KC * kMultiBlockCells];
-                    a2 += se[2 * KC * kMultiBlockCells];
+                    float t[KC];
+                    ld_vec<KC>(sE + ((corner * 3 + cc) * kMultiBlockCells + cell) * KC, t);
+#pragma unroll
+                    for (int rr = 0; rr < KC; ++rr) acc[rr] += t[rr];
                 }
                 const uint32_t id = slot_node[s0 + i];
-                float* o = out + 3 * K * (int64_t)(id & ~kSharedBitM) + r0 + rr;
+                float* o = out + 3 * K * (int64_t)(id & ~kSharedBitM) + cc * K + r0;
                 if (id & kSharedBitM) {
-                    red_add(o, a0);
-                    red_add(o + K, a1);
-                    red_add(o + 2 * K, a2);
+                    red_vec<KC>(o, acc);
                 } else {
-                    o[0] += a0;
-                    o[K] += a1;
-                    o[2 * K] += a2;
+                    float t[KC];
+                    ld_vec<KC>(o, t);
+#pragma unroll
+                    for (int rr = 0; rr < KC; ++rr) t[rr] += acc[rr];
+                    st_vec<KC>(o, t);
                 }
             }
             __syncthreads();
@@ -213,8 +258,8 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 
 template <int K>
 size_t multi_smem(int ld) {
-    return (size_t)12 * MultiChunk<K>::value * kMultiBlockCells * sizeof(float) + (size_t)ld * 3 * sizeof(double) +
-           (size_t)ld * 3 * K * sizeof(float);
+    return (size_t)12 * MultiChunk<K>::value * kMultiBlockCells * sizeof(float) +
+           ((size_t)ld * 3 * K * sizeof(float) + 15) / 16 * 16 + (size_t)ld * 3 * sizeof(double);
 }
 
 // ---- batched vector kernels, layout [n][K] -------------------------------------------------
