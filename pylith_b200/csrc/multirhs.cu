@@ -100,11 +100,33 @@ PL_D void red_vec(float* p, const float (&v)[W]) {
 // work item per (node, component) sums its incident corners over the block-local incidence list
 // in a fixed order, KC right-hand sides per vector, and adds the node into the output (one vector
 // reduction when the node is shared with other blocks).
+// Asynchronous copies of block b's node rows (K field values per component) and coordinates
+// into shared memory.
+template <int K>
+PL_D void prefetch_multi(const DomainParams& p, const int32_t* __restrict__ slot_begin,
+                         const uint32_t* __restrict__ slot_node, int64_t b, int ld, const float* __restrict__ v,
+                         float* sV, double* sX) {
+    constexpr int CB = K % 4 == 0 ? 16 : (K % 2 == 0 ? 8 : 4);  // bytes per copy; rows are 12 K bytes
+    const int s0 = slot_begin[b];
+    const int ns = slot_begin[b + 1] - s0;
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+        const int64_t nd = slot_node[s0 + i] & ~kSharedBitM;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) __pipeline_memcpy_async(&sX[d * ld + i], &p.coords[3 * nd + d], sizeof(double));
+        const float* vr = v + 3 * K * nd;
+        float* sr = sV + 3 * K * i;
+#pragma unroll
+        for (int j = 0; j < 3 * K; j += CB / 4) __pipeline_memcpy_async(sr + j, vr + j, CB);
+    }
+}
+
+// store_owned: nodes owned by one block are stored (the output was zeroed and this is the first
+// integrator); otherwise they are added.
 template <int K>
 __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     DomainParams p, const int32_t* __restrict__ slot_begin, const uint32_t* __restrict__ slot_node,
     const ushort4* __restrict__ lconn, const uint32_t* __restrict__ inc_off, const uint16_t* __restrict__ inc,
-    int64_t nblocks, int ld, const float* __restrict__ v, float* out) {
+    int64_t nblocks, int ld, const float* __restrict__ v, float* out, bool store_owned) {
     constexpr int KC = MultiChunk<K>::value;
     using L = AuxLayout<RHEO_ILE, false>;
     extern __shared__ __align__(16) char smem_raw[];
@@ -114,22 +136,12 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     // [3][ld], at a 16-byte boundary after sV
     double* sX = reinterpret_cast<double*>(reinterpret_cast<char*>(sV) + ((size_t)ld * 3 * K * sizeof(float) + 15) / 16 * 16);
     const int tc = threadIdx.x;
+    if (blockIdx.x < nblocks) prefetch_multi<K>(p, slot_begin, slot_node, blockIdx.x, ld, v, sV, sX);
+    __pipeline_commit();
     for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int s0 = slot_begin[b];
         const int ns = slot_begin[b + 1] - s0;
-        for (int i = tc; i < ns; i += blockDim.x) {
-            const int64_t nd = slot_node[s0 + i] & ~kSharedBitM;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) sX[d * ld + i] = p.coords[3 * nd + d];
-            const float* vr = v + 3 * K * nd;
-            float* sr = sV + 3 * K * i;
-#pragma unroll
-            for (int j = 0; j < 3 * K; j += KC) {
-                float t[KC];
-                ld_vec<KC>(vr + j, t);
-                st_vec<KC>(sr + j, t);
-            }
-        }
+        __pipeline_wait_prior(0);
         __syncthreads();
         const int64_t c = b * kMultiBlockCells + tc;
         const bool live = c < p.ncells;
@@ -223,6 +235,10 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                 }
             }
             __syncthreads();
+            // the node rows are no longer read in this block: copy the next block's while gathering
+            if (r0 + KC >= K && b + gridDim.x < nblocks)
+                prefetch_multi<K>(p, slot_begin, slot_node, b + gridDim.x, ld, v, sV, sX);
+            __pipeline_commit();
             // one work item per (node, component): consecutive threads take consecutive nodes
             for (int w = tc; w < ns * 3; w += blockDim.x) {
                 const int cc = w / ns, i = w - cc * ns;
@@ -243,6 +259,8 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                 float* o = out + 3 * K * (int64_t)(id & ~kSharedBitM) + cc * K + r0;
                 if (id & kSharedBitM) {
                     red_vec<KC>(o, acc);
+                } else if (store_owned) {
+                    st_vec<KC>(o, acc);
                 } else {
                     float t[KC];
                     ld_vec<KC>(o, t);
@@ -254,6 +272,7 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
             __syncthreads();
         }
     }
+    __pipeline_wait_prior(0);
 }
 
 template <int K>
@@ -487,6 +506,7 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
         count_launch();
     }
     PLB_CUDA(cudaMemsetAsync(out, 0, B->n * K * sizeof(float), s));
+    bool first = true;
     for (pl_integrator ig : S->ops) {
         DomainParams pp;
         int rc = bind_domain_jacobian(ig, &pp);
@@ -512,7 +532,8 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
         const int grid = (int)std::min<int64_t>(L.num_blocks, (int64_t)nsm * std::max(per_sm, 1));
         k_tet_blocked_jv32_multi<K><<<grid, kMultiBlockCells, smem, s>>>(
             pp, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
-            L.num_blocks, L.max_local_nodes, v, out);
+            L.num_blocks, L.max_local_nodes, v, out, first);
+        first = false;
         count_launch();
     }
     if (S->npairs > 0) {
