@@ -103,3 +103,33 @@ def test_host_pointwise_matches_reference_golden(L, name):
             fn(*common, 0.0, x.ctypes.data_as(P), n.ctypes.data_as(P), nc, c.ctypes.data_as(P),
                out.ctypes.data_as(P))
         np.testing.assert_array_equal(out, g[f"{key}.out"][i])
+
+
+def test_argument_validation_without_a_device(L):
+    """Host-side checks run before any CUDA call: null handles and bad arguments return
+    PL_ERR_INVALID_ARG (-1) with a message, and every error code has a name."""
+    from pylith_b200 import _lib
+
+    P = ctypes.c_void_p
+    null = P(0)
+    out = P()
+    assert L.pl_context_create(0, None) == -1
+    assert L.pl_mesh_create(null, 0, 10, None, 5, None, ctypes.byref(out)) == -1
+    assert L.pl_integrator_domain_create(null, 0, None, ctypes.byref(out)) == -1
+    assert L.pl_integrator_set_scatter(null, 0) == -1
+    assert L.pl_integrator_set_aux(null, b"shear_modulus", 0, 1, None) == -1
+    assert L.pl_integrator_set_kernels_derived_field(null, None, 0) == -1
+    assert L.pl_compute_lhs_residual(null, 0.0, 0.0, None, None, None, 0) == -1
+    assert L.pl_compute_lhs_jacobian_action(null, 0.0, 0.0, 0.0, None, None, None, 0) == -1
+    assert L.pl_compute_lhs_residual_host(null, 0.0, 0.0, None, None) == -1
+    assert L.pl_compute_lhs_residual_host_noalloc(null, 0.0, 0.0, None, None) == -1
+    assert L.pl_compute_derived_field(null, 0.0, 0.0, None, None) == -1
+    assert L.pl_solver_solve(null, None, None) == -1
+    assert L.pl_batch_solver_create(null, 3, ctypes.byref(out)) == -1
+    assert L.pl_last_error()
+    for code, name in _lib.ERRORS.items():
+        assert L.pl_error_string(code) not in (None, b"unknown error"), name
+    assert L.pl_error_string(0) == b"ok"
+    # destroying nothing is a no-op
+    assert L.pl_integrator_destroy(null) == 0
+    assert L.pl_matrix_destroy(null) == 0
