@@ -90,7 +90,7 @@ def test_elastic_residual_matches_oracle(oracle_lib, torch_cuda, ctx, kind, scat
     assert rel_l2(dr.cpu().numpy(), 2 * r_ref) <= TOL64
 
 
-@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+@pytest.mark.parametrize("kind", ["tet4", "hex8", "hex27"])
 def test_body_force_residual(oracle_lib, torch_cuda, ctx, kind):
     from pylith_b200 import feassemble as FA
 
@@ -161,7 +161,7 @@ def genmaxwell_oracle_aux(O, g):
                         (g.shear_modulus_ratio, "cell"), (g.viscous_strain, "qp"), (g.total_strain, "qp")])
 
 
-@pytest.mark.parametrize("kind", ["hex8", "tet4"])
+@pytest.mark.parametrize("kind", ["hex8", "tet4", "hex27"])
 def test_genmaxwell_residual_jacobian_and_state_update(oracle_lib, torch_cuda, ctx, kind):
     from pylith_b200 import feassemble as FA
 
@@ -395,7 +395,7 @@ def test_derived_genmaxwell_stress(oracle_lib, torch_cuda, ctx):
     assert e.value.code == -7
 
 
-@pytest.mark.parametrize("kind", ["tet4", "hex8"])
+@pytest.mark.parametrize("kind", ["tet4", "hex8", "hex27"])
 def test_two_materials_on_cell_subsets(oracle_lib, torch_cuda, ctx, kind):
     """Two materials on complementary cell subsets (one IntegratorDomain per material label,
     IntegratorDomain.cc:422-453) summed into one residual and one Jacobian action; an integrator
