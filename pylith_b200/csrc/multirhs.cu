@@ -94,30 +94,65 @@ PL_D void red_vec(float* p, const float (&v)[W]) {
 
 // v, out: [ndof][K] FP32 (ndof = 3 * nodes, node-major); out must be zeroed or hold the sum to add to.
 // Per cell block: the block's node coordinates (FP64, [3][ld]) and K field vectors (FP32, one row
-// of 3K values per node, as in global memory) are staged in shared memory. One thread per cell
+// of 3K values per node, as in global memory) are staged in shared memory with the block's node ids
+// and incidence list, all copied asynchronously one block ahead. One thread per cell
 // forms the geometry and the isotropic tangent once and then, KC right-hand sides at a time (one
 // vector load per node and component), the element vectors, staged as [12][cells][KC]; then one
 // work item per (node, component) sums its incident corners over the block-local incidence list
 // in a fixed order, KC right-hand sides per vector, and adds the node into the output (one vector
 // reduction when the node is shared with other blocks).
-// Asynchronous copies of block b's node rows (K field values per component) and coordinates
-// into shared memory.
+
+// Block metadata in shared memory (two buffers: the gather reads one while the next block's is
+// copied into the other): node ids [ld], incidence offsets [ld + 1], incidence list
+// [4 * cells] (cell * 4 + corner).
+struct MultiMeta {
+    uint32_t* id;
+    uint32_t* off;
+    uint16_t* inc;
+};
+
+PL_HD size_t multi_r16(size_t x) { return (x + 15) & ~size_t(15); }
+
+PL_HD size_t multi_meta_bytes(int ld) {
+    return multi_r16(4 * (size_t)ld) + multi_r16(4 * ((size_t)ld + 1)) + (size_t)2 * 4 * kMultiBlockCells;
+}
+
+PL_D MultiMeta multi_meta(char* base, int ld) {
+    MultiMeta m;
+    m.id = reinterpret_cast<uint32_t*>(base);
+    base += multi_r16(4 * (size_t)ld);
+    m.off = reinterpret_cast<uint32_t*>(base);
+    base += multi_r16(4 * ((size_t)ld + 1));
+    m.inc = reinterpret_cast<uint16_t*>(base);
+    return m;
+}
+
+// Asynchronous copies of block b's node rows (K field values per component), coordinates and
+// metadata into shared memory.
 template <int K>
 PL_D void prefetch_multi(const DomainParams& p, const int32_t* __restrict__ slot_begin,
-                         const uint32_t* __restrict__ slot_node, int64_t b, int ld, const float* __restrict__ v,
-                         float* sV, double* sX) {
+                         const uint32_t* __restrict__ slot_node, const uint32_t* __restrict__ inc_off,
+                         const uint16_t* __restrict__ inc, int64_t b, int ld, const float* __restrict__ v,
+                         float* sV, double* sX, const MultiMeta& mm) {
     constexpr int CB = K % 4 == 0 ? 16 : (K % 2 == 0 ? 8 : 4);  // bytes per copy; rows are 12 K bytes
     const int s0 = slot_begin[b];
     const int ns = slot_begin[b + 1] - s0;
     for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-        const int64_t nd = slot_node[s0 + i] & ~kSharedBitM;
+        const uint32_t id = slot_node[s0 + i];
+        const int64_t nd = id & ~kSharedBitM;
 #pragma unroll
         for (int d = 0; d < 3; ++d) __pipeline_memcpy_async(&sX[d * ld + i], &p.coords[3 * nd + d], sizeof(double));
         const float* vr = v + 3 * K * nd;
         float* sr = sV + 3 * K * i;
 #pragma unroll
         for (int j = 0; j < 3 * K; j += CB / 4) __pipeline_memcpy_async(sr + j, vr + j, CB);
+        mm.id[i] = id;
     }
+    for (int i = threadIdx.x; i <= ns; i += blockDim.x)
+        __pipeline_memcpy_async(&mm.off[i], &inc_off[s0 + b + i], sizeof(uint32_t));
+    // 4 * kMultiBlockCells uint16 = kMultiBlockCells / 2 chunks of 16 bytes
+    for (int i = threadIdx.x; i < kMultiBlockCells / 2; i += blockDim.x)
+        __pipeline_memcpy_async(&mm.inc[8 * i], &inc[b * 4 * kMultiBlockCells + 8 * i], 16);
 }
 
 // store_owned: nodes owned by one block are stored (the output was zeroed and this is the first
@@ -134,25 +169,45 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     float* sE = reinterpret_cast<float*>(smem_raw);                                              // [12][cells][KC]
     float* sV = sE + 12 * kMultiBlockCells * KC;                                                 // [ld][3K]
     // [3][ld], at a 16-byte boundary after sV
-    double* sX = reinterpret_cast<double*>(reinterpret_cast<char*>(sV) + ((size_t)ld * 3 * K * sizeof(float) + 15) / 16 * 16);
+    double* sX = reinterpret_cast<double*>(reinterpret_cast<char*>(sV) + multi_r16((size_t)ld * 3 * K * sizeof(float)));
+    // two metadata buffers after sX
+    char* metabase = reinterpret_cast<char*>(sX) + multi_r16((size_t)ld * 3 * sizeof(double));
+    const size_t mb = multi_meta_bytes(ld);
+    int cur = 0;
     const int tc = threadIdx.x;
-    if (blockIdx.x < nblocks) prefetch_multi<K>(p, slot_begin, slot_node, blockIdx.x, ld, v, sV, sX);
+    if (blockIdx.x < nblocks)
+        prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, blockIdx.x, ld, v, sV, sX, multi_meta(metabase, ld));
     __pipeline_commit();
     for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
-        const int s0 = slot_begin[b];
-        const int ns = slot_begin[b + 1] - s0;
-        __pipeline_wait_prior(0);
-        __syncthreads();
+        const int ns = slot_begin[b + 1] - slot_begin[b];
         const int64_t c = b * kMultiBlockCells + tc;
         const bool live = c < p.ncells;
         int ln[4] = {0, 0, 0, 0};
         float inv[3][3], cf[3][3], lam = 0.f, mu = 0.f;
+        // per-cell inputs from global memory first: their latency overlaps the staging copies
         if (live) {
             const ushort4 lc = lconn[c];
             ln[0] = lc.x;
             ln[1] = lc.y;
             ln[2] = lc.z;
             ln[3] = lc.w;
+            // The registered tangent (Jf3vu_infinitesimalStrain) is isotropic: Jf3 = -C with
+            // C = lambda d_ij d_kl + mu (d_ik d_jl + d_il d_jk); its (f,g,df,dg) = (0,1,0,1) and
+            // (0,1,1,0) entries are -lambda and -mu.
+            double a[L::size];
+            L::load_cell(p, c, a);
+            double x[3] = {0, 0, 0};
+            double Jf3d[81];
+#pragma unroll
+            for (int i = 0; i < 81; ++i) Jf3d[i] = 0.0;
+            call_jf3<RHEO_ILE>(L::numA, aoff.v, a, p, x, Jf3d);
+            lam = (float)(-Jf3d[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
+            mu = (float)(-Jf3d[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
+        }
+        __pipeline_wait_prior(0);
+        __syncthreads();
+        const MultiMeta mm = multi_meta(metabase + cur * mb, ld);
+        if (live) {
             double X[4][3];
 #pragma unroll
             for (int k = 0; k < 4; ++k)
@@ -169,20 +224,7 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                     inv[i][j] = (float)(cof[i][j] * rdet);
                     cf[i][j] = (float)(cof[i][j] * (1.0 / 6.0));
                 }
-            // The registered tangent (Jf3vu_infinitesimalStrain) is isotropic: Jf3 = -C with
-            // C = lambda d_ij d_kl + mu (d_ik d_jl + d_il d_jk); its (f,g,df,dg) = (0,1,0,1) and
-            // (0,1,1,0) entries are -lambda and -mu.
-            double a[L::size];
-            L::load_cell(p, c, a);
-            double x[3] = {0, 0, 0};
-            double Jf3d[81];
-#pragma unroll
-            for (int i = 0; i < 81; ++i) Jf3d[i] = 0.0;
-            call_jf3<RHEO_ILE>(L::numA, aoff.v, a, p, x, Jf3d);
-            lam = (float)(-Jf3d[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
-            mu = (float)(-Jf3d[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
         }
-        const uint16_t* lst = inc + b * 4 * kMultiBlockCells;
 #pragma unroll 1
         for (int r0 = 0; r0 < K; r0 += KC) {
             if (live) {
@@ -237,25 +279,26 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
             __syncthreads();
             // the node rows are no longer read in this block: copy the next block's while gathering
             if (r0 + KC >= K && b + gridDim.x < nblocks)
-                prefetch_multi<K>(p, slot_begin, slot_node, b + gridDim.x, ld, v, sV, sX);
+                prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, b + gridDim.x, ld, v, sV, sX,
+                                  multi_meta(metabase + (cur ^ 1) * mb, ld));
             __pipeline_commit();
             // one work item per (node, component): consecutive threads take consecutive nodes
             for (int w = tc; w < ns * 3; w += blockDim.x) {
                 const int cc = w / ns, i = w - cc * ns;
-                const int j0 = inc_off[s0 + b + i], j1 = inc_off[s0 + b + i + 1];
+                const int j0 = mm.off[i], j1 = mm.off[i + 1];
                 float acc[KC];
 #pragma unroll
                 for (int rr = 0; rr < KC; ++rr) acc[rr] = 0.f;
 #pragma unroll 4
                 for (int j = j0; j < j1; ++j) {
-                    const int e = lst[j];
+                    const int e = mm.inc[j];
                     const int cell = e >> 2, corner = e & 3;
                     float t[KC];
                     ld_vec<KC>(sE + ((corner * 3 + cc) * kMultiBlockCells + cell) * KC, t);
 #pragma unroll
                     for (int rr = 0; rr < KC; ++rr) acc[rr] += t[rr];
                 }
-                const uint32_t id = slot_node[s0 + i];
+                const uint32_t id = mm.id[i];
                 float* o = out + 3 * K * (int64_t)(id & ~kSharedBitM) + cc * K + r0;
                 if (id & kSharedBitM) {
                     red_vec<KC>(o, acc);
@@ -271,6 +314,7 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
             }
             __syncthreads();
         }
+        cur ^= 1;
     }
     __pipeline_wait_prior(0);
 }
@@ -278,7 +322,8 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 template <int K>
 size_t multi_smem(int ld) {
     return (size_t)12 * MultiChunk<K>::value * kMultiBlockCells * sizeof(float) +
-           ((size_t)ld * 3 * K * sizeof(float) + 15) / 16 * 16 + (size_t)ld * 3 * sizeof(double);
+           multi_r16((size_t)ld * 3 * K * sizeof(float)) + multi_r16((size_t)ld * 3 * sizeof(double)) +
+           2 * multi_meta_bytes(ld);
 }
 
 // ---- batched vector kernels, layout [n][K] -------------------------------------------------
