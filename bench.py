@@ -126,14 +126,40 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(mesh):
-    """DRAM bytes per residual launch from the committed ncu summary, scaled to this mesh."""
+def _profile_summary():
     path = os.path.join(ROOT, "profiles", "tet4_residual_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
-        d = json.load(f)
-    return float(d["dram_bytes_per_cell"]) * mesh.num_cells
+        return json.load(f)
+
+
+def profiled_traffic(mesh):
+    """DRAM bytes per residual launch from the committed ncu summary, scaled to this mesh."""
+    d = _profile_summary()
+    return None if d is None else float(d["dram_bytes_per_cell"]) * mesh.num_cells
+
+
+def issue_limiter(mesh, seconds_per_launch, sm_mhz):
+    """What bounds the residual kernel below the HBM roofline: the instruction-issue and FP64
+    floors from the committed ncu warp-instruction counts (per cell, scaled to this mesh), at the
+    clock sampled during the timed region. One warp-instruction per scheduler per cycle (4 per
+    SM); an FP64 warp-instruction holds a scheduler's FP64 pipe for 2 cycles (64 FP64 lanes per
+    SM)."""
+    d = _profile_summary()
+    if d is None or "warp_instructions_per_cell" not in d:
+        return None
+    import torch
+
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    slots = 4 * sms * (sm_mhz or 1965.0) * 1e6
+    t_issue = float(d["warp_instructions_per_cell"]) * mesh.num_cells / slots
+    t_fp64 = 2.0 * float(d["fp64_warp_instructions_per_cell"]) * mesh.num_cells / slots
+    return {"kind": "instruction issue and latency (FP64 arithmetic, shared-memory gather), not HBM",
+            "issue_floor_us": t_issue * 1e6, "issue_frac": t_issue / seconds_per_launch,
+            "fp64_floor_us": t_fp64 * 1e6, "fp64_frac": t_fp64 / seconds_per_launch,
+            "warp_instructions_per_cell": d["warp_instructions_per_cell"],
+            "source": "ncu warp-instruction counts of the same kernel (profiles/tet4_residual_traffic.json)"}
 
 
 def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
@@ -386,6 +412,9 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
         }
+        lim = issue_limiter(mesh, t_res / args.steps, line["clocks"].get("sm_mhz"))
+        if lim is not None:
+            line["roofline"]["limiter"] = lim
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(mesh, mat, "oracle")
         print(json.dumps(line), flush=True)
