@@ -333,6 +333,17 @@ typedef struct pl_batch_solver_s* pl_batch_solver;
 int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out);
 int pl_batch_solver_solve(pl_batch_solver solver, int nrhs, const double* const* b_dev,
                           double* const* x_dev);
+/* Preconditioner of the FP32 tile PCG. degree 0 or 1: point-block Jacobi (the default). degree
+ * 2-8: Chebyshev-Jacobi, the Chebyshev iteration of that degree for A z = r from z = 0 with the
+ * point-block Jacobi inverse P (degree - 1 operator applications per PCG iteration), on the
+ * interval [lower_ratio b, b] with b = 1.1 lambda_max(P A); lambda_max is estimated by eig_iters
+ * power iterations at the next solve (and again after the integrators change). The reference
+ * smooths the fine level of its algebraic multigrid with the same kind of iteration: PETSc GAMG
+ * (-pc_type gamg, -mg_fine_ksp_max_it 5, -mg_fine_pc_type vpbjacobi with faults;
+ * libsrc/pylith/materials/Elasticity.cc:310-317), whose level smoother is PETSc's Chebyshev
+ * iteration with bounds 0.1 and 1.1 times an estimated largest eigenvalue. */
+int pl_batch_solver_set_chebyshev(pl_batch_solver solver, int degree, double lower_ratio, int eig_iters);
+int pl_batch_solver_get_chebyshev(pl_batch_solver solver, double* lambda_max);
 int pl_batch_solver_get_stats(pl_batch_solver solver, int64_t* solves, int64_t* inner_iterations,
                               int64_t* outer_iterations, double* max_rel_residual);
 int pl_batch_solver_destroy(pl_batch_solver solver);

@@ -120,6 +120,8 @@ SIGNATURES = {
     "pl_batch_solver_get_stats": (_I, [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64),
                                        ctypes.POINTER(_D)]),
     "pl_batch_solver_destroy": (_I, [_P]),
+    "pl_batch_solver_set_chebyshev": (_I, [_P, _I, _D, _I]),
+    "pl_batch_solver_get_chebyshev": (_I, [_P, ctypes.POINTER(_D)]),
 }
 PL_SOLVER_FP64, PL_SOLVER_FP32_REFINED = 0, 1
 

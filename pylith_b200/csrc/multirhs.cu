@@ -484,6 +484,137 @@ __global__ void k_b_pupdate(float* p, const float* z, int64_t n, const double* r
         p[e] = z[e] + beta * p[e];
 }
 
+// ---- Chebyshev-Jacobi preconditioner: z = q(P A) P r, with A = -J and the point-block
+// Jacobi inverse P; Chebyshev iteration of a given degree for A z = r from z = 0 (Saad,
+// "Iterative Methods for Sparse Linear Systems", 2nd ed., Algorithm 12.1), so the preconditioner is a
+// fixed polynomial, symmetric and positive definite while the eigenvalues of P A lie below the
+// upper bound. ----
+
+PL_D void pinv_local(const float* __restrict__ P, int64_t node, const float in[3], float out[3]) {
+    const float* B = P + 9 * node;
+    out[0] = B[0] * in[0] + B[1] * in[1] + B[2] * in[2];
+    out[1] = B[3] * in[0] + B[4] * in[1] + B[5] * in[2];
+    out[2] = B[6] * in[0] + B[7] * in[1] + B[8] * in[2];
+}
+
+// x += alpha p; r += alpha q on free DOFs; partial r.r (the preconditioner runs after).
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* x, float* r, const float* p, const float* q,
+                                                           const uint8_t* mask, int64_t n, const double* rz,
+                                                           const double* pq, const int* active, double* part_rr) {
+    const int k = threadIdx.x % K;
+    const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
+    double srr = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
+        if (mask[e / K]) continue;
+        x[e] += alpha * p[e];
+        const float ri = r[e] + alpha * q[e];
+        r[e] = ri;
+        srr += (double)ri * ri;
+    }
+    block_sum_by_rhs<K>(srr, part_rr);
+}
+
+// First Chebyshev step: d = s P r, z = d (constrained DOFs zero). One thread per (node, rhs).
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_cheb_first(const float* r, float* d, float* z, const uint8_t* mask,
+                                                          const float* P, int64_t nnodes, float s) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        const int k = (int)(t % K);
+        float zz[3];
+        pinv_apply<K>(P, r, nd, k, zz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const float v = mask[3 * nd + c] ? 0.0f : s * zz[c];
+            d[i] = v;
+            z[i] = v;
+        }
+    }
+}
+
+// Later steps: res = src + q (= src - A d; src is r for the first of them, res after), then
+// d = c1 d + c2 P res, z += d, all on free DOFs; the last step also sums r.z per right-hand side.
+template <int K, bool LAST>
+__global__ void __launch_bounds__(kBThreads) k_cheb_step(const float* src, const float* q, float* res, float* d,
+                                                         float* z, const float* r, const uint8_t* mask, const float* P,
+                                                         int64_t nnodes, float c1, float c2, double* part_rz) {
+    double srz = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        const int k = (int)(t % K);
+        float rs[3], pr[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            rs[c] = mask[3 * nd + c] ? 0.0f : src[i] + q[i];
+            res[i] = rs[c];
+        }
+        pinv_local(P, nd, rs, pr);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const bool m = mask[3 * nd + c];
+            const float dv = m ? 0.0f : c1 * d[i] + c2 * pr[c];
+            const float zv = m ? 0.0f : z[i] + dv;
+            d[i] = dv;
+            z[i] = zv;
+            if (LAST) srz += (double)r[i] * zv;
+        }
+    }
+    if (LAST) block_sum_by_rhs<K>(srz, part_rz);
+}
+
+// Power iteration for the largest eigenvalue of P A: w = -P (J v) on free DOFs, partial |w|^2
+// and |v|^2 per right-hand side.
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_power_step(const float* v, const float* q, float* w, const uint8_t* mask,
+                                                          const float* P, int64_t nnodes, double* part_ww,
+                                                          double* part_vv) {
+    double sww = 0.0, svv = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        const int k = (int)(t % K);
+        float zz[3];
+        pinv_apply<K>(P, q, nd, k, zz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const bool m = mask[3 * nd + c];
+            const float wi = m ? 0.0f : -zz[c];
+            w[i] = wi;
+            sww += (double)wi * wi;
+            if (!m) svv += (double)v[i] * v[i];
+        }
+    }
+    block_sum_by_rhs<K>(sww, part_ww);
+    __syncthreads();
+    block_sum_by_rhs<K>(svv, part_vv);
+}
+
+// v = s_k w (per right-hand side), or a deterministic pseudo-random start when w is null.
+struct ColScale {
+    float s[8];
+};
+template <int K>
+__global__ void k_power_scale(float* v, const float* w, const uint8_t* mask, int64_t n, ColScale cs) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(e % K);
+        float val;
+        if (w) {
+            val = cs.s[k] * w[e];
+        } else {
+            uint32_t h = (uint32_t)(e * 2654435761ull) ^ 0x9e3779b9u;
+            h ^= h >> 15;
+            h *= 0x85ebca6bu;
+            h ^= h >> 13;
+            val = (float)(h & 0xffffff) / 16777216.0f - 0.5f;
+        }
+        v[e] = mask[e / K] ? 0.0f : val;
+    }
+}
+
 // fault unfold / fold on [n][K]
 template <int K>
 __global__ void k_b_unfold(float* v, const int32_t* neg, const int32_t* pos, int64_t npairs) {
@@ -531,6 +662,17 @@ struct pl_batch_solver_s {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     unsigned long long graph_epoch = 0;
+    int graph_cheb = -1;      // cheb_version the graph was captured with
+    // Chebyshev-Jacobi preconditioner (degree >= 2; 0 or 1: point-block Jacobi)
+    int cheb_degree = 0;
+    double cheb_lower_ratio = 0.05;
+    int cheb_eig_iters = 20;
+    double cheb_lmax = 0.0;   // estimated largest eigenvalue of P A (before the safety factor)
+    int cheb_version = 0;     // bumped when the coefficients change
+    unsigned long long cheb_epoch = 0;  // state epoch of the estimate
+    float cheb_s0 = 0.0f;
+    float cheb_c1[8] = {}, cheb_c2[8] = {};
+    float *res = nullptr, *d = nullptr;
     // The solve runs on a private stream (graph capture is not possible on the legacy default
     // stream a caller may use), fenced against the caller's stream with events.
     cudaStream_t stream = nullptr;
@@ -538,6 +680,10 @@ struct pl_batch_solver_s {
     int64_t solves = 0, inner_iterations = 0, outer_iterations = 0;
     double max_rel_residual = 0.0;
 };
+
+namespace plb {
+constexpr int kMaxChebDegree = 8;
+}
 
 namespace {
 
@@ -588,6 +734,30 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
     return PL_OK;
 }
 
+// z = q(P A) P r with the Chebyshev coefficients of the solver; partial r.z into part_a.
+template <int K>
+int cheb_apply(pl_batch_solver B) {
+    pl_solver S = B->base;
+    cudaStream_t s = S->mesh->ctx->stream;
+    k_cheb_first<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->d, B->z, S->d_mask, S->d_pinv32, B->nnodes, B->cheb_s0);
+    count_launch();
+    for (int i = 1; i < B->cheb_degree; ++i) {
+        int rc = jv32_multi<K>(B, B->d, B->q);
+        if (rc) return rc;
+        const float* src = i == 1 ? B->r : B->res;
+        if (i == B->cheb_degree - 1)
+            k_cheb_step<K, true><<<kBBlocks, kBThreads, 0, s>>>(src, B->q, B->res, B->d, B->z, B->r, S->d_mask,
+                                                                S->d_pinv32, B->nnodes, B->cheb_c1[i], B->cheb_c2[i],
+                                                                B->part_a);
+        else
+            k_cheb_step<K, false><<<kBBlocks, kBThreads, 0, s>>>(src, B->q, B->res, B->d, B->z, B->r, S->d_mask,
+                                                                 S->d_pinv32, B->nnodes, B->cheb_c1[i], B->cheb_c2[i],
+                                                                 nullptr);
+        count_launch();
+    }
+    return PL_OK;
+}
+
 // One PCG iteration for all K vectors of the tile (capturable: kernels and memsets only).
 template <int K>
 int pcg_iteration(pl_batch_solver B) {
@@ -601,12 +771,69 @@ int pcg_iteration(pl_batch_solver B) {
     if (rc) return rc;
     k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a);
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, pq, nullptr);
-    k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes, rz, pq,
-                                                 B->active, B->part_a, B->part_b);
+    if (B->cheb_degree >= 2) {
+        k_b_update_xr<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, S->d_mask, B->n, rz, pq, B->active,
+                                                        B->part_b);
+        count_launch();
+        rc = cheb_apply<K>(B);
+        if (rc) return rc;
+    } else {
+        k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes,
+                                                     rz, pq, B->active, B->part_a, B->part_b);
+        count_launch();
+    }
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, rz, rz_old);
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, rr, nullptr);
     k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->z, B->n, rz, rz_old, B->active);
-    count_launch(6);
+    count_launch(5);
+    return PL_OK;
+}
+
+// Largest eigenvalue of P A by power iteration on the tile's K vectors (deterministic start);
+// sets the Chebyshev coefficients for the interval [lower_ratio b, b], b = 1.1 lambda_max.
+template <int K>
+int cheb_setup(pl_batch_solver B) {
+    pl_solver S = B->base;
+    cudaStream_t s = S->mesh->ctx->stream;
+    const int64_t n = B->n;
+    ColScale cs{};
+    k_power_scale<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, nullptr, S->d_mask, n, cs);
+    count_launch();
+    double lam = 0.0;
+    double h[16];
+    for (int it = 0; it < B->cheb_eig_iters; ++it) {
+        int rc = jv32_multi<K>(B, B->p, B->q);
+        if (rc) return rc;
+        k_power_step<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes, B->part_a,
+                                                       B->part_b);
+        k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+        k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, B->scal + K, nullptr);
+        count_launch(3);
+        PLB_CUDA(cudaMemcpyAsync(h, B->scal, 2 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PLB_CUDA(cudaStreamSynchronize(s));
+        lam = 0.0;
+        for (int k = 0; k < K; ++k) {
+            const double ww = h[k], vv = h[K + k];
+            if (vv > 0.0 && ww > 0.0) lam = std::max(lam, std::sqrt(ww / vv));
+            cs.s[k] = ww > 0.0 ? (float)(1.0 / std::sqrt(ww)) : 0.0f;
+        }
+        if (!(lam > 0.0) || !std::isfinite(lam)) return fail(PL_ERR_NOT_CONVERGED, "eigenvalue estimate failed");
+        k_power_scale<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->z, S->d_mask, n, cs);
+        count_launch();
+    }
+    B->cheb_lmax = lam;
+    const double b = 1.1 * lam, a = B->cheb_lower_ratio * b;
+    const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    B->cheb_s0 = (float)(1.0 / theta);
+    for (int i = 1; i < B->cheb_degree; ++i) {
+        const double rho_new = 1.0 / (2.0 * sigma - rho);
+        B->cheb_c1[i] = (float)(rho_new * rho);
+        B->cheb_c2[i] = (float)(2.0 * rho_new / delta);
+        rho = rho_new;
+    }
+    B->cheb_version++;
+    B->cheb_epoch = state_epoch();
     return PL_OK;
 }
 
@@ -622,6 +849,14 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     count_launch(3);
     double h[4 * 8];
     int act[8];
+    if (B->cheb_degree >= 2) {
+        // z = q(P A) P r, p = z, rz = r.z
+        int rc = cheb_apply<K>(B);
+        if (rc) return rc;
+        k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+        count_launch();
+        PLB_CUDA(cudaMemcpyAsync(B->p, B->z, B->n * K * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
     PLB_CUDA(cudaMemcpyAsync(h, B->scal, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
     PLB_CUDA(cudaStreamSynchronize(s));
     double r0[8];
@@ -632,7 +867,7 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
     const int chunk = S->check_every;
     // capture `chunk` iterations once per tile size, replay between checks
-    if (!B->graph || B->graph_iters != chunk || B->graph_epoch != state_epoch()) {
+    if (!B->graph || B->graph_iters != chunk || B->graph_epoch != state_epoch() || B->graph_cheb != B->cheb_version) {
         if (B->graph) cudaGraphExecDestroy(B->graph);
         B->graph = nullptr;
         cudaGraph_t g;
@@ -647,6 +882,7 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
         if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
         B->graph_iters = chunk;
         B->graph_epoch = state_epoch();
+        B->graph_cheb = B->cheb_version;
     }
     *iters = 0;
     for (int it = 0; it < max_iter; it += chunk) {
@@ -812,6 +1048,14 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
     PLB_CUDA(cudaStreamWaitEvent(B->stream, B->ev_in, 0));
     c->stream = B->stream;
     int rc = PL_OK;
+    if (nrhs > 0 && B->cheb_degree >= 2 && (B->cheb_version == 0 || B->cheb_epoch != state_epoch())) {
+        switch (B->K) {
+            case 1: rc = cheb_setup<1>(B); break;
+            case 2: rc = cheb_setup<2>(B); break;
+            case 4: rc = cheb_setup<4>(B); break;
+            default: rc = cheb_setup<8>(B); break;
+        }
+    }
     for (int r0 = 0; r0 < nrhs && rc == PL_OK; r0 += B->K) {
         const int nact = std::min(B->K, nrhs - r0);
         switch (B->K) {
@@ -826,6 +1070,36 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
     cudaEventRecord(B->ev_out, B->stream);
     cudaStreamWaitEvent(user, B->ev_out, 0);
     return rc;
+}
+
+int pl_batch_solver_set_chebyshev(pl_batch_solver B, int degree, double lower_ratio, int eig_iters) {
+    if (!B || degree < 0 || degree > kMaxChebDegree || !(lower_ratio > 0.0 && lower_ratio < 1.0) || eig_iters < 1 ||
+        eig_iters > 1000)
+        return fail(PL_ERR_INVALID_ARG, "degree 0-8, lower_ratio in (0, 1), eig_iters 1-1000");
+    PLB_CUDA(cudaSetDevice(B->base->mesh->ctx->device));
+    if (degree >= 2 && !B->res) {
+        const size_t nk = (size_t)B->n * B->K;
+        PLB_CUDA(cudaMalloc((void**)&B->res, nk * sizeof(float)));
+        cudaError_t e = cudaMalloc((void**)&B->d, nk * sizeof(float));
+        if (e != cudaSuccess) {
+            cudaFree(B->res);
+            B->res = nullptr;
+            return cuda_fail(e, "pl_batch_solver_set_chebyshev");
+        }
+    }
+    B->cheb_degree = degree;
+    B->cheb_lower_ratio = lower_ratio;
+    B->cheb_eig_iters = eig_iters;
+    B->cheb_version = 0;  // estimate again at the next solve
+    B->cheb_lmax = 0.0;
+    B->graph_cheb = -1;
+    return PL_OK;
+}
+
+int pl_batch_solver_get_chebyshev(pl_batch_solver B, double* lambda_max) {
+    if (!B || !lambda_max) return fail(PL_ERR_INVALID_ARG, "bad arguments");
+    *lambda_max = B->cheb_lmax;
+    return PL_OK;
 }
 
 int pl_batch_solver_get_stats(pl_batch_solver B, int64_t* solves, int64_t* inner_iterations, int64_t* outer_iterations,
@@ -848,7 +1122,7 @@ int pl_batch_solver_destroy(pl_batch_solver B) {
     if (B->ev_in) cudaEventDestroy(B->ev_in);
     if (B->ev_out) cudaEventDestroy(B->ev_out);
     if (B->stream) cudaStreamDestroy(B->stream);
-    void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64};
+    void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64, B->res, B->d};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete B;

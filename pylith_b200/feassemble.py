@@ -370,6 +370,8 @@ class BatchSolver:
 
     def __init__(self, solver: Solver, tile: int = 8):
         self.solver = solver
+        self.tile = tile
+        self.degree = 0
         self.handle = ctypes.c_void_p()
         check(C.lib().pl_batch_solver_create(solver.handle, tile, ctypes.byref(self.handle)))
 
@@ -378,6 +380,19 @@ class BatchSolver:
         pb = (ctypes.c_void_p * max(n, 1))(*[_ptr(b) for b in bs])
         px = (ctypes.c_void_p * max(n, 1))(*[_ptr(x) for x in xs])
         check(C.lib().pl_batch_solver_solve(self.handle, n, pb, px))
+
+    def set_chebyshev(self, degree: int, lower_ratio: float = 0.05, eig_iters: int = 20) -> None:
+        """Preconditioner of the FP32 tile PCG: degree 0 or 1 point-block Jacobi, 2-8 Chebyshev-
+        Jacobi on [lower_ratio b, b], b = 1.1 lambda_max(P A), estimated at the next solve."""
+        check(C.lib().pl_batch_solver_set_chebyshev(self.handle, int(degree), float(lower_ratio), int(eig_iters)))
+        self.degree = int(degree)
+
+    @property
+    def lambda_max(self) -> float:
+        """The power-iteration estimate of lambda_max(P A) (0 before the first Chebyshev solve)."""
+        v = ctypes.c_double()
+        check(C.lib().pl_batch_solver_get_chebyshev(self.handle, ctypes.byref(v)))
+        return v.value
 
     def stats(self):
         s, i, o, r = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()

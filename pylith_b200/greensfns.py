@@ -46,7 +46,8 @@ class Impulse:
 
 class GreensFunctions:
     def __init__(self, ctx, mesh, material, constrained, patches, components=("left_lateral", "reverse"),
-                 rtol=1e-10, inner_rtol=1e-4, tile=8, ref_dir_1=(0.0, 0.0, 1.0), ref_dir_2=(0.0, 1.0, 0.0)):
+                 rtol=1e-10, inner_rtol=1e-4, tile=8, ref_dir_1=(0.0, 0.0, 1.0), ref_dir_2=(0.0, 1.0, 0.0),
+                 cheb_degree=0, cheb_lower_ratio=0.05):
         from . import materials as MAT
 
         self.ctx = ctx
@@ -64,6 +65,9 @@ class GreensFunctions:
                                   precision=FA.Solver.FP32_REFINED, inner_rtol=inner_rtol)
         self.solver32.setup()
         self.batch = FA.BatchSolver(self.solver32, tile)
+        self.cheb_lower_ratio = cheb_lower_ratio
+        if cheb_degree >= 2:
+            self.batch.set_chebyshev(cheb_degree, cheb_lower_ratio)
 
     def impulse_rhs(self, imp: Impulse):
         """(u_slip, b): the displacement carrying unit slip on the patch, and b = F(u_slip)."""
@@ -77,6 +81,39 @@ class GreensFunctions:
         b = torch.zeros_like(u)
         self.domain.compute_lhs_residual(0.0, 0.0, u, b)
         return u, b
+
+    def autotune(self, impulses, tiles=(4, 8), degrees=(0, 2, 3, 4)):
+        """Picks the tile size and the preconditioner degree (0: point-block Jacobi, >= 2:
+        Chebyshev-Jacobi) with the highest batched solves/s on `impulses` (a sample of the
+        impulses to be solved; each configuration solves them once to warm up and once timed)
+        and keeps that batched solver. Returns [(tile, degree, solves_per_s)], best first."""
+        rhs = [self.impulse_rhs(imp)[1] for imp in impulses]
+        import torch
+
+        results = []
+        best = None
+        for tile in tiles:
+            for degree in degrees:
+                bs = FA.BatchSolver(self.solver32, tile)
+                if degree >= 2:
+                    bs.set_chebyshev(degree, self.cheb_lower_ratio)
+                xs = [torch.zeros_like(b) for b in rhs]
+                bs.solve(rhs[:tile], xs[:tile])  # graph capture and eigenvalue estimate
+                self.ctx.synchronize()
+                t0 = time.perf_counter()
+                bs.solve(rhs, xs)
+                self.ctx.synchronize()
+                rate = len(rhs) / (time.perf_counter() - t0)
+                results.append((tile, degree, rate))
+                if best is None or rate > best[2]:
+                    if best is not None:
+                        best[3].close()
+                    best = (tile, degree, rate, bs)
+                else:
+                    bs.close()
+        self.batch.close()
+        self.batch = best[3]
+        return sorted(results, key=lambda r: -r[2])
 
     def solve(self, impulses, batched=True):
         """Solutions u = u_slip + du of the given impulses; returns (solutions, seconds)."""

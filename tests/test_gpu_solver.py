@@ -306,3 +306,87 @@ def test_batched_green_functions_match_single_fp64_solves(ctx):
             assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
         st = g.batch.stats()
         assert st["solves"] == len(imps) and st["inner_iterations"] > 0
+
+
+def test_batched_chebyshev_jacobi_eigen_estimate_and_solutions(ctx, oracle_lib):
+    """Chebyshev-Jacobi preconditioning of the batched FP32 PCG on a Kuhn tetrahedral mesh: the
+    power-iteration estimate of lambda_max(P A) lies within [0.85, 1.0001] of the largest
+    generalized eigenvalue of the oracle-assembled stiffness against its 3x3 node blocks
+    (scipy), the solutions match one-at-a-time FP64 solves to <= 1e-8, and degree 3 needs fewer
+    inner iterations than point-block Jacobi."""
+    import scipy.linalg as sla
+    import torch
+    from pylith_b200 import feassemble as FA
+
+    O = oracle_lib
+    mesh = M.box_tet_kuhn(8, 6, 5, seed=3)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=5)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg")] = True
+    cons[M.boundary_mask(mesh, 0, "pos")] = True
+    cons[M.boundary_mask(mesh, 2, "neg"), 2] = True
+    cons = cons.ravel()
+    aux = O.AuxFields([(rho[:, None], "cell"), (mu[:, None], "cell"), (K[:, None], "cell")])
+    J = O.assemble(mesh, O.jacobian_elements(mesh, aux, g3="IsotropicLinearElasticity3D::Jf3vu_infinitesimalStrain"))
+    A = -J.toarray()
+    free = ~cons
+    D = np.zeros_like(A)
+    for nd in range(mesh.num_nodes):
+        s = slice(3 * nd, 3 * nd + 3)
+        D[s, s] = A[s, s]
+    lam_true = sla.eigh(A[free][:, free], D[free][:, free], eigvals_only=True)[-1]
+
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm)
+    S64 = FA.Solver(dm, cons, [ig], rtol=1e-11)
+    S64.setup()
+    S32 = FA.Solver(dm, cons, [ig], rtol=1e-11, precision=FA.Solver.FP32_REFINED, inner_rtol=1e-4)
+    S32.setup()
+    g = torch.Generator(device="cuda").manual_seed(11)
+    bs = [torch.randn(dm.num_dof, dtype=torch.float64, device="cuda", generator=g) * torch.from_numpy(free).cuda()
+          for _ in range(8)]
+    ref = []
+    for b in bs:
+        x = torch.zeros_like(b)
+        S64.solve(b, x)
+        ref.append(x.cpu().numpy())
+    iters = {}
+    for degree in (0, 3):
+        B = FA.BatchSolver(S32, 8)
+        B.set_chebyshev(degree, lower_ratio=0.05)
+        xs = [torch.zeros_like(b) for b in bs]
+        B.solve(bs, xs)
+        ctx.synchronize()
+        for a, r in zip(xs, ref):
+            assert np.linalg.norm(a.cpu().numpy() - r) <= 1e-8 * np.linalg.norm(r), degree
+        iters[degree] = B.stats()["inner_iterations"]
+        if degree == 3:
+            assert 0.85 * lam_true <= B.lambda_max <= 1.0001 * lam_true, (B.lambda_max, lam_true)
+        B.close()
+    assert iters[3] < iters[0], iters
+
+
+def test_green_functions_autotune_keeps_the_fastest_configuration(ctx):
+    """The tile/preconditioner autotuner times every (tile, degree) pair on a sample of impulses
+    and keeps the fastest batched solver, whose solutions still match FP64 solves to <= 1e-8."""
+    from pylith_b200 import greensfns as GF
+
+    mesh = M.box_tet_kuhn(8, 6, 5, fault_x=0.0, seed=3)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=5)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg")] = True
+    cons[M.boundary_mask(mesh, 0, "pos")] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    patches = GF.fault_patches(mesh, (-6000.0, 6000.0), (-9000.0, 0.0), 3, 2)
+    g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-11)
+    res = g.autotune(g.impulses[:8], tiles=(2, 4), degrees=(0, 3))
+    assert len(res) == 4 and res[0][2] >= res[-1][2]
+    assert (g.batch.tile, g.batch.degree) == res[0][:2]
+    imps = g.impulses[:6]
+    ref, _ = g.solve(imps, batched=False)
+    got, _ = g.solve(imps, batched=True)
+    for a, b in zip(got, ref):
+        a, b = a.cpu().numpy(), b.cpu().numpy()
+        assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
