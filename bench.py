@@ -639,9 +639,9 @@ def config_c3(args):
     step = max(1, len(usable) // nb)
     sample_b = usable[::step][:nb]
     # the autotuner picks the tile size and the preconditioner (point-block Jacobi or Chebyshev-
-    # Jacobi of degree 2-4) on a separate sample of 16 impulses
-    tune = usable[step // 2::step][:16]
-    table = g.autotune(tune, tiles=(4, 8), degrees=(0, 2, 3, 4))
+    # Jacobi of degree 2-3) on a separate sample of 32 impulses
+    tune = usable[step // 2::step][:32]
+    table = g.autotune(tune, tiles=(8, 16), degrees=(0, 2, 3))
     g.solve(sample_b[:8], batched=True)  # warm-up
     g.solve(sample_b[:1], batched=False)
     sol_b, t_b = g.solve(sample_b, batched=True)

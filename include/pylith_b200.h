@@ -325,7 +325,7 @@ int pl_solver_destroy(pl_solver solver);
 /* ---- batched right-hand sides (Green's functions; replaces the one-impulse-at-a-time
  *      SNES loop of libsrc/pylith/problems/GreensFns.cc:291-337) ------------------------------ */
 /* Solves A x_i = b_i for many right-hand sides with the operator, constraints, preconditioner and
- * tolerances of `base` (after pl_solver_setup). Tiles of `tile` (1, 2, 4 or 8) right-hand sides
+ * tolerances of `base` (after pl_solver_setup). Tiles of `tile` (1, 2, 4, 8 or 16) right-hand sides
  * share every launch of an FP32 PCG (FP64 dot products, CUDA-graph replay between convergence
  * checks) inside FP64 iterative refinement per right-hand side. b_dev/x_dev are arrays of nrhs
  * device pointers to full local vectors. P1 tetrahedra with isotropic linear elasticity. */

@@ -331,6 +331,7 @@ size_t multi_smem(int ld) {
 // consecutive threads to consecutive elements (thread index % K == right-hand side).
 constexpr int kBThreads = 256;
 constexpr int kBBlocks = 1184;
+constexpr int kMaxTile = 16;  // right-hand sides per tile: 1, 2, 4, 8 or 16
 
 // Per-block sums of one value per thread, by right-hand side (thread index % K), in a fixed
 // order -> partials[blk][K].
@@ -595,7 +596,7 @@ __global__ void __launch_bounds__(kBThreads) k_power_step(const float* v, const 
 
 // v = s_k w (per right-hand side), or a deterministic pseudo-random start when w is null.
 struct ColScale {
-    float s[8];
+    float s[kMaxTile];
 };
 template <int K>
 __global__ void k_power_scale(float* v, const float* w, const uint8_t* mask, int64_t n, ColScale cs) {
@@ -800,7 +801,7 @@ int cheb_setup(pl_batch_solver B) {
     k_power_scale<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, nullptr, S->d_mask, n, cs);
     count_launch();
     double lam = 0.0;
-    double h[16];
+    double h[2 * kMaxTile];
     for (int it = 0; it < B->cheb_eig_iters; ++it) {
         int rc = jv32_multi<K>(B, B->p, B->q);
         if (rc) return rc;
@@ -847,8 +848,8 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, B->scal + 3 * K, nullptr);
     count_launch(3);
-    double h[4 * 8];
-    int act[8];
+    double h[4 * kMaxTile];
+    int act[kMaxTile];
     if (B->cheb_degree >= 2) {
         // z = q(P A) P r, p = z, rz = r.z
         int rc = cheb_apply<K>(B);
@@ -859,7 +860,7 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     }
     PLB_CUDA(cudaMemcpyAsync(h, B->scal, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
     PLB_CUDA(cudaStreamSynchronize(s));
-    double r0[8];
+    double r0[kMaxTile];
     for (int k = 0; k < K; ++k) {
         r0[k] = std::sqrt(h[3 * K + k]);
         act[k] = (k < nact && r0[k] > 0.0) ? 1 : 0;
@@ -937,7 +938,7 @@ int solve_tile(pl_batch_solver B, int nact, const double* const* bs, double* con
     pl_solver S = B->base;
     cudaStream_t s = S->mesh->ctx->stream;
     const int64_t n = B->n;
-    double bnorm[8] = {0}, rn[8] = {0};
+    double bnorm[kMaxTile] = {0}, rn[kMaxTile] = {0};
     for (int k = 0; k < nact; ++k) PLB_CUDA(cudaMemsetAsync(xs[k], 0, n * sizeof(double), s));
     for (int outer = 0; outer < 30; ++outer) {
         // FP64 outer residual of every RHS of the tile, packed into the FP32 tile
@@ -995,8 +996,8 @@ int solve_tile(pl_batch_solver B, int nact, const double* const* bs, double* con
 extern "C" {
 
 int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
-    if (!base || !out || !(tile == 1 || tile == 2 || tile == 4 || tile == 8))
-        return fail(PL_ERR_INVALID_ARG, "tile must be 1, 2, 4 or 8");
+    if (!base || !out || !(tile == 1 || tile == 2 || tile == 4 || tile == 8 || tile == 16))
+        return fail(PL_ERR_INVALID_ARG, "tile must be 1, 2, 4, 8 or 16");
     *out = nullptr;
     pl_batch_solver B = new pl_batch_solver_s();
     B->base = base;
@@ -1010,10 +1011,10 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     };
     const size_t nk = (size_t)B->n * tile;
     A(&B->r, nk); A(&B->z, nk); A(&B->p, nk); A(&B->q, nk); A(&B->x, nk);
-    A(&B->scal, 4 * 8);
-    A(&B->active, 8);
-    A(&B->part_a, (size_t)kBBlocks * 8);
-    A(&B->part_b, (size_t)kBBlocks * 8);
+    A(&B->scal, 4 * kMaxTile);
+    A(&B->active, kMaxTile);
+    A(&B->part_a, (size_t)kBBlocks * kMaxTile);
+    A(&B->part_b, (size_t)kBBlocks * kMaxTile);
     A(&B->r64, B->n);
     A(&B->jx64, B->n);
     // the cell-block layout is built here, outside any stream capture
@@ -1053,7 +1054,8 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
             case 1: rc = cheb_setup<1>(B); break;
             case 2: rc = cheb_setup<2>(B); break;
             case 4: rc = cheb_setup<4>(B); break;
-            default: rc = cheb_setup<8>(B); break;
+            case 8: rc = cheb_setup<8>(B); break;
+            default: rc = cheb_setup<16>(B); break;
         }
     }
     for (int r0 = 0; r0 < nrhs && rc == PL_OK; r0 += B->K) {
@@ -1062,7 +1064,8 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
             case 1: rc = solve_tile<1>(B, nact, b_dev + r0, x_dev + r0); break;
             case 2: rc = solve_tile<2>(B, nact, b_dev + r0, x_dev + r0); break;
             case 4: rc = solve_tile<4>(B, nact, b_dev + r0, x_dev + r0); break;
-            default: rc = solve_tile<8>(B, nact, b_dev + r0, x_dev + r0); break;
+            case 8: rc = solve_tile<8>(B, nact, b_dev + r0, x_dev + r0); break;
+            default: rc = solve_tile<16>(B, nact, b_dev + r0, x_dev + r0); break;
         }
         if (rc == PL_OK) B->solves += nact;
     }
