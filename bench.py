@@ -645,13 +645,21 @@ def config_c3(args):
     g.solve(sample_b[:8], batched=True)  # warm-up
     g.solve(sample_b[:1], batched=False)
     sol_b, t_b = g.solve(sample_b, batched=True)
+    st_b = g.batch.stats()
+    # the same sample with restarted FP64 refinement in place of reliable updates
+    g.batch.set_reliable(False)
+    g.solve(sample_b[:8], batched=True)
+    _, t_r = g.solve(sample_b, batched=True)
+    restarted = {"solves_per_s": len(sample_b) / t_r, **g.batch.stats()}
+    g.batch.set_reliable(True)
     sample_s = sample_b[:ns]
     sol_s, t_s = g.solve(sample_s, batched=False)
     err = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(sol_b[:ns], sol_s))
     return {"config": "c3", "cells": mesh.num_cells, "dof": mesh.num_dof, "impulses_total": len(g.impulses),
             "batched": {"sample": len(sample_b), "solves_per_s": len(sample_b) / t_b, "tile": g.batch.tile,
                         "chebyshev_degree": g.batch.degree, "lambda_max_estimate": g.batch.lambda_max,
-                        **g.batch.stats()},
+                        "fp64_accuracy": "reliable updates (residual replacement, delta 0.1)", **st_b},
+            "restarted_refinement": restarted,
             "autotune": [{"tile": t, "chebyshev_degree": d, "solves_per_s": r} for t, d, r in table],
             "fp64_one_at_a_time": {"sample": len(sample_s), "solves_per_s": len(sample_s) / t_s,
                                    "iterations_last": g.solver64.stats()["iterations"]},

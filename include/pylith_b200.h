@@ -312,6 +312,14 @@ int pl_solver_create(pl_mesh mesh, const uint8_t* constrained_host, pl_solver* o
 int pl_solver_add_integrator(pl_solver solver, pl_integrator integ);
 int pl_solver_set_tolerances(pl_solver solver, double rtol, double atol, int max_iter);
 int pl_solver_set_precision(pl_solver solver, int precision, double inner_rtol);
+/* How PL_SOLVER_FP32_REFINED reaches FP64 accuracy. enable != 0 (the default, delta 0.1):
+ * reliable updates, one FP32 PCG without restarts whose iterated residual is replaced by the FP64
+ * true residual (the FP32 correction added to the FP64 solution) whenever it has dropped by
+ * `delta`. enable == 0: iterative refinement that restarts the FP32 PCG from every new FP64
+ * residual until it has dropped by inner_rtol. Either way the solve ends when the FP64 residual
+ * meets the tolerances. pl_solver_get_stats reports the replacements (or refinement passes) as
+ * outer iterations. */
+int pl_solver_set_reliable(pl_solver solver, int enable, double delta);
 /* Builds the preconditioner at (t, dt). */
 int pl_solver_setup(pl_solver solver, double t, double dt);
 int pl_solver_solve(pl_solver solver, const double* b_dev, double* x_dev);
@@ -343,6 +351,14 @@ int pl_batch_solver_solve(pl_batch_solver solver, int nrhs, const double* const*
  * libsrc/pylith/materials/Elasticity.cc:310-317), whose level smoother is PETSc's Chebyshev
  * iteration with bounds 0.1 and 1.1 times an estimated largest eigenvalue. */
 int pl_batch_solver_set_chebyshev(pl_batch_solver solver, int degree, double lower_ratio, int eig_iters);
+/* FP64 accuracy of the FP32 tile PCG. enable != 0 (the default, delta 0.1): reliable updates, one
+ * FP32 PCG per right-hand side without restarts, whose iterated residual is replaced by the FP64
+ * true residual (the FP32 correction added to the FP64 solution) whenever it has dropped by
+ * `delta`; the solve ends when the true residual meets the base solver's rtol. enable == 0: FP64
+ * iterative refinement that restarts the FP32 PCG from every new FP64 residual until it has
+ * dropped by the base solver's inner_rtol. pl_batch_solver_get_stats counts FP64 true residuals
+ * after the first as outer iterations with reliable updates, refinement passes without. */
+int pl_batch_solver_set_reliable(pl_batch_solver solver, int enable, double delta);
 int pl_batch_solver_get_chebyshev(pl_batch_solver solver, double* lambda_max);
 int pl_batch_solver_get_stats(pl_batch_solver solver, int64_t* solves, int64_t* inner_iterations,
                               int64_t* outer_iterations, double* max_rel_residual);

@@ -109,6 +109,7 @@ SIGNATURES = {
     "pl_solver_add_integrator": (_I, [_P, _P]),
     "pl_solver_set_tolerances": (_I, [_P, _D, _D, _I]),
     "pl_solver_set_precision": (_I, [_P, _I, _D]),
+    "pl_solver_set_reliable": (_I, [_P, _I, _D]),
     "pl_solver_setup": (_I, [_P, _D, _D]),
     "pl_solver_solve": (_I, [_P, _P, _P]),
     "pl_solver_get_stats": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
@@ -122,6 +123,7 @@ SIGNATURES = {
     "pl_batch_solver_destroy": (_I, [_P]),
     "pl_batch_solver_set_chebyshev": (_I, [_P, _I, _D, _I]),
     "pl_batch_solver_get_chebyshev": (_I, [_P, ctypes.POINTER(_D)]),
+    "pl_batch_solver_set_reliable": (_I, [_P, _I, _D]),
 }
 PL_SOLVER_FP64, PL_SOLVER_FP32_REFINED = 0, 1
 

@@ -177,6 +177,10 @@ struct pl_solver_s {
     double* d_pair_normal = nullptr;  // fault normal at each fault node
     double rtol = 1e-12, atol = 0.0, inner_rtol = 1e-5;
     int max_iter = 10000, precision = 0, check_every = 10;
+    // FP32_REFINED: reliable updates (residual replacement when the iterated residual has dropped
+    // by reliable_delta) or, when off, restarted iterative refinement to inner_rtol per pass
+    bool reliable = true;
+    double reliable_delta = 0.1;
     double t = 0.0, dt = 0.0;
     int iterations = 0, inner_iterations = 0, outer_iterations = 0;
     double rel_residual = 0.0;

@@ -643,6 +643,33 @@ __global__ void k_b_unpack_add(const float* d, int64_t n, int K, int kk, const u
         if (!mask[i]) x[i] += (double)d[i * K + kk];
 }
 
+// d[:, kk] = 0
+__global__ void k_b_col_zero(float* d, int64_t n, int K, int kk) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i * K + kk] = 0.0f;
+}
+
+// z[:, kk] = P r[:, kk] (constrained DOFs zero); partial r.z of the column
+__global__ void __launch_bounds__(kBThreads) k_b_col_prec(const float* r, float* z, const uint8_t* mask,
+                                                          const float* P, int64_t nnodes, int K, int kk,
+                                                          double* part) {
+    double s = 0.0;
+    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
+        float in[3], out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) in[c] = r[(3 * nd + c) * K + kk];
+        pinv_local(P, nd, in, out);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float v = mask[3 * nd + c] ? 0.0f : out[c];
+            z[(3 * nd + c) * K + kk] = v;
+            s += (double)in[c] * v;
+        }
+    }
+    double acc[1] = {s};
+    block_sumK<1>(acc, part);
+}
+
 static int bgrid(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 8); }
 
 }  // namespace plb
@@ -674,6 +701,13 @@ struct pl_batch_solver_s {
     float cheb_s0 = 0.0f;
     float cheb_c1[8] = {}, cheb_c2[8] = {};
     float *res = nullptr, *d = nullptr;
+    // Reliable updates (default): one FP32 CG per right-hand side, whose iterated residual is
+    // replaced by the FP64 true residual (and the FP32 correction folded into the FP64 solution)
+    // each time it has dropped by reliable_delta; off: FP64 refinement that restarts the FP32 PCG
+    // from each new FP64 residual until it has dropped by the solver's inner_rtol.
+    bool reliable = true;
+    double reliable_delta = 0.1;
+    int64_t reliable_updates = 0;
     // The solve runs on a private stream (graph capture is not possible on the legacy default
     // stream a caller may use), fenced against the caller's stream with events.
     cudaStream_t stream = nullptr;
@@ -838,6 +872,33 @@ int cheb_setup(pl_batch_solver B) {
     return PL_OK;
 }
 
+// Captures (once per tile size, state epoch and preconditioner) the graph of check_every PCG
+// iterations.
+template <int K>
+int ensure_pcg_graph(pl_batch_solver B) {
+    pl_solver S = B->base;
+    cudaStream_t s = S->mesh->ctx->stream;
+    const int chunk = S->check_every;
+    if (B->graph && B->graph_iters == chunk && B->graph_epoch == state_epoch() && B->graph_cheb == B->cheb_version)
+        return PL_OK;
+    if (B->graph) cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+    cudaGraph_t g;
+    PLB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    int rc = PL_OK;
+    for (int i = 0; i < chunk && rc == PL_OK; ++i) rc = pcg_iteration<K>(B);
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    B->graph_iters = chunk;
+    B->graph_epoch = state_epoch();
+    B->graph_cheb = B->cheb_version;
+    return PL_OK;
+}
+
 // FP32 PCG on the tile: r holds the right-hand sides on entry; x returns the corrections.
 template <int K>
 int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters) {
@@ -867,24 +928,8 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     }
     PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
     const int chunk = S->check_every;
-    // capture `chunk` iterations once per tile size, replay between checks
-    if (!B->graph || B->graph_iters != chunk || B->graph_epoch != state_epoch() || B->graph_cheb != B->cheb_version) {
-        if (B->graph) cudaGraphExecDestroy(B->graph);
-        B->graph = nullptr;
-        cudaGraph_t g;
-        PLB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
-        int rc = PL_OK;
-        for (int i = 0; i < chunk && rc == PL_OK; ++i) rc = pcg_iteration<K>(B);
-        cudaError_t e = cudaStreamEndCapture(s, &g);
-        if (rc) return rc;
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&B->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
-        B->graph_iters = chunk;
-        B->graph_epoch = state_epoch();
-        B->graph_cheb = B->cheb_version;
-    }
+    int rc = ensure_pcg_graph<K>(B);
+    if (rc) return rc;
     *iters = 0;
     for (int it = 0; it < max_iter; it += chunk) {
         PLB_CUDA(cudaGraphLaunch(B->graph, s));
@@ -933,8 +978,137 @@ __global__ void k_outer64(const double* bf, const double* Jx, const uint8_t* mas
     block_sumK<1>(acc, part);
 }
 
+// FP64 true residual of right-hand side kk, r = P^T (b + J x) on free DOFs (x unfolded first for
+// faults), packed into column kk of the FP32 tile residual; returns |r|.
+int col_true_residual(pl_batch_solver B, int K, int kk, const double* b, double* x, double* rnorm) {
+    pl_solver S = B->base;
+    cudaStream_t s = S->mesh->ctx->stream;
+    const int64_t n = B->n;
+    if (S->npairs > 0) {
+        k_unfold64<<<bgrid(3 * S->npairs), 256, 0, s>>>(x, S->d_pair_neg, S->d_pair_pos, S->npairs);
+        count_launch();
+    }
+    int rc = apply_J64(S, x, B->jx64);
+    if (rc) return rc;
+    PLB_CUDA(cudaMemcpyAsync(B->r64, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (S->npairs > 0) {
+        k_fold64<<<bgrid(3 * S->npairs), 256, 0, s>>>(B->jx64, S->d_pair_neg, S->d_pair_pos, S->npairs);
+        k_fold64<<<bgrid(3 * S->npairs), 256, 0, s>>>(B->r64, S->d_pair_neg, S->d_pair_pos, S->npairs);
+        count_launch(2);
+    }
+    k_outer64<<<kBBlocks, kBThreads, 0, s>>>(B->r64, B->jx64, S->d_mask, n, B->r64, B->part_a);
+    k_b_finish<1><<<1, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal + 4 * kMaxTile, nullptr);
+    k_b_pack<<<bgrid(n), 256, 0, s>>>(B->r64, n, K, kk, B->r);
+    count_launch(3);
+    double h;
+    PLB_CUDA(cudaMemcpyAsync(&h, B->scal + 4 * kMaxTile, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PLB_CUDA(cudaStreamSynchronize(s));
+    *rnorm = std::sqrt(h);
+    return PL_OK;
+}
+
+// The tile with reliable updates (van der Vorst and Ye, "Residual replacement strategies for
+// Krylov subspace iterative methods for the convergence of true residuals", SIAM J. Sci. Comput.
+// 22 (2000); as in the mixed-precision CG of Clark et al., Comput. Phys. Commun. 181 (2010)):
+// the FP32 PCG of every right-hand side runs without restarts; at a convergence check, a column
+// whose iterated residual has dropped below reliable_delta times its last true residual adds its
+// FP32 correction to the FP64 solution, gets the FP64 true residual (and z = P r, r.z) in place of
+// the iterated one and keeps its search direction; it is done when the true residual meets rtol.
+template <int K>
+int solve_tile_reliable(pl_batch_solver B, int nact, const double* const* bs, double* const* xs) {
+    pl_solver S = B->base;
+    cudaStream_t s = S->mesh->ctx->stream;
+    const int64_t n = B->n;
+    double bnorm[kMaxTile] = {0}, rref[kMaxTile] = {0};
+    int act[kMaxTile] = {0};
+    PLB_CUDA(cudaMemsetAsync(B->r, 0, n * K * sizeof(float), s));
+    PLB_CUDA(cudaMemsetAsync(B->x, 0, n * K * sizeof(float), s));
+    for (int k = 0; k < nact; ++k) {
+        PLB_CUDA(cudaMemsetAsync(xs[k], 0, n * sizeof(double), s));
+        int rc = col_true_residual(B, K, k, bs[k], xs[k], &bnorm[k]);
+        if (rc) return rc;
+        rref[k] = bnorm[k];
+        act[k] = bnorm[k] > 0.0 ? 1 : 0;
+    }
+    B->outer_iterations++;
+    k_b_init<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, B->p, S->d_mask, S->d_pinv32, B->nnodes, B->part_a, B->part_b);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, B->scal + 3 * K, nullptr);
+    count_launch(3);
+    if (B->cheb_degree >= 2) {
+        int rc = cheb_apply<K>(B);
+        if (rc) return rc;
+        k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+        count_launch();
+        PLB_CUDA(cudaMemcpyAsync(B->p, B->z, n * K * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
+    PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
+    int rc = ensure_pcg_graph<K>(B);
+    if (rc) return rc;
+    const int chunk = S->check_every;
+    const int max_iter = S->max_iter;
+    double h[4 * kMaxTile];
+    bool any = false;
+    for (int k = 0; k < K; ++k) any = any || act[k];
+    for (int it = 0; any; it += chunk) {
+        if (it >= max_iter) return fail(PL_ERR_NOT_CONVERGED, "batched PCG reached the iteration limit");
+        PLB_CUDA(cudaGraphLaunch(B->graph, s));
+        B->inner_iterations += chunk;
+        PLB_CUDA(cudaMemcpyAsync(h, B->scal, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PLB_CUDA(cudaStreamSynchronize(s));
+        bool changed = false, replaced = false;
+        any = false;
+        for (int k = 0; k < K; ++k) {
+            if (!act[k]) continue;
+            const double rn = std::sqrt(h[3 * K + k]);
+            if (!(rn == rn)) return fail(PL_ERR_NOT_CONVERGED, "batched PCG diverged (NaN residual)");
+            if (rn <= B->reliable_delta * rref[k] || rn <= 0.5 * S->rtol * bnorm[k]) {
+                k_b_unpack_add<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k, S->d_mask, xs[k]);
+                k_b_col_zero<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k);
+                count_launch(2);
+                double rt = 0.0;
+                rc = col_true_residual(B, K, k, bs[k], xs[k], &rt);
+                if (rc) return rc;
+                B->reliable_updates++;
+                B->outer_iterations++;
+                if (rt <= S->rtol * bnorm[k]) {
+                    act[k] = 0;
+                    changed = true;
+                    B->max_rel_residual = std::max(B->max_rel_residual, rt / bnorm[k]);
+                    continue;
+                }
+                rref[k] = rt;
+                replaced = true;
+                if (B->cheb_degree < 2) {
+                    k_b_col_prec<<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, S->d_mask, S->d_pinv32, B->nnodes, K, k,
+                                                                B->part_a);
+                    k_b_finish<1><<<1, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal + k, nullptr);
+                    count_launch(2);
+                }
+            }
+            any = true;
+        }
+        if (replaced && B->cheb_degree >= 2) {
+            // z = q(P A) P r with the same polynomial for the whole tile (the columns not replaced
+            // get their own z and r.z again), so the preconditioner stays fixed
+            rc = cheb_apply<K>(B);
+            if (rc) return rc;
+            k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+            count_launch();
+        }
+        if (changed) PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+    for (int k = 0; k < nact; ++k)
+        if (S->npairs > 0) {
+            k_unfold64<<<bgrid(3 * S->npairs), 256, 0, s>>>(xs[k], S->d_pair_neg, S->d_pair_pos, S->npairs);
+            count_launch();
+        }
+    return PL_OK;
+}
+
 template <int K>
 int solve_tile(pl_batch_solver B, int nact, const double* const* bs, double* const* xs) {
+    if (B->reliable) return solve_tile_reliable<K>(B, nact, bs, xs);
     pl_solver S = B->base;
     cudaStream_t s = S->mesh->ctx->stream;
     const int64_t n = B->n;
@@ -1011,7 +1185,7 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     };
     const size_t nk = (size_t)B->n * tile;
     A(&B->r, nk); A(&B->z, nk); A(&B->p, nk); A(&B->q, nk); A(&B->x, nk);
-    A(&B->scal, 4 * kMaxTile);
+    A(&B->scal, 4 * kMaxTile + 1);
     A(&B->active, kMaxTile);
     A(&B->part_a, (size_t)kBBlocks * kMaxTile);
     A(&B->part_b, (size_t)kBBlocks * kMaxTile);
@@ -1096,6 +1270,13 @@ int pl_batch_solver_set_chebyshev(pl_batch_solver B, int degree, double lower_ra
     B->cheb_version = 0;  // estimate again at the next solve
     B->cheb_lmax = 0.0;
     B->graph_cheb = -1;
+    return PL_OK;
+}
+
+int pl_batch_solver_set_reliable(pl_batch_solver B, int enable, double delta) {
+    if (!B || !(delta > 0.0 && delta < 1.0)) return fail(PL_ERR_INVALID_ARG, "delta must lie in (0, 1)");
+    B->reliable = enable != 0;
+    B->reliable_delta = delta;
     return PL_OK;
 }
 

@@ -177,6 +177,23 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update(T* x, T* r, const T* 
     block_sum2(rz, rr, partials);
 }
 
+// z = P^{-1} r; partial (r.z) (after the residual of a reliable update replaced r).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_prec_rz(const T* r, const T* pinv, int64_t nnodes, T* z,
+                                                         double* partials) {
+    double rz = 0.0;
+    for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
+        T zz[3];
+        apply_pinv(pinv, r, nd, zz);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            z[3 * nd + k] = zz[k];
+            rz += to_d(r[3 * nd + k]) * to_d(zz[k]);
+        }
+    }
+    block_sum2(rz, 0.0, partials);
+}
+
 // beta = rz / rz_old; p = z + beta p.
 template <typename T>
 __global__ void k_cg_pupdate(T* p, const T* z, int64_t n, double* scal) {
@@ -383,6 +400,48 @@ int apply_J32(pl_solver S, const float* v, float* out) {
     return PL_OK;
 }
 
+// One PCG iteration on the solver's private stream (capturable).
+template <typename T>
+int cg_iteration(pl_solver S, T* x, T* r, T* p, T* q, T* z, const T* pinv) {
+    const int64_t n = S->n, nn = S->nnodes;
+    double* part = S->d_partials;
+    double* scal = S->d_scal;
+    int rc;
+    if constexpr (sizeof(T) == 8) rc = apply_J(S, (const double*)p, (double*)q);
+    else rc = apply_J32(S, (const float*)p, (float*)q);
+    if (rc) return rc;
+    k_cg_pq<T><<<kRedBlocks, kRedThreads, 0, S->cstream>>>(p, q, S->d_mask, n, part);
+    k_finish2<<<1, 1024, 0, S->cstream>>>(part, kRedBlocks, scal, S_PQ, -1);
+    k_copy_scalar<<<1, 1, 0, S->cstream>>>(scal, S_RZ, S_RZ_OLD);
+    k_cg_update<T><<<kRedBlocks, kRedThreads, 0, S->cstream>>>(x, r, p, q, z, S->d_mask, pinv, nn, scal, part);
+    k_finish2<<<1, 1024, 0, S->cstream>>>(part, kRedBlocks, scal, S_RZ, S_RR);
+    k_cg_pupdate<T><<<vec_grid(n), 256, 0, S->cstream>>>(p, z, n, scal);
+    count_launch(6);
+    return PL_OK;
+}
+
+// The graph of check_every iterations (index 0: FP64, 1: FP32), captured again when the
+// integrators changed. The caller has switched the context to the private stream.
+template <typename T>
+int ensure_cg_graph(pl_solver S, T* x, T* r, T* p, T* q, T* z, const T* pinv) {
+    const int gi = sizeof(T) == 8 ? 0 : 1;
+    const int chunk = std::max(1, S->check_every);
+    if (S->graph[gi] && S->graph_iters[gi] == chunk && S->graph_epoch[gi] == state_epoch()) return PL_OK;
+    if (S->graph[gi]) cudaGraphExecDestroy(S->graph[gi]);
+    S->graph[gi] = nullptr;
+    int rc = PL_OK;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(S->cstream, cudaStreamCaptureModeRelaxed);
+    for (int i = 0; i < chunk && rc == PL_OK && e == cudaSuccess; ++i) rc = cg_iteration<T>(S, x, r, p, q, z, pinv);
+    if (e == cudaSuccess) e = cudaStreamEndCapture(S->cstream, &g);
+    if (e == cudaSuccess && rc == PL_OK) e = cudaGraphInstantiate(&S->graph[gi], g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc == PL_OK && e != cudaSuccess) rc = cuda_fail(e, "PCG graph capture");
+    S->graph_iters[gi] = chunk;
+    S->graph_epoch[gi] = state_epoch();
+    return rc;
+}
+
 template <typename T>
 int pcg(pl_solver S, const T* b, T* x, double rtol, double atol, int max_iter, const T* pinv, T* r, T* p, T* q, T* z,
         int* iters, double* rel) {
@@ -416,34 +475,7 @@ int pcg(pl_solver S, const T* b, T* x, double rtol, double atol, int max_iter, c
     PLB_CUDA(cudaEventRecord(S->ev_in, s));
     PLB_CUDA(cudaStreamWaitEvent(S->cstream, S->ev_in, 0));
     c->stream = S->cstream;
-    auto iteration = [&]() -> int {
-        int rc;
-        if constexpr (sizeof(T) == 8) rc = apply_J(S, (const double*)p, (double*)q);
-        else rc = apply_J32(S, (const float*)p, (float*)q);
-        if (rc) return rc;
-        k_cg_pq<T><<<kRedBlocks, kRedThreads, 0, S->cstream>>>(p, q, S->d_mask, n, part);
-        k_finish2<<<1, 1024, 0, S->cstream>>>(part, kRedBlocks, scal, S_PQ, -1);
-        k_copy_scalar<<<1, 1, 0, S->cstream>>>(scal, S_RZ, S_RZ_OLD);
-        k_cg_update<T><<<kRedBlocks, kRedThreads, 0, S->cstream>>>(x, r, p, q, z, S->d_mask, pinv, nn, scal, part);
-        k_finish2<<<1, 1024, 0, S->cstream>>>(part, kRedBlocks, scal, S_RZ, S_RR);
-        k_cg_pupdate<T><<<vec_grid(n), 256, 0, S->cstream>>>(p, z, n, scal);
-        count_launch(6);
-        return PL_OK;
-    };
-    int rc = PL_OK;
-    if (!S->graph[gi] || S->graph_iters[gi] != chunk || S->graph_epoch[gi] != state_epoch()) {
-        if (S->graph[gi]) cudaGraphExecDestroy(S->graph[gi]);
-        S->graph[gi] = nullptr;
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(S->cstream, cudaStreamCaptureModeRelaxed);
-        for (int i = 0; i < chunk && rc == PL_OK && e == cudaSuccess; ++i) rc = iteration();
-        if (e == cudaSuccess) e = cudaStreamEndCapture(S->cstream, &g);
-        if (e == cudaSuccess && rc == PL_OK) e = cudaGraphInstantiate(&S->graph[gi], g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (rc == PL_OK && e != cudaSuccess) rc = cuda_fail(e, "PCG graph capture");
-        S->graph_iters[gi] = chunk;
-        S->graph_epoch[gi] = state_epoch();
-    }
+    int rc = ensure_cg_graph<T>(S, x, r, p, q, z, pinv);
     for (int it = 0; rc == PL_OK && it < max_iter; it += chunk) {
         cudaError_t e = cudaGraphLaunch(S->graph[gi], S->cstream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, S->cstream);
@@ -468,6 +500,102 @@ int pcg(pl_solver S, const T* b, T* x, double rtol, double atol, int max_iter, c
     return rc;
 }
 
+// FP32 PCG with reliable updates (residual replacement; van der Vorst and Ye, SIAM J. Sci.
+// Comput. 22 (2000); the mixed-precision CG of Clark et al., Comput. Phys. Commun. 181 (2010)):
+// one FP32 PCG without restarts; whenever its iterated residual has dropped below
+// reliable_delta times the last FP64 true residual, the FP32 correction is added to the FP64
+// solution x, r is replaced by the FP64 true residual b - A x (and z = P r, r.z recomputed), and
+// the search direction is kept. Ends when the true residual meets rtol (or atol).
+int pcg32_reliable(pl_solver S, const double* b, double* x) {
+    cudaStream_t s = S->mesh->ctx->stream;
+    pl_context c = S->mesh->ctx;
+    const int64_t n = S->n, nn = S->nnodes;
+    double* scal = S->d_scal;
+    double h[S_COUNT];
+    if (S->mesh->cell_type == PL_CELL_TET4)
+        for (pl_integrator ig : S->ops) {
+            int rcl = prepare_blocked(ig);  // allocates: outside any capture
+            if (rcl) return rcl;
+        }
+    PLB_CUDA(cudaEventRecord(S->ev_in, s));
+    PLB_CUDA(cudaStreamWaitEvent(S->cstream, S->ev_in, 0));
+    c->stream = S->cstream;
+    cudaStream_t cs = S->cstream;
+    int rc = PL_OK;
+    // FP64 true residual of x into d_r (and f_r); returns |r|
+    auto true_residual = [&](double* rn) -> int {
+        int r2 = apply_J(S, x, S->d_q);
+        if (r2) return r2;
+        k_outer_residual<<<kRedBlocks, kRedThreads, 0, cs>>>(b, S->d_q, S->d_mask, n, S->d_r, S->f_r, S->d_partials);
+        k_finish2<<<1, 1024, 0, cs>>>(S->d_partials, kRedBlocks, scal, S_BB, -1);
+        count_launch(2);
+        PLB_CUDA(cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, cs));
+        PLB_CUDA(cudaStreamSynchronize(cs));
+        *rn = std::sqrt(h[S_BB]);
+        return PL_OK;
+    };
+    double b0 = 0.0, rt = 0.0;
+    do {
+        if (cudaMemsetAsync(x, 0, n * sizeof(double), cs) != cudaSuccess ||
+            cudaMemsetAsync(S->f_x, 0, n * sizeof(float), cs) != cudaSuccess) {
+            rc = fail(PL_ERR_CUDA, "memset");
+            break;
+        }
+        if ((rc = true_residual(&b0)) != PL_OK) break;
+        rt = b0;
+        const double stop = std::max(S->rtol * b0, S->atol);
+        if (b0 == 0.0 || b0 <= stop) break;
+        k_cg_init<float><<<kRedBlocks, kRedThreads, 0, cs>>>(S->f_r, S->d_mask, S->d_pinv32, nn, S->f_r, S->f_z, S->f_p,
+                                                               S->d_partials);
+        k_finish2<<<1, 1024, 0, cs>>>(S->d_partials, kRedBlocks, scal, S_RZ, S_RR);
+        count_launch(2);
+        if ((rc = ensure_cg_graph<float>(S, S->f_x, S->f_r, S->f_p, S->f_q, S->f_z, S->d_pinv32)) != PL_OK) break;
+        const int chunk = std::max(1, S->check_every);
+        double rref = b0;
+        bool done = false;
+        for (int it = 0; !done; it += chunk) {
+            if (it >= S->max_iter) {
+                rc = fail(PL_ERR_NOT_CONVERGED, "PCG reached the iteration limit");
+                break;
+            }
+            cudaError_t e = cudaGraphLaunch(S->graph[1], cs);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h, scal, sizeof(h), cudaMemcpyDeviceToHost, cs);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(e, "PCG iterations");
+                break;
+            }
+            S->inner_iterations += chunk;
+            const double rn = std::sqrt(h[S_RR]);
+            if (!(rn == rn)) {
+                rc = fail(PL_ERR_NOT_CONVERGED, "PCG diverged (NaN residual)");
+                break;
+            }
+            if (rn > S->reliable_delta * rref && rn > 0.5 * stop) continue;
+            k_add_correction<<<vec_grid(n), 256, 0, cs>>>(x, S->f_x, S->d_mask, n);
+            count_launch();
+            if (cudaMemsetAsync(S->f_x, 0, n * sizeof(float), cs) != cudaSuccess) {
+                rc = fail(PL_ERR_CUDA, "memset");
+                break;
+            }
+            if ((rc = true_residual(&rt)) != PL_OK) break;
+            S->outer_iterations++;
+            if (rt <= stop) {
+                done = true;
+                break;
+            }
+            rref = rt;
+            k_prec_rz<float><<<kRedBlocks, kRedThreads, 0, cs>>>(S->f_r, S->d_pinv32, nn, S->f_z, S->d_partials);
+            k_finish2<<<1, 1024, 0, cs>>>(S->d_partials, kRedBlocks, scal, S_RZ, -1);
+            count_launch(2);
+        }
+    } while (false);
+    S->rel_residual = b0 > 0.0 ? rt / b0 : 0.0;
+    c->stream = s;
+    cudaEventRecord(S->ev_out, cs);
+    cudaStreamWaitEvent(s, S->ev_out, 0);
+    return rc;
+}
 
 }  // namespace
 
@@ -576,6 +704,13 @@ int pl_solver_set_tolerances(pl_solver S, double rtol, double atol, int max_iter
     return PL_OK;
 }
 
+int pl_solver_set_reliable(pl_solver S, int enable, double delta) {
+    if (!S || !(delta > 0.0 && delta < 1.0)) return fail(PL_ERR_INVALID_ARG, "delta must lie in (0, 1)");
+    S->reliable = enable != 0;
+    S->reliable_delta = delta;
+    return PL_OK;
+}
+
 int pl_solver_set_precision(pl_solver S, int precision, double inner_rtol) {
     if (!S || (precision != PL_SOLVER_FP64 && precision != PL_SOLVER_FP32_REFINED) || !(inner_rtol > 0 && inner_rtol < 1))
         return fail(PL_ERR_INVALID_ARG, "bad precision settings");
@@ -636,6 +771,7 @@ int pl_solver_solve(pl_solver S, const double* b, double* x) {
         S->rel_residual = rel;
         return rc;
     }
+    if (S->reliable) return pcg32_reliable(S, b, x);
     // FP64 iterative refinement around FP32 PCG (apply_J unfolds x on every outer pass).
     PLB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
     double h[S_COUNT];

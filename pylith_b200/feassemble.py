@@ -323,7 +323,8 @@ class Solver:
     FP32_REFINED = C.PL_SOLVER_FP32_REFINED
 
     def __init__(self, mesh: DeviceMesh, constrained: Optional[np.ndarray], integrators,
-                 rtol=1e-12, atol=0.0, max_iter=20000, precision=C.PL_SOLVER_FP64, inner_rtol=1e-5):
+                 rtol=1e-12, atol=0.0, max_iter=20000, precision=C.PL_SOLVER_FP64, inner_rtol=1e-5,
+                 reliable=True, reliable_delta=0.1):
         self.dmesh = mesh
         self.integrators = list(integrators)
         self.handle = ctypes.c_void_p()
@@ -335,6 +336,8 @@ class Solver:
             check(C.lib().pl_solver_add_integrator(self.handle, ig.handle))
         check(C.lib().pl_solver_set_tolerances(self.handle, rtol, atol, max_iter))
         check(C.lib().pl_solver_set_precision(self.handle, precision, inner_rtol))
+        # FP32_REFINED: reliable updates (residual replacement) or restarted iterative refinement
+        check(C.lib().pl_solver_set_reliable(self.handle, 1 if reliable else 0, reliable_delta))
 
     def setup(self, t=0.0, dt=0.0):
         check(C.lib().pl_solver_setup(self.handle, t, dt))
@@ -372,6 +375,7 @@ class BatchSolver:
         self.solver = solver
         self.tile = tile
         self.degree = 0
+        self.reliable = True
         self.handle = ctypes.c_void_p()
         check(C.lib().pl_batch_solver_create(solver.handle, tile, ctypes.byref(self.handle)))
 
@@ -386,6 +390,12 @@ class BatchSolver:
         Jacobi on [lower_ratio b, b], b = 1.1 lambda_max(P A), estimated at the next solve."""
         check(C.lib().pl_batch_solver_set_chebyshev(self.handle, int(degree), float(lower_ratio), int(eig_iters)))
         self.degree = int(degree)
+
+    def set_reliable(self, enable: bool = True, delta: float = 0.1) -> None:
+        """FP64 accuracy of the FP32 tile PCG: reliable updates (residual replacement whenever the
+        iterated residual has dropped by `delta`; the default) or restarted iterative refinement."""
+        check(C.lib().pl_batch_solver_set_reliable(self.handle, 1 if enable else 0, float(delta)))
+        self.reliable = bool(enable)
 
     @property
     def lambda_max(self) -> float:

@@ -390,3 +390,75 @@ def test_green_functions_autotune_keeps_the_fastest_configuration(ctx):
     for a, b in zip(got, ref):
         a, b = a.cpu().numpy(), b.cpu().numpy()
         assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
+
+
+def test_batched_reliable_updates_match_fp64_with_fewer_iterations(ctx):
+    """Reliable updates (one FP32 PCG per right-hand side, residual replacement by the FP64 true
+    residual) and restarted FP64 refinement both match one-at-a-time FP64 solves to <= 1e-8; the
+    reliable updates need no more tile iterations than the restarts."""
+    import torch
+    from pylith_b200 import greensfns as GF
+
+    mesh = M.box_tet_kuhn(12, 10, 8, fault_x=0.0, seed=4)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=6)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg")] = True
+    cons[M.boundary_mask(mesh, 0, "pos")] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    patches = GF.fault_patches(mesh, (-6000.0, 6000.0), (-9000.0, 0.0), 4, 3)
+    g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
+    imps = g.impulses[:8]
+    ref, _ = g.solve(imps, batched=False)
+    iters = {}
+    for reliable in (True, False):
+        g.batch.set_reliable(reliable, 0.1)
+        got, _ = g.solve(imps, batched=True)
+        for a, b in zip(got, ref):
+            a, b = a.cpu().numpy(), b.cpu().numpy()
+            assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b), reliable
+        st = g.batch.stats()
+        assert st["max_rel_residual"] <= 1e-11
+        iters[reliable] = st["inner_iterations"]
+    assert iters[True] <= iters[False], iters
+
+
+def test_fp32_reliable_updates_and_restarted_refinement_match_the_oracle(ctx, oracle_lib):
+    """The single-right-hand-side FP32 solver with reliable updates and with restarted iterative
+    refinement both reach the FP64 tolerance on a heterogeneous tetrahedral problem and match
+    scipy's direct solve of the oracle-assembled system to <= 1e-8; the reliable updates need no
+    more FP32 iterations."""
+    import torch
+    from pylith_b200 import feassemble as FA
+
+    O = oracle_lib
+    mesh = M.box_tet_delaunay(8000, seed=4)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=3)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg")] = True
+    cons[M.boundary_mask(mesh, 0, "pos")] = True
+    cons = cons.ravel()
+    aux = O.AuxFields([(rho[:, None], "cell"), (mu[:, None], "cell"), (K[:, None], "cell")])
+    J = O.assemble(mesh, O.jacobian_elements(mesh, aux, g3="IsotropicLinearElasticity3D::Jf3vu_infinitesimalStrain"))
+    b = np.random.default_rng(9).standard_normal(3 * mesh.num_nodes) * (~cons)
+    free = ~cons
+    x_ref = np.zeros_like(b)
+    x_ref[free] = spla.spsolve((-J)[free][:, free].tocsc(), b[free])
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm)
+    inner = {}
+    for reliable in (True, False):
+        S = FA.Solver(dm, cons, [ig], rtol=1e-11, precision=FA.Solver.FP32_REFINED, inner_rtol=1e-4,
+                      reliable=reliable)
+        S.setup()
+        x = torch.zeros(dm.num_dof, dtype=torch.float64, device="cuda")
+        S.solve(torch.from_numpy(b).cuda(), x)
+        ctx.synchronize()
+        st = S.stats()
+        assert st["rel_residual"] <= 1e-11, (reliable, st)
+        err = np.linalg.norm(x.cpu().numpy() - x_ref) / np.linalg.norm(x_ref)
+        assert err <= 1e-8, (reliable, err, st)
+        inner[reliable] = st["inner_iterations"]
+        S.close()
+    assert inner[True] <= inner[False], inner
