@@ -299,8 +299,8 @@ int pl_matrix_destroy(pl_matrix mat);
  *      libsrc/pylith/materials/Elasticity.cc:298-330, petsc/Options.cc:320-331) ------------ */
 /* Solves A x = b with A = -(sum of the added domain integrators' Jacobians), on the DOFs whose
  * constrained flag is 0 (Dirichlet DOFs of x are returned as 0). Preconditioned conjugate
- * gradients with point-block Jacobi. PL_SOLVER_FP32_REFINED runs the inner iterations in FP32
- * (FP64 dot products) inside FP64 iterative refinement.
+ * gradients with point-block Jacobi. PL_SOLVER_FP32_REFINED runs the iterations in FP32 (FP64
+ * dot products) and reaches FP64 accuracy through FP64 residuals (pl_solver_set_reliable).
  * Meshes with cohesive cells are solved in the reduced space of the slip constraint
  * u+ = u- + d: the positive-side DOFs of fault nodes follow the negative side and the two sides'
  * equations are summed, where the Lagrange-multiplier terms of f0u_neg/f0u_pos cancel; this
@@ -335,7 +335,7 @@ int pl_solver_destroy(pl_solver solver);
 /* Solves A x_i = b_i for many right-hand sides with the operator, constraints, preconditioner and
  * tolerances of `base` (after pl_solver_setup). Tiles of `tile` (1, 2, 4, 8 or 16) right-hand sides
  * share every launch of an FP32 PCG (FP64 dot products, CUDA-graph replay between convergence
- * checks) inside FP64 iterative refinement per right-hand side. b_dev/x_dev are arrays of nrhs
+ * checks), brought to FP64 accuracy per right-hand side (pl_batch_solver_set_reliable). b_dev/x_dev are arrays of nrhs
  * device pointers to full local vectors. P1 tetrahedra with isotropic linear elasticity. */
 typedef struct pl_batch_solver_s* pl_batch_solver;
 int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out);

@@ -369,7 +369,7 @@ class Solver:
 
 class BatchSolver:
     """Many right-hand sides with the operator and preconditioner of a set-up `Solver`
-    (pl_batch_solver_*): tiles of `tile` RHS share each FP32 PCG launch, FP64 refinement per RHS."""
+    (pl_batch_solver_*): tiles of `tile` RHS share each FP32 PCG launch, FP64 residuals per RHS."""
 
     def __init__(self, solver: Solver, tile: int = 8):
         self.solver = solver
