@@ -59,6 +59,14 @@ struct MultiChunk {
     static constexpr int value = K < 4 ? K : 4;
 };
 
+// Floats per staged node row in shared memory: the 3K field values, padded so that for K a
+// multiple of 4 the row is an odd number of 16-byte units; the 16-byte loads of a warp from
+// random rows then reach all 8 bank groups (a 96-byte row for K = 8 reaches only 4).
+template <int K>
+struct MultiRow {
+    static constexpr int value = (K % 4 == 0 && ((3 * K / 4) % 2 == 0)) ? 3 * K + 4 : 3 * K;
+};
+
 template <int W>
 PL_D void ld_vec(const float* p, float (&v)[W]) {
     if (W == 4) {
@@ -94,7 +102,7 @@ PL_D void red_vec(float* p, const float (&v)[W]) {
 
 // v, out: [ndof][K] FP32 (ndof = 3 * nodes, node-major); out must be zeroed or hold the sum to add to.
 // Per cell block: the block's node coordinates (FP64, [3][ld]) and K field vectors (FP32, one row
-// of 3K values per node, as in global memory) are staged in shared memory with the block's node ids
+// of 3K values per node as in global memory, padded to MultiRow<K>) are staged in shared memory with the block's node ids
 // and incidence list, all copied asynchronously one block ahead. One thread per cell
 // forms the geometry and the isotropic tangent once and then, KC right-hand sides at a time (one
 // vector load per node and component), the element vectors, staged as [12][cells][KC]; then one
@@ -143,7 +151,7 @@ PL_D void prefetch_multi(const DomainParams& p, const int32_t* __restrict__ slot
 #pragma unroll
         for (int d = 0; d < 3; ++d) __pipeline_memcpy_async(&sX[d * ld + i], &p.coords[3 * nd + d], sizeof(double));
         const float* vr = v + 3 * K * nd;
-        float* sr = sV + 3 * K * i;
+        float* sr = sV + MultiRow<K>::value * i;
 #pragma unroll
         for (int j = 0; j < 3 * K; j += CB / 4) __pipeline_memcpy_async(sr + j, vr + j, CB);
         mm.id[i] = id;
@@ -167,9 +175,10 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     extern __shared__ __align__(16) char smem_raw[];
     const AuxOffsets<RHEO_ILE, false> aoff;
     float* sE = reinterpret_cast<float*>(smem_raw);                                              // [12][cells][KC]
-    float* sV = sE + 12 * kMultiBlockCells * KC;                                                 // [ld][3K]
+    float* sV = sE + 12 * kMultiBlockCells * KC;  // [ld][MultiRow<K>]
     // [3][ld], at a 16-byte boundary after sV
-    double* sX = reinterpret_cast<double*>(reinterpret_cast<char*>(sV) + multi_r16((size_t)ld * 3 * K * sizeof(float)));
+    double* sX = reinterpret_cast<double*>(reinterpret_cast<char*>(sV) +
+                                           multi_r16((size_t)ld * MultiRow<K>::value * sizeof(float)));
     // two metadata buffers after sX
     char* metabase = reinterpret_cast<char*>(sX) + multi_r16((size_t)ld * 3 * sizeof(double));
     const size_t mb = multi_meta_bytes(ld);
@@ -233,10 +242,10 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 #pragma unroll
                 for (int cc = 0; cc < 3; ++cc) {
                     float u0[KC], u1[KC], u2[KC], u3[KC];
-                    ld_vec<KC>(sV + 3 * K * ln[0] + cc * K + r0, u0);
-                    ld_vec<KC>(sV + 3 * K * ln[1] + cc * K + r0, u1);
-                    ld_vec<KC>(sV + 3 * K * ln[2] + cc * K + r0, u2);
-                    ld_vec<KC>(sV + 3 * K * ln[3] + cc * K + r0, u3);
+                    ld_vec<KC>(sV + MultiRow<K>::value * ln[0] + cc * K + r0, u0);
+                    ld_vec<KC>(sV + MultiRow<K>::value * ln[1] + cc * K + r0, u1);
+                    ld_vec<KC>(sV + MultiRow<K>::value * ln[2] + cc * K + r0, u2);
+                    ld_vec<KC>(sV + MultiRow<K>::value * ln[3] + cc * K + r0, u3);
 #pragma unroll
                     for (int rr = 0; rr < KC; ++rr) {
                         const float g0 = u1[rr] - u0[rr], g1 = u2[rr] - u0[rr], g2 = u3[rr] - u0[rr];
@@ -322,7 +331,7 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
 template <int K>
 size_t multi_smem(int ld) {
     return (size_t)12 * MultiChunk<K>::value * kMultiBlockCells * sizeof(float) +
-           multi_r16((size_t)ld * 3 * K * sizeof(float)) + multi_r16((size_t)ld * 3 * sizeof(double)) +
+           multi_r16((size_t)ld * MultiRow<K>::value * sizeof(float)) + multi_r16((size_t)ld * 3 * sizeof(double)) +
            2 * multi_meta_bytes(ld);
 }
 
@@ -394,6 +403,51 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish(const double* __restrict
     }
 }
 
+// Final sums fused into the kernel that produced the per-block partials: the last block to finish
+// (a ticket counter; the partials are fenced before the ticket is taken) sums partials[blk][K] in
+// block order, like k_b_finish, into out[k] (copying the old out[k] to prev[k] first when prev is
+// set). FinSpec::counter null: no fused sum (the caller launches k_b_finish).
+struct FinSpec {
+    unsigned int* counter = nullptr;
+    double* out_a = nullptr;   // sums of the first partial array
+    double* prev_a = nullptr;
+    double* out_b = nullptr;   // sums of the second partial array (kernels with two)
+};
+
+PL_D bool take_last_ticket(unsigned int* counter) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+        if (last) *counter = 0u;  // every other block has taken its ticket
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+template <int K>
+PL_D void sum_partials_last_block(const double* partials, double* out, double* prev) {
+    __shared__ double sh[kBThreads / 32][K];
+    const int k = threadIdx.x % K;
+    double s = 0.0;
+    for (int b = threadIdx.x / K; b < (int)gridDim.x; b += kBThreads / K) s += __ldcg(&partials[b * K + k]);
+#pragma unroll
+    for (int o = K; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l < K) sh[w][l] = s;
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < kBThreads / 32; ++i) t += sh[i][threadIdx.x];
+        if (prev) prev[threadIdx.x] = out[threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
 template <int K>
 PL_D void pinv_apply(const float* __restrict__ P, const float* r, int64_t node, int k, float z[3]) {
     const float* B = P + 9 * node;
@@ -434,11 +488,12 @@ __global__ void __launch_bounds__(kBThreads) k_b_init(float* r, float* z, float*
 // partial p.(A p) with q = J p: -p.q over free DOFs
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_b_pq(const float* p, const float* q, const uint8_t* mask, int64_t n,
-                                                    double* part) {
+                                                    double* part, FinSpec fin) {
     double s = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
         if (!mask[e / K]) s -= (double)p[e] * q[e];
     block_sum_by_rhs<K>(s, part);
+    if (fin.counter && take_last_ticket(fin.counter)) sum_partials_last_block<K>(part, fin.out_a, fin.prev_a);
 }
 
 // alpha_k = active_k ? rz_k / pq_k : 0; x += alpha p; r += alpha q; z = P r; partial rz, rr.
@@ -447,7 +502,7 @@ template <int K>
 __global__ void __launch_bounds__(kBThreads) k_b_update(float* x, float* r, const float* p, const float* q, float* z,
                                                         const uint8_t* mask, const float* P, int64_t nnodes,
                                                         const double* rz, const double* pq, const int* active,
-                                                        double* part_rz, double* part_rr) {
+                                                        double* part_rz, double* part_rr, FinSpec fin) {
     const int k = threadIdx.x % K;  // blockDim and the grid stride are multiples of K
     const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
     double srz = 0.0, srr = 0.0;
@@ -474,6 +529,10 @@ __global__ void __launch_bounds__(kBThreads) k_b_update(float* x, float* r, cons
     block_sum_by_rhs<K>(srz, part_rz);
     __syncthreads();
     block_sum_by_rhs<K>(srr, part_rr);
+    if (fin.counter && take_last_ticket(fin.counter)) {
+        sum_partials_last_block<K>(part_rz, fin.out_a, fin.prev_a);
+        sum_partials_last_block<K>(part_rr, fin.out_b, nullptr);
+    }
 }
 
 // beta_k = rz_k / rz_old_k; p = z + beta p
@@ -502,7 +561,8 @@ PL_D void pinv_local(const float* __restrict__ P, int64_t node, const float in[3
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* x, float* r, const float* p, const float* q,
                                                            const uint8_t* mask, int64_t n, const double* rz,
-                                                           const double* pq, const int* active, double* part_rr) {
+                                                           const double* pq, const int* active, double* part_rr,
+                                                           FinSpec fin) {
     const int k = threadIdx.x % K;
     const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
     double srr = 0.0;
@@ -514,6 +574,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* x, float* r, c
         srr += (double)ri * ri;
     }
     block_sum_by_rhs<K>(srr, part_rr);
+    if (fin.counter && take_last_ticket(fin.counter)) sum_partials_last_block<K>(part_rr, fin.out_a, nullptr);
 }
 
 // First Chebyshev step: d = s P r, z = d (constrained DOFs zero). One thread per (node, rhs).
@@ -540,7 +601,8 @@ __global__ void __launch_bounds__(kBThreads) k_cheb_first(const float* r, float*
 template <int K, bool LAST>
 __global__ void __launch_bounds__(kBThreads) k_cheb_step(const float* src, const float* q, float* res, float* d,
                                                          float* z, const float* r, const uint8_t* mask, const float* P,
-                                                         int64_t nnodes, float c1, float c2, double* part_rz) {
+                                                         int64_t nnodes, float c1, float c2, double* part_rz,
+                                                         FinSpec fin) {
     double srz = 0.0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t nd = t / K;
@@ -564,7 +626,10 @@ __global__ void __launch_bounds__(kBThreads) k_cheb_step(const float* src, const
             if (LAST) srz += (double)r[i] * zv;
         }
     }
-    if (LAST) block_sum_by_rhs<K>(srz, part_rz);
+    if (LAST) {
+        block_sum_by_rhs<K>(srz, part_rz);
+        if (fin.counter && take_last_ticket(fin.counter)) sum_partials_last_block<K>(part_rz, fin.out_a, fin.prev_a);
+    }
 }
 
 // Power iteration for the largest eigenvalue of P A: w = -P (J v) on free DOFs, partial |w|^2
@@ -685,6 +750,7 @@ struct pl_batch_solver_s {
     int* active = nullptr;
     double* part_a = nullptr;
     double* part_b = nullptr;
+    unsigned int* ticket = nullptr;  // last-block counter of the fused reductions (zero between kernels)
     double* r64 = nullptr;    // single-RHS FP64 outer residual
     double* jx64 = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -769,9 +835,10 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
     return PL_OK;
 }
 
-// z = q(P A) P r with the Chebyshev coefficients of the solver; partial r.z into part_a.
+// z = q(P A) P r with the Chebyshev coefficients of the solver; partial r.z into part_a (and,
+// with fin.counter, the final r.z into fin.out_a, the old value into fin.prev_a).
 template <int K>
-int cheb_apply(pl_batch_solver B) {
+int cheb_apply(pl_batch_solver B, FinSpec fin = FinSpec()) {
     pl_solver S = B->base;
     cudaStream_t s = S->mesh->ctx->stream;
     k_cheb_first<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->d, B->z, S->d_mask, S->d_pinv32, B->nnodes, B->cheb_s0);
@@ -783,11 +850,11 @@ int cheb_apply(pl_batch_solver B) {
         if (i == B->cheb_degree - 1)
             k_cheb_step<K, true><<<kBBlocks, kBThreads, 0, s>>>(src, B->q, B->res, B->d, B->z, B->r, S->d_mask,
                                                                 S->d_pinv32, B->nnodes, B->cheb_c1[i], B->cheb_c2[i],
-                                                                B->part_a);
+                                                                B->part_a, fin);
         else
             k_cheb_step<K, false><<<kBBlocks, kBThreads, 0, s>>>(src, B->q, B->res, B->d, B->z, B->r, S->d_mask,
                                                                  S->d_pinv32, B->nnodes, B->cheb_c1[i], B->cheb_c2[i],
-                                                                 nullptr);
+                                                                 nullptr, FinSpec());
         count_launch();
     }
     return PL_OK;
@@ -804,23 +871,36 @@ int pcg_iteration(pl_batch_solver B) {
     double* rr = B->scal + 3 * K;
     int rc = jv32_multi<K>(B, B->p, B->q);
     if (rc) return rc;
-    k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a);
-    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, pq, nullptr);
+    // the final sums are formed by the last block of each reduction kernel (no k_b_finish launches)
+    FinSpec fpq;
+    fpq.counter = B->ticket;
+    fpq.out_a = pq;
+    k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a, fpq);
     if (B->cheb_degree >= 2) {
+        FinSpec frr;
+        frr.counter = B->ticket;
+        frr.out_a = rr;
         k_b_update_xr<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, S->d_mask, B->n, rz, pq, B->active,
-                                                        B->part_b);
+                                                        B->part_b, frr);
         count_launch();
-        rc = cheb_apply<K>(B);
+        FinSpec frz;
+        frz.counter = B->ticket;
+        frz.out_a = rz;
+        frz.prev_a = rz_old;
+        rc = cheb_apply<K>(B, frz);
         if (rc) return rc;
     } else {
+        FinSpec fu;
+        fu.counter = B->ticket;
+        fu.out_a = rz;
+        fu.prev_a = rz_old;
+        fu.out_b = rr;
         k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes,
-                                                     rz, pq, B->active, B->part_a, B->part_b);
+                                                     rz, pq, B->active, B->part_a, B->part_b, fu);
         count_launch();
     }
-    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, rz, rz_old);
-    k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, rr, nullptr);
     k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->z, B->n, rz, rz_old, B->active);
-    count_launch(5);
+    count_launch(2);
     return PL_OK;
 }
 
@@ -1189,6 +1269,8 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     A(&B->active, kMaxTile);
     A(&B->part_a, (size_t)kBBlocks * kMaxTile);
     A(&B->part_b, (size_t)kBBlocks * kMaxTile);
+    A(&B->ticket, 1);
+    if (e == cudaSuccess) e = cudaMemset(B->ticket, 0, sizeof(unsigned int));
     A(&B->r64, B->n);
     A(&B->jx64, B->n);
     // the cell-block layout is built here, outside any stream capture
@@ -1306,7 +1388,7 @@ int pl_batch_solver_destroy(pl_batch_solver B) {
     if (B->ev_in) cudaEventDestroy(B->ev_in);
     if (B->ev_out) cudaEventDestroy(B->ev_out);
     if (B->stream) cudaStreamDestroy(B->stream);
-    void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64, B->res, B->d};
+    void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64, B->res, B->d, B->ticket};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete B;
