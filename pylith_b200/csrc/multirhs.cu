@@ -714,6 +714,12 @@ __global__ void k_b_col_zero(float* d, int64_t n, int K, int kk) {
         d[i * K + kk] = 0.0f;
 }
 
+// dst[:, kk] = src[:, kk]
+__global__ void k_b_col_copy(float* dst, const float* src, int64_t n, int K, int kk) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i * K + kk] = src[i * K + kk];
+}
+
 // z[:, kk] = P r[:, kk] (constrained DOFs zero); partial r.z of the column
 __global__ void __launch_bounds__(kBThreads) k_b_col_prec(const float* r, float* z, const uint8_t* mask,
                                                           const float* P, int64_t nnodes, int K, int kk,
@@ -1087,108 +1093,145 @@ int col_true_residual(pl_batch_solver B, int K, int kk, const double* b, double*
     return PL_OK;
 }
 
-// The tile with reliable updates (van der Vorst and Ye, "Residual replacement strategies for
-// Krylov subspace iterative methods for the convergence of true residuals", SIAM J. Sci. Comput.
-// 22 (2000); as in the mixed-precision CG of Clark et al., Comput. Phys. Commun. 181 (2010)):
-// the FP32 PCG of every right-hand side runs without restarts; at a convergence check, a column
-// whose iterated residual has dropped below reliable_delta times its last true residual adds its
-// FP32 correction to the FP64 solution, gets the FP64 true residual (and z = P r, r.z) in place of
-// the iterated one and keeps its search direction; it is done when the true residual meets rtol.
+// All right-hand sides with reliable updates (van der Vorst and Ye, "Residual replacement
+// strategies for Krylov subspace iterative methods for the convergence of true residuals", SIAM J.
+// Sci. Comput. 22 (2000); as in the mixed-precision CG of Clark et al., Comput. Phys. Commun. 181
+// (2010)). Each of the K columns of the tile runs the FP32 PCG of one right-hand side without
+// restarts. At a convergence check, a column whose iterated residual has dropped below
+// reliable_delta times its last true residual adds its FP32 correction to the FP64 solution and
+// gets the FP64 true residual (with z = M r and r.z) in place of the iterated one, keeping its
+// search direction. A right-hand side is done when its true residual meets rtol; its column then
+// starts the next pending right-hand side (r = b, z = M r, p = z), so no column idles while
+// right-hand sides remain.
 template <int K>
-int solve_tile_reliable(pl_batch_solver B, int nact, const double* const* bs, double* const* xs) {
+int solve_reliable(pl_batch_solver B, int nrhs, const double* const* bs, double* const* xs) {
     pl_solver S = B->base;
     cudaStream_t s = S->mesh->ctx->stream;
     const int64_t n = B->n;
     double bnorm[kMaxTile] = {0}, rref[kMaxTile] = {0};
-    int act[kMaxTile] = {0};
+    int act[kMaxTile] = {0}, slot[kMaxTile], iters[kMaxTile] = {0};
+    bool fresh[kMaxTile] = {false}, replaced[kMaxTile] = {false};
+    for (int k = 0; k < K; ++k) slot[k] = -1;
+    int next = 0;
+    int rc = PL_OK;
     PLB_CUDA(cudaMemsetAsync(B->r, 0, n * K * sizeof(float), s));
     PLB_CUDA(cudaMemsetAsync(B->x, 0, n * K * sizeof(float), s));
-    for (int k = 0; k < nact; ++k) {
-        PLB_CUDA(cudaMemsetAsync(xs[k], 0, n * sizeof(double), s));
-        int rc = col_true_residual(B, K, k, bs[k], xs[k], &bnorm[k]);
-        if (rc) return rc;
-        rref[k] = bnorm[k];
-        act[k] = bnorm[k] > 0.0 ? 1 : 0;
-    }
-    B->outer_iterations++;
+    // final FP64 solution of right-hand side j (faults: the positive side follows the negative)
+    auto finish_rhs = [&](int j) {
+        if (S->npairs > 0) {
+            k_unfold64<<<bgrid(3 * S->npairs), 256, 0, s>>>(xs[j], S->d_pair_neg, S->d_pair_pos, S->npairs);
+            count_launch();
+        }
+    };
+    // column k takes the next pending right-hand side with a nonzero residual (r = b, x = 0)
+    auto assign = [&](int k) -> int {
+        slot[k] = -1;
+        act[k] = 0;
+        while (next < nrhs) {
+            const int j = next++;
+            PLB_CUDA(cudaMemsetAsync(xs[j], 0, n * sizeof(double), s));
+            double bn = 0.0;
+            int r2 = col_true_residual(B, K, k, bs[j], xs[j], &bn);
+            if (r2) return r2;
+            B->outer_iterations++;
+            if (bn > 0.0) {
+                slot[k] = j;
+                act[k] = 1;
+                bnorm[k] = rref[k] = bn;
+                iters[k] = 0;
+                return PL_OK;
+            }
+            finish_rhs(j);
+        }
+        // no right-hand side left: the column's residual is cleared (it stays inactive)
+        k_b_col_zero<<<bgrid(n), 256, 0, s>>>(B->r, n, K, k);
+        count_launch();
+        return PL_OK;
+    };
+    for (int k = 0; k < K; ++k)
+        if ((rc = assign(k)) != PL_OK) return rc;
     k_b_init<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, B->p, S->d_mask, S->d_pinv32, B->nnodes, B->part_a, B->part_b);
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, B->scal + 3 * K, nullptr);
     count_launch(3);
     if (B->cheb_degree >= 2) {
-        int rc = cheb_apply<K>(B);
-        if (rc) return rc;
+        if ((rc = cheb_apply<K>(B)) != PL_OK) return rc;
         k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
         count_launch();
         PLB_CUDA(cudaMemcpyAsync(B->p, B->z, n * K * sizeof(float), cudaMemcpyDeviceToDevice, s));
     }
     PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
-    int rc = ensure_pcg_graph<K>(B);
-    if (rc) return rc;
+    if ((rc = ensure_pcg_graph<K>(B)) != PL_OK) return rc;
     const int chunk = S->check_every;
-    const int max_iter = S->max_iter;
     double h[4 * kMaxTile];
     bool any = false;
     for (int k = 0; k < K; ++k) any = any || act[k];
-    for (int it = 0; any; it += chunk) {
-        if (it >= max_iter) return fail(PL_ERR_NOT_CONVERGED, "batched PCG reached the iteration limit");
+    while (any) {
         PLB_CUDA(cudaGraphLaunch(B->graph, s));
         B->inner_iterations += chunk;
         PLB_CUDA(cudaMemcpyAsync(h, B->scal, 4 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
         PLB_CUDA(cudaStreamSynchronize(s));
-        bool changed = false, replaced = false;
-        any = false;
+        bool changed = false, update_z = false;
         for (int k = 0; k < K; ++k) {
+            fresh[k] = replaced[k] = false;
             if (!act[k]) continue;
+            iters[k] += chunk;
+            if (iters[k] > S->max_iter) return fail(PL_ERR_NOT_CONVERGED, "batched PCG reached the iteration limit");
             const double rn = std::sqrt(h[3 * K + k]);
             if (!(rn == rn)) return fail(PL_ERR_NOT_CONVERGED, "batched PCG diverged (NaN residual)");
-            if (rn <= B->reliable_delta * rref[k] || rn <= 0.5 * S->rtol * bnorm[k]) {
-                k_b_unpack_add<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k, S->d_mask, xs[k]);
-                k_b_col_zero<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k);
-                count_launch(2);
-                double rt = 0.0;
-                rc = col_true_residual(B, K, k, bs[k], xs[k], &rt);
-                if (rc) return rc;
-                B->reliable_updates++;
-                B->outer_iterations++;
-                if (rt <= S->rtol * bnorm[k]) {
-                    act[k] = 0;
-                    changed = true;
-                    B->max_rel_residual = std::max(B->max_rel_residual, rt / bnorm[k]);
-                    continue;
-                }
-                rref[k] = rt;
-                replaced = true;
-                if (B->cheb_degree < 2) {
+            if (rn > B->reliable_delta * rref[k] && rn > 0.5 * S->rtol * bnorm[k]) continue;
+            const int j = slot[k];
+            k_b_unpack_add<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k, S->d_mask, xs[j]);
+            k_b_col_zero<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k);
+            count_launch(2);
+            double rt = 0.0;
+            if ((rc = col_true_residual(B, K, k, bs[j], xs[j], &rt)) != PL_OK) return rc;
+            B->reliable_updates++;
+            B->outer_iterations++;
+            if (rt <= S->rtol * bnorm[k]) {
+                B->max_rel_residual = std::max(B->max_rel_residual, rt / bnorm[k]);
+                finish_rhs(j);
+                if ((rc = assign(k)) != PL_OK) return rc;
+                changed = true;
+                if (act[k]) fresh[k] = update_z = true;
+                continue;
+            }
+            rref[k] = rt;
+            replaced[k] = update_z = true;
+        }
+        if (update_z) {
+            if (B->cheb_degree >= 2) {
+                // z = q(P A) P r with the same polynomial for the whole tile (the other columns get
+                // their own z and r.z again), so the preconditioner stays fixed
+                if ((rc = cheb_apply<K>(B)) != PL_OK) return rc;
+                k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+                count_launch();
+            } else {
+                for (int k = 0; k < K; ++k) {
+                    if (!fresh[k] && !replaced[k]) continue;
                     k_b_col_prec<<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, S->d_mask, S->d_pinv32, B->nnodes, K, k,
                                                                 B->part_a);
                     k_b_finish<1><<<1, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal + k, nullptr);
                     count_launch(2);
                 }
             }
-            any = true;
-        }
-        if (replaced && B->cheb_degree >= 2) {
-            // z = q(P A) P r with the same polynomial for the whole tile (the columns not replaced
-            // get their own z and r.z again), so the preconditioner stays fixed
-            rc = cheb_apply<K>(B);
-            if (rc) return rc;
-            k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
-            count_launch();
+            // a new right-hand side starts from p = z
+            for (int k = 0; k < K; ++k)
+                if (fresh[k]) {
+                    k_b_col_copy<<<bgrid(n), 256, 0, s>>>(B->p, B->z, n, K, k);
+                    count_launch();
+                }
         }
         if (changed) PLB_CUDA(cudaMemcpyAsync(B->active, act, K * sizeof(int), cudaMemcpyHostToDevice, s));
+        any = false;
+        for (int k = 0; k < K; ++k) any = any || act[k];
     }
-    for (int k = 0; k < nact; ++k)
-        if (S->npairs > 0) {
-            k_unfold64<<<bgrid(3 * S->npairs), 256, 0, s>>>(xs[k], S->d_pair_neg, S->d_pair_pos, S->npairs);
-            count_launch();
-        }
+    B->solves += nrhs;
     return PL_OK;
 }
 
 template <int K>
 int solve_tile(pl_batch_solver B, int nact, const double* const* bs, double* const* xs) {
-    if (B->reliable) return solve_tile_reliable<K>(B, nact, bs, xs);
     pl_solver S = B->base;
     cudaStream_t s = S->mesh->ctx->stream;
     const int64_t n = B->n;
@@ -1314,7 +1357,16 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
             default: rc = cheb_setup<16>(B); break;
         }
     }
-    for (int r0 = 0; r0 < nrhs && rc == PL_OK; r0 += B->K) {
+    if (rc == PL_OK && B->reliable && nrhs > 0) {
+        switch (B->K) {
+            case 1: rc = solve_reliable<1>(B, nrhs, b_dev, x_dev); break;
+            case 2: rc = solve_reliable<2>(B, nrhs, b_dev, x_dev); break;
+            case 4: rc = solve_reliable<4>(B, nrhs, b_dev, x_dev); break;
+            case 8: rc = solve_reliable<8>(B, nrhs, b_dev, x_dev); break;
+            default: rc = solve_reliable<16>(B, nrhs, b_dev, x_dev); break;
+        }
+    }
+    for (int r0 = 0; !B->reliable && r0 < nrhs && rc == PL_OK; r0 += B->K) {
         const int nact = std::min(B->K, nrhs - r0);
         switch (B->K) {
             case 1: rc = solve_tile<1>(B, nact, b_dev + r0, x_dev + r0); break;
