@@ -351,7 +351,7 @@ int pl_batch_solver_solve(pl_batch_solver solver, int nrhs, const double* const*
  * libsrc/pylith/materials/Elasticity.cc:310-317), whose level smoother is PETSc's Chebyshev
  * iteration with bounds 0.1 and 1.1 times an estimated largest eigenvalue. */
 int pl_batch_solver_set_chebyshev(pl_batch_solver solver, int degree, double lower_ratio, int eig_iters);
-/* FP64 accuracy of the FP32 tile PCG. enable != 0 (the default, delta 0.1): reliable updates, one
+/* FP64 accuracy of the FP32 tile PCG. enable != 0 (the default, delta 0.01): reliable updates, one
  * FP32 PCG per right-hand side without restarts, whose iterated residual is replaced by the FP64
  * true residual (the FP32 correction added to the FP64 solution) whenever it has dropped by
  * `delta`; the solve ends when the true residual meets the base solver's rtol. enable == 0: FP64

@@ -778,7 +778,7 @@ struct pl_batch_solver_s {
     // each time it has dropped by reliable_delta; off: FP64 refinement that restarts the FP32 PCG
     // from each new FP64 residual until it has dropped by the solver's inner_rtol.
     bool reliable = true;
-    double reliable_delta = 0.1;
+    double reliable_delta = 0.01;
     int64_t reliable_updates = 0;
     // The solve runs on a private stream (graph capture is not possible on the legacy default
     // stream a caller may use), fenced against the caller's stream with events.

@@ -391,9 +391,10 @@ class BatchSolver:
         check(C.lib().pl_batch_solver_set_chebyshev(self.handle, int(degree), float(lower_ratio), int(eig_iters)))
         self.degree = int(degree)
 
-    def set_reliable(self, enable: bool = True, delta: float = 0.1) -> None:
+    def set_reliable(self, enable: bool = True, delta: float = 0.01) -> None:
         """FP64 accuracy of the FP32 tile PCG: reliable updates (residual replacement whenever the
-        iterated residual has dropped by `delta`; the default) or restarted iterative refinement."""
+        iterated residual has dropped by `delta`; the default, with delta 0.01) or restarted
+        iterative refinement."""
         check(C.lib().pl_batch_solver_set_reliable(self.handle, 1 if enable else 0, float(delta)))
         self.reliable = bool(enable)
 
