@@ -508,6 +508,316 @@ __global__ void __launch_bounds__(SumFact::WARPS * 32) k_hex27_sumfact(DomainPar
     }
 }
 
+// Q2 hexahedra by sum factorisation with one 1-D line of 3 points per lane: a warp holds 3
+// cells, 9 lanes each. A 1-D pass along a line runs in the lane's registers; the values move
+// through shared memory only when the pass direction changes (x-lines, y-lines, z-lines: lane l
+// of a cell owns the line with fixed indices (l % 3, l / 3) in the other two directions). The
+// pointwise stage runs on the z-lines, each lane evaluating its line's 3 Gauss points one after
+// the other. Compared with one point per lane (k_hex27_sumfact, where every pass reads three
+// neighbours from a stage buffer and writes one value), this moves each staged value through
+// shared memory once per direction change instead of once per pass.
+struct Lines {
+    static constexpr int WARPS = 2;
+    static constexpr int T_D = 9, T_W = 18, T_END = 18 + 27;  // B[3][3], D[3][3] (point i, node a), weights[27]
+    // per cell: A and Bf stage buffers [12][27] each, corner coordinates [8][3]. The cell stride,
+    // 11 modulo the 16 eight-byte bank pairs, staggers the three cells of a warp; with the point
+    // orders of the kernel a warp's line accesses take 2 or 3 shared-memory wavefronts (2 is the
+    // least for 27 eight-byte accesses).
+    static constexpr int O_B = 12 * 27, O_X = 24 * 27, CS = 683;
+    static_assert(CS >= O_X + 24 && CS % 16 == 11, "cell stride");
+    static constexpr size_t smem_bytes() { return sizeof(double) * ((size_t)T_END + (size_t)WARPS * 3 * CS); }
+};
+
+template <int RHEO, bool BF, int OP>
+__global__ void __launch_bounds__(Lines::WARPS * 32) k_hex27_lines(DomainParams p) {
+    using LN = Lines;
+    using L = AuxLayout<RHEO, BF>;
+    const AuxOffsets<RHEO, BF> aoff;
+    extern __shared__ __align__(16) double lsm[];
+    double* tB = lsm;
+    double* tD = lsm + LN::T_D;
+    double* tW = lsm + LN::T_W;
+    for (int i = threadIdx.x; i < 9; i += blockDim.x) {
+        const double x = gauss3_x(i / 3);
+        tB[i] = quad_v(i % 3, x);
+        tD[i] = quad_d(i % 3, x);
+    }
+    for (int q = threadIdx.x; q < 27; q += blockDim.x) tW[q] = gauss3_w(q % 3) * gauss3_w((q / 3) % 3) * gauss3_w(q / 9);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool inwarp = lane < 27;
+    const int g = inwarp ? lane / 9 : 0, l = inwarp ? lane - 9 * (lane / 9) : 0;
+    const int la = l % 3, lb = l / 3;
+    double* cb = lsm + LN::T_END + (warp * 3 + g) * LN::CS;
+    double* A = cb;
+    double* Bf = cb + LN::O_B;
+    double* sX = cb + LN::O_X;
+    const double* __restrict__ field = OP == OP_RESIDUAL ? p.u : p.v;
+    // Position of point (i0, i1, i2) in a stage buffer: two orders, each keeping both the
+    // writing and the reading lines of its transposes on distinct banks within a cell
+    // (i0 + 3 i1 + 9 i2 would put a y-line's 9 lanes on 7 bank pairs).
+    auto iy = [](int a0, int a1, int a2) { return a0 + 9 * a1 + 3 * a2; };  // x <-> y transposes
+    auto iz = [](int a0, int a1, int a2) { return 3 * a0 + a1 + 9 * a2; };  // y <-> z and the z stage
+    const int64_t stride = (int64_t)gridDim.x * LN::WARPS * 3;
+    // every lane of a warp runs the same number of passes (the __syncwarp calls need them all)
+    for (int64_t c0 = ((int64_t)blockIdx.x * LN::WARPS + warp) * 3; c0 < p.ncells; c0 += stride) {
+        const int64_t c = c0 + g;
+        const bool live = inwarp && c < p.ncells;
+        const int64_t mc = live ? (p.cell_ids ? p.cell_ids[c] : c) : 0;
+        // x-line (i1, i2) = (la, lb): the nodes a + 3 la + 9 lb
+        int nodes[3] = {0, 0, 0};
+        double u[3][3];
+        if (live) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                nodes[a] = p.cells[mc * 27 + a + 3 * la + 9 * lb];
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) u[a][cc] = field[3 * (int64_t)nodes[a] + cc];
+            }
+            if (l < 8) {
+                const int cn = p.cells[mc * 27 + Elem<HEX27>::corner(l)];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) sX[l * 3 + k] = p.coords[3 * (int64_t)cn + k];
+            }
+            // forward x: B u and D u along the line
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    double vb = 0.0, vd = 0.0;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        vb += tB[i * 3 + a] * u[a][cc];
+                        vd += tD[i * 3 + a] * u[a][cc];
+                    }
+                    A[cc * 27 + iy(i, la, lb)] = vb;
+                    A[(3 + cc) * 27 + iy(i, la, lb)] = vd;
+                }
+        }
+        __syncwarp();
+        // forward y on y-lines (i0, i2) = (la, lb): BB, BD (y derivative), DB (x derivative)
+        if (live) {
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                double bx[3], dx[3];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    bx[b] = A[cc * 27 + iy(la, b, lb)];
+                    dx[b] = A[(3 + cc) * 27 + iy(la, b, lb)];
+                }
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double bb = 0.0, bd = 0.0, db = 0.0;
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        bb += tB[j * 3 + b] * bx[b];
+                        bd += tD[j * 3 + b] * bx[b];
+                        db += tB[j * 3 + b] * dx[b];
+                    }
+                    Bf[cc * 27 + iz(la, j, lb)] = bb;
+                    Bf[(3 + cc) * 27 + iz(la, j, lb)] = bd;
+                    Bf[(6 + cc) * 27 + iz(la, j, lb)] = db;
+                }
+            }
+        }
+        __syncwarp();
+        // z-lines (i0, i1) = (la, lb): forward z, geometry and the pointwise function at the
+        // line's 3 Gauss points; the test-function weights go to A at the points' positions
+        if (live) {
+            double a[L::size] = {};
+            L::load_cell(p, c, a);
+#pragma unroll 1
+            for (int k = 0; k < 3; ++k) {
+                const int q = la + 3 * lb + 9 * k;
+                double Gr[3][3];
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+                    for (int c3 = 0; c3 < 3; ++c3) {
+                        const int pt = iz(la, lb, c3);
+                        gx += tB[k * 3 + c3] * Bf[(6 + cc) * 27 + pt];
+                        gy += tB[k * 3 + c3] * Bf[(3 + cc) * 27 + pt];
+                        gz += tD[k * 3 + c3] * Bf[cc * 27 + pt];
+                    }
+                    Gr[cc][0] = gx;
+                    Gr[cc][1] = gy;
+                    Gr[cc][2] = gz;
+                }
+                double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+                for (int cr = 0; cr < 8; ++cr) {
+                    double d[3];
+                    hex_corner_dN<3>(cr, la, lb, k, d);
+#pragma unroll
+                    for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+                        for (int jj = 0; jj < 3; ++jj) J[ii][jj] += sX[cr * 3 + ii] * d[jj];
+                }
+                double inv[3][3];
+                const double detJ = invert3(J, inv);
+                if (!(detJ > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+                const double wdetJ = tW[q] * detJ;
+                double s_x[9];
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                    for (int e = 0; e < 3; ++e)
+                        s_x[cc * 3 + e] = Gr[cc][0] * inv[0][e] + Gr[cc][1] * inv[1][e] + Gr[cc][2] * inv[2][e];
+                if (OP == OP_RESIDUAL) L::load_qp(p, c, q, 27, a);  // the tangents read no state
+                double x[3] = {0, 0, 0}, s3[3] = {0, 0, 0};
+                double f0[3] = {0, 0, 0}, f1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                if (OP == OP_RESIDUAL) {
+                    if (BF) {
+                        const int sOff[1] = {0}, sOff_x[1] = {0};
+                        pw::g0v_bodyforce<double>(3, 1, L::numA, sOff, sOff_x, s3, nullptr, s_x, aoff.v, nullptr, a,
+                                                  nullptr, nullptr, p.t, x, p.num_constants, p.constants, f0);
+                    }
+                    call_f1<RHEO>(L::numA, aoff.v, a, s3, s_x, p, x, f1);
+                } else {
+                    double Jf3[81];
+#pragma unroll
+                    for (int ii = 0; ii < 81; ++ii) Jf3[ii] = 0.0;
+                    call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
+#pragma unroll
+                    for (int f = 0; f < 3; ++f)
+#pragma unroll
+                        for (int df = 0; df < 3; ++df) {
+                            double acc1 = 0.0;
+#pragma unroll
+                            for (int gg = 0; gg < 3; ++gg)
+#pragma unroll
+                                for (int dg = 0; dg < 3; ++dg)
+                                    acc1 += Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
+                            f1[f * 3 + df] = acc1;
+                        }
+                }
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        A[(cc * 3 + d) * 27 + iz(la, lb, k)] =
+                            wdetJ * (inv[d][0] * f1[cc * 3 + 0] + inv[d][1] * f1[cc * 3 + 1] + inv[d][2] * f1[cc * 3 + 2]);
+                    if (BF && OP == OP_RESIDUAL) A[(9 + cc) * 27 + iz(la, lb, k)] = wdetJ * f0[cc];
+                }
+            }
+            // reverse z on the same line (this lane's own points): Tx, Ty, Tz, T0 into Bf
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                double wx[3], wy[3], wz[3], w0[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const int pt = iz(la, lb, k);
+                    wx[k] = A[(cc * 3 + 0) * 27 + pt];
+                    wy[k] = A[(cc * 3 + 1) * 27 + pt];
+                    wz[k] = A[(cc * 3 + 2) * 27 + pt];
+                    w0[k] = (BF && OP == OP_RESIDUAL) ? A[(9 + cc) * 27 + pt] : 0.0;
+                }
+#pragma unroll
+                for (int c3 = 0; c3 < 3; ++c3) {
+                    double tx = 0.0, ty = 0.0, tz = 0.0, t0 = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const double bk = tB[k * 3 + c3], dk = tD[k * 3 + c3];
+                        tx += bk * wx[k];
+                        ty += bk * wy[k];
+                        tz += dk * wz[k];
+                        if (BF && OP == OP_RESIDUAL) t0 += bk * w0[k];
+                    }
+                    const int pt = iz(la, lb, c3);
+                    Bf[cc * 27 + pt] = tx;
+                    Bf[(3 + cc) * 27 + pt] = ty;
+                    Bf[(6 + cc) * 27 + pt] = tz + t0;
+                }
+            }
+        }
+        __syncwarp();
+        // reverse y on y-lines (i0, i2) = (la, lb): QD (x-derivative channel), QB (the others)
+        if (live) {
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                double tx[3], ty[3], tz[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int pt = iz(la, j, lb);
+                    tx[j] = Bf[cc * 27 + pt];
+                    ty[j] = Bf[(3 + cc) * 27 + pt];
+                    tz[j] = Bf[(6 + cc) * 27 + pt];
+                }
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    double px = 0.0, py = 0.0, pz = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const double bj = tB[j * 3 + b], dj = tD[j * 3 + b];
+                        px += bj * tx[j];
+                        py += dj * ty[j];
+                        pz += bj * tz[j];
+                    }
+                    const int pt = iy(la, b, lb);
+                    A[cc * 27 + pt] = px;
+                    A[(3 + cc) * 27 + pt] = py + pz;
+                }
+            }
+        }
+        __syncwarp();
+        // reverse x on x-lines (i1, i2) = (la, lb): node values, added into the output
+        if (live) {
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                double qd[3], qb[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    qd[i] = A[cc * 27 + iy(i, la, lb)];
+                    qb[i] = A[(3 + cc) * 27 + iy(i, la, lb)];
+                }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    double r = 0.0;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) r += tD[i * 3 + a] * qd[i] + tB[i * 3 + a] * qb[i];
+                    red_add(p.out + 3 * (int64_t)nodes[a] + cc, r);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int RHEO, bool BF, int OP>
+static void launch_lines_t(const DomainParams& p, cudaStream_t s) {
+    auto kern = k_hex27_lines<RHEO, BF, OP>;
+    const size_t smem = Lines::smem_bytes();
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Lines::WARPS * 32, smem);
+    const int64_t blocks = (p.ncells + 3 * Lines::WARPS - 1) / (3 * Lines::WARPS);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)nsm * std::max(per_sm, 1)));
+    kern<<<grid, Lines::WARPS * 32, smem, s>>>(p);
+    count_launch();
+}
+
+#ifndef PLB_Q2_LINES
+#define PLB_Q2_LINES 1
+#endif
+
+static void launch_lines(const DomainParams& p, int rheo, bool bf, int op, cudaStream_t s) {
+    if (op == OP_RESIDUAL) {
+        if (rheo == RHEO_ILE) {
+            if (bf) launch_lines_t<RHEO_ILE, true, OP_RESIDUAL>(p, s);
+            else launch_lines_t<RHEO_ILE, false, OP_RESIDUAL>(p, s);
+        } else {
+            if (bf) launch_lines_t<RHEO_GENMAXWELL, true, OP_RESIDUAL>(p, s);
+            else launch_lines_t<RHEO_GENMAXWELL, false, OP_RESIDUAL>(p, s);
+        }
+    } else {
+        if (rheo == RHEO_ILE) launch_lines_t<RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, s);
+        else launch_lines_t<RHEO_GENMAXWELL, false, OP_JACOBIAN_ACTION>(p, s);
+    }
+}
+
 template <int RHEO, bool BF, int OP, typename T = double>
 static void launch_sumfact_t(const DomainParams& p, cudaStream_t s) {
     auto kern = k_hex27_sumfact<RHEO, BF, OP, T>;
@@ -577,6 +887,7 @@ static void launch_sumfact(const DomainParams& p, int rheo, bool bf, int op, cud
 bool launch_domain_apply_hexgroup(const DomainParams& p, int cell, int rheo, bool bf, int op, cudaStream_t s) {
     if (p.ncells == 0) return true;
     if (cell == HEX8) launch_group_cell<HEX8>(p, rheo, bf, op, s);
+    else if (cell == HEX27 && PLB_Q2_LINES) launch_lines(p, rheo, bf, op, s);
     else if (cell == HEX27 && PLB_Q2_SUMFACT) launch_sumfact(p, rheo, bf, op, s);
     else if (cell == HEX27) launch_group_cell<HEX27>(p, rheo, bf, op, s);
     else return false;
