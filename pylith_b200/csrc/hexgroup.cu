@@ -47,6 +47,23 @@ struct HexGroup {
     }
 };
 
+// f1 = Jf3 : s_x for the registered tangent of either rheology on this path. Both are isotropic,
+// Jf3 = -C with C = lambda d_ij d_kl + mu (d_ik d_jl + d_il d_jk) (generalized Maxwell with its
+// effective shear modulus), so the tangent is evaluated by its registered function and contracted
+// in closed form from its (f,g,df,dg) = (0,1,0,1) and (0,1,1,0) entries, -lambda and -mu: 12
+// multiply-adds instead of 81 (the 81-entry contraction cannot drop its zero entries).
+template <int RHEO, typename T>
+PL_D void isotropic_jf3_contract(const double Jf3[81], const T s_x[9], T f1[9]) {
+    static_assert(RHEO == RHEO_ILE || RHEO == RHEO_GENMAXWELL, "isotropic tangents only");
+    const T lam = (T)(-Jf3[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
+    const T mu = (T)(-Jf3[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
+    const T ltr = lam * (s_x[0] + s_x[4] + s_x[8]);
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int df = 0; df < 3; ++df) f1[f * 3 + df] = -(mu * (s_x[f * 3 + df] + s_x[df * 3 + f]) + (f == df ? ltr : T(0)));
+}
+
 template <int CELL, typename T>
 PL_D void fill_tables(double* t64, T* tt) {
     using H = HexGroup<CELL, T>;
@@ -184,18 +201,7 @@ __global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(Dom
 #pragma unroll
                 for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
                 call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
-#pragma unroll
-                for (int f = 0; f < 3; ++f)
-#pragma unroll
-                    for (int df = 0; df < 3; ++df) {
-                        T acc1 = 0;
-#pragma unroll
-                        for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                            for (int dg = 0; dg < 3; ++dg)
-                                acc1 += (T)Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                        f1[f * 3 + df] = acc1;
-                    }
+                isotropic_jf3_contract<RHEO>(Jf3, s_x, f1);
             }
             // test-function weights: grad(phi_n) . f1 = tB_n . (J^{-1} f1^T), so stage
             // W[cc][d] = wdetJ sum_e inv[d][e] f1[cc][e]
@@ -404,17 +410,7 @@ __global__ void __launch_bounds__(SumFact::WARPS * 32) k_hex27_sumfact(DomainPar
 #pragma unroll
                 for (int ii = 0; ii < 81; ++ii) Jf3[ii] = 0.0;
                 call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
-#pragma unroll
-                for (int f = 0; f < 3; ++f)
-#pragma unroll
-                    for (int df = 0; df < 3; ++df) {
-                        double acc1 = 0.0;
-#pragma unroll
-                        for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                            for (int dg = 0; dg < 3; ++dg) acc1 += Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                        f1[f * 3 + df] = acc1;
-                    }
+                isotropic_jf3_contract<RHEO>(Jf3, s_x, f1);
             }
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) {
@@ -679,18 +675,7 @@ __global__ void __launch_bounds__(Lines::WARPS * 32) k_hex27_lines(DomainParams 
 #pragma unroll
                     for (int ii = 0; ii < 81; ++ii) Jf3[ii] = 0.0;
                     call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
-#pragma unroll
-                    for (int f = 0; f < 3; ++f)
-#pragma unroll
-                        for (int df = 0; df < 3; ++df) {
-                            double acc1 = 0.0;
-#pragma unroll
-                            for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                                for (int dg = 0; dg < 3; ++dg)
-                                    acc1 += Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                            f1[f * 3 + df] = acc1;
-                        }
+                    isotropic_jf3_contract<RHEO>(Jf3, s_x, f1);
                 }
 #pragma unroll
                 for (int cc = 0; cc < 3; ++cc) {
