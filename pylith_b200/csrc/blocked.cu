@@ -200,17 +200,7 @@ PL_D void tet_cell_element(const DomainParams& p, const int* aoff, const double*
 #pragma unroll
         for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
         call_jf3<RHEO>(L::numA, aoff, a, p, x, Jf3);
-#pragma unroll
-        for (int f = 0; f < 3; ++f)
-#pragma unroll
-            for (int df = 0; df < 3; ++df) {
-                double acc1 = 0.0;
-#pragma unroll
-                for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                    for (int dg = 0; dg < 3; ++dg) acc1 += Jf3[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                f1[f * 3 + df] = acc1;
-            }
+        isotropic_jf3_contract<RHEO>(Jf3, s_x, f1);
     }
     // corners 1..3: |J|/6 * f1 . grad(phi_a) = f1 . cof_{a-1} / 6; corner 0: minus their sum,
     // plus the body-force term |J|/6 * f0 / 4 at every corner.
@@ -401,18 +391,7 @@ __global__ void __launch_bounds__(kTetBlockCells, 4) k_tet_blocked_jv32(DomainPa
                 for (int d = 0; d < 3; ++d) s_x[cc * 3 + d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
             }
             float f1[9];
-#pragma unroll
-            for (int f = 0; f < 3; ++f)
-#pragma unroll
-                for (int df = 0; df < 3; ++df) {
-                    float acc1 = 0.0f;
-#pragma unroll
-                    for (int gg = 0; gg < 3; ++gg)
-#pragma unroll
-                        for (int dg = 0; dg < 3; ++dg)
-                            acc1 += (float)Jf3d[((f * 3 + gg) * 3 + df) * 3 + dg] * s_x[gg * 3 + dg];
-                    f1[f * 3 + df] = acc1;
-                }
+            isotropic_jf3_contract<RHEO_ILE>(Jf3d, s_x, f1);
             float e0[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int k = 0; k < 3; ++k)

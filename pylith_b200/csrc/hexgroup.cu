@@ -47,23 +47,6 @@ struct HexGroup {
     }
 };
 
-// f1 = Jf3 : s_x for the registered tangent of either rheology on this path. Both are isotropic,
-// Jf3 = -C with C = lambda d_ij d_kl + mu (d_ik d_jl + d_il d_jk) (generalized Maxwell with its
-// effective shear modulus), so the tangent is evaluated by its registered function and contracted
-// in closed form from its (f,g,df,dg) = (0,1,0,1) and (0,1,1,0) entries, -lambda and -mu: 12
-// multiply-adds instead of 81 (the 81-entry contraction cannot drop its zero entries).
-template <int RHEO, typename T>
-PL_D void isotropic_jf3_contract(const double Jf3[81], const T s_x[9], T f1[9]) {
-    static_assert(RHEO == RHEO_ILE || RHEO == RHEO_GENMAXWELL, "isotropic tangents only");
-    const T lam = (T)(-Jf3[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
-    const T mu = (T)(-Jf3[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
-    const T ltr = lam * (s_x[0] + s_x[4] + s_x[8]);
-#pragma unroll
-    for (int f = 0; f < 3; ++f)
-#pragma unroll
-        for (int df = 0; df < 3; ++df) f1[f * 3 + df] = -(mu * (s_x[f * 3 + df] + s_x[df * 3 + f]) + (f == df ? ltr : T(0)));
-}
-
 template <int CELL, typename T>
 PL_D void fill_tables(double* t64, T* tt) {
     using H = HexGroup<CELL, T>;
