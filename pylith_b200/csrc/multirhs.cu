@@ -496,10 +496,10 @@ __global__ void __launch_bounds__(kBThreads) k_b_pq(const float* p, const float*
     if (fin.counter && take_last_ticket(fin.counter)) sum_partials_last_block<K>(part, fin.out_a, fin.prev_a);
 }
 
-// alpha_k = active_k ? rz_k / pq_k : 0; x += alpha p; r += alpha q; z = P r; partial rz, rr.
+// alpha_k = active_k ? rz_k / pq_k : 0; r += alpha q; z = P r; partial rz, rr (x is updated by k_b_pupdate).
 // One thread per (node, rhs).
 template <int K>
-__global__ void __launch_bounds__(kBThreads) k_b_update(float* x, float* r, const float* p, const float* q, float* z,
+__global__ void __launch_bounds__(kBThreads) k_b_update(float* r, const float* q, float* z,
                                                         const uint8_t* mask, const float* P, int64_t nnodes,
                                                         const double* rz, const double* pq, const int* active,
                                                         double* part_rz, double* part_rr, FinSpec fin) {
@@ -512,7 +512,6 @@ __global__ void __launch_bounds__(kBThreads) k_b_update(float* x, float* r, cons
         for (int c = 0; c < 3; ++c) {
             if (mask[3 * nd + c]) continue;
             const int64_t i = (3 * nd + c) * K + k;
-            x[i] += alpha * p[i];
             r[i] += alpha * q[i];
         }
         float zz[3];
@@ -535,13 +534,20 @@ __global__ void __launch_bounds__(kBThreads) k_b_update(float* x, float* r, cons
     }
 }
 
-// beta_k = rz_k / rz_old_k; p = z + beta p
+// x += alpha p (free DOFs; alpha_k = rz_old_k / pq_k, the step of this iteration, whose r.z is
+// rz_old now) and then p = z + beta p, beta_k = rz_k / rz_old_k: the solution update rides on the
+// pass that reads p anyway.
 template <int K>
-__global__ void k_b_pupdate(float* p, const float* z, int64_t n, const double* rz, const double* rz_old, const int* active) {
+__global__ void k_b_pupdate(float* x, float* p, const float* z, const uint8_t* mask, int64_t n, const double* rz,
+                            const double* rz_old, const double* pq, const int* active) {
     const int k = threadIdx.x % K;
+    const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz_old[k] / pq[k]) : 0.0f;
     const float beta = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
-        p[e] = z[e] + beta * p[e];
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
+        const float pe = p[e];
+        if (!mask[e / K]) x[e] += alpha * pe;
+        p[e] = z[e] + beta * pe;
+    }
 }
 
 // ---- Chebyshev-Jacobi preconditioner: z = q(P A) P r, with A = -J and the point-block
@@ -557,9 +563,10 @@ PL_D void pinv_local(const float* __restrict__ P, int64_t node, const float in[3
     out[2] = B[6] * in[0] + B[7] * in[1] + B[8] * in[2];
 }
 
-// x += alpha p; r += alpha q on free DOFs; partial r.r (the preconditioner runs after).
+// r += alpha q on free DOFs; partial r.r (the preconditioner runs after; x is updated by
+// k_b_pupdate).
 template <int K>
-__global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* x, float* r, const float* p, const float* q,
+__global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* r, const float* q,
                                                            const uint8_t* mask, int64_t n, const double* rz,
                                                            const double* pq, const int* active, double* part_rr,
                                                            FinSpec fin) {
@@ -568,7 +575,6 @@ __global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* x, float* r, c
     double srr = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
         if (mask[e / K]) continue;
-        x[e] += alpha * p[e];
         const float ri = r[e] + alpha * q[e];
         r[e] = ri;
         srr += (double)ri * ri;
@@ -886,8 +892,8 @@ int pcg_iteration(pl_batch_solver B) {
         FinSpec frr;
         frr.counter = B->ticket;
         frr.out_a = rr;
-        k_b_update_xr<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, S->d_mask, B->n, rz, pq, B->active,
-                                                        B->part_b, frr);
+        k_b_update_xr<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->q, S->d_mask, B->n, rz, pq, B->active, B->part_b,
+                                                        frr);
         count_launch();
         FinSpec frz;
         frz.counter = B->ticket;
@@ -901,11 +907,11 @@ int pcg_iteration(pl_batch_solver B) {
         fu.out_a = rz;
         fu.prev_a = rz_old;
         fu.out_b = rr;
-        k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->r, B->p, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes,
-                                                     rz, pq, B->active, B->part_a, B->part_b, fu);
+        k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes, rz, pq,
+                                                     B->active, B->part_a, B->part_b, fu);
         count_launch();
     }
-    k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->z, B->n, rz, rz_old, B->active);
+    k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->p, B->z, S->d_mask, B->n, rz, rz_old, pq, B->active);
     count_launch(2);
     return PL_OK;
 }
