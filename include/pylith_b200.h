@@ -172,7 +172,8 @@ void* pl_fekernel_lookup(const char* name);
 /* ---- context -------------------------------------------------------------------------- */
 int pl_context_create(int device, pl_context* out);
 /* Destroy calls may come in any order: an object still referenced by a dependent one (a mesh by
- * an integrator, a context by a mesh) is released when its last dependent is destroyed. */
+ * an integrator, a context by a mesh, a solver by a batched solver) is released when its last
+ * dependent is destroyed. A solver uses its integrators until it is destroyed. */
 int pl_context_destroy(pl_context ctx);
 /* Enqueue all work on a caller-owned cudaStream_t; NULL is CUDA's legacy default stream
  * (torch's default stream). A new context starts on its own non-blocking stream. */

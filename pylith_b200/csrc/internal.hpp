@@ -73,12 +73,15 @@ struct BlockedLayout {
 
 void mesh_retain(pl_mesh_s* m);
 void mesh_release(pl_mesh_s* m);
+void solver_retain(pl_solver_s* S);
+void solver_release(pl_solver_s* S);
 
 }  // namespace plb
 
 // Object lifetimes: meshes hold a reference on their context, integrators, matrices and solvers
-// on their mesh; a destroy request on an object that is still referenced is deferred until the
-// last dependent object is destroyed, so any destroy order is safe.
+// on their mesh, batched solvers on their solver; a destroy request on an object that is still
+// referenced is deferred until the last dependent object is destroyed, so any destroy order is
+// safe.
 struct pl_context_s {
     int refs = 0;
     bool destroy_requested = false;
@@ -159,6 +162,8 @@ struct pl_matrix_s {
 // Device Krylov solver state (csrc/solver.cu); the batched solver (csrc/multirhs.cu) reuses its
 // operator, mask, preconditioner and fault pairs.
 struct pl_solver_s {
+    int refs = 0;
+    bool destroy_requested = false;
     pl_mesh mesh = nullptr;
     std::vector<pl_integrator> ops;
     int64_t n = 0;       // DOFs (3 per node)

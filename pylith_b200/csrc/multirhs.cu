@@ -1308,6 +1308,7 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     B->n = base->n;
     B->nnodes = base->nnodes;
     mesh_retain(base->mesh);
+    solver_retain(base);
     cudaError_t e = cudaSuccess;
     auto A = [&](auto** p, size_t cnt) {
         if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(**p));
@@ -1449,8 +1450,10 @@ int pl_batch_solver_destroy(pl_batch_solver B) {
     void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64, B->res, B->d, B->ticket};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    pl_solver base = B->base;
     delete B;
     mesh_release(m);
+    solver_release(base);
     return PL_OK;
 }
 

@@ -832,8 +832,9 @@ int pl_solver_get_stats(pl_solver S, int* iterations, int* inner_iterations, int
     return PL_OK;
 }
 
-int pl_solver_destroy(pl_solver S) {
-    if (!S) return PL_OK;
+}  // extern "C"
+
+static void solver_free(pl_solver S) {
     cudaSetDevice(S->mesh->ctx->device);
     cudaStreamSynchronize(S->mesh->ctx->stream);
     for (cudaGraphExec_t g : S->graph)
@@ -850,6 +851,24 @@ int pl_solver_destroy(pl_solver S) {
     pl_mesh m = S->mesh;
     delete S;
     mesh_release(m);
+}
+
+namespace plb {
+void solver_retain(pl_solver_s* S) { S->refs++; }
+void solver_release(pl_solver_s* S) {
+    if (--S->refs == 0 && S->destroy_requested) solver_free(S);
+}
+}  // namespace plb
+
+extern "C" {
+
+int pl_solver_destroy(pl_solver S) {
+    if (!S) return PL_OK;
+    if (S->refs > 0) {
+        S->destroy_requested = true;
+        return PL_OK;
+    }
+    solver_free(S);
     return PL_OK;
 }
 

@@ -462,3 +462,36 @@ def test_fp32_reliable_updates_and_restarted_refinement_match_the_oracle(ctx, or
         inner[reliable] = st["inner_iterations"]
         S.close()
     assert inner[True] <= inner[False], inner
+
+
+def test_handles_can_be_destroyed_in_any_order():
+    """Handles are reference-counted: closing the context, mesh and solver before the batched
+    solver that uses them defers their release to the batched solver's destroy, which still solves
+    and then frees everything (the order in which a garbage collector may run finalizers)."""
+    import torch
+    from pylith_b200 import feassemble as FA
+
+    mesh = M.box_tet_kuhn(4, 4, 3, seed=2)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=2)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg")] = True
+    cons = cons.ravel()
+    c = FA.Context(0)
+    dm = FA.DeviceMesh(c, mesh)
+    ig = mat.create_integrator(dm)
+    S = FA.Solver(dm, cons, [ig], rtol=1e-10, precision=FA.Solver.FP32_REFINED, inner_rtol=1e-4)
+    S.setup()
+    B = FA.BatchSolver(S, 4)
+    b = torch.from_numpy(np.random.default_rng(1).standard_normal(dm.num_dof) * ~cons).cuda()
+    x0 = torch.zeros_like(b)
+    B.solve([b], [x0])
+    S.close()
+    dm.close()
+    c.close()
+    x1 = torch.zeros_like(b)
+    B.solve([b], [x1])
+    torch.cuda.synchronize()
+    assert float(torch.linalg.norm(x1 - x0)) <= 1e-8 * float(torch.linalg.norm(x0)) and float(torch.linalg.norm(x0)) > 0.0
+    B.close()
+    ig.close()
