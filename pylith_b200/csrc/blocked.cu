@@ -19,6 +19,7 @@
 #include <cuda_pipeline.h>
 
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "domain_kernels.cuh"
@@ -545,6 +546,142 @@ bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, i
     return true;
 }
 
+// Host: bank-aware numbering of one block's local nodes and order of their incidence sums.
+//
+// The kernels keep node values component-major in shared memory, so the bank pair of node i in
+// an FP64 array is i mod 16 (and the 16-byte bank group of an FP32 row of 28 floats is 7 i mod 8):
+// the 32 reads of one corner by a warp's 32 cells conflict when distinct nodes share an index
+// residue. Starting from the nodes sorted by global id, a local search over swaps of two nodes'
+// indices (deterministic, seeded by the block index) lowers the sum over (warp, corner) of the
+// largest number of distinct nodes on one residue. Within each residue class the nodes are then
+// placed by decreasing incidence count, so each warp of the per-node sums gets nodes of similar
+// counts and runs fewer steps. Finally each node's incidences are ordered, warp by warp and step
+// by step, so that the staged element entries read in one step (bank pair = cell mod 16) spread
+// over the banks. Any fixed order keeps the sums identical from run to run.
+struct BlockPlan {
+    std::vector<int32_t> loc;     // global ids of the local nodes, sorted
+    std::vector<int32_t> newidx;  // local index of loc[l]
+    std::vector<uint16_t> inc;    // incidence entries (cell * 4 + corner) by local index
+    std::vector<uint32_t> off;    // [nloc + 1] offsets into inc
+};
+
+static uint64_t splitmix64(uint64_t& x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static void plan_block(const int32_t* bc, int ncell, uint64_t seed, BlockPlan& P) {
+    constexpr int R = 16, W = 32, kIters = 4000;
+    P.loc.assign(bc, bc + 4 * (size_t)ncell);
+    std::sort(P.loc.begin(), P.loc.end());
+    P.loc.erase(std::unique(P.loc.begin(), P.loc.end()), P.loc.end());
+    const int nloc = (int)P.loc.size();
+    std::vector<int> lcs(4 * (size_t)ncell);
+    for (int i = 0; i < 4 * ncell; ++i)
+        lcs[i] = (int)(std::lower_bound(P.loc.begin(), P.loc.end(), bc[i]) - P.loc.begin());
+    // groups: (warp of cells, corner) -> distinct nodes; each node's groups
+    const int ng = (ncell + W - 1) / W * 4;
+    std::vector<std::vector<int>> node_groups(nloc);
+    std::vector<int> stamp(nloc, -1);
+    for (int g = 0; g < ng; ++g) {
+        const int w = g / 4, k = g % 4;
+        for (int c = w * W; c < std::min(ncell, (w + 1) * W); ++c) {
+            const int l = lcs[4 * c + k];
+            if (stamp[l] != g) {
+                stamp[l] = g;
+                node_groups[l].push_back(g);
+            }
+        }
+    }
+    std::vector<int>& perm = P.newidx;
+    perm.resize(nloc);
+    for (int l = 0; l < nloc; ++l) perm[l] = l;
+    std::vector<int> cnt((size_t)ng * R, 0);
+    for (int l = 0; l < nloc; ++l)
+        for (int g : node_groups[l]) cnt[(size_t)g * R + (perm[l] & (R - 1))]++;
+    auto gmax = [&](int g) {
+        int m = 0;
+        for (int r = 0; r < R; ++r) m = std::max(m, cnt[(size_t)g * R + r]);
+        return m;
+    };
+    auto move = [&](int l, int from, int to) {
+        for (int g : node_groups[l]) {
+            cnt[(size_t)g * R + from]--;
+            cnt[(size_t)g * R + to]++;
+        }
+    };
+    std::vector<int> mark(ng, -1), aff;
+    uint64_t rs = seed;
+    for (int it = 0; it < kIters && nloc > 1; ++it) {
+        const int a = (int)(splitmix64(rs) % (uint64_t)nloc), b = (int)(splitmix64(rs) % (uint64_t)nloc);
+        const int ra = perm[a] & (R - 1), rb = perm[b] & (R - 1);
+        if (ra == rb) continue;
+        aff.clear();
+        for (int g : node_groups[a])
+            if (mark[g] != it) mark[g] = it, aff.push_back(g);
+        for (int g : node_groups[b])
+            if (mark[g] != it) mark[g] = it, aff.push_back(g);
+        int before = 0, after = 0;
+        for (int g : aff) before += gmax(g);
+        move(a, ra, rb);
+        move(b, rb, ra);
+        for (int g : aff) after += gmax(g);
+        if (after <= before) {
+            std::swap(perm[a], perm[b]);
+        } else {
+            move(a, rb, ra);
+            move(b, ra, rb);
+        }
+    }
+    // within each residue class: decreasing incidence count
+    std::vector<int> deg(nloc, 0);
+    for (int i = 0; i < 4 * ncell; ++i) deg[lcs[i]]++;
+    for (int r = 0; r < R; ++r) {
+        std::vector<int> nodes, slots;
+        for (int l = 0; l < nloc; ++l)
+            if ((perm[l] & (R - 1)) == r) nodes.push_back(l), slots.push_back(perm[l]);
+        std::sort(slots.begin(), slots.end());
+        std::stable_sort(nodes.begin(), nodes.end(), [&](int x, int y) { return deg[x] > deg[y]; });
+        for (size_t i = 0; i < nodes.size(); ++i) perm[nodes[i]] = slots[i];
+    }
+    // incidences by new index, in (cell, corner) order, then ordered warp by warp
+    std::vector<std::vector<int>> lists(nloc);
+    for (int c = 0; c < ncell; ++c)
+        for (int k = 0; k < 4; ++k) lists[perm[lcs[4 * c + k]]].push_back(4 * c + k);
+    P.off.assign(nloc + 1, 0);
+    P.inc.clear();
+    P.inc.reserve(4 * (size_t)ncell);
+    for (int w0 = 0; w0 < nloc; w0 += W) {
+        const int nl = std::min(W, nloc - w0);
+        std::vector<std::vector<int>> ordered(nl);
+        std::vector<int> lanes(nl);
+        int depth = 0;
+        for (int i = 0; i < nl; ++i) depth = std::max(depth, (int)lists[w0 + i].size());
+        for (int j = 0; j < depth; ++j) {
+            int c16[R] = {0};
+            for (int i = 0; i < nl; ++i) lanes[i] = i;
+            std::stable_sort(lanes.begin(), lanes.end(),
+                             [&](int x, int y) { return lists[w0 + x].size() > lists[w0 + y].size(); });
+            for (int i : lanes) {
+                std::vector<int>& L = lists[w0 + i];
+                if (L.empty()) continue;
+                size_t best = 0;
+                for (size_t t = 1; t < L.size(); ++t)
+                    if (c16[(L[t] >> 2) & (R - 1)] < c16[(L[best] >> 2) & (R - 1)]) best = t;
+                c16[(L[best] >> 2) & (R - 1)]++;
+                ordered[i].push_back(L[best]);
+                L.erase(L.begin() + best);
+            }
+        }
+        for (int i = 0; i < nl; ++i) {
+            for (int e : ordered[i]) P.inc.push_back((uint16_t)e);
+            P.off[w0 + i + 1] = (uint32_t)P.inc.size();
+        }
+    }
+}
+
 // Host: block layout from the cell connectivity (cells should be in a locality-preserving order).
 int ensure_blocked_layout(pl_mesh_s* m) {
     if (m->blocked) return PL_OK;
@@ -564,36 +701,40 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     node_ids.reserve((size_t)nc);
     inc_off.reserve((size_t)nc + nb);
     int maxloc = 0;
-    std::vector<int32_t> loc;
-    std::vector<int> count;
+    // the blocks' numberings and incidence orders, planned in parallel
+    std::vector<BlockPlan> plans(nb);
+    {
+        const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 0; t < nth; ++t)
+            th.emplace_back([&, t] {
+                for (int64_t b = t; b < nb; b += nth) {
+                    const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
+                    plan_block(m->h_cells.data() + c0 * 4, (int)(c1 - c0), (uint64_t)b, plans[b]);
+                }
+            });
+        for (std::thread& x : th) x.join();
+    }
     for (int64_t b = 0; b < nb; ++b) {
+        BlockPlan& P = plans[b];
         const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
-        loc.assign(m->h_cells.begin() + c0 * 4, m->h_cells.begin() + c1 * 4);
-        std::sort(loc.begin(), loc.end());
-        loc.erase(std::unique(loc.begin(), loc.end()), loc.end());
-        maxloc = std::max<int>(maxloc, (int)loc.size());
+        const int nloc = (int)P.loc.size();
+        maxloc = std::max(maxloc, nloc);
         begin[b] = (int32_t)node_ids.size();
-        for (int32_t nd : loc) {
-            node_ids.push_back((uint32_t)nd);
-            nblocks_of[nd]++;
+        node_ids.resize(node_ids.size() + nloc);
+        for (int l = 0; l < nloc; ++l) {
+            node_ids[begin[b] + P.newidx[l]] = (uint32_t)P.loc[l];
+            nblocks_of[P.loc[l]]++;
         }
-        count.assign(loc.size() + 1, 0);
         for (int64_t c = c0; c < c1; ++c)
             for (int k = 0; k < 4; ++k) {
                 const int32_t nd = m->h_cells[c * 4 + k];
-                const int l = (int)(std::lower_bound(loc.begin(), loc.end(), nd) - loc.begin());
-                lconn[c * 4 + k] = (uint16_t)l;
-                count[l + 1]++;
+                const int l = (int)(std::lower_bound(P.loc.begin(), P.loc.end(), nd) - P.loc.begin());
+                lconn[c * 4 + k] = (uint16_t)P.newidx[l];
             }
-        for (size_t i = 0; i < loc.size(); ++i) count[i + 1] += count[i];
-        for (size_t i = 0; i <= loc.size(); ++i) inc_off.push_back((uint32_t)count[i]);
-        // incidence entries in (cell, corner) order for every node: a fixed summation order
-        std::vector<int> fill(count.begin(), count.end() - 1);
-        for (int64_t c = c0; c < c1; ++c)
-            for (int k = 0; k < 4; ++k) {
-                const int l = lconn[c * 4 + k];
-                inc[(size_t)b * 4 * B + fill[l]++] = (uint16_t)((c - c0) * 4 + k);
-            }
+        for (int i = 0; i <= nloc; ++i) inc_off.push_back(P.off[i]);
+        std::copy(P.inc.begin(), P.inc.end(), inc.begin() + (size_t)b * 4 * B);
+        P = BlockPlan();
     }
     begin[nb] = (int32_t)node_ids.size();
     for (uint32_t& id : node_ids)
