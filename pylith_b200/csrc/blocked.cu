@@ -558,6 +558,9 @@ bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, i
 // counts and runs fewer steps. Finally each node's incidences are ordered, warp by warp and step
 // by step, so that the staged element entries read in one step (bank pair = cell mod 16) spread
 // over the banks. Any fixed order keeps the sums identical from run to run.
+#ifndef PLB_PLAN_ITERS
+#define PLB_PLAN_ITERS 12000
+#endif
 struct BlockPlan {
     std::vector<int32_t> loc;     // global ids of the local nodes, sorted
     std::vector<int32_t> newidx;  // local index of loc[l]
@@ -573,7 +576,7 @@ static uint64_t splitmix64(uint64_t& x) {
 }
 
 static void plan_block(const int32_t* bc, int ncell, uint64_t seed, BlockPlan& P) {
-    constexpr int R = 16, W = 32, kIters = 4000;
+    constexpr int R = 16, W = 32, kIters = PLB_PLAN_ITERS;
     P.loc.assign(bc, bc + 4 * (size_t)ncell);
     std::sort(P.loc.begin(), P.loc.end());
     P.loc.erase(std::unique(P.loc.begin(), P.loc.end()), P.loc.end());

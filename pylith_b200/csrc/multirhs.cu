@@ -291,9 +291,12 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                 prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, b + gridDim.x, ld, v, sV, sX,
                                   multi_meta(metabase + (cur ^ 1) * mb, ld));
             __pipeline_commit();
-            // one work item per (node, component): consecutive threads take consecutive nodes
-            for (int w = tc; w < ns * 3; w += blockDim.x) {
-                const int cc = w / ns, i = w - cc * ns;
+            // one work item per (node, component): a warp takes one component of 32 consecutive
+            // nodes, the groups whose incidence order the layout spread over the banks
+            const int nitems = (ns + 31) / 32 * 96;
+            for (int w = tc; w < nitems; w += blockDim.x) {
+                const int chunk = w >> 5, g = chunk / 3, cc = chunk - 3 * g, i = g * 32 + (w & 31);
+                if (i >= ns) continue;
                 const int j0 = mm.off[i], j1 = mm.off[i + 1];
                 float acc[KC];
 #pragma unroll
