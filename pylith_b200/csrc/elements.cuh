@@ -61,12 +61,13 @@ struct Geom {
 };
 
 // 3x3 inverse by cofactors; returns det.
-PL_HD double invert3(const double J[3][3], double inv[3][3]) {
-    const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-    const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-    const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-    const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-    const double r = 1.0 / det;
+template <typename R>
+PL_HD R invert3(const R J[3][3], R inv[3][3]) {
+    const R c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const R c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const R c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const R det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    const R r = R(1) / det;
     inv[0][0] = c00 * r;
     inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
     inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;

@@ -126,22 +126,41 @@ __global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(Dom
         __syncwarp();
         if (live && l < H::NQ) {
             const int q = l;
-            double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            T inv[3][3];
+            T wdetJ;
+            if constexpr (sizeof(T) == 4 && CELL == HEX8) {
+                // FP32 Jacobian action: FP32 geometry from the corners relative to corner 0 (the
+                // basis gradients sum to zero, so J is unchanged and no large coordinates cancel),
+                // with the field-basis gradient table (the Q1 field basis is the geometry basis)
+                float J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
+                for (int k = 1; k < 8; ++k)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const float dx = (float)(sX[k * 3 + i] - sX[i]);
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) J[i][j] += dx * tB[q * H::LDB + k * 3 + j];
+                    }
+                const float detJ = invert3(J, inv);
+                if (!(detJ > 0.f)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+                wdetJ = (float)tW[q] * detJ;
+            } else {
+                double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) J[i][j] += sX[k * 3 + i] * tN[q * 25 + k * 3 + j];
+                double inv64[3][3];
+                const double detJ = invert3(J, inv64);
+                if (!(detJ > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+                wdetJ = (T)(tW[q] * detJ);
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) J[i][j] += sX[k * 3 + i] * tN[q * 25 + k * 3 + j];
-            double inv64[3][3];
-            const double detJ = invert3(J, inv64);
-            if (!(detJ > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
-            const T wdetJ = (T)(tW[q] * detJ);
-            T inv[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) inv[i][j] = (T)inv64[i][j];
+                    for (int j = 0; j < 3; ++j) inv[i][j] = (T)inv64[i][j];
+            }
             // reference gradient of the field, then s_x = Gref J^{-1}
             T Gr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll 9
