@@ -492,6 +492,7 @@ int pl_integrator_interface_set_kernels_jacobian(pl_integrator ig, const pl_inte
 int pl_integrator_set_aux(pl_integrator ig, const char* name, int storage, int ncomp, const double* values) {
     bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || !name || !values || ncomp <= 0 || ncomp > 64) return fail(PL_ERR_INVALID_ARG, "bad aux arguments");
+    ig->lm32_valid = false;
     pl_mesh m = ig->mesh;
     int64_t nc = ig->ncells;
     int nq = 1;
@@ -564,6 +565,7 @@ int pl_integrator_get_aux(pl_integrator ig, const char* name, double* values) {
 int pl_integrator_set_constants(pl_integrator ig, int num, const double* constants) {
     bump_state_epoch();  // captured solver graphs hold kernel arguments
     if (!ig || num < 0 || num > 8 || (num > 0 && !constants)) return fail(PL_ERR_INVALID_ARG, "bad constants (at most 8)");
+    ig->lm32_valid = false;
     ig->constants.assign(constants, constants + num);
     return PL_OK;
 }
@@ -584,6 +586,7 @@ int pl_integrator_destroy(pl_integrator ig) {
         if (f.d) cudaFree(f.d);
     if (ig->d_cell_ids) cudaFree(ig->d_cell_ids);
     if (ig->d_block_partial) cudaFree(ig->d_block_partial);
+    if (ig->d_lm32) cudaFree(ig->d_lm32);
     pl_mesh m = ig->mesh;
     delete ig;
     mesh_release(m);
@@ -595,6 +598,26 @@ int pl_integrator_destroy(pl_integrator ig) {
 
 extern "C++" {
 namespace plb {
+int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt) {
+    pl_mesh m = ig->mesh;
+    if (ig->is_interface || m->cell_type != PL_CELL_HEX8 || ig->j3 == K_NONE) return PL_OK;
+    const Rheology rheo = rheology_of(ig, true);
+    if (rheo != RHEO_ILE && rheo != RHEO_GENMAXWELL) return PL_OK;
+    if (ig->lm32_valid && ig->lm32_t == t && ig->lm32_dt == dt) return PL_OK;
+    DomainParams p;
+    int rc = bind_domain(ig, rheo, false, &p);
+    if (rc) return rc;
+    p.t = t;
+    p.dt = dt;
+    if (!ig->d_lm32 && ig->ncells > 0) PLB_CUDA(cudaMalloc((void**)&ig->d_lm32, 2 * ig->ncells * sizeof(float)));
+    launch_tangent_lm32(p, rheo, ig->d_lm32, m->ctx->stream);
+    PLB_CUDA(cudaGetLastError());
+    ig->lm32_valid = true;
+    ig->lm32_t = t;
+    ig->lm32_dt = dt;
+    return PL_OK;
+}
+
 int prepare_blocked(pl_integrator_s* ig) {
     pl_mesh m = ig->mesh;
     int rc = ensure_blocked_layout(m);
@@ -735,6 +758,7 @@ int pl_compute_lhs_jacobian_action_f32(pl_integrator ig, double t, double dt, co
     p.out32 = jv;
     p.t = t;
     p.dt = dt;
+    if (m->cell_type == PL_CELL_HEX8 && ig->lm32_valid && ig->lm32_t == t && ig->lm32_dt == dt) p.lm32 = ig->d_lm32;
     if (use_blocked(ig) && (rc = ensure_blocked_layout(m)) == PL_OK &&
         launch_domain_jv32_blocked(p, *m->blocked, m->cell_type, rheo, m->nnodes, s)) {
         PLB_CUDA(cudaGetLastError());

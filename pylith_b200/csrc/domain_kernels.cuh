@@ -38,6 +38,8 @@ struct DomainParams {
     int num_constants;
     double constants[8];
     unsigned int* err;
+    const float* lm32;  // FP32 Jacobian action of hexahedra: per-cell (lambda, mu) of the
+                        // isotropic tangent at (t, dt), or NULL to evaluate the tangent per point
 };
 
 // ---- elements --------------------------------------------------------------------------
@@ -214,16 +216,18 @@ PL_D void call_jf3(int numA, const int* aOff, const double* a, const DomainParam
 // effective shear modulus), so the tangent is evaluated by its registered function and contracted
 // in closed form from its (f,g,df,dg) = (0,1,0,1) and (0,1,1,0) entries, -lambda and -mu: 12
 // multiply-adds instead of 81 (the 81-entry contraction cannot drop its zero entries).
-template <int RHEO, typename T>
-PL_D void isotropic_jf3_contract(const double Jf3[81], const T s_x[9], T f1[9]) {
-    static_assert(RHEO == RHEO_ILE || RHEO == RHEO_GENMAXWELL, "isotropic tangents only");
-    const T lam = (T)(-Jf3[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
-    const T mu = (T)(-Jf3[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
+template <typename T>
+PL_D void isotropic_contract(T lam, T mu, const T s_x[9], T f1[9]) {
     const T ltr = lam * (s_x[0] + s_x[4] + s_x[8]);
 #pragma unroll
     for (int f = 0; f < 3; ++f)
 #pragma unroll
         for (int df = 0; df < 3; ++df) f1[f * 3 + df] = -(mu * (s_x[f * 3 + df] + s_x[df * 3 + f]) + (f == df ? ltr : T(0)));
+}
+template <int RHEO, typename T>
+PL_D void isotropic_jf3_contract(const double Jf3[81], const T s_x[9], T f1[9]) {
+    static_assert(RHEO == RHEO_ILE || RHEO == RHEO_GENMAXWELL, "isotropic tangents only");
+    isotropic_contract<T>((T)(-Jf3[((0 * 3 + 1) * 3 + 0) * 3 + 1]), (T)(-Jf3[((0 * 3 + 1) * 3 + 1) * 3 + 0]), s_x, f1);
 }
 
 }  // namespace plb

@@ -181,12 +181,15 @@ __global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(Dom
                 for (int e = 0; e < 3; ++e)
                     s_x[cc * 3 + e] = Gr[cc][0] * inv[0][e] + Gr[cc][1] * inv[1][e] + Gr[cc][2] * inv[2][e];
             double a[L::size] = {};
-            L::load_cell(p, c, a);
+            const bool cached = f32 && OP == OP_JACOBIAN_ACTION && p.lm32;
+            if (!cached) L::load_cell(p, c, a);
             if (OP == OP_RESIDUAL) L::load_qp(p, c, q, H::NQ, a);  // the tangents read no state
             double x[3] = {0, 0, 0}, s[3] = {0, 0, 0};
             double f0[3] = {0, 0, 0};
             T f1[9];
-            if (OP == OP_RESIDUAL) {
+            if (cached) {
+                isotropic_contract<T>((T)p.lm32[2 * c], (T)p.lm32[2 * c + 1], s_x, f1);
+            } else if (OP == OP_RESIDUAL) {
                 double s_x64[9], f164[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
                 for (int i = 0; i < 9; ++i) s_x64[i] = (double)s_x[i];
@@ -878,6 +881,35 @@ bool launch_domain_apply_hexgroup(const DomainParams& p, int cell, int rheo, boo
     else if (cell == HEX27 && PLB_Q2_SUMFACT) launch_sumfact(p, rheo, bf, op, s);
     else if (cell == HEX27) launch_group_cell<HEX27>(p, rheo, bf, op, s);
     else return false;
+    return true;
+}
+
+// (lambda, mu) of the isotropic tangent per integrator cell at p.t, p.dt, from the registered
+// Jacobian kernel: the FP32 Jacobian action of hexahedra reads them instead of evaluating the
+// tangent (for generalized Maxwell, three exponentials in FP64) at each quadrature point.
+template <int RHEO>
+__global__ void k_tangent_lm32(DomainParams p, float* __restrict__ out) {
+    using L = AuxLayout<RHEO, false>;
+    const AuxOffsets<RHEO, false> aoff;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < p.ncells; c += (int64_t)gridDim.x * blockDim.x) {
+        double a[L::size] = {};
+        L::load_cell(p, c, a);
+        double x[3] = {0, 0, 0}, Jf3[81];
+#pragma unroll
+        for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
+        call_jf3<RHEO>(L::numA, aoff.v, a, p, x, Jf3);
+        out[2 * c] = (float)(-Jf3[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
+        out[2 * c + 1] = (float)(-Jf3[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
+    }
+}
+
+bool launch_tangent_lm32(const DomainParams& p, int rheo, float* out, cudaStream_t s) {
+    if (rheo != RHEO_ILE && rheo != RHEO_GENMAXWELL) return false;
+    if (p.ncells == 0) return true;
+    const int grid = (int)std::min<int64_t>((p.ncells + 255) / 256, 148 * 16);
+    if (rheo == RHEO_GENMAXWELL) k_tangent_lm32<RHEO_GENMAXWELL><<<grid, 256, 0, s>>>(p, out);
+    else k_tangent_lm32<RHEO_ILE><<<grid, 256, 0, s>>>(p, out);
+    count_launch();
     return true;
 }
 

@@ -146,6 +146,11 @@ struct pl_integrator_s {
     std::vector<plb::AuxField> aux;
     std::vector<double> constants;
     int scatter = PL_SCATTER_AUTO;
+    // per-cell (lambda, mu) for the FP32 Jacobian action of hexahedra, valid for (lm32_t,
+    // lm32_dt) until the aux fields or constants change
+    float* d_lm32 = nullptr;
+    bool lm32_valid = false;
+    double lm32_t = 0.0, lm32_dt = 0.0;
 };
 
 struct pl_matrix_s {

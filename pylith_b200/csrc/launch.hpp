@@ -17,6 +17,7 @@ struct BlockedLayout;
 
 // Counts kernel launches made by this library (reported by pl_kernel_launches).
 void count_launch(int n = 1);
+bool launch_tangent_lm32(const DomainParams& p, int rheo, float* out, cudaStream_t s);
 
 void launch_domain_apply_atomic(const DomainParams& p, int cell, int rheo, bool bf, int op,
                                 cudaStream_t s);
@@ -48,6 +49,9 @@ bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, 
 // The cell-block layout of the integrator's mesh and the integrator's partial-sum buffer
 // (allocations: call outside stream capture).
 int prepare_blocked(pl_integrator_s* ig);
+// Fills the integrator's per-cell FP32 (lambda, mu) for the Jacobian action of hexahedra at
+// (t, dt) when that path applies (no-op otherwise); call outside stream capture.
+int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt);
 
 // FP32 Jacobian action on the cell blocks (the output must be zeroed or hold the sum to add to).
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,

@@ -735,6 +735,7 @@ int pl_solver_setup(pl_solver S, double t, double dt) {
         p.t = t;
         p.dt = dt;
         launch_domain_diag_blocks(p, m->cell_type, ig->j3 == K_ILE_JF3VU ? RHEO_ILE : RHEO_GENMAXWELL, S->d_diag, s);
+        if (S->precision != PL_SOLVER_FP64 && (rc = prepare_jv32_tangent(ig, t, dt)) != PL_OK) return rc;
     }
     if (S->npairs > 0) {
         k_fault_fold_blocks<<<vec_grid(9 * S->npairs), 256, 0, s>>>(S->d_diag, S->d_pair_neg, S->d_pair_pos, S->npairs);

@@ -495,3 +495,57 @@ def test_handles_can_be_destroyed_in_any_order():
     assert float(torch.linalg.norm(x1 - x0)) <= 1e-8 * float(torch.linalg.norm(x0)) and float(torch.linalg.norm(x0)) > 0.0
     B.close()
     ig.close()
+
+
+def test_fp32_hex_jacobian_action_uses_the_tangent_cached_by_solver_setup(ctx):
+    """A FP32 solver's setup caches, per Q1 cell, the (lambda, mu) of the registered isotropic
+    tangent; the FP32 Jacobian action then reads them instead of evaluating the generalized-
+    Maxwell tangent (three exponentials of dt / tau) at every quadrature point. The cached action
+    matches the per-point one, and new constants (the time step) or new aux values make the cache
+    stale until the next setup."""
+    import torch
+    from pylith_b200 import feassemble as FA
+
+    mesh = M.box_hex(6, 5, 4, lo=(-4000.0, -4000.0, -8000.0), hi=(4000.0, 4000.0, 0.0))
+    mu, K, lam, tau = KA.genmaxwell_params()
+    nc, nq = mesh.num_cells, 8
+    rng = np.random.default_rng(5)
+    g = MAT.IsotropicLinearGenMaxwell(
+        np.full(nc, KA.GM_DENSITY), mu * rng.uniform(0.5, 1.5, nc), np.full(nc, K), np.tile(tau, (nc, 1)),
+        np.tile(KA.GM_RATIO, (nc, 1)), np.zeros((nc, nq, 18)), np.zeros((nc, nq, 6)))
+    dt = KA.GM_DT
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = g.create_integrator(dm, dt)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 2, "neg")] = True
+    v = torch.from_numpy(rng.standard_normal(dm.num_dof).astype(np.float32)).cuda()
+
+    def jv():
+        out = torch.zeros_like(v)
+        ig.compute_lhs_jacobian_action_f32(0.0, dt, v, out)
+        torch.cuda.synchronize()
+        return out.double()
+
+    def close(a, b):
+        return float(torch.linalg.norm(a - b)) <= 1e-6 * float(torch.linalg.norm(b))
+
+    def setup():
+        S = FA.Solver(dm, cons.ravel(), [ig], precision=FA.Solver.FP32_REFINED)
+        S.setup(0.0, dt)
+        return S
+
+    ref = jv()  # no cache yet: the tangent at every point
+    S1 = setup()
+    assert close(jv(), ref)
+    ig.set_constants([4.0 * dt])  # another time step: the cache is stale
+    fresh = jv()
+    assert not close(fresh, ref)
+    S2 = setup()
+    assert close(jv(), fresh)
+    ig.set_aux("shear_modulus", FA.PER_CELL, np.full((nc, 1), 2.0 * mu))
+    fresh2 = jv()
+    assert not close(fresh2, fresh)
+    S3 = setup()
+    assert close(jv(), fresh2)
+    for S in (S1, S2, S3):
+        S.close()
