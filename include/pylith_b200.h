@@ -321,7 +321,10 @@ int pl_solver_set_precision(pl_solver solver, int precision, double inner_rtol);
  * meets the tolerances. pl_solver_get_stats reports the replacements (or refinement passes) as
  * outer iterations. */
 int pl_solver_set_reliable(pl_solver solver, int enable, double delta);
-/* Builds the preconditioner at (t, dt). */
+/* Builds the preconditioner at (t, dt). For PL_SOLVER_FP32_REFINED on hexahedra it also evaluates
+ * each integrator's isotropic tangent once per cell at (t, dt), which the FP32 Jacobian action
+ * (pl_compute_lhs_jacobian_action_f32) then reads until the integrator's aux fields or constants
+ * change; call it again after such a change or a new time step. */
 int pl_solver_setup(pl_solver solver, double t, double dt);
 int pl_solver_solve(pl_solver solver, const double* b_dev, double* x_dev);
 /* Sets the positive side of every fault node to u+ = u- + d from the interface integrator's
