@@ -19,6 +19,7 @@
 #include <cuda_pipeline.h>
 
 #include <algorithm>
+#include <atomic>
 #include <thread>
 #include <vector>
 
@@ -704,18 +705,25 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     node_ids.reserve((size_t)nc);
     inc_off.reserve((size_t)nc + nb);
     int maxloc = 0;
-    // the blocks' numberings and incidence orders, planned in parallel
+    // the blocks' numberings and incidence orders, planned in parallel (a block's plan depends
+    // only on its cells and index; the calling thread takes blocks too, so the layout is complete
+    // even where no helper thread can be started)
     std::vector<BlockPlan> plans(nb);
     {
-        const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::atomic<int64_t> next{0};
+        auto work = [&] {
+            for (int64_t b; (b = next.fetch_add(1)) < nb;) {
+                const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
+                plan_block(m->h_cells.data() + c0 * 4, (int)(c1 - c0), (uint64_t)b, plans[b]);
+            }
+        };
+        const int nth = (int)std::min(15u, std::thread::hardware_concurrency());
         std::vector<std::thread> th;
-        for (int t = 0; t < nth; ++t)
-            th.emplace_back([&, t] {
-                for (int64_t b = t; b < nb; b += nth) {
-                    const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
-                    plan_block(m->h_cells.data() + c0 * 4, (int)(c1 - c0), (uint64_t)b, plans[b]);
-                }
-            });
+        try {
+            for (int t = 1; t < nth; ++t) th.emplace_back(work);
+        } catch (...) {
+        }
+        work();
         for (std::thread& x : th) x.join();
     }
     for (int64_t b = 0; b < nb; ++b) {
