@@ -172,8 +172,8 @@ void* pl_fekernel_lookup(const char* name);
 /* ---- context -------------------------------------------------------------------------- */
 int pl_context_create(int device, pl_context* out);
 /* Destroy calls may come in any order: an object still referenced by a dependent one (a mesh by
- * an integrator, a context by a mesh, a solver by a batched solver) is released when its last
- * dependent is destroyed. A solver uses its integrators until it is destroyed. */
+ * an integrator, a context by a mesh, an integrator by a solver it was added to, a solver by a
+ * batched solver) is released when its last dependent is destroyed. */
 int pl_context_destroy(pl_context ctx);
 /* Enqueue all work on a caller-owned cudaStream_t; NULL is CUDA's legacy default stream
  * (torch's default stream). A new context starts on its own non-blocking stream. */
@@ -217,7 +217,8 @@ int pl_integrator_set_aux(pl_integrator integ, const char* name, int storage, in
                           const double* values_host);
 /* Copies an aux subfield back in the host layout of pl_integrator_set_aux. */
 int pl_integrator_get_aux(pl_integrator integ, const char* name, double* values_host);
-/* Integrator::_setKernelConstants (Integrator.cc:264-290). */
+/* Integrator::_setKernelConstants (Integrator.cc:264-290). At most 8 constants (the kernels on
+ * this path use 1 or 6); more return PL_ERR_UNSUPPORTED and leave the previous constants. */
 int pl_integrator_set_constants(pl_integrator integ, int num, const double* constants);
 int pl_integrator_set_scatter(pl_integrator integ, int scatter);
 int pl_integrator_destroy(pl_integrator integ);
@@ -257,7 +258,9 @@ int pl_compute_lhs_residual_host(pl_integrator integ, double t, double dt, const
  * stages u and r through one fixed 16 MiB device array built into the library (held on every
  * GPU that loads it until exit) and so accepts meshes of at most 1048576 DOFs, returning
  * PL_ERR_INVALID_ARG beyond that. Uses the thread-per-cell kernels. The first call on each
- * device looks up the array's address and should come before any stream capture. All calls
+ * device looks up the array's address and should come before any stream capture; the address is
+ * kept for the life of the process and not looked up again, so the entry point must not be used
+ * on a device after cudaDeviceReset (or another teardown of its primary context). All calls
  * share the array: calls whose GPU work overlaps (two host threads, two streams) race on it;
  * each call waits for its stream before returning. */
 int pl_compute_lhs_residual_host_noalloc(pl_integrator integ, double t, double dt,

@@ -384,6 +384,99 @@ int64_t oracle_jacobian_elements(int cell_type, int64_t ncells, const int* cells
     return bad;
 }
 
+// Matrix-free Jacobian action (DMPlexComputeJacobianActionByKey, called at
+// libsrc/pylith/feassemble/IntegratorDomain.cc:540): jv += sum over cells of K_e v_e, with K_e
+// the element Jacobian of oracle_jacobian_elements, applied at each quadrature point to the
+// values and gradient of v instead of being formed: jv_a,fc += wdetJ (phi_a (G0 v + G1 grad v)
+// + grad phi_a . (G2 v + G3 grad v)). The pointwise Jacobians are evaluated at u.
+int64_t oracle_jacobian_action(int cell_type, int64_t ncells, const int* cells, const double* coords,
+                               int64_t nnodes, const double* u, const double* v, int numA,
+                               const int* aux_kind, const int* aux_ncomp, const double* const* aux_data,
+                               double t, double s_tshift, int numConstants, const double* constants,
+                               PointJacFn g0, PointJacFn g1, PointJacFn g2, PointJacFn g3, double* jv,
+                               int nthreads) {
+    const Element e = make_element(cell_type);
+    const Aux aux(numA, aux_kind, aux_ncomp, aux_data);
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    std::vector<std::vector<double>> bufs(nthreads);
+    int64_t bad = 0;
+#pragma omp parallel num_threads(nthreads)
+    {
+        const int tid = omp_get_thread_num();
+        std::vector<double>& rb = bufs[tid];
+        rb.assign(nnodes * 3, 0.0);
+        std::vector<double> a(aux.total > 0 ? aux.total : 1);
+        std::vector<double> re(e.nen * 3);
+        QPoint p;
+        const int sOff[1] = {0}, sOff_x[1] = {0};
+        double s[3], s_t[3] = {0, 0, 0}, s_x[9], w[3], w_x[9], G0[9], G1[27], G2[27], G3[81];
+#pragma omp for schedule(static)
+        for (int64_t cell = 0; cell < ncells; ++cell) {
+            const int* cn = &cells[cell * e.nen];
+            std::fill(re.begin(), re.end(), 0.0);
+            for (int q = 0; q < e.nq; ++q) {
+                if (!eval_geometry(e, q, cn, coords, &p)) {
+#pragma omp critical
+                    { if (!bad) bad = -(cell + 1); }
+                    continue;
+                }
+                if (u) {
+                    eval_field(e, q, p, cn, u, s, s_x);
+                } else {
+                    std::fill(s, s + 3, 0.0);
+                    std::fill(s_x, s_x + 9, 0.0);
+                }
+                eval_field(e, q, p, cn, v, w, w_x);
+                aux.eval(e, cell, q, cn, a.data());
+                std::fill(G0, G0 + 9, 0.0); std::fill(G1, G1 + 27, 0.0);
+                std::fill(G2, G2 + 27, 0.0); std::fill(G3, G3 + 81, 0.0);
+#define ORACLE_CALLJ(fn, out) \
+    if (fn) fn(3, 1, numA, sOff, sOff_x, s, s_t, s_x, aux.off.data(), nullptr, a.data(), nullptr, \
+               nullptr, t, s_tshift, p.x, numConstants, constants, out)
+                ORACLE_CALLJ(g0, G0);
+                ORACLE_CALLJ(g1, G1);
+                ORACLE_CALLJ(g2, G2);
+                ORACLE_CALLJ(g3, G3);
+#undef ORACLE_CALLJ
+                double f0v[3], f1v[9];
+                for (int fc = 0; fc < 3; ++fc) {
+                    double acc0 = 0.0;
+                    for (int gc = 0; gc < 3; ++gc) {
+                        const int fg = fc * 3 + gc;
+                        acc0 += G0[fg] * w[gc];
+                        for (int dg = 0; dg < 3; ++dg) acc0 += G1[fg * 3 + dg] * w_x[gc * 3 + dg];
+                    }
+                    f0v[fc] = acc0;
+                    for (int df = 0; df < 3; ++df) {
+                        double acc1 = 0.0;
+                        for (int gc = 0; gc < 3; ++gc) {
+                            const int fg = fc * 3 + gc;
+                            acc1 += G2[fg * 3 + df] * w[gc];
+                            for (int dg = 0; dg < 3; ++dg) acc1 += G3[(fg * 3 + df) * 3 + dg] * w_x[gc * 3 + dg];
+                        }
+                        f1v[fc * 3 + df] = acc1;
+                    }
+                }
+                for (int n = 0; n < e.nen; ++n) {
+                    const double ph = e.phi[q * e.nen + n];
+                    const double* g = &p.gphi[n * 3];
+                    for (int c = 0; c < 3; ++c)
+                        re[n * 3 + c] += p.wdetJ * (f0v[c] * ph + f1v[c * 3 + 0] * g[0] + f1v[c * 3 + 1] * g[1] +
+                                                    f1v[c * 3 + 2] * g[2]);
+                }
+            }
+            for (int n = 0; n < e.nen; ++n)
+                for (int c = 0; c < 3; ++c) rb[3 * (int64_t)cn[n] + c] += re[n * 3 + c];
+        }
+    }
+    for (int th = 0; th < nthreads; ++th) {
+        const std::vector<double>& rb = bufs[th];
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (int64_t i = 0; i < nnodes * 3; ++i) jv[i] += rb[i];
+    }
+    return bad;
+}
+
 // Projection of pointwise functions at quadrature points (DMProjectFieldLocal with
 // point-space outputs): out_k[cell][q][ncomp_k] = fn_k(solution at q, aux at q). All functions
 // see the same (previous) aux values, as the reference evaluates every kernel on the input

@@ -34,11 +34,20 @@ _lib = None
 _ref = None
 
 
+def source_tree():
+    """The PyLith source tree named by the PYLITH_SRC environment variable, or None when it is
+    unset or holds no libsrc/ (tests that read the tree skip then)."""
+    src = os.environ.get("PYLITH_SRC")
+    return src if src and os.path.isdir(os.path.join(src, "libsrc")) else None
+
+
 def build(ref: bool = True) -> None:
-    """Compile the oracle (and the reference kernels when the PyLith sources are present)."""
+    """Compile the oracle, and the reference kernels when PYLITH_SRC names the PyLith sources
+    (an existing oracle/_ref build is kept otherwise)."""
     subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
-    if ref and os.path.isdir(os.environ.get("PYLITH_SRC", "/root/reference") + "/libsrc"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"], stdout=subprocess.DEVNULL)
+    src = source_tree()
+    if ref and src:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"PYLITH_SRC={src}"], stdout=subprocess.DEVNULL)
 
 
 def lib():
@@ -49,6 +58,7 @@ def lib():
         _lib = ctypes.CDLL(LIB_PATH)
         _lib.oracle_residual.restype = _I64
         _lib.oracle_jacobian_elements.restype = _I64
+        _lib.oracle_jacobian_action.restype = _I64
         _lib.oracle_project_qp.restype = _I64
         _lib.oracle_project_centroid.restype = _I64
     return _lib
@@ -144,6 +154,29 @@ def residual(mesh, u, aux: AuxFields, f0=None, f1=None, t=0.0, constants=None, u
     if bad:
         raise ValueError(f"non-positive Jacobian determinant in cell {-bad - 1}")
     return r
+
+
+def jacobian_action(mesh, v, aux: AuxFields, g3, g0=None, u=None, t=0.0, s_tshift=0.0,
+                    constants=None, nthreads=0, source="oracle"):
+    """Matrix-free Jacobian action J v (ADD into zeros) over all cells of `mesh`
+    (DMPlexComputeJacobianActionByKey, IntegratorDomain.cc:540), the pointwise Jacobians
+    evaluated at u (zero when None)."""
+    L = lib()
+    cells = np.ascontiguousarray(mesh.cells, dtype=np.int32)
+    coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    uu = None if u is None else np.ascontiguousarray(u, dtype=np.float64)
+    jv = np.zeros(mesh.num_nodes * 3)
+    c = np.ascontiguousarray(constants if constants is not None else [0.0], dtype=np.float64)
+    nc = 0 if constants is None else len(constants)
+    ptr = lambda n: _P(kernel(n, source) if n else None)  # noqa: E731
+    bad = L.oracle_jacobian_action(_I(mesh.cell_type), _I64(mesh.num_cells), _p(cells), _p(coords),
+                                   _I64(mesh.num_nodes), _p(uu), _p(v), _I(aux.num), _p(aux.kinds),
+                                   _p(aux.ncomp), aux.ptrs, _D(t), _D(s_tshift), _I(nc), _p(c),
+                                   ptr(g0), _P(None), _P(None), ptr(g3), _p(jv), _I(nthreads))
+    if bad:
+        raise ValueError(f"non-positive Jacobian determinant in cell {-bad - 1}")
+    return jv
 
 
 def jacobian_elements(mesh, aux: AuxFields, g3, g0=None, u=None, t=0.0, s_tshift=0.0,

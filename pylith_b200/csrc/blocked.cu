@@ -687,7 +687,7 @@ static void plan_block(const int32_t* bc, int ncell, uint64_t seed, BlockPlan& P
 }
 
 // Host: block layout from the cell connectivity (cells should be in a locality-preserving order).
-int ensure_blocked_layout(pl_mesh_s* m) {
+static int build_blocked_layout(pl_mesh_s* m) {
     if (m->blocked) return PL_OK;
     if (m->cell_type != PL_CELL_TET4 || m->nnodes >= (int64_t)kSharedBit) {
         m->blocked = new BlockedLayout();  // empty: not supported for this mesh
@@ -711,10 +711,17 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     std::vector<BlockPlan> plans(nb);
     {
         std::atomic<int64_t> next{0};
-        auto work = [&] {
-            for (int64_t b; (b = next.fetch_add(1)) < nb;) {
-                const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
-                plan_block(m->h_cells.data() + c0 * 4, (int)(c1 - c0), (uint64_t)b, plans[b]);
+        std::atomic<bool> failed{false};
+        // an exception (bad_alloc in a plan) must not leave a thread: it stops the block loop of
+        // every thread, and the layout reports the failure after all threads are joined
+        auto work = [&]() noexcept {
+            try {
+                for (int64_t b; !failed.load() && (b = next.fetch_add(1)) < nb;) {
+                    const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
+                    plan_block(m->h_cells.data() + c0 * 4, (int)(c1 - c0), (uint64_t)b, plans[b]);
+                }
+            } catch (...) {
+                failed.store(true);
             }
         };
         const int nth = (int)std::min(15u, std::thread::hardware_concurrency());
@@ -725,6 +732,7 @@ int ensure_blocked_layout(pl_mesh_s* m) {
         }
         work();
         for (std::thread& x : th) x.join();
+        if (failed.load()) return fail(PL_ERR_OUT_OF_MEMORY, "cell-block layout planning ran out of host memory");
     }
     for (int64_t b = 0; b < nb; ++b) {
         BlockPlan& P = plans[b];
@@ -809,6 +817,16 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     }
     m->blocked = L;
     return PL_OK;
+}
+
+int ensure_blocked_layout(pl_mesh_s* m) {
+    try {
+        return build_blocked_layout(m);
+    } catch (const std::bad_alloc&) {
+        return fail(PL_ERR_OUT_OF_MEMORY, "cell-block layout: out of host memory");
+    } catch (...) {
+        return fail(PL_ERR_INVALID_ARG, "cell-block layout failed");
+    }
 }
 
 void free_blocked_layout(BlockedLayout* b) {

@@ -103,7 +103,8 @@ static int bind_domain(pl_integrator_s* ig, Rheology rheo, bool bf, DomainParams
         p->total = tot->d;
         if (ig->constants.empty()) return fail(PL_ERR_INVALID_ARG, "generalized Maxwell needs constants[0] = dt");
     }
-    p->num_constants = (int)std::min<size_t>(ig->constants.size(), 8);
+    if (ig->constants.size() > 8) return fail(PL_ERR_UNSUPPORTED, "at most 8 kernel constants are supported");
+    p->num_constants = (int)ig->constants.size();
     for (int i = 0; i < p->num_constants; ++i) p->constants[i] = ig->constants[i];
     return PL_OK;
 }
@@ -118,7 +119,8 @@ static int bind_cohesive(pl_integrator_s* ig, CohesiveParams* p) {
     p->lag_offset = 3 * m->nnodes;
     const AuxField* slip = find_aux(ig, "slip");
     p->slip = slip ? slip->d : nullptr;
-    p->num_constants = (int)std::min<size_t>(ig->constants.size(), 8);
+    if (ig->constants.size() > 8) return fail(PL_ERR_UNSUPPORTED, "at most 8 kernel constants are supported");
+    p->num_constants = (int)ig->constants.size();
     for (int i = 0; i < p->num_constants; ++i) p->constants[i] = ig->constants[i];
     for (int f = 0; f < 3; ++f) {
         p->kr[f] = ig->if_r[f];
@@ -415,6 +417,7 @@ int pl_integrator_set_kernels_jacobian(pl_integrator ig, const pl_jacobian_kerne
         if (c != K_NONE) j3 = c;
     }
     ig->j3 = j3;
+    ig->lm32_valid = false;  // the cached FP32 tangent was evaluated with the previous Jf3
     return PL_OK;
 }
 
@@ -564,7 +567,8 @@ int pl_integrator_get_aux(pl_integrator ig, const char* name, double* values) {
 
 int pl_integrator_set_constants(pl_integrator ig, int num, const double* constants) {
     bump_state_epoch();  // captured solver graphs hold kernel arguments
-    if (!ig || num < 0 || num > 8 || (num > 0 && !constants)) return fail(PL_ERR_INVALID_ARG, "bad constants (at most 8)");
+    if (!ig || num < 0 || (num > 0 && !constants)) return fail(PL_ERR_INVALID_ARG, "bad constants");
+    if (num > 8) return fail(PL_ERR_UNSUPPORTED, "at most 8 kernel constants are supported");
     ig->lm32_valid = false;
     ig->constants.assign(constants, constants + num);
     return PL_OK;
@@ -577,9 +581,7 @@ int pl_integrator_set_scatter(pl_integrator ig, int scatter) {
     return PL_OK;
 }
 
-int pl_integrator_destroy(pl_integrator ig) {
-    bump_state_epoch();  // captured solver graphs hold kernel arguments
-    if (!ig) return PL_OK;
+static void integrator_free(pl_integrator ig) {
     cudaSetDevice(ig->mesh->ctx->device);
     cudaStreamSynchronize(ig->mesh->ctx->stream);
     for (AuxField& f : ig->aux)
@@ -590,6 +592,16 @@ int pl_integrator_destroy(pl_integrator ig) {
     pl_mesh m = ig->mesh;
     delete ig;
     mesh_release(m);
+}
+
+int pl_integrator_destroy(pl_integrator ig) {
+    bump_state_epoch();  // captured solver graphs hold kernel arguments
+    if (!ig) return PL_OK;
+    if (ig->refs > 0) {  // still used by a solver: freed when the last one releases it
+        ig->destroy_requested = true;
+        return PL_OK;
+    }
+    integrator_free(ig);
     return PL_OK;
 }
 
@@ -598,6 +610,11 @@ int pl_integrator_destroy(pl_integrator ig) {
 
 extern "C++" {
 namespace plb {
+void integrator_retain(pl_integrator_s* ig) { ig->refs++; }
+void integrator_release(pl_integrator_s* ig) {
+    if (--ig->refs == 0 && ig->destroy_requested) integrator_free(ig);
+}
+
 int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt) {
     pl_mesh m = ig->mesh;
     if (ig->is_interface || m->cell_type != PL_CELL_HEX8 || ig->j3 == K_NONE) return PL_OK;

@@ -75,13 +75,15 @@ void mesh_retain(pl_mesh_s* m);
 void mesh_release(pl_mesh_s* m);
 void solver_retain(pl_solver_s* S);
 void solver_release(pl_solver_s* S);
+void integrator_retain(pl_integrator_s* ig);
+void integrator_release(pl_integrator_s* ig);
 
 }  // namespace plb
 
 // Object lifetimes: meshes hold a reference on their context, integrators, matrices and solvers
-// on their mesh, batched solvers on their solver; a destroy request on an object that is still
-// referenced is deferred until the last dependent object is destroyed, so any destroy order is
-// safe.
+// on their mesh, solvers on the integrators added to them, batched solvers on their solver; a
+// destroy request on an object that is still referenced is deferred until the last dependent
+// object is destroyed, so any destroy order is safe.
 struct pl_context_s {
     int refs = 0;
     bool destroy_requested = false;
@@ -126,6 +128,8 @@ struct AuxField {
 }  // namespace plb
 
 struct pl_integrator_s {
+    int refs = 0;
+    bool destroy_requested = false;
     pl_mesh mesh = nullptr;
     bool is_interface = false;
     int64_t ncells = 0;                 // cells integrated over

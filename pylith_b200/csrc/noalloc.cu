@@ -19,7 +19,10 @@
 //    (2 x 2^20 doubles = 16 MiB). Every GPU on which the library's module is loaded holds it
 //    until the process exits. Meshes with more DOFs are rejected with PL_ERR_INVALID_ARG.
 //  * Its device address is looked up on the first call made on each device (with that device
-//    current); make that first call before any stream capture begins.
+//    current); make that first call before any stream capture begins. The address is kept for the
+//    life of the process: after cudaDeviceReset (or any teardown of the device's primary context)
+//    the module may be loaded at another address, so the entry point must not be used on that
+//    device again.
 //  * All calls share the array, and it keeps the last call's contents; the residual half is
 //    cleared at the start of every call. Calls whose GPU work overlaps (from two host threads,
 //    or on two contexts with different streams) race on the array. Each call ends by waiting

@@ -691,6 +691,7 @@ int pl_solver_add_integrator(pl_solver S, pl_integrator ig) {
         return fail(PL_ERR_INVALID_ARG, "interface integrators are not part of the reduced operator; "
                                         "pass them to pl_solver_apply_fault_slip");
     if (ig->j3 == K_NONE) return fail(PL_ERR_NOT_READY, "integrator has no Jacobian kernels");
+    integrator_retain(ig);  // kept alive until the solver is freed (the solver's graphs use it)
     S->ops.push_back(ig);
     S->ready = false;
     return PL_OK;
@@ -849,8 +850,11 @@ static void solver_free(pl_solver S) {
                     S->d_pair_neg, S->d_pair_pos, S->d_pair_normal};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    std::vector<pl_integrator> ops;
+    ops.swap(S->ops);
     pl_mesh m = S->mesh;
     delete S;
+    for (pl_integrator ig : ops) integrator_release(ig);
     mesh_release(m);
 }
 

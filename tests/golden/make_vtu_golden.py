@@ -6,7 +6,7 @@ those files (the PyLith source tree must be present), keeps their mesh, cell typ
 arrays (names and values, in file order) and the SHA-256 of every file, so that the writer in
 pylith_b200/output.py can be checked byte for byte against them without the PyLith sources.
 
-    python tests/golden/make_vtu_golden.py [path/to/pylith]
+    PYLITH_SRC=path/to/pylith python tests/golden/make_vtu_golden.py
 """
 import hashlib
 import json
@@ -22,7 +22,10 @@ from pylith_b200 import output as OUT  # noqa: E402
 FILES = ["tet4_vertex_t10.vtu", "tet4_cell_t10.vtu", "hex8_vertex_t10.vtu", "hex8_cell_t10.vtu"]
 
 
-def main(pylith="/root/reference"):
+def main(pylith=None):
+    pylith = pylith or os.environ.get("PYLITH_SRC")
+    if not pylith:
+        sys.exit("set PYLITH_SRC to the PyLith source tree")
     data_dir = os.path.join(pylith, "tests", "libtests", "meshio", "data")
     arrays, meta = {}, {}
     for i, name in enumerate(FILES):

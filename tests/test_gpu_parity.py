@@ -306,6 +306,26 @@ def test_unknown_kernel_is_rejected(torch_cuda, ctx):
     assert e.value.code == -1
 
 
+def test_more_than_eight_constants_are_rejected(torch_cuda, ctx):
+    """Integrator::_setKernelConstants takes any number of constants; this build holds at most 8
+    (the kernels on the path use 1 or 6) and rejects more with PL_ERR_UNSUPPORTED instead of
+    dropping the extra ones; the previous constants stay in place."""
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+
+    torch = torch_cuda
+    mesh = MESHES["hex8"]()
+    mat = elastic_setup(mesh)
+    ig = mat.create_integrator(FA.DeviceMesh(ctx, mesh))
+    ig.set_constants([1.0] * 8)
+    with pytest.raises(_lib.PylithB200Error) as e:
+        ig.set_constants([1.0] * 9)
+    assert e.value.code == -7
+    du = torch.zeros(mesh.num_dof, dtype=torch.float64, device="cuda")
+    ig.compute_lhs_residual(0.0, 0.0, du, torch.empty_like(du))
+    ctx.synchronize()
+
+
 def test_inverted_cell_is_reported(torch_cuda, ctx):
     from pylith_b200 import _lib
     from pylith_b200 import feassemble as FA

@@ -547,5 +547,14 @@ def test_fp32_hex_jacobian_action_uses_the_tangent_cached_by_solver_setup(ctx):
     assert not close(fresh2, fresh)
     S3 = setup()
     assert close(jv(), fresh2)
-    for S in (S1, S2, S3):
+    # a new Jf3 kernel (here the elastic one, reading the same shear and bulk moduli) also makes
+    # the cache stale: the action follows the new kernel at once, and again after the next setup
+    ig.set_kernels_jacobian([FA.JacobianKernels(
+        "displacement", "displacement", FA.LHS, None, None, None,
+        FA.fekernels.IsotropicLinearElasticity3D.Jf3vu_infinitesimalStrain)])
+    elastic = jv()
+    assert not close(elastic, fresh2)
+    S4 = setup()
+    assert close(jv(), elastic)
+    for S in (S1, S2, S3, S4):
         S.close()

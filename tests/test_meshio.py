@@ -1,9 +1,11 @@
-"""Mesh ingest (pylith_b200.meshio): Gmsh 4.1 ASCII/binary round trips, and — where the PyLith
-source tree is present — the reference's own test meshes read and solved with the oracle against
-the reference tests' known answers:
+"""Mesh ingest (pylith_b200.meshio): Gmsh 4.1 ASCII/binary round trips, and the reference's own
+test meshes solved with the oracle against the reference tests' known answers:
   * UniformStrain3D MMS on tests/mmstests/linearelasticity/nofaults-3d/data/{tet,hex}.msh;
   * axial displacement on tests/fullscale/linearelasticity/nofaults-3d/mesh_{tet,hex}.exo with the
-    Dirichlet groups and components of axialdisp.cfg."""
+    Dirichlet groups and components of axialdisp.cfg.
+The meshes come from tests/golden/reference_meshes.npz (written by make_mesh_golden.py with this
+reader); where PYLITH_SRC names the PyLith source tree, reading the files again must reproduce
+the fixture."""
 import os
 
 import numpy as np
@@ -11,21 +13,18 @@ import pytest
 import scipy.sparse.linalg as spla
 
 import known_answers as KA
+from golden import make_mesh_golden as MG
 from pylith_b200 import materials as MAT
 from pylith_b200 import meshing as M
 from pylith_b200 import meshio as MIO
 
 F1_ILE = "IsotropicLinearElasticity3D::f1v_infinitesimalStrain"
 JF3_ILE = "IsotropicLinearElasticity3D::Jf3vu_infinitesimalStrain"
-REF = os.environ.get("PYLITH_REFERENCE_TREE", "/root/reference")
-MMS_DATA = os.path.join(REF, "tests/mmstests/linearelasticity/nofaults-3d/data")
-AXIAL = os.path.join(REF, "tests/fullscale/linearelasticity/nofaults-3d")
 
 
-def _needs(path):
-    if not os.path.exists(path):
-        pytest.skip(f"{path} not present")
-    return path
+@pytest.fixture(scope="module")
+def ref_meshes():
+    return MG.load()
 
 
 @pytest.mark.parametrize("binary", [False, True], ids=["ascii", "binary"])
@@ -70,13 +69,31 @@ def test_rejects_unknown_format(tmp_path):
         MIO.read(str(p))
 
 
-@pytest.mark.parametrize("name,ctype,ncells", [("tet.msh", M.CELL_TET4, 307), ("hex.msh", M.CELL_HEX8, 125)])
-def test_reference_gmsh_meshes_mms_uniform_strain(oracle_lib, name, ctype, ncells):
+def test_reading_the_reference_files_reproduces_the_fixture():
+    src = os.environ.get("PYLITH_SRC")
+    if not src or not os.path.isdir(src):
+        pytest.skip("PYLITH_SRC (the PyLith source tree) is not set")
+    fresh = MG.read_all(src)
+    fixture = MG.load()
+    assert sorted(fresh) == sorted(fixture)
+    for key, d in fresh.items():
+        f = fixture[key]
+        assert d.mesh.cell_type == f.mesh.cell_type
+        np.testing.assert_array_equal(d.mesh.coords, f.mesh.coords)
+        np.testing.assert_array_equal(d.mesh.cells, f.mesh.cells)
+        np.testing.assert_array_equal(d.material_ids, f.material_ids)
+        assert sorted(d.vertex_groups) == sorted(f.vertex_groups)
+        for g in d.vertex_groups:
+            np.testing.assert_array_equal(d.vertex_groups[g], f.vertex_groups[g])
+
+
+@pytest.mark.parametrize("key,ctype,ncells", [("mms_tet", M.CELL_TET4, 307), ("mms_hex", M.CELL_HEX8, 125)])
+def test_reference_gmsh_meshes_mms_uniform_strain(oracle_lib, ref_meshes, key, ctype, ncells):
     """The reference's MMS meshes: 8 km box, material 24, vertex group `boundary`; a linear
     displacement field gives zero residual at every vertex outside `boundary`
     (UniformStrain3D.cc)."""
     O = oracle_lib
-    d = MIO.read(_needs(os.path.join(MMS_DATA, name)))
+    d = ref_meshes[key]
     m = d.mesh
     assert m.cell_type == ctype and m.num_cells == ncells
     np.testing.assert_allclose(m.coords.min(0), [-4000, -4000, -8000])
@@ -94,12 +111,12 @@ def test_reference_gmsh_meshes_mms_uniform_strain(oracle_lib, name, ctype, ncell
     assert np.abs(r[interior]).max() <= 1e-12 * np.abs(r).max()
 
 
-@pytest.mark.parametrize("name", ["mesh_tet.exo", "mesh_hex.exo"])
-def test_reference_exodus_meshes_axial_displacement(oracle_lib, name):
+@pytest.mark.parametrize("key", ["axial_tet", "axial_hex"])
+def test_reference_exodus_meshes_axial_displacement(oracle_lib, ref_meshes, key):
     """axialdisp.cfg on the reference's ExodusII meshes: ux on boundary_x*, uy on boundary_y*,
     uz on boundary_zneg from the analytic solution; the oracle's solve reproduces it."""
     O = oracle_lib
-    d = MIO.read(_needs(os.path.join(AXIAL, name)))
+    d = ref_meshes[key]
     m = d.mesh
     assert set(d.material_ids.tolist()) == {1, 2}
     cons = MIO.constrained_mask(d, [("boundary_xneg", [0]), ("boundary_xpos", [0]), ("boundary_yneg", [1]),

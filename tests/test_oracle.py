@@ -229,3 +229,26 @@ def test_derived_fields_known_answer(oracle_lib, make):
         s_ref, e_ref = O.project_centroid(mesh, u, aux, fns, [6, 6], source="ref")
         np.testing.assert_array_equal(stress, s_ref)
         np.testing.assert_array_equal(strain, e_ref)
+
+
+@pytest.mark.parametrize("make", [lambda: M.box_tet_delaunay(2000, seed=3), lambda: M.box_hex(4, 3, 3),
+                                  lambda: M.box_hex27(2, 2, 2)], ids=["tet4", "hex8", "hex27"])
+def test_jacobian_action_equals_assembled_elements(oracle_lib, make):
+    """The matrix-free action (DMPlexComputeJacobianActionByKey) is the assembled element Jacobians
+    applied to v, for the elastic and the generalized-Maxwell tangents."""
+    O = oracle_lib
+    mesh = make()
+    rng = np.random.default_rng(7)
+    nc, nq = mesh.num_cells, M.QUAD_POINTS[mesh.cell_type]
+    rho, mu, K = MAT.lognormal_elastic(nc, seed=2)
+    tau = MAT.genmaxwell_times(rho, np.sqrt(mu / rho), [1e18, 1e19, 1e20], [0.3, 0.3, 0.3])
+    gm = O.AuxFields([(rho[:, None], "cell"), (mu[:, None], "cell"), (K[:, None], "cell"), (tau, "cell"),
+                      (np.tile([0.3, 0.3, 0.3], (nc, 1)), "cell"), (np.zeros((nc, nq, 18)), "qp"),
+                      (np.zeros((nc, nq, 6)), "qp")])
+    el = O.AuxFields([(rho[:, None], "cell"), (mu[:, None], "cell"), (K[:, None], "cell")])
+    v = rng.standard_normal(mesh.num_dof)
+    for aux, g3, consts in ((el, "IsotropicLinearElasticity3D::Jf3vu_infinitesimalStrain", None),
+                            (gm, "IsotropicLinearGenMaxwell3D::Jf3vu_infinitesimalStrain", [MAT.YEAR])):
+        J = O.assemble(mesh, O.jacobian_elements(mesh, aux, g3=g3, constants=consts))
+        jv = O.jacobian_action(mesh, v, aux, g3=g3, constants=consts)
+        assert np.linalg.norm(jv - J @ v) <= 1e-13 * np.linalg.norm(J @ v)
