@@ -12,8 +12,12 @@ application's working set (~53 MB) would otherwise stay cached between applicati
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pylith_b200|reference]
   python bench.py --config c0|c1q2|c2|c3|c4     (the other configurations, one JSON line each)
 
-Under torchrun (N > 1) every rank runs the same workload on its own GPU (weak scaling, its own
-seeded mesh); the slowest rank's device time defines the step time.
+Under torchrun (N > 1) the ranks share one mesh of N x 1.2 M cells (the same Delaunay box
+stretched N times along x, so every rank's part is the single-GPU workload: weak scaling), cut into
+N contiguous ranges of its Morton order. Every application on every rank computes its part's
+residual (or J v) and sums the shared nodes with its neighbours: one pack kernel, NCCL send/receive
+per neighbour, one add kernel (the DMLocalToGlobal ADD_VALUES step of the reference). The slowest
+rank's device time defines the step time; value counts the global mesh's DOFs.
 """
 from __future__ import annotations
 
@@ -41,18 +45,35 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def load_mesh(cells: int, seed: int):
-    """The seeded benchmark mesh, cached under the temp directory between processes."""
-    from pylith_b200 import meshing as M
-
+def _mesh_path(cells: int, seed: int, stretch: int = 1):
     cache = os.path.join(tempfile.gettempdir(), "pylith_b200_mesh_cache")
     os.makedirs(cache, exist_ok=True)
-    path = os.path.join(cache, f"tet_{cells}_{seed}_v1.npz")
+    tag = f"tet_{cells}_{seed}_v1" if stretch == 1 else f"tet_{cells}_{seed}_x{stretch}_v1"
+    return os.path.join(cache, tag + ".npz")
+
+
+def load_mesh(cells: int, seed: int, stretch: int = 1, build: bool = True):
+    """The seeded benchmark mesh, cached under the temp directory between processes. stretch > 1:
+    the box [-6, -6 + 12 stretch] x [-6, 6] x [-9, 0] km with `cells` tetrahedra (the multi-GPU
+    mesh). With build=False, waits for another process to write the cache."""
+    from pylith_b200 import meshing as M
+
+    path = _mesh_path(cells, seed, stretch)
+    if not build:
+        t0 = time.time()
+        while not os.path.exists(path):
+            if time.time() - t0 > 1800:
+                raise TimeoutError(f"{path} was not written")
+            time.sleep(1.0)
     if os.path.exists(path):
         d = np.load(path)
         return M.Mesh(M.CELL_TET4, d["coords"], d["cells"])
     t0 = time.time()
-    mesh = M.box_tet_delaunay(cells, seed=seed)
+    if stretch == 1:
+        mesh = M.box_tet_delaunay(cells, seed=seed)
+    else:
+        lo, hi = M.BOX_LO, M.BOX_HI
+        mesh = M.box_tet_delaunay(cells, seed=seed, lo=lo, hi=(lo[0] + stretch * (hi[0] - lo[0]), hi[1], hi[2]))
     log(f"mesh: {mesh.num_cells} tets, {mesh.num_nodes} nodes in {time.time() - t0:.1f} s")
     tmp = path + f".{os.getpid()}.tmp.npz"
     np.savez(tmp, coords=mesh.coords, cells=mesh.cells)
@@ -254,19 +275,40 @@ def main():
 
         import torch.distributed as dist
 
+        # rank 0 builds the shared mesh (minutes for 8 x 1.2 M cells) before the process group
+        # starts its collective timeouts; the other ranks wait for its cache file
+        load_mesh(args.cells * world, seed=0, stretch=world, build=rank == 0)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from pylith_b200 import _lib
     from pylith_b200 import feassemble as FA
     from pylith_b200 import materials as MAT
 
-    mesh = load_mesh(args.cells, seed=rank)
-    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=rank)
+    halo = None
+    if world == 1:
+        mesh = load_mesh(args.cells, seed=0)
+        rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+        global_dof = mesh.num_dof
+    else:
+        from pylith_b200.parallel import HaloExchange, partition_mesh
+
+        gmesh = load_mesh(args.cells * world, seed=0, stretch=world)
+        grho, gmu, gK = MAT.lognormal_elastic(gmesh.num_cells, seed=0)
+        global_dof = gmesh.num_dof
+        part = partition_mesh(gmesh, world)[rank]
+        mesh = part.mesh
+        ids = part.cell_ids
+        rho, mu, K = grho[ids], gmu[ids], gK[ids]
+        del gmesh, grho, gmu, gK
     mat = MAT.IsotropicLinearElasticity(rho, mu, K)
     ctx = FA.Context(local_rank)
     dmesh = FA.DeviceMesh(ctx, mesh)
     ig = mat.create_integrator(dmesh)
     n = dmesh.num_dof
+    if world > 1:
+        halo = HaloExchange(part, device="cuda", ctx=ctx)
+        hsend = torch.empty(3 * halo.total, dtype=torch.float64, device="cuda")
+        hrecv = torch.empty_like(hsend)
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     u = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
     v = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
@@ -275,11 +317,17 @@ def main():
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
+    def exchange(out):
+        if halo is not None:
+            halo.sum_shared(out, hsend, hrecv)
+
     def app_residual():
         ig.compute_lhs_residual(0.0, 0.0, u, r)
+        exchange(r)
 
     def app_jv():
         ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, u, v, jv)
+        exchange(jv)
 
     for _ in range(args.warmup):
         flush.zero_()
@@ -316,7 +364,7 @@ def main():
         tt = torch.tensor([t_total, t_res, t_jv], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_total, t_res, t_jv = tt.tolist()
-    value = world * 2 * n * args.steps / t_total / 1e9
+    value = 2 * global_dof * args.steps / t_total / 1e9
 
     # End to end through the public API with host buffers: every step copies its u and v from
     # pinned host memory, computes the residual and J v, and copies both results back. Copies in
@@ -350,8 +398,10 @@ def main():
         comp.wait_event(ev_in[i])
         comp.wait_event(ev_out[i])  # results of step k - 2 copied out
         ig.compute_lhs_residual(0.0, 0.0, du[i], dr[i])
+        exchange(dr[i])
         ev_res[i].record(comp)
         ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, du[i], dv[i], djv[i])
+        exchange(djv[i])
         ev_done[i].record(comp)
         s_out.wait_event(ev_res[i])
         with torch.cuda.stream(s_out):
@@ -388,7 +438,7 @@ def main():
         e2e_step(k, stream)
     torch.cuda.synchronize()
     t_e2e = timed(eager)
-    e2e_value = world * 2 * n * args.steps / t_e2e / 1e9
+    e2e_value = 2 * global_dof * args.steps / t_e2e / 1e9
 
     # the host link on this box: pinned copies of one step's input bytes, each direction alone and
     # both directions at once (the bound of the overlapped end-to-end steps)
@@ -439,10 +489,11 @@ def main():
         torch.cuda.synchronize()
         t = timed(gr.replay)
         del gr
-        return world * 2 * n * args.steps / t / 1e9
+        return 2 * global_dof * args.steps / t / 1e9
 
     try:
-        e2e_graph = graph_e2e()
+        # the exchange's NCCL calls stay out of graph capture
+        e2e_graph = graph_e2e() if world == 1 else None
     except RuntimeError as exc:  # capture not possible here: report the per-call figure only
         log(f"graph e2e skipped: {exc}")
         e2e_graph = None
@@ -463,7 +514,11 @@ def main():
             "data": "synthetic",
             "config": {"workload": "elasticity P1 tet residual+Jv", "cells": mesh.num_cells,
                        "nodes": mesh.num_nodes, "dof": n, "l2": "flushed before every application (256 MiB write)",
-                       "ms_residual": t_res / args.steps * 1e3, "ms_jv": t_jv / args.steps * 1e3},
+                       "ms_residual": t_res / args.steps * 1e3, "ms_jv": t_jv / args.steps * 1e3,
+                       "parallelism": "single GPU" if world == 1 else
+                       f"{world} cell partitions of one {global_dof // 3}-node mesh; shared-node sums "
+                       "by pack kernel + NCCL send/recv + add kernel inside every application",
+                       "global_dof": global_dof},
             "roofline": {"bound": "hbm", "kernel": "residual (P1 tet, FP64)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "algorithmic_bytes": alg, "traffic": traffic},
@@ -481,7 +536,7 @@ def main():
         lim = issue_limiter(mesh, t_res / args.steps, line["clocks"].get("sm_mhz"))
         if lim is not None:
             line["roofline"]["limiter"] = lim
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(mesh, mat, "oracle")
         print(json.dumps(line), flush=True)
     if dist:
@@ -735,17 +790,28 @@ def config_c3(args):
 
 def config_c4(args):
     """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
-    material, random rectangular left-lateral slip patch of 0.1-3 m. Server (FP32-refined, 8 slots,
-    HBM-budget admission) vs the FP64 one-at-a-time path on the same stream."""
+    material, random rectangular left-lateral slip patch of 0.1-3 m. Server (continuous batching in
+    one ragged batch, FP32-refined, HBM-budget admission) vs the FP64 one-at-a-time path. The
+    requests' host-side meshes are built before the stream starts, for both."""
     from pylith_b200 import serving as SV
 
     count = max(8, int(40 * args.scale))
     reqs = SV.poisson_requests(count, rate=200.0, seed=0, n_min=8, n_max=max(8, int(96 * min(1.0, args.scale))))
-    served = SV.Server(slots=8).run(reqs)
-    seq = SV.serve_sequential(reqs)
+    t0 = time.perf_counter()
+    hps = [SV.prepare(r) for r in reqs]
+    t_host = time.perf_counter() - t0
+    SV.Server(slots=64).run(hps[:2])  # warm-up: device code loading and the first graph capture
+    server = SV.Server(slots=64)
+    served = server.run(hps)
+    seq = SV.serve_sequential(hps)
     a, b = SV.summarize(served), SV.summarize(seq)
+    mem = np.array([(p, m) for _, p, m in server.memory], dtype=float)
     return {"config": "c4", "requests": count, "server": a, "fp64_one_at_a_time": b,
-            "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"]}
+            "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"],
+            "host_mesh_build_s_excluded": t_host,
+            "admission_bytes": {"predicted_total": float(mem[:, 0].sum()), "measured_total": float(mem[:, 1].sum()),
+                                "how": "predicted: estimate_bytes(n) formula used for admission; measured: "
+                                       "free device memory before and after each request's build"}}
 
 
 CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c4": config_c4}

@@ -168,6 +168,18 @@ int64_t pl_kernel_launches(void);
  * "IsotropicLinearElasticity3D::f1v_infinitesimalStrain"; NULL if unknown. The addresses are
  * those of the pylith::fekernels declarations in include/pylith_b200/fekernels.hh. */
 void* pl_fekernel_lookup(const char* name);
+/* Registers the caller's own compiled copy of a pointwise kernel under its PyLith name, so that a
+ * material or fault compiled against the reference's libsrc/pylith/fekernels/*.hh can pass the
+ * same function pointers it hands to PetscWeakFormAddResidual / PetscWeakFormAddJacobian
+ * (IntegratorDomain.cc:135-205, IntegratorInterface.cc:243-310) to the registration calls below.
+ * The function is first run on the host on a fixed set of probe inputs and must compute what the
+ * named kernel computes (relative 1e-12); the engine then runs its device implementation of that
+ * name for the address. Returns PL_ERR_UNKNOWN_KERNEL for a name without a device implementation
+ * or a function that computes something else, PL_ERR_INVALID_ARG for an address already
+ * registered under another name. Registering the same pair again is a no-op. Thread-safe. */
+int pl_fekernel_register(const char* name, const void* fn);
+/* PyLith name of a known or registered kernel address; NULL if the address is unknown. */
+const char* pl_fekernel_name(const void* fn);
 
 /* ---- context -------------------------------------------------------------------------- */
 int pl_context_create(int device, pl_context* out);
@@ -370,6 +382,56 @@ int pl_batch_solver_get_chebyshev(pl_batch_solver solver, double* lambda_max);
 int pl_batch_solver_get_stats(pl_batch_solver solver, int64_t* solves, int64_t* inner_iterations,
                               int64_t* outer_iterations, double* max_rel_residual);
 int pl_batch_solver_destroy(pl_batch_solver solver);
+
+/* ---- ragged batches: many meshes of uneven size solved together (replaces one problem per
+ *      solve, libsrc/pylith/problems/GreensFns.cc:291-337 and one run per forward problem) ---- */
+/* A ragged batch runs the FP32 PCG iterations (with reliable updates to FP64 accuracy) of many
+ * solvers at once: per iteration one operator launch covers the cells of every active member and
+ * seven vector/reduction launches cover all their vectors, with dot products, step lengths and
+ * convergence kept per member, so each member follows exactly its own PCG. Members join
+ * (pl_ragged_add) and leave (on convergence, or pl_ragged_remove) between iteration chunks.
+ * Members: solvers of Q1 hexahedral meshes with one domain integrator (and any faults), set up
+ * with PL_SOLVER_FP32_REFINED, all on the batch's context. */
+typedef struct pl_ragged_s* pl_ragged;
+int pl_ragged_create(pl_context ctx, int capacity, pl_ragged* out);
+/* Adds a solve A x = b (b_dev, x_dev: the solver's full local vectors, device memory that must
+ * stay valid while the member is in the batch). Computes the member's initial FP64 residual with
+ * its own launches (synchronises the context's stream); *member is its slot. */
+int pl_ragged_add(pl_ragged batch, pl_solver solver, const double* b_dev, double* x_dev, int* member);
+/* Runs one chunk of PCG iterations (pl_ragged_set_chunk, default 10) on every active member as
+ * one CUDA graph, then checks each member: residual replacement (FP64 true residual) when its
+ * iterated residual has dropped by the solver's reliable delta, completion when the true residual
+ * meets the solver's tolerances. *active_left: members still iterating. */
+int pl_ragged_iterate(pl_ragged batch, int* active_left);
+/* status: PL_ERR_NOT_READY while iterating, PL_OK when converged (x_dev holds the solution), an
+ * error code otherwise; iterations and the final relative FP64 residual. */
+int pl_ragged_member_status(pl_ragged batch, int member, int* status, int* iterations, double* rel_residual);
+/* Frees a member's slot (for a later pl_ragged_add); the other members keep theirs. */
+int pl_ragged_remove(pl_ragged batch, int member);
+int pl_ragged_set_chunk(pl_ragged batch, int iterations);
+int pl_ragged_destroy(pl_ragged batch);
+
+/* ---- partitioned meshes: shared-node exchange (replaces DMLocalToGlobal with ADD_VALUES
+ *      over the PetscSF, libsrc/pylith/topology/Field.cc:394-402, TimeDependent.cc:667) ------ */
+/* Exchange plan of one partition: npeers neighbouring partitions, counts[p] nodes shared with
+ * neighbour p, and nodes_host the local node indices of those lists concatenated neighbour after
+ * neighbour, each list in an order both partitions agree on (e.g. by global node id). */
+typedef struct pl_halo_s* pl_halo;
+int pl_halo_create(pl_context ctx, int npeers, const int64_t* counts, const int32_t* nodes_host,
+                   pl_halo* out);
+/* Number of listed entries (the send and receive buffers hold 3 values per entry). */
+int64_t pl_halo_num_entries(pl_halo halo);
+/* Copies the 3 values of every listed node of r_dev, neighbour after neighbour, into send_dev
+ * (one launch on the context's stream). */
+int pl_halo_pack(pl_halo halo, const double* r_dev, double* send_dev);
+/* Adds the neighbours' partial sums recv_dev (laid out as send_dev) into r_dev: each shared node
+ * gets its neighbours' values summed in neighbour order and added once (no atomics: the same
+ * result every run). After it every partition holds the global residual at all of its nodes. */
+int pl_halo_unpack_add(pl_halo halo, const double* recv_dev, double* r_dev);
+/* FP32 versions for the inner iterations of the mixed-precision solvers. */
+int pl_halo_pack_f32(pl_halo halo, const float* r_dev, float* send_dev);
+int pl_halo_unpack_add_f32(pl_halo halo, const float* recv_dev, float* r_dev);
+int pl_halo_destroy(pl_halo halo);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,7 @@ _I64 = ctypes.c_int64
 _D = ctypes.c_double
 
 PL_OK = 0
+ERRORS_NOT_READY = -8
 ERRORS = {
     -1: "PL_ERR_INVALID_ARG", -2: "PL_ERR_UNKNOWN_KERNEL", -3: "PL_ERR_CUDA",
     -4: "PL_ERR_OUT_OF_MEMORY", -5: "PL_ERR_NOT_CONVERGED", -6: "PL_ERR_DEVICE_CHECK",
@@ -65,6 +66,8 @@ SIGNATURES = {
     "pl_last_error": (ctypes.c_char_p, []),
     "pl_kernel_launches": (_I64, []),
     "pl_fekernel_lookup": (_P, [ctypes.c_char_p]),
+    "pl_fekernel_register": (_I, [ctypes.c_char_p, _P]),
+    "pl_fekernel_name": (ctypes.c_char_p, [_P]),
     "pl_context_create": (_I, [_I, ctypes.POINTER(_P)]),
     "pl_context_destroy": (_I, [_P]),
     "pl_context_set_stream": (_I, [_P, _P]),
@@ -124,6 +127,20 @@ SIGNATURES = {
     "pl_batch_solver_set_chebyshev": (_I, [_P, _I, _D, _I]),
     "pl_batch_solver_get_chebyshev": (_I, [_P, ctypes.POINTER(_D)]),
     "pl_batch_solver_set_reliable": (_I, [_P, _I, _D]),
+    "pl_ragged_create": (_I, [_P, _I, ctypes.POINTER(_P)]),
+    "pl_ragged_add": (_I, [_P, _P, _P, _P, ctypes.POINTER(_I)]),
+    "pl_ragged_iterate": (_I, [_P, ctypes.POINTER(_I)]),
+    "pl_ragged_member_status": (_I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D)]),
+    "pl_ragged_remove": (_I, [_P, _I]),
+    "pl_ragged_set_chunk": (_I, [_P, _I]),
+    "pl_ragged_destroy": (_I, [_P]),
+    "pl_halo_create": (_I, [_P, _I, _P, _P, ctypes.POINTER(_P)]),
+    "pl_halo_num_entries": (_I64, [_P]),
+    "pl_halo_pack": (_I, [_P, _P, _P]),
+    "pl_halo_unpack_add": (_I, [_P, _P, _P]),
+    "pl_halo_pack_f32": (_I, [_P, _P, _P]),
+    "pl_halo_unpack_add_f32": (_I, [_P, _P, _P]),
+    "pl_halo_destroy": (_I, [_P]),
 }
 PL_SOLVER_FP64, PL_SOLVER_FP32_REFINED = 0, 1
 

@@ -20,6 +20,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -332,6 +334,278 @@ __global__ void __launch_bounds__(kTetThreads, PLB_TET_MIN_BLOCKS) k_tet_blocked
     __pipeline_wait_prior(0);
 }
 
+// ---- cell-block kernels over the padded layout ---------------------------------------------------
+// The same cell blocks, staged from padded per-block arrays (built with the layout): per block the
+// CTA copies, one block ahead, its coordinates, node ids, incidence offsets and incidence list as
+// 16-byte cp.async runs, and gathers the input field of its nodes with 8-byte cp.async; the
+// incidence list holds staging offsets (corner * 3 * cells + cell), so the node sums do no index
+// arithmetic. Two schedules:
+//  * PIPE: one barrier per block: iteration i computes the element vectors of block b_i into one
+//    staging buffer while the node sums of block b_{i-1} read the other (element vectors x2, node
+//    data x2, block metadata x3; 3 CTAs per SM);
+//  * two barriers per block (element vectors, then node sums of the same block; element vectors
+//    x1, node data x2, metadata x2; 4 CTAs per SM).
+#ifndef PLB_PIPE_MIN_BLOCKS
+#define PLB_PIPE_MIN_BLOCKS 3
+#endif
+#ifndef PLB_PAD2_MIN_BLOCKS
+#define PLB_PAD2_MIN_BLOCKS 4
+#endif
+
+struct PipeArrays {
+    const int32_t* slot_begin;  // [nblocks + 1] unpadded slots (slot counts, deterministic partials)
+    const int32_t* pbeg;        // [nblocks + 1] padded slot starts (multiples of 4)
+    const uint32_t* ids;        // per padded slot: node id | kSharedBit
+    const double* coords;       // per block [3][padded slots]
+    const uint32_t* off;        // per block at pbeg[b] + 4 b: ns + 1 incidence offsets
+    const uint16_t* inc;        // [nblocks][4 * kTetBlockCells] staging offsets
+    const ushort4* lconn;       // [ncells] block-local slots of the 4 corners
+    double* partial;            // [slots][3] deterministic partial sums (unpadded slot index)
+    int64_t nblocks;
+    int ld;                     // padded slots of the largest block (multiple of 4)
+};
+
+PL_HD size_t pipe_meta_bytes(int ld) {
+    return round16(4 * (size_t)ld) + round16(4 * ((size_t)ld + 4)) + round16(2 * 4 * (size_t)kTetBlockCells);
+}
+
+PL_HD size_t pipe_smem_bytes(int ld) {
+    return 2 * 12 * (size_t)kTetBlockCells * sizeof(double) + 2 * 6 * (size_t)ld * sizeof(double) + 3 * pipe_meta_bytes(ld);
+}
+
+PL_HD size_t pad2_smem_bytes(int ld) {
+    return 12 * (size_t)kTetBlockCells * sizeof(double) + 2 * 6 * (size_t)ld * sizeof(double) + 2 * pipe_meta_bytes(ld);
+}
+
+struct PipeMeta {
+    uint32_t* ids;
+    uint32_t* off;
+    uint16_t* inc;
+};
+
+PL_D PipeMeta pipe_meta(char* base, int ld) {
+    PipeMeta m;
+    m.ids = reinterpret_cast<uint32_t*>(base);
+    base += round16(4 * (size_t)ld);
+    m.off = reinterpret_cast<uint32_t*>(base);
+    base += round16(4 * ((size_t)ld + 4));
+    m.inc = reinterpret_cast<uint16_t*>(base);
+    return m;
+}
+
+PL_D void pipe_load_ids(const PipeArrays& A, int64_t b, uint32_t nd[kMaxSlotsPerThread]) {
+#pragma unroll
+    for (int k = 0; k < kMaxSlotsPerThread; ++k) nd[k] = 0u;
+    if (b >= A.nblocks) return;
+    const int p0 = A.pbeg[b];
+    const int ns = A.slot_begin[b + 1] - A.slot_begin[b];
+#pragma unroll
+    for (int k = 0; k < kMaxSlotsPerThread; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        if (i < ns) nd[k] = A.ids[p0 + i];
+    }
+}
+
+// Asynchronous copies of block b: coordinates, ids, offsets and incidences as aligned 16-byte
+// runs, the field of its nodes (ids in nd, read one block earlier) as 8-byte gathers.
+PL_D void pipe_stage(const double* __restrict__ field, const PipeArrays& A, int64_t b,
+                     const uint32_t nd[kMaxSlotsPerThread], double* node, const PipeMeta& M, int ld) {
+    const int p0 = A.pbeg[b];
+    const int np = A.pbeg[b + 1] - p0;
+    const int ns = A.slot_begin[b + 1] - A.slot_begin[b];
+    const int half = np >> 1;  // 16-byte chunks per coordinate component
+    for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
+        const int d = t / half, j = t - d * half;
+        __pipeline_memcpy_async(&node[d * ld + 2 * j], &A.coords[3 * (int64_t)p0 + (int64_t)d * np + 2 * j], 16);
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxSlotsPerThread; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        if (i < ns) {
+            const int64_t n = nd[k] & ~kSharedBit;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) __pipeline_memcpy_async(&node[(3 + d) * ld + i], &field[3 * n + d], sizeof(double));
+        }
+    }
+    const int q = np >> 2;  // 16-byte chunks of ids; offsets take one more
+    for (int t = threadIdx.x; t < q; t += blockDim.x) __pipeline_memcpy_async(&M.ids[4 * t], &A.ids[p0 + 4 * t], 16);
+    for (int t = threadIdx.x; t <= q; t += blockDim.x)
+        __pipeline_memcpy_async(&M.off[4 * t], &A.off[(int64_t)p0 + 4 * b + 4 * t], 16);
+    for (int t = threadIdx.x; t < kTetBlockCells / 2; t += blockDim.x)
+        __pipeline_memcpy_async(&M.inc[8 * t], &A.inc[b * 4 * kTetBlockCells + 8 * t], 16);
+}
+
+// Node sums of block b (element vectors in sE, metadata in M): one thread per node.
+template <bool INSERT, bool DET>
+PL_D void pipe_node_sums(const DomainParams& p, const PipeArrays& A, int64_t b, const double* sE, const PipeMeta& M) {
+    const int s0 = A.slot_begin[b];
+    const int ns = A.slot_begin[b + 1] - s0;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        const int j0 = M.off[k], j1 = M.off[k + 1];
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+#pragma unroll 4
+        for (int j = j0; j < j1; ++j) {
+            const int e = M.inc[j];
+            r0 += sE[e];
+            r1 += sE[e + kTetBlockCells];
+            r2 += sE[e + 2 * kTetBlockCells];
+        }
+        const uint32_t id = M.ids[k];
+        double* o = p.out + 3 * (int64_t)(id & ~kSharedBit);
+        if ((id & kSharedBit) && DET) {
+            double* pp = A.partial + 3 * (int64_t)(s0 + k);
+            pp[0] = r0;
+            pp[1] = r1;
+            pp[2] = r2;
+        } else if (id & kSharedBit) {
+            red_add(o, r0);
+            red_add(o + 1, r1);
+            red_add(o + 2, r2);
+        } else if (INSERT) {
+            o[0] = r0;
+            o[1] = r1;
+            o[2] = r2;
+        } else {
+            o[0] += r0;
+            o[1] += r1;
+            o[2] += r2;
+        }
+    }
+}
+
+template <int RHEO, bool BF, int OP, bool INSERT, bool DET>
+__global__ void __launch_bounds__(kTetBlockCells, PLB_PIPE_MIN_BLOCKS) k_tet_pipe(DomainParams p, PipeArrays A) {
+    using L = AuxLayout<RHEO, BF>;
+    extern __shared__ __align__(16) char smem_raw[];
+    const AuxOffsets<RHEO, BF> aoff;
+    const double* __restrict__ field = OP == OP_RESIDUAL ? p.u : p.v;
+    const int ld = A.ld;
+    double* sEb = reinterpret_cast<double*>(smem_raw);            // [2][12][kTetBlockCells]
+    double* nodeb = sEb + 2 * 12 * kTetBlockCells;                // [2][6][ld]
+    char* metab = reinterpret_cast<char*>(nodeb + 2 * 6 * ld);   // [3][pipe_meta_bytes]
+    const size_t mb = pipe_meta_bytes(ld);
+    const int64_t G = gridDim.x;
+    const int tc = threadIdx.x;
+    int64_t b = blockIdx.x;
+    if (b >= A.nblocks) return;
+    uint32_t nd_next[kMaxSlotsPerThread];
+    {
+        uint32_t nd0[kMaxSlotsPerThread];
+        pipe_load_ids(A, b, nd0);
+        pipe_stage(field, A, b, nd0, nodeb, pipe_meta(metab, ld), ld);
+        __pipeline_commit();
+        pipe_load_ids(A, b + G, nd_next);
+    }
+    int it = 0;
+    int64_t bprev = -1;
+    for (; b < A.nblocks; b += G, ++it) {
+        // this block's per-cell inputs and the slot ids two blocks ahead: issued before the wait
+        const int64_t c = b * kTetBlockCells + tc;
+        ushort4 lc = make_ushort4(0, 0, 0, 0);
+        double a[L::size];
+        if (c < p.ncells) {
+            lc = A.lconn[c];
+            L::load_cell(p, c, a);
+        }
+        uint32_t nd_after[kMaxSlotsPerThread];
+        pipe_load_ids(A, b + 2 * G, nd_after);
+        __pipeline_wait_prior(0);
+        // block b's copies have landed, and every thread has finished iteration it - 1 (its
+        // element vectors are complete; the buffers staged below are no longer read)
+        __syncthreads();
+        if (b + G < A.nblocks) {
+            pipe_stage(field, A, b + G, nd_next, nodeb + ((it + 1) & 1) * 6 * ld, pipe_meta(metab + ((it + 1) % 3) * mb, ld), ld);
+            const int64_t cn = (b + G) * kTetBlockCells + tc;
+            if (cn < p.ncells) {
+                prefetch_l2(&A.lconn[cn]);
+                prefetch_l2(&p.mu[cn]);
+                prefetch_l2(&p.K[cn]);
+                if (BF)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) prefetch_l2(&p.body_force[d * p.ncells + cn]);
+            }
+        }
+        __pipeline_commit();
+#pragma unroll
+        for (int k = 0; k < kMaxSlotsPerThread; ++k) nd_next[k] = nd_after[k];
+        SmemBuf S;
+        S.node = nodeb + (it & 1) * 6 * ld;
+        S.ld = ld;
+        double* sE = sEb + (it & 1) * 12 * kTetBlockCells;
+        if (c < p.ncells) tet_cell_element<RHEO, BF, OP>(p, aoff.v, a, lc, S, sE, tc);
+        if (bprev >= 0)
+            pipe_node_sums<INSERT, DET>(p, A, bprev, sEb + ((it + 1) & 1) * 12 * kTetBlockCells,
+                                        pipe_meta(metab + ((it + 2) % 3) * mb, ld));
+        bprev = b;
+    }
+    __syncthreads();
+    pipe_node_sums<INSERT, DET>(p, A, bprev, sEb + ((it + 1) & 1) * 12 * kTetBlockCells,
+                                pipe_meta(metab + ((it + 2) % 3) * mb, ld));
+    __pipeline_wait_prior(0);
+}
+
+template <int RHEO, bool BF, int OP, bool INSERT, bool DET>
+__global__ void __launch_bounds__(kTetBlockCells, PLB_PAD2_MIN_BLOCKS) k_tet_pad2(DomainParams p, PipeArrays A) {
+    using L = AuxLayout<RHEO, BF>;
+    extern __shared__ __align__(16) char smem_raw[];
+    const AuxOffsets<RHEO, BF> aoff;
+    const double* __restrict__ field = OP == OP_RESIDUAL ? p.u : p.v;
+    const int ld = A.ld;
+    double* sE = reinterpret_cast<double*>(smem_raw);             // [12][kTetBlockCells]
+    double* nodeb = sE + 12 * kTetBlockCells;                      // [2][6][ld]
+    char* metab = reinterpret_cast<char*>(nodeb + 2 * 6 * ld);    // [2][pipe_meta_bytes]
+    const size_t mb = pipe_meta_bytes(ld);
+    const int64_t G = gridDim.x;
+    const int tc = threadIdx.x;
+    int64_t b = blockIdx.x;
+    if (b >= A.nblocks) return;
+    uint32_t nd_next[kMaxSlotsPerThread];
+    {
+        uint32_t nd0[kMaxSlotsPerThread];
+        pipe_load_ids(A, b, nd0);
+        pipe_stage(field, A, b, nd0, nodeb, pipe_meta(metab, ld), ld);
+        __pipeline_commit();
+        pipe_load_ids(A, b + G, nd_next);
+    }
+    for (int it = 0; b < A.nblocks; b += G, ++it) {
+        const int64_t c = b * kTetBlockCells + tc;
+        ushort4 lc = make_ushort4(0, 0, 0, 0);
+        double a[L::size];
+        if (c < p.ncells) {
+            lc = A.lconn[c];
+            L::load_cell(p, c, a);
+        }
+        uint32_t nd_after[kMaxSlotsPerThread];
+        pipe_load_ids(A, b + 2 * G, nd_after);
+        __pipeline_wait_prior(0);
+        // block b's copies have landed; every thread has finished the node sums of the previous
+        // block (its buffers are free for block b + G)
+        __syncthreads();
+        if (b + G < A.nblocks) {
+            pipe_stage(field, A, b + G, nd_next, nodeb + ((it + 1) & 1) * 6 * ld, pipe_meta(metab + ((it + 1) & 1) * mb, ld), ld);
+            const int64_t cn = (b + G) * kTetBlockCells + tc;
+            if (cn < p.ncells) {
+                prefetch_l2(&A.lconn[cn]);
+                prefetch_l2(&p.mu[cn]);
+                prefetch_l2(&p.K[cn]);
+                if (BF)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) prefetch_l2(&p.body_force[d * p.ncells + cn]);
+            }
+        }
+        __pipeline_commit();
+#pragma unroll
+        for (int k = 0; k < kMaxSlotsPerThread; ++k) nd_next[k] = nd_after[k];
+        SmemBuf S;
+        S.node = nodeb + (it & 1) * 6 * ld;
+        S.ld = ld;
+        if (c < p.ncells) tet_cell_element<RHEO, BF, OP>(p, aoff.v, a, lc, S, sE, tc);
+        __syncthreads();
+        pipe_node_sums<INSERT, DET>(p, A, b, sE, pipe_meta(metab + (it & 1) * mb, ld));
+    }
+    __pipeline_wait_prior(0);
+}
+
 // FP32 Jacobian action of isotropic linear elasticity on the cell blocks: geometry (cofactors,
 // 1/det) and the elastic tangent in FP64 per cell, the field, gradient, flux and element vectors
 // in FP32. Used by the inner iterations of the mixed-precision solver.
@@ -511,6 +785,64 @@ static void launch_t(const DomainParams& p, const BlockedLayout& b, bool insert,
     }
 }
 
+static PipeArrays pipe_arrays_of(const BlockedLayout& b, double* partial) {
+    PipeArrays A;
+    A.slot_begin = b.d_block_node_begin;
+    A.pbeg = b.d_pipe_begin;
+    A.ids = b.d_pipe_ids;
+    A.coords = b.d_pipe_coords;
+    A.off = b.d_pipe_off;
+    A.inc = b.d_pipe_inc;
+    A.lconn = (const ushort4*)b.d_local_cells;
+    A.partial = partial;
+    A.nblocks = b.num_blocks;
+    A.ld = (b.max_local_nodes + 3) & ~3;
+    return A;
+}
+
+template <bool PIPE, int RHEO, bool BF, int OP, bool INSERT, bool DET>
+static void launch_pipe_one(const DomainParams& p, const PipeArrays& A, size_t smem, int grid, cudaStream_t s) {
+    auto kern = PIPE ? k_tet_pipe<RHEO, BF, OP, INSERT, DET> : k_tet_pad2<RHEO, BF, OP, INSERT, DET>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, kTetBlockCells, smem, s>>>(p, A);
+    count_launch();
+}
+
+template <bool PIPE, int RHEO, bool BF, int OP>
+static void launch_pipe_t(const DomainParams& p, const BlockedLayout& b, bool insert, double* partial, cudaStream_t s) {
+    const PipeArrays A = pipe_arrays_of(b, partial);
+    const size_t smem = PIPE ? pipe_smem_bytes(A.ld) : pad2_smem_bytes(A.ld);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)std::min<int64_t>(b.num_blocks, (int64_t)nsm * (PIPE ? PLB_PIPE_MIN_BLOCKS : PLB_PAD2_MIN_BLOCKS));
+    const bool det = partial != nullptr;
+    if (insert && det) launch_pipe_one<PIPE, RHEO, BF, OP, true, true>(p, A, smem, grid, s);
+    else if (insert) launch_pipe_one<PIPE, RHEO, BF, OP, true, false>(p, A, smem, grid, s);
+    else if (det) launch_pipe_one<PIPE, RHEO, BF, OP, false, true>(p, A, smem, grid, s);
+    else launch_pipe_one<PIPE, RHEO, BF, OP, false, false>(p, A, smem, grid, s);
+    if (det && b.num_fix > 0) {
+        const int fg = (int)std::min<int64_t>((b.num_fix + 255) / 256, 148 * 8);
+        if (insert) k_blocked_fixup<true><<<fg, 256, 0, s>>>(p.out, partial, b.d_fix_node, b.d_fix_off, b.d_fix_slot, b.num_fix);
+        else k_blocked_fixup<false><<<fg, 256, 0, s>>>(p.out, partial, b.d_fix_node, b.d_fix_off, b.d_fix_slot, b.num_fix);
+        count_launch();
+    }
+}
+
+// Which FP64 cell-block kernel runs, read once per process from PYLITH_B200_TET_KERNEL: "pad2" (the
+// default: two barriers per block over the padded layout), "pipe" (one barrier per block over the
+// padded layout) or "twophase" (two barriers per block, per-thread 8-byte gathers of all node data).
+enum TetKernel { TK_PAD2, TK_PIPE, TK_TWOPHASE };
+static TetKernel tet_kernel_choice() {
+    static const TetKernel k = [] {
+        const char* v = std::getenv("PYLITH_B200_TET_KERNEL");
+        if (v && std::strcmp(v, "pipe") == 0) return TK_PIPE;
+        if (v && std::strcmp(v, "twophase") == 0) return TK_TWOPHASE;
+        return TK_PAD2;
+    }();
+    return k;
+}
+
 static bool blocked_usable(const BlockedLayout& b) {
     return b.num_blocks > 0 && b.max_local_nodes <= kMaxSlotsPerThread * kTetThreads &&
            blocked_smem(b) <= 200 * 1024;
@@ -525,11 +857,21 @@ bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, 
     // Without one, shared nodes get FP64 reductions, and for INSERT the output starts from zero.
     if (!partial && insert && (b.num_shared_nodes > 0 || b.num_untouched > 0))
         if (cudaMemsetAsync(p.out, 0, 3 * nnodes * sizeof(double), s) != cudaSuccess) return false;
+    const int ld = (b.max_local_nodes + 3) & ~3;
+    TetKernel k = tet_kernel_choice();
+    if (!b.d_pipe_begin || (k == TK_PIPE && pipe_smem_bytes(ld) > 75 * 1024) || (k == TK_PAD2 && pad2_smem_bytes(ld) > 56 * 1024))
+        k = TK_TWOPHASE;
     if (op == OP_RESIDUAL) {
-        if (bf) launch_t<RHEO_ILE, true, OP_RESIDUAL>(p, b, insert, partial, s);
+        if (k == TK_PIPE && bf) launch_pipe_t<true, RHEO_ILE, true, OP_RESIDUAL>(p, b, insert, partial, s);
+        else if (k == TK_PIPE) launch_pipe_t<true, RHEO_ILE, false, OP_RESIDUAL>(p, b, insert, partial, s);
+        else if (k == TK_PAD2 && bf) launch_pipe_t<false, RHEO_ILE, true, OP_RESIDUAL>(p, b, insert, partial, s);
+        else if (k == TK_PAD2) launch_pipe_t<false, RHEO_ILE, false, OP_RESIDUAL>(p, b, insert, partial, s);
+        else if (bf) launch_t<RHEO_ILE, true, OP_RESIDUAL>(p, b, insert, partial, s);
         else launch_t<RHEO_ILE, false, OP_RESIDUAL>(p, b, insert, partial, s);
     } else {
-        launch_t<RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, insert, partial, s);
+        if (k == TK_PIPE) launch_pipe_t<true, RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, insert, partial, s);
+        else if (k == TK_PAD2) launch_pipe_t<false, RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, insert, partial, s);
+        else launch_t<RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, insert, partial, s);
     }
     return true;
 }
@@ -563,11 +905,49 @@ bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, i
 #define PLB_PLAN_ITERS 12000
 #endif
 struct BlockPlan {
-    std::vector<int32_t> loc;     // global ids of the local nodes, sorted
-    std::vector<int32_t> newidx;  // local index of loc[l]
-    std::vector<uint16_t> inc;    // incidence entries (cell * 4 + corner) by local index
-    std::vector<uint32_t> off;    // [nloc + 1] offsets into inc
+    std::vector<int32_t> loc;       // global ids of the local nodes, sorted
+    std::vector<int32_t> newidx;    // local index of loc[l]
+    std::vector<uint16_t> inc;      // incidence entries (cell * 4 + corner) by local index
+    std::vector<uint32_t> off;      // [nloc + 1] offsets into inc
+    std::vector<uint16_t> inc_pipe; // the same incidences in the same order, as staging offsets
+                                    // corner * 3 * kTetBlockCells + cell (padded-layout kernels)
 };
+
+// Orders each node's incidences (lists[k], entries cell * 4 + corner) so that the entries that
+// the lanes of one warp read in one step (bank pair = cell mod 16) spread over the banks; the
+// warp of node k is group(k) and its lanes run the group's nodes in increasing k. Returns the
+// per-node ordered lists.
+template <typename Group>
+static std::vector<std::vector<int>> order_for_banks(std::vector<std::vector<int>> lists, int ngroups, Group group) {
+    constexpr int R = 16;
+    const int nloc = (int)lists.size();
+    std::vector<std::vector<int>> members(ngroups), ordered(nloc);
+    for (int k = 0; k < nloc; ++k) members[group(k)].push_back(k);
+    for (const std::vector<int>& mem : members) {
+        const int nl = (int)mem.size();
+        if (nl == 0) continue;
+        std::vector<int> lanes(nl);
+        int depth = 0;
+        for (int k : mem) depth = std::max(depth, (int)lists[k].size());
+        for (int j = 0; j < depth; ++j) {
+            int c16[R] = {0};
+            for (int i = 0; i < nl; ++i) lanes[i] = i;
+            std::stable_sort(lanes.begin(), lanes.end(),
+                             [&](int x, int y) { return lists[mem[x]].size() > lists[mem[y]].size(); });
+            for (int i : lanes) {
+                std::vector<int>& L = lists[mem[i]];
+                if (L.empty()) continue;
+                size_t best = 0;
+                for (size_t t = 1; t < L.size(); ++t)
+                    if (c16[(L[t] >> 2) & (R - 1)] < c16[(L[best] >> 2) & (R - 1)]) best = t;
+                c16[(L[best] >> 2) & (R - 1)]++;
+                ordered[mem[i]].push_back(L[best]);
+                L.erase(L.begin() + best);
+            }
+        }
+    }
+    return ordered;
+}
 
 static uint64_t splitmix64(uint64_t& x) {
     uint64_t z = (x += 0x9E3779B97F4A7C15ull);
@@ -650,39 +1030,21 @@ static void plan_block(const int32_t* bc, int ncell, uint64_t seed, BlockPlan& P
         std::stable_sort(nodes.begin(), nodes.end(), [&](int x, int y) { return deg[x] > deg[y]; });
         for (size_t i = 0; i < nodes.size(); ++i) perm[nodes[i]] = slots[i];
     }
-    // incidences by new index, in (cell, corner) order, then ordered warp by warp
+    // incidences by new index, in (cell, corner) order, then ordered for the banks (the warps of
+    // the node sums take 32 consecutive nodes)
     std::vector<std::vector<int>> lists(nloc);
     for (int c = 0; c < ncell; ++c)
         for (int k = 0; k < 4; ++k) lists[perm[lcs[4 * c + k]]].push_back(4 * c + k);
+    const std::vector<std::vector<int>> by_warp = order_for_banks(lists, (nloc + W - 1) / W, [](int k) { return k / W; });
     P.off.assign(nloc + 1, 0);
     P.inc.clear();
     P.inc.reserve(4 * (size_t)ncell);
-    for (int w0 = 0; w0 < nloc; w0 += W) {
-        const int nl = std::min(W, nloc - w0);
-        std::vector<std::vector<int>> ordered(nl);
-        std::vector<int> lanes(nl);
-        int depth = 0;
-        for (int i = 0; i < nl; ++i) depth = std::max(depth, (int)lists[w0 + i].size());
-        for (int j = 0; j < depth; ++j) {
-            int c16[R] = {0};
-            for (int i = 0; i < nl; ++i) lanes[i] = i;
-            std::stable_sort(lanes.begin(), lanes.end(),
-                             [&](int x, int y) { return lists[w0 + x].size() > lists[w0 + y].size(); });
-            for (int i : lanes) {
-                std::vector<int>& L = lists[w0 + i];
-                if (L.empty()) continue;
-                size_t best = 0;
-                for (size_t t = 1; t < L.size(); ++t)
-                    if (c16[(L[t] >> 2) & (R - 1)] < c16[(L[best] >> 2) & (R - 1)]) best = t;
-                c16[(L[best] >> 2) & (R - 1)]++;
-                ordered[i].push_back(L[best]);
-                L.erase(L.begin() + best);
-            }
-        }
-        for (int i = 0; i < nl; ++i) {
-            for (int e : ordered[i]) P.inc.push_back((uint16_t)e);
-            P.off[w0 + i + 1] = (uint32_t)P.inc.size();
-        }
+    P.inc_pipe.clear();
+    P.inc_pipe.reserve(4 * (size_t)ncell);
+    for (int k = 0; k < nloc; ++k) {
+        for (int e : by_warp[k]) P.inc.push_back((uint16_t)e);
+        for (int e : by_warp[k]) P.inc_pipe.push_back((uint16_t)((e & 3) * 3 * kTetBlockCells + (e >> 2)));
+        P.off[k + 1] = (uint32_t)P.inc.size();
     }
 }
 
@@ -734,6 +1096,14 @@ static int build_blocked_layout(pl_mesh_s* m) {
         for (std::thread& x : th) x.join();
         if (failed.load()) return fail(PL_ERR_OUT_OF_MEMORY, "cell-block layout planning ran out of host memory");
     }
+    // padded per-block regions of the pipelined kernel: block b's slots start at pbeg[b], a
+    // multiple of 4, so that its node ids, coordinates ([3][ns rounded up to 4]) and incidence
+    // offsets are 16-byte aligned runs that the kernel copies with 16-byte cp.async
+    std::vector<int32_t> pbeg(nb + 1, 0);
+    std::vector<uint32_t> pids;
+    std::vector<double> pcoords;
+    std::vector<uint32_t> poff;
+    std::vector<uint16_t> pinc((size_t)nb * 4 * B, 0);
     for (int64_t b = 0; b < nb; ++b) {
         BlockPlan& P = plans[b];
         const int64_t c0 = b * B, c1 = std::min<int64_t>(nc, c0 + B);
@@ -745,6 +1115,18 @@ static int build_blocked_layout(pl_mesh_s* m) {
             node_ids[begin[b] + P.newidx[l]] = (uint32_t)P.loc[l];
             nblocks_of[P.loc[l]]++;
         }
+        const int npad = (nloc + 3) & ~3;
+        pbeg[b + 1] = pbeg[b] + npad;
+        pids.resize(pbeg[b + 1], 0u);
+        pcoords.resize(3 * (size_t)pbeg[b + 1], 0.0);
+        for (int l = 0; l < nloc; ++l) {
+            const int i = P.newidx[l];
+            pids[pbeg[b] + i] = (uint32_t)P.loc[l];
+            for (int d = 0; d < 3; ++d) pcoords[3 * (size_t)pbeg[b] + (size_t)d * npad + i] = m->h_coords[3 * (size_t)P.loc[l] + d];
+        }
+        poff.resize((size_t)pbeg[b + 1] + 4 * (b + 1), 0u);
+        for (int i = 0; i <= nloc; ++i) poff[(size_t)pbeg[b] + 4 * b + i] = P.off[i];
+        std::copy(P.inc_pipe.begin(), P.inc_pipe.end(), pinc.begin() + (size_t)b * 4 * B);
         for (int64_t c = c0; c < c1; ++c)
             for (int k = 0; k < 4; ++k) {
                 const int32_t nd = m->h_cells[c * 4 + k];
@@ -758,6 +1140,9 @@ static int build_blocked_layout(pl_mesh_s* m) {
     begin[nb] = (int32_t)node_ids.size();
     for (uint32_t& id : node_ids)
         if (nblocks_of[id] > 1) id |= kSharedBit;
+    for (int64_t b = 0; b < nb; ++b)
+        for (int i = 0; i < begin[b + 1] - begin[b]; ++i)
+            if (nblocks_of[pids[pbeg[b] + i]] > 1) pids[pbeg[b] + i] |= kSharedBit;
     int64_t nshared = 0, nuntouched = 0;
     for (int64_t nd = 0; nd < m->nnodes; ++nd) {
         nshared += nblocks_of[nd] > 1;
@@ -810,6 +1195,11 @@ static int build_blocked_layout(pl_mesh_s* m) {
     up(&L->d_fix_node, fix_node);
     up(&L->d_fix_off, fix_off);
     up(&L->d_fix_slot, fix_slot);
+    up(&L->d_pipe_begin, pbeg);
+    up(&L->d_pipe_ids, pids);
+    up(&L->d_pipe_coords, pcoords);
+    up(&L->d_pipe_off, poff);
+    up(&L->d_pipe_inc, pinc);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         free_blocked_layout(L);
@@ -839,6 +1229,11 @@ void free_blocked_layout(BlockedLayout* b) {
     cudaFree(b->d_fix_node);
     cudaFree(b->d_fix_off);
     cudaFree(b->d_fix_slot);
+    cudaFree(b->d_pipe_begin);
+    cudaFree(b->d_pipe_ids);
+    cudaFree(b->d_pipe_coords);
+    cudaFree(b->d_pipe_off);
+    cudaFree(b->d_pipe_inc);
     delete b;
 }
 

@@ -329,6 +329,10 @@ int pl_mesh_destroy(pl_mesh m) {
 
 extern "C++" {
 namespace plb {
+void context_retain(pl_context_s* c) { c->refs++; }
+void context_release(pl_context_s* c) {
+    if (--c->refs == 0 && c->destroy_requested) context_free(c);
+}
 void mesh_retain(pl_mesh_s* m) { m->refs++; }
 void mesh_release(pl_mesh_s* m) {
     if (--m->refs == 0 && m->destroy_requested) mesh_free(m);

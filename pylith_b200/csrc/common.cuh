@@ -25,6 +25,13 @@ PL_D void flag_error(unsigned int* err, unsigned int code) {
 }
 
 // Reduction into global memory without a return value (red.global.add).
+// CG step length rz / pq for the SPD operator: 0 when pq <= 0 or the step is not a finite float
+// (a search direction that collapsed to rounding noise in FP32 iterations past convergence).
+PL_D float safe_step_f32(double rz, double pq) {
+    const float a = pq > 0.0 ? (float)(rz / pq) : 0.0f;
+    return isfinite(a) ? a : 0.0f;
+}
+
 PL_D void red_add(double* p, double v) { atomicAdd(p, v); }
 PL_D void red_add(float* p, float v) { atomicAdd(p, v); }
 

@@ -78,34 +78,60 @@ PL_D void fill_tables(double* t64, T* tt) {
         t64[H::T_W + q] = CELL == HEX8 ? 1.0 : gauss3_w(q % 3) * gauss3_w((q / 3) % 3) * gauss3_w(q / 9);
 }
 
-// T = double: residual (OP_RESIDUAL) or Jacobian action into p.out from p.u / p.v;
-// T = float: Jacobian action into p.out32 from p.v32.
+// Per-block tables and per-group staging of the group-of-lanes hexahedral kernels.
+template <int CELL, typename T>
+struct HexGroupSmem {
+    const double* tN;  // geometry gradients [NQ][25]
+    const double* tW;  // quadrature weights
+    const T* tB;       // field-basis gradients [NQ][LDB]
+    const T* tPhi;     // basis values [NQ][NEN]
+    double* sX;        // this group's corner coordinates
+    T* su;             // this group's node field
+    T* sF;             // test-function weights
+    T* sF0;            // body-force weights
+    int grp, l;        // group of this lane within its warp, lane within the group
+};
+
+template <int CELL, typename T>
+PL_D HexGroupSmem<CELL, T> hex_group_smem(double* hsm) {
+    using H = HexGroup<CELL, T>;
+    HexGroupSmem<CELL, T> g;
+    double* t64 = hsm;
+    T* tt = reinterpret_cast<T*>(hsm + H::T_END64 + H::GROUPS * H::PER_GROUP_X);
+    g.tN = t64;
+    g.tW = t64 + H::T_W;
+    g.tB = tt;
+    g.tPhi = tt + H::T_PHI;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    g.grp = lane / H::G;
+    g.l = lane % H::G;
+    const int gid = warp * H::CPW + g.grp;
+    g.sX = hsm + H::T_END64 + gid * H::PER_GROUP_X;
+    T* sg = tt + H::T_ENDT + gid * H::PER_GROUP_T;
+    g.su = sg;
+    g.sF = sg + H::OFF_F;
+    g.sF0 = sg + H::OFF_F0;
+    return g;
+}
+
+// The CPW cells base .. base + CPW - 1 of p, one per group of lanes of the calling warp (every
+// lane of the warp calls it: it synchronises the warp).
 template <int CELL, int RHEO, bool BF, int OP, typename T>
-__global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(DomainParams p) {
+PL_D void hex_group_cells(const DomainParams& p, int64_t base, const HexGroupSmem<CELL, T>& g) {
     using H = HexGroup<CELL, T>;
     using L = AuxLayout<RHEO, BF>;
     const AuxOffsets<RHEO, BF> aoff;
-    extern __shared__ __align__(16) double hsm[];
-    double* t64 = hsm;
-    T* tt = reinterpret_cast<T*>(hsm + H::T_END64 + H::GROUPS * H::PER_GROUP_X);
-    fill_tables<CELL, T>(t64, tt);
-    __syncthreads();
-    const double* tN = t64;
-    const double* tW = t64 + H::T_W;
-    const T* tB = tt;
-    const T* tPhi = tt + H::T_PHI;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane / H::G, l = lane % H::G;
-    const int gid = warp * H::CPW + grp;
-    double* sX = hsm + H::T_END64 + gid * H::PER_GROUP_X;
-    T* sg = tt + H::T_ENDT + gid * H::PER_GROUP_T;
-    T* su = sg;
-    T* sF = sg + H::OFF_F;
-    T* sF0 = sg + H::OFF_F0;
+    const double* tN = g.tN;
+    const double* tW = g.tW;
+    const T* tB = g.tB;
+    const T* tPhi = g.tPhi;
+    double* sX = g.sX;
+    T* su = g.su;
+    T* sF = g.sF;
+    T* sF0 = g.sF0;
+    const int grp = g.grp, l = g.l;
     const bool f32 = sizeof(T) == 4;
-    const int64_t cells_per_pass = (int64_t)gridDim.x * H::WARPS * H::CPW;
-    // every lane of a warp runs the same number of passes (the __syncwarp calls need them all)
-    for (int64_t base = ((int64_t)blockIdx.x * H::WARPS + warp) * H::CPW; base < p.ncells; base += cells_per_pass) {
+    {
         const int64_t c = base + grp;
         const bool live = c < p.ncells;
         const int64_t mc = live ? (p.cell_ids ? p.cell_ids[c] : c) : 0;
@@ -252,6 +278,66 @@ __global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(Dom
         }
         __syncwarp();
     }
+}
+
+// T = double: residual (OP_RESIDUAL) or Jacobian action into p.out from p.u / p.v;
+// T = float: Jacobian action into p.out32 from p.v32.
+template <int CELL, int RHEO, bool BF, int OP, typename T>
+__global__ void __launch_bounds__(HexGroup<CELL, T>::WARPS * 32) k_hex_group(DomainParams p) {
+    using H = HexGroup<CELL, T>;
+    extern __shared__ __align__(16) double hsm[];
+    fill_tables<CELL, T>(hsm, reinterpret_cast<T*>(hsm + H::T_END64 + H::GROUPS * H::PER_GROUP_X));
+    __syncthreads();
+    const HexGroupSmem<CELL, T> g = hex_group_smem<CELL, T>(hsm);
+    const int warp = threadIdx.x >> 5;
+    const int64_t cells_per_pass = (int64_t)gridDim.x * H::WARPS * H::CPW;
+    // every lane of a warp runs the same number of passes (the __syncwarp calls need them all)
+    for (int64_t base = ((int64_t)blockIdx.x * H::WARPS + warp) * H::CPW; base < p.ncells; base += cells_per_pass)
+        hex_group_cells<CELL, RHEO, BF, OP, T>(p, base, g);
+}
+
+// FP32 Jacobian action of Q1 hexahedra over the cells of many meshes in one launch (the ragged
+// batch of solvers, ragged.cu): member m's cells form warp chunks chunk0[m] .. chunk0[m + 1] - 1
+// of one index space (4 cells per chunk), so a warp never mixes members; ops[m] holds member m's
+// operator arguments (its own cells, coordinates, cached per-cell tangent, input and output).
+// Members must have the cached isotropic tangent (lm32).
+__global__ void __launch_bounds__(HexGroup<HEX8, float>::WARPS * 32)
+    k_hex8_jv32_ragged(const DomainParams* __restrict__ ops, const int64_t* __restrict__ chunk0,
+                       const int* __restrict__ active, const int* __restrict__ nmembers) {
+    using H = HexGroup<HEX8, float>;
+    extern __shared__ __align__(16) double hsm[];
+    fill_tables<HEX8, float>(hsm, reinterpret_cast<float*>(hsm + H::T_END64 + H::GROUPS * H::PER_GROUP_X));
+    __syncthreads();
+    const HexGroupSmem<HEX8, float> g = hex_group_smem<HEX8, float>(hsm);
+    const int M = *nmembers;
+    const int64_t total = chunk0[M];
+    const int warp = threadIdx.x >> 5;
+    for (int64_t w = (int64_t)blockIdx.x * H::WARPS + warp; w < total; w += (int64_t)gridDim.x * H::WARPS) {
+        int lo = 0, hi = M;  // the member of chunk w: largest m with chunk0[m] <= w
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (chunk0[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        if (!active[lo]) continue;  // the whole warp shares w
+        hex_group_cells<HEX8, RHEO_ILE, false, OP_JACOBIAN_ACTION, float>(ops[lo], (w - chunk0[lo]) * H::CPW, g);
+    }
+}
+
+void launch_hex8_jv32_ragged(const DomainParams* ops, const int64_t* chunk0, const int* active, const int* nmembers,
+                             cudaStream_t s) {
+    using H = HexGroup<HEX8, float>;
+    const size_t smem = H::smem_bytes();
+    static int per_sm = 0, nsm = 0;
+    if (!per_sm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k_hex8_jv32_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hex8_jv32_ragged, H::WARPS * 32, smem);
+        per_sm = std::max(per_sm, 1);
+    }
+    k_hex8_jv32_ragged<<<nsm * per_sm, H::WARPS * 32, smem, s>>>(ops, chunk0, active, nmembers);
 }
 
 // ---- Q2 hexahedra by sum factorisation --------------------------------------------------------

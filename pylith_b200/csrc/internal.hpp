@@ -68,9 +68,20 @@ struct BlockedLayout {
     int32_t* d_fix_node = nullptr;          // [num_fix] node ids
     int32_t* d_fix_off = nullptr;           // [num_fix + 1] offsets into d_fix_slot
     int32_t* d_fix_slot = nullptr;          // global slot ids of each node, in block order
+    // Padded per-block regions of the pipelined kernel (k_tet_pipe): block b's slots start at
+    // d_pipe_begin[b] (a multiple of 4) and span its slot count rounded up to 4.
+    int32_t* d_pipe_begin = nullptr;        // [num_blocks + 1]
+    uint32_t* d_pipe_ids = nullptr;         // node id | shared bit, per padded slot
+    double* d_pipe_coords = nullptr;        // per block [3][padded slots] coordinates
+    uint32_t* d_pipe_off = nullptr;         // per block, at d_pipe_begin[b] + 4 b: ns + 1 offsets
+    uint16_t* d_pipe_inc = nullptr;         // [num_blocks][4 * cells_per_block] staging offsets
+                                            // corner * 3 * cells_per_block + cell, node groups of
+                                            // the pipelined kernel
     size_t device_bytes = 0;
 };
 
+void context_retain(pl_context_s* c);
+void context_release(pl_context_s* c);
 void mesh_retain(pl_mesh_s* m);
 void mesh_release(pl_mesh_s* m);
 void solver_retain(pl_solver_s* S);

@@ -8,6 +8,7 @@
 struct pl_mesh_s;
 
 struct pl_integrator_s;
+struct pl_solver_s;
 
 namespace plb {
 
@@ -52,6 +53,14 @@ int prepare_blocked(pl_integrator_s* ig);
 // Fills the integrator's per-cell FP32 (lambda, mu) for the Jacobian action of hexahedra at
 // (t, dt) when that path applies (no-op otherwise); call outside stream capture.
 int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt);
+
+// FP32 Q1 Jacobian action over many members' cells in one launch (the ragged batch; device
+// tables: per-member operator arguments, warp-chunk prefix, active flags, member count).
+void launch_hex8_jv32_ragged(const DomainParams* ops, const int64_t* chunk0, const int* active, const int* nmembers,
+                             cudaStream_t s);
+// Step-by-step FP32 reliable-update PCG of one solver for an outside iteration loop (solver.cu).
+int solver32_begin(pl_solver_s* S, const double* b, double* x, double* b0);
+int solver32_replace(pl_solver_s* S, const double* b, double* x, bool restart, double* rt);
 
 // FP32 Jacobian action on the cell blocks (the output must be zeroed or hold the sum to add to).
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,

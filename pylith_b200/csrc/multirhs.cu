@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_update(float* r, const float* q
                                                         const double* rz, const double* pq, const int* active,
                                                         double* part_rz, double* part_rr, FinSpec fin) {
     const int k = threadIdx.x % K;  // blockDim and the grid stride are multiples of K
-    const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
+    const float alpha = active[k] ? safe_step_f32(rz[k], pq[k]) : 0.0f;
     double srz = 0.0, srr = 0.0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t nd = t / K;
@@ -544,7 +544,7 @@ template <int K>
 __global__ void k_b_pupdate(float* x, float* p, const float* z, const uint8_t* mask, int64_t n, const double* rz,
                             const double* rz_old, const double* pq, const int* active) {
     const int k = threadIdx.x % K;
-    const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz_old[k] / pq[k]) : 0.0f;
+    const float alpha = active[k] ? safe_step_f32(rz_old[k], pq[k]) : 0.0f;
     const float beta = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
         const float pe = p[e];
@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_update_xr(float* r, const float
                                                            const double* pq, const int* active, double* part_rr,
                                                            FinSpec fin) {
     const int k = threadIdx.x % K;
-    const float alpha = (active[k] && pq[k] != 0.0) ? (float)(rz[k] / pq[k]) : 0.0f;
+    const float alpha = active[k] ? safe_step_f32(rz[k], pq[k]) : 0.0f;
     double srr = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
         if (mask[e / K]) continue;

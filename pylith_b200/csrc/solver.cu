@@ -16,48 +16,12 @@
 #include <cstring>
 #include <vector>
 
+#include "cg.cuh"
 #include "domain_kernels.cuh"
 #include "internal.hpp"
 #include "launch.hpp"
 
 namespace plb {
-
-constexpr int kRedThreads = 256;
-constexpr int kRedBlocks = 296;  // 2 per SM
-
-enum Scalar { S_RZ = 0, S_RZ_OLD, S_PQ, S_RR, S_ALPHA, S_BETA, S_BB, S_COUNT };
-
-template <typename T>
-PL_D double to_d(T v) { return (double)v; }
-
-// Block-level sum of up to 2 values; thread 0 of each block writes partials[blk*2 + k].
-PL_D void block_sum2(double a, double b, double* partials) {
-    __shared__ double sa[kRedThreads / 32], sb[kRedThreads / 32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        sa[w] = a;
-        sb[w] = b;
-    }
-    __syncthreads();
-    if (w == 0) {
-        a = l < (int)(blockDim.x >> 5) ? sa[l] : 0.0;
-        b = l < (int)(blockDim.x >> 5) ? sb[l] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xffffffffu, a, o);
-            b += __shfl_down_sync(0xffffffffu, b, o);
-        }
-        if (l == 0) {
-            partials[2 * blockIdx.x] = a;
-            partials[2 * blockIdx.x + 1] = b;
-        }
-    }
-}
 
 // Sum the partials of the previous pass in a fixed order into scal[i0], scal[i1].
 __global__ void k_finish2(const double* __restrict__ partials, int nblk, double* scal, int i0, int i1) {
@@ -106,17 +70,6 @@ __global__ void __launch_bounds__(kRedThreads) k_dot2(const T* a, const T* b, co
     block_sum2(s0, s1, partials);
 }
 
-// z = P^{-1} r with point blocks; constrained entries of r are zero and P^{-1} is the identity
-// on them, so z stays zero there.
-template <typename T>
-PL_D void apply_pinv(const T* pinv, const T* r, int64_t node, T out[3]) {
-    const T* B = pinv + 9 * node;
-    const T r0 = r[3 * node], r1 = r[3 * node + 1], r2 = r[3 * node + 2];
-    out[0] = B[0] * r0 + B[1] * r1 + B[2] * r2;
-    out[1] = B[3] * r0 + B[4] * r1 + B[5] * r2;
-    out[2] = B[6] * r0 + B[7] * r1 + B[8] * r2;
-}
-
 // r := b (masked), z := P^{-1} r, p := z; partial (r.z, r.r).
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_cg_init(const T* b, const uint8_t* mask, const T* pinv, int64_t nnodes,
@@ -153,8 +106,11 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_cg_update(T* x, T* r, const T* p, const T* q, T* z, const uint8_t* mask,
                                                            const T* pinv, int64_t nnodes, const double* scal,
                                                            double* partials) {
+    // p.(A p) > 0 for the SPD operator; a search direction that has collapsed to rounding noise
+    // (FP32 iterations past convergence) can give pq <= 0 or an alpha beyond T's range: no step
     const double pq = scal[S_PQ];
-    const T alpha = (T)(pq != 0.0 ? scal[S_RZ] / pq : 0.0);
+    const double a64 = pq > 0.0 ? scal[S_RZ] / pq : 0.0;
+    const T alpha = (T)(isfinite((T)a64) ? a64 : 0.0);
     double rz = 0.0, rr = 0.0;
     for (int64_t nd = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; nd < nnodes; nd += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
@@ -588,6 +544,13 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
             k_prec_rz<float><<<kRedBlocks, kRedThreads, 0, cs>>>(S->f_r, S->d_pinv32, nn, S->f_z, S->d_partials);
             k_finish2<<<1, 1024, 0, cs>>>(S->d_partials, kRedBlocks, scal, S_RZ, -1);
             count_launch(2);
+            // The FP32 iterations had run below the stopping threshold while the true residual had
+            // not: their search direction is rounding noise, so restart it from z.
+            if (rn <= 0.5 * stop &&
+                cudaMemcpyAsync(S->f_p, S->f_z, n * sizeof(float), cudaMemcpyDeviceToDevice, cs) != cudaSuccess) {
+                rc = fail(PL_ERR_CUDA, "search direction restart");
+                break;
+            }
         }
     } while (false);
     S->rel_residual = b0 > 0.0 ? rt / b0 : 0.0;
@@ -598,6 +561,68 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
 }
 
 }  // namespace
+
+namespace plb {
+
+// The FP32 reliable-update PCG of one solver, driven step by step by an outside loop (the ragged
+// batch runs the iterations of many solvers in shared launches). Both run on the context's
+// stream and synchronise it.
+//
+// Start: x = 0, FP64 residual r = b - A x (d_r, and f_r in FP32), z = P r, p = z, r.z and r.r in
+// the solver's scalars, q = 0; *b0 = |r|.
+int solver32_begin(pl_solver S, const double* b, double* x, double* b0) {
+    pl_context c = S->mesh->ctx;
+    cudaStream_t s = c->stream;
+    const int64_t n = S->n;
+    double h[S_COUNT];
+    PLB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    PLB_CUDA(cudaMemsetAsync(S->f_x, 0, n * sizeof(float), s));
+    PLB_CUDA(cudaMemsetAsync(S->f_q, 0, n * sizeof(float), s));
+    if (S->mesh->cell_type == PL_CELL_TET4)
+        for (pl_integrator ig : S->ops) {
+            int rcl = prepare_blocked(ig);
+            if (rcl) return rcl;
+        }
+    int rc = apply_J(S, x, S->d_q);
+    if (rc) return rc;
+    k_outer_residual<<<kRedBlocks, kRedThreads, 0, s>>>(b, S->d_q, S->d_mask, n, S->d_r, S->f_r, S->d_partials);
+    k_finish2<<<1, 1024, 0, s>>>(S->d_partials, kRedBlocks, S->d_scal, S_BB, -1);
+    k_cg_init<float><<<kRedBlocks, kRedThreads, 0, s>>>(S->f_r, S->d_mask, S->d_pinv32, S->nnodes, S->f_r, S->f_z, S->f_p,
+                                                         S->d_partials);
+    k_finish2<<<1, 1024, 0, s>>>(S->d_partials, kRedBlocks, S->d_scal, S_RZ, S_RR);
+    count_launch(4);
+    PLB_CUDA(cudaMemcpyAsync(h, S->d_scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PLB_CUDA(cudaStreamSynchronize(s));
+    *b0 = std::sqrt(h[S_BB]);
+    return PL_OK;
+}
+
+// Residual replacement: x += f_x, f_x = 0, r = b - A x in FP64 (*rt = |r|), r.z for the new r
+// (z = P r); with restart the search direction starts again from z; q = 0.
+int solver32_replace(pl_solver S, const double* b, double* x, bool restart, double* rt) {
+    pl_context c = S->mesh->ctx;
+    cudaStream_t s = c->stream;
+    const int64_t n = S->n;
+    double h[S_COUNT];
+    k_add_correction<<<vec_grid(n), 256, 0, s>>>(x, S->f_x, S->d_mask, n);
+    count_launch();
+    PLB_CUDA(cudaMemsetAsync(S->f_x, 0, n * sizeof(float), s));
+    int rc = apply_J(S, x, S->d_q);
+    if (rc) return rc;
+    k_outer_residual<<<kRedBlocks, kRedThreads, 0, s>>>(b, S->d_q, S->d_mask, n, S->d_r, S->f_r, S->d_partials);
+    k_finish2<<<1, 1024, 0, s>>>(S->d_partials, kRedBlocks, S->d_scal, S_BB, -1);
+    k_prec_rz<float><<<kRedBlocks, kRedThreads, 0, s>>>(S->f_r, S->d_pinv32, S->nnodes, S->f_z, S->d_partials);
+    k_finish2<<<1, 1024, 0, s>>>(S->d_partials, kRedBlocks, S->d_scal, S_RZ, -1);
+    count_launch(4);
+    if (restart) PLB_CUDA(cudaMemcpyAsync(S->f_p, S->f_z, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    PLB_CUDA(cudaMemsetAsync(S->f_q, 0, n * sizeof(float), s));
+    PLB_CUDA(cudaMemcpyAsync(h, S->d_scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PLB_CUDA(cudaStreamSynchronize(s));
+    *rt = std::sqrt(h[S_BB]);
+    return PL_OK;
+}
+
+}  // namespace plb
 
 extern "C" {
 

@@ -46,6 +46,19 @@ class _KernelClass:
 fekernels = _Kernels()
 
 
+def register_fekernel(name: str, address: int) -> None:
+    """Registers a caller-compiled copy of the pointwise kernel `name` (e.g.
+    "IsotropicLinearElasticity3D::f1v_infinitesimalStrain") so that its address can be passed to
+    the set_kernels_* calls (pl_fekernel_register)."""
+    check(C.lib().pl_fekernel_register(name.encode(), address))
+
+
+def fekernel_name(address: int):
+    """PyLith name of a known or registered kernel address, or None."""
+    n = C.lib().pl_fekernel_name(address)
+    return n.decode() if n else None
+
+
 def _ptr(t) -> int:
     if t is None:
         return 0
@@ -416,6 +429,55 @@ class BatchSolver:
         if self.handle:
             C.lib().pl_batch_solver_destroy(self.handle)
             self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RaggedBatch:
+    """Many solvers on meshes of uneven size iterated together (pl_ragged_*): every PCG iteration
+    of every active member shares one operator launch and seven vector launches, with dot products
+    and convergence kept per member. Members are FP32-refined Q1 hexahedral solvers."""
+
+    def __init__(self, ctx: Context, capacity: int = 256, chunk: int = 10):
+        self.ctx = ctx
+        self.handle = ctypes.c_void_p()
+        check(C.lib().pl_ragged_create(ctx.handle, capacity, ctypes.byref(self.handle)))
+        check(C.lib().pl_ragged_set_chunk(self.handle, chunk))
+        self._keep = {}
+
+    def add(self, solver: Solver, b, x) -> int:
+        """Adds the solve solver.A x = b (device vectors kept alive while the member is here)."""
+        m = ctypes.c_int()
+        check(C.lib().pl_ragged_add(self.handle, solver.handle, _ptr(b), _ptr(x), ctypes.byref(m)))
+        self._keep[m.value] = (solver, b, x)
+        return m.value
+
+    def iterate(self) -> int:
+        """One chunk of iterations for every active member; returns how many are still active."""
+        left = ctypes.c_int()
+        check(C.lib().pl_ragged_iterate(self.handle, ctypes.byref(left)))
+        return left.value
+
+    def status(self, member: int):
+        st, it, rel = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(C.lib().pl_ragged_member_status(self.handle, member, ctypes.byref(st), ctypes.byref(it),
+                                              ctypes.byref(rel)))
+        return {"status": st.value, "done": st.value != C.ERRORS_NOT_READY, "iterations": it.value,
+                "rel_residual": rel.value}
+
+    def remove(self, member: int) -> None:
+        check(C.lib().pl_ragged_remove(self.handle, member))
+        self._keep.pop(member, None)
+
+    def close(self):
+        if self.handle:
+            C.lib().pl_ragged_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+            self._keep.clear()
 
     def __del__(self):
         try:

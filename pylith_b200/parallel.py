@@ -10,9 +10,9 @@ their shared vertices in DMLocalToGlobal(ADD_VALUES) over a PetscSF
     node numbering, the local-to-global node map, and, per neighbouring part, the list of
     shared local nodes sorted by global node id (so both sides agree on the order);
   * `HaloExchange.sum_shared` adds the neighbours' partial sums into the local residual at the
-    shared nodes: one packed send and one receive per neighbour over torch.distributed (NCCL on
-    the GPU, gloo on CPU), then one index_add. After it every rank holds, for each of its nodes,
-    the same value the global residual has there.
+    shared nodes: one pack kernel, one send and one receive per neighbour over torch.distributed
+    (NCCL on the GPU, gloo on CPU), then one add kernel. After it every rank holds, for each of
+    its nodes, the same value the global residual has there.
 """
 from __future__ import annotations
 
@@ -69,32 +69,104 @@ def partition_mesh(mesh: Mesh, nparts: int) -> List[LocalMesh]:
 
 
 class HaloExchange:
-    """Sum of partial nodal values across the parts that share nodes (ADD_VALUES)."""
+    """Sum of partial nodal values across the parts that share nodes (ADD_VALUES).
 
-    def __init__(self, local: LocalMesh, device=None, group=None):
+    On CUDA tensors the shared nodes' values are packed into one send buffer and the neighbours'
+    values added back by the library's kernels (pl_halo_pack / pl_halo_unpack_add, one launch
+    each, on the context's stream); between them each neighbour's slice moves by point-to-point
+    send/receive (NCCL). On CPU tensors (the gloo transport of the multi-process CPU tests) the
+    same two steps are index_select and index_add.
+    """
+
+    def __init__(self, local: LocalMesh, device=None, group=None, ctx=None):
         import torch
 
         self.local = local
         self.group = group
-        self.device = device if device is not None else torch.device("cpu")
+        self.device = torch.device(device) if device is not None else torch.device("cpu")
         self.peers = sorted(local.shared)
-        self.index = {q: torch.as_tensor(local.shared[q], dtype=torch.int64, device=self.device)
-                      for q in self.peers}
+        self.counts = [len(local.shared[q]) for q in self.peers]
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.total = int(self.offsets[-1])
+        nodes = (np.concatenate([local.shared[q] for q in self.peers]) if self.peers
+                 else np.zeros(0, dtype=np.int64))
+        self.halo = None
+        if self.device.type == "cuda":
+            import ctypes
 
-    def sum_shared(self, r) -> None:
-        """r: tensor [3 * num_local_nodes] (any float dtype), updated in place."""
+            from . import _lib as C
+
+            if ctx is None:
+                raise ValueError("a CUDA exchange needs the pylith_b200 Context of its device")
+            self.ctx = ctx
+            counts = np.ascontiguousarray(self.counts, dtype=np.int64)
+            nodes32 = np.ascontiguousarray(nodes, dtype=np.int32)
+            h = ctypes.c_void_p()
+            C.check(C.lib().pl_halo_create(ctx.handle, len(self.peers), counts.ctypes.data,
+                                           nodes32.ctypes.data, ctypes.byref(h)))
+            self.halo = h
+        else:
+            self.index = torch.as_tensor(nodes, dtype=torch.int64)
+
+    def close(self):
+        if self.halo:
+            from . import _lib as C
+
+            C.lib().pl_halo_destroy(self.halo)
+            self.halo = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def slices(self, buf):
+        """{neighbour: its part of a send or receive buffer}."""
+        return {q: buf[3 * self.offsets[i]:3 * self.offsets[i + 1]] for i, q in enumerate(self.peers)}
+
+    def pack(self, r, out=None):
+        """The shared nodes' values of r, neighbour after neighbour: [3 * entries]."""
+        import torch
+
+        if out is None:
+            out = torch.empty(3 * self.total, dtype=r.dtype, device=r.device)
+        if self.halo is not None:
+            from . import _lib as C
+
+            fn = C.lib().pl_halo_pack if r.dtype == torch.float64 else C.lib().pl_halo_pack_f32
+            C.check(fn(self.halo, r.data_ptr(), out.data_ptr()))
+        else:
+            out.view(-1, 3).copy_(r.view(-1, 3).index_select(0, self.index))
+        return out
+
+    def unpack_add(self, recv, r) -> None:
+        """Adds the neighbours' values (laid out as `pack`'s output) into r at the shared nodes."""
+        import torch
+
+        if self.halo is not None:
+            from . import _lib as C
+
+            fn = C.lib().pl_halo_unpack_add if r.dtype == torch.float64 else C.lib().pl_halo_unpack_add_f32
+            C.check(fn(self.halo, recv.data_ptr(), r.data_ptr()))
+        else:
+            r.view(-1, 3).index_add_(0, self.index, recv.view(-1, 3))
+
+    def sum_shared(self, r, send=None, recv=None) -> None:
+        """r: tensor [3 * num_local_nodes], updated in place; send/recv: optional buffers of
+        3 * entries values reused between calls."""
         import torch
         import torch.distributed as dist
 
-        r3 = r.view(-1, 3)
-        sends = {q: r3.index_select(0, self.index[q]).contiguous() for q in self.peers}
-        recvs = {q: torch.empty_like(sends[q]) for q in self.peers}
+        send = self.pack(r, send)
+        if recv is None:
+            recv = torch.empty_like(send)
+        ss, rs = self.slices(send), self.slices(recv)
         ops = []
         for q in self.peers:
-            ops.append(dist.P2POp(dist.isend, sends[q], q, group=self.group))
-            ops.append(dist.P2POp(dist.irecv, recvs[q], q, group=self.group))
+            ops.append(dist.P2POp(dist.isend, ss[q], q, group=self.group))
+            ops.append(dist.P2POp(dist.irecv, rs[q], q, group=self.group))
         if ops:
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
-        for q in self.peers:
-            r3.index_add_(0, self.index[q], recvs[q])
+        self.unpack_add(recv, r)

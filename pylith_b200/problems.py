@@ -78,24 +78,41 @@ class QuasistaticProblem:
             ig.compute_lhs_residual(t, self.dt, u, out, mode=FA.INSERT if i == 0 else FA.ADD)
         return out
 
-    def step(self, t: float) -> StepStats:
+    def begin_step(self, t: float):
+        """Everything of a step before the linear solve: the solution takes its Dirichlet values
+        and the prescribed slip, F is the domain residual (the fault's lambda terms cancel in the
+        reduced, slip-constrained space) and the solver is set up when its trigger fires. Returns
+        (F, du): the solve is A du = F."""
         import torch
 
-        # solution with Dirichlet values and the prescribed slip on the positive fault side
         self.u = torch.where(self._mask, self._bc, self.u)
         for iface in self.interfaces:
             self.solver.apply_fault_slip(iface, self.u)
-        # domain residual; the fault's lambda terms cancel in the reduced (slip-constrained) space
         for i, ig in enumerate(self.domain):
             ig.compute_lhs_residual(t, self.dt, self.u, self.F, mode=FA.INSERT if i == 0 else FA.ADD)
         if self._setup_dt is None or (self.viscous and self._setup_dt != self.dt):
             self.solver.setup(t, self.dt)
             self._setup_dt = self.dt
-        self.solver.solve(self.F, self.du)
+        return self.F, self.du
+
+    def end_step(self, t: float) -> None:
+        """After the solve: u += du and the state variables' update (poststep)."""
         self.u += self.du
         for ig in self.viscous:
             ig.update_state_vars(t, self.dt, self.u)
+
+    def step(self, t: float) -> StepStats:
+        F, du = self.begin_step(t)
+        self.solver.solve(F, du)
+        self.end_step(t)
         s = self.solver.stats()
         st = StepStats(t, s["iterations"], s["inner_iterations"], s["outer_iterations"], s["rel_residual"])
         self.history.append(st)
         return st
+
+    def close(self) -> None:
+        """Releases the device objects (solver, integrators, mesh) now rather than at collection."""
+        self.solver.close()
+        for ig in self.domain + self.interfaces:
+            ig.close()
+        self.dmesh.close()

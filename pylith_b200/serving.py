@@ -1,21 +1,23 @@
-"""Serving forward solves: a request loop with HBM-budget admission and concurrent device slots.
+"""Serving forward solves: a request loop with HBM-budget admission and continuous batching.
 
-Each request is a quasi-static forward solve (the same path as problems.QuasistaticProblem) on
-its own box mesh with a prescribed-slip fault. The server admits a request when it has arrived,
-a slot is free and the request's estimated device memory fits the remaining HBM budget; every
-slot has its own CUDA stream and host thread, so requests that arrive while others run are
-started at once and their kernels overlap on the GPU. Meshes, aux fields and solver state live on
-the device for the life of the request. Latency is measured from arrival to completion.
+Each request is a quasi-static forward solve (the same path as problems.QuasistaticProblem) on its
+own box mesh with a prescribed-slip fault. The server keeps one ragged batch (pl_ragged_*): a
+request is admitted when it has arrived, a slot is free and its estimated device memory fits the
+remaining HBM budget; its mesh, aux fields and solver are then built on the device, and its solve
+joins the batch at the next iteration boundary. Every PCG iteration of every admitted request
+shares the same launches (one operator launch over all their cells), each request converging on
+its own dot products; a request leaves the batch when its FP64 residual meets the tolerance, and
+its slot and memory go to the next arrival. Latency is measured from arrival to completion.
 
-The baseline is the same stream of requests served one at a time with the FP64 solver.
+Host mesh generation is not part of serving: the requests' host-side problem data (mesh, material
+fields, slip, constraints) is prepared before the request stream starts, for the server and the
+baseline alike. The baseline is the same stream served one at a time with the FP64 solver.
 """
 from __future__ import annotations
 
-import heapq
-import queue
-import threading
 import time
-from dataclasses import dataclass, field
+from collections import deque
+from dataclasses import dataclass
 from typing import List, Optional
 
 import numpy as np
@@ -75,13 +77,23 @@ def estimate_bytes(n: int) -> int:
     return cells * (32 + 40) + nodes * 3 * 8 * 24 + (64 << 20)
 
 
-def build_problem(ctx, req: Request, precision: int, rtol: float):
-    from . import problems as P
+@dataclass
+class HostProblem:
+    """A request's host-side data, prepared before the request stream starts."""
+    req: Request
+    mesh: object
+    rho: np.ndarray
+    mu: np.ndarray
+    K: np.ndarray
+    slip: np.ndarray
+    constrained: np.ndarray
+    bc: np.ndarray
 
+
+def prepare(req: Request) -> HostProblem:
     lo, hi = M.BOX_LO, M.BOX_HI
     mesh = M.insert_fault_x(M.box_hex(req.n, req.n, req.n))
     rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=req.seed)
-    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
     lag_nodes = np.zeros(mesh.num_lagrange, dtype=np.int64)
     lag_nodes[mesh.cohesive[:, 8:].ravel()] = mesh.cohesive[:, :4].ravel()
     yz = mesh.coords[lag_nodes][:, 1:]
@@ -91,115 +103,120 @@ def build_problem(ctx, req: Request, precision: int, rtol: float):
     on = (fy >= y0) & (fy <= y1) & (fz >= z0) & (fz <= z1)
     slip = np.zeros((mesh.num_lagrange, 3))
     slip[on, 1] = req.slip
-    fault = MAT.FaultCohesiveKin(slip)
     cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
     cons[M.boundary_mask(mesh, 0, "neg")] = True
     cons[M.boundary_mask(mesh, 0, "pos")] = True
     cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
-    bc = np.zeros(mesh.num_dof)
-    return P.QuasistaticProblem(ctx, mesh, [(mat, None)], cons, bc, faults=[fault], precision=precision,
+    return HostProblem(req, mesh, rho, mu, K, slip, cons, np.zeros(mesh.num_dof))
+
+
+def build_problem(ctx, hp: HostProblem, precision: int, rtol: float):
+    from . import problems as P
+
+    return P.QuasistaticProblem(ctx, hp.mesh, [(MAT.IsotropicLinearElasticity(hp.rho, hp.mu, hp.K), None)],
+                                hp.constrained, hp.bc, faults=[MAT.FaultCohesiveKin(hp.slip)], precision=precision,
                                 rtol=rtol)
 
 
-def solve_one(ctx, req: Request, precision: int, rtol: float, keep_solution: bool):
-    prob = build_problem(ctx, req, precision, rtol)
-    st = prob.step(0.0)
-    ctx.synchronize()
-    u = prob.u.cpu().numpy() if keep_solution else None
-    return prob.dmesh.num_dof, st.iterations + st.inner_iterations, u
-
-
 class Server:
-    def __init__(self, device: int = 0, slots: int = 8, hbm_budget: Optional[int] = None,
-                 precision: int = FA.Solver.FP32_REFINED, rtol: float = 1e-10, keep_solutions=False):
+    """Continuous batching of FP32-refined solves in one ragged batch (single host thread)."""
+
+    def __init__(self, device: int = 0, slots: int = 64, hbm_budget: Optional[int] = None, rtol: float = 1e-10,
+                 keep_solutions=False, chunk: int = 10):
         import torch
 
         self.device = device
         self.slots = slots
         free, total = torch.cuda.mem_get_info(device)
         self.budget = hbm_budget if hbm_budget is not None else int(0.8 * free)
-        self.precision = precision
         self.rtol = rtol
         self.keep = keep_solutions
+        self.chunk = chunk
+        self.memory = []  # (request, predicted bytes, measured bytes)
 
-    def run(self, requests: List[Request]) -> List[Result]:
+    def run(self, problems: List[HostProblem]) -> List[Result]:
         import torch
 
-        pending = sorted(requests, key=lambda r: r.arrival)
-        work = queue.Queue()
+        torch.cuda.set_device(self.device)
+        ctx = FA.Context(self.device)
+        batch = FA.RaggedBatch(ctx, capacity=self.slots, chunk=self.chunk)
+        pending = deque(sorted(problems, key=lambda hp: hp.req.arrival))
+        for hp in pending:
+            if estimate_bytes(hp.req.n) > self.budget:
+                raise ValueError(f"request {hp.req.rid} ({hp.req.n}^3) exceeds the HBM budget")
+        active = {}
+        used = 0
         results: List[Result] = []
-        lock = threading.Lock()
-        freed = threading.Condition(lock)
-        state = {"used": 0, "busy": 0}
+        self.memory = []
         t0 = time.perf_counter()
-        errors = []
-
-        def worker():
-            torch.cuda.set_device(self.device)
-            stream = torch.cuda.Stream(device=self.device)
-            ctx = FA.Context(self.device, use_torch_stream=False)
-            ctx.set_stream(stream.cuda_stream)
-            with torch.cuda.stream(stream):
-                while True:
-                    item = work.get()
-                    if item is None:
-                        break
-                    req, nbytes = item
-                    start = time.perf_counter() - t0
-                    try:
-                        dof, iters, u = solve_one(ctx, req, self.precision, self.rtol, self.keep)
-                    except Exception as e:  # surfaced after the run
-                        errors.append((req.rid, repr(e)))
-                        dof, iters, u = 0, 0, None
-                    end = time.perf_counter() - t0
-                    with lock:
-                        results.append(Result(req.rid, req.n, dof, req.arrival, start, end, iters, u))
-                        state["used"] -= nbytes
-                        state["busy"] -= 1
-                        freed.notify_all()
-            ctx.close()
-
-        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.slots)]
-        for th in threads:
-            th.start()
-        for req in pending:
-            nbytes = estimate_bytes(req.n)
-            if nbytes > self.budget:
-                raise ValueError(f"request {req.rid} ({req.n}^3) exceeds the HBM budget")
-            wait = req.arrival - (time.perf_counter() - t0)
-            if wait > 0:
-                time.sleep(wait)
-            with lock:
-                while state["busy"] >= self.slots or state["used"] + nbytes > self.budget:
-                    freed.wait()
-                state["used"] += nbytes
-                state["busy"] += 1
-            work.put((req, nbytes))
-        for _ in threads:
-            work.put(None)
-        for th in threads:
-            th.join()
-        if errors:
-            raise RuntimeError(f"requests failed: {errors[:3]}")
+        while pending or active:
+            now = time.perf_counter() - t0
+            while (pending and pending[0].req.arrival <= now and len(active) < self.slots
+                   and used + estimate_bytes(pending[0].req.n) <= self.budget):
+                hp = pending.popleft()
+                start = time.perf_counter() - t0
+                predicted = estimate_bytes(hp.req.n)
+                free0 = torch.cuda.mem_get_info(self.device)[0]
+                prob = build_problem(ctx, hp, FA.Solver.FP32_REFINED, self.rtol)
+                F, du = prob.begin_step(0.0)
+                member = batch.add(prob.solver, F, du)
+                measured = free0 - torch.cuda.mem_get_info(self.device)[0]
+                self.memory.append((hp.req.rid, predicted, measured))
+                used += predicted
+                active[member] = (hp, prob, start, predicted)
+            if not active:
+                time.sleep(max(0.0, pending[0].req.arrival - (time.perf_counter() - t0)))
+                continue
+            batch.iterate()
+            for member in list(active):
+                st = batch.status(member)
+                if not st["done"]:
+                    continue
+                hp, prob, start, nbytes = active.pop(member)
+                if st["status"] != 0:
+                    raise RuntimeError(f"request {hp.req.rid} failed: {C_error(st['status'])}")
+                prob.end_step(0.0)
+                ctx.synchronize()
+                end = time.perf_counter() - t0
+                u = prob.u.cpu().numpy() if self.keep else None
+                results.append(Result(hp.req.rid, hp.req.n, prob.dmesh.num_dof, hp.req.arrival, start, end,
+                                      st["iterations"], u))
+                batch.remove(member)
+                prob.close()
+                used -= nbytes
+        batch.close()
+        ctx.close()
         return sorted(results, key=lambda r: r.rid)
 
 
-def serve_sequential(requests: List[Request], device: int = 0, precision: int = FA.Solver.FP64,
+def C_error(code: int) -> str:
+    from . import _lib as C
+
+    return C.ERRORS.get(code, str(code))
+
+
+def serve_sequential(problems: List[HostProblem], device: int = 0, precision: int = FA.Solver.FP64,
                      rtol: float = 1e-10, keep_solutions=False) -> List[Result]:
-    """The baseline: requests in arrival order, one at a time, on one stream."""
+    """The baseline: requests in arrival order, one at a time, each with its own solver."""
     import torch
 
     torch.cuda.set_device(device)
     ctx = FA.Context(device)
     t0 = time.perf_counter()
     out = []
-    for req in sorted(requests, key=lambda r: r.arrival):
-        wait = req.arrival - (time.perf_counter() - t0)
+    for hp in sorted(problems, key=lambda hp: hp.req.arrival):
+        wait = hp.req.arrival - (time.perf_counter() - t0)
         if wait > 0:
             time.sleep(wait)
         start = time.perf_counter() - t0
-        dof, iters, u = solve_one(ctx, req, precision, rtol, keep_solutions)
-        out.append(Result(req.rid, req.n, dof, req.arrival, start, time.perf_counter() - t0, iters, u))
+        prob = build_problem(ctx, hp, precision, rtol)
+        st = prob.step(0.0)
+        ctx.synchronize()
+        u = prob.u.cpu().numpy() if keep_solutions else None
+        out.append(Result(hp.req.rid, hp.req.n, prob.dmesh.num_dof, hp.req.arrival, start,
+                          time.perf_counter() - t0, st.iterations + st.inner_iterations, u))
+        prob.close()
+    ctx.close()
     return out
 
 

@@ -4,7 +4,8 @@
 // permutation; every (cell, corner) appears once, under its node's new index) and the simulated
 // shared-memory wavefronts of the corner gathers (FP64 node arrays: bank pair = local index mod 16)
 // and of the per-node sums (bank pair = cell mod 16), with the nodes sorted by id and incidences in
-// cell order, and with the planned layout.
+// cell order, and with the planned layout. The pipelined kernel's incidence list must hold the same
+// incidences per node, as staging offsets.
 #include <cstdio>
 #include <cstdlib>
 #include <set>
@@ -59,11 +60,17 @@ int main(int argc, char** argv) {
             ok = ok && P.newidx[l] >= 0 && P.newidx[l] < nloc && seen[P.newidx[l]]++ == 0;
         ok = ok && (int)P.off.size() == nloc + 1 && (int)P.inc.size() == 4 * ncell && P.off[nloc] == (uint32_t)(4 * ncell);
         if (!ok) break;
-        std::vector<int> hit(4 * ncell, 0);
-        for (int i = 0; i < nloc; ++i)
+        std::vector<int> hit(4 * ncell, 0), hit_pipe(4 * ncell, 0);
+        ok = ok && P.inc_pipe.size() == P.inc.size();
+        for (int i = 0; ok && i < nloc; ++i)
             for (uint32_t j = P.off[i]; j < P.off[i + 1]; ++j) {
                 const int e = P.inc[j];
                 ok = ok && e < 4 * ncell && P.newidx[sorted_index(bc[e])] == i && hit[e]++ == 0;
+                // the pipelined kernel's list: the same incidences of node i, as staging offsets
+                // corner * 3 * 256 + cell
+                const int q = P.inc_pipe[j], corner = q / (3 * 256), cell = q % (3 * 256);
+                ok = ok && corner < 4 && cell < ncell && P.newidx[sorted_index(bc[4 * cell + corner])] == i &&
+                     hit_pipe[4 * cell + corner]++ == 0;
             }
         for (int w = 0; w < ncell; w += 32)
             for (int k = 0; k < 4; ++k) {

@@ -456,3 +456,58 @@ def test_two_materials_on_cell_subsets(oracle_lib, torch_cuda, ctx, kind):
     empty.compute_lhs_residual(0.0, 0.0, du, dr, mode=FA.INSERT)
     ctx.synchronize()
     assert float(dr.abs().max()) == 0.0
+
+
+def test_reference_compiled_kernels_drive_the_device_path(oracle_lib, torch_cuda, ctx):
+    """The reference's own pointwise kernels compiled from libsrc/pylith/fekernels/*.hh
+    (oracle/_ref) are registered under their names (pl_fekernel_register) and passed to the
+    integrator exactly as PyLith passes them to PetscWeakForm: the device path runs with them and
+    gives what it gives with the library's own addresses, for a material and a fault."""
+    from pylith_b200 import feassemble as FA
+
+    O, torch = oracle_lib, torch_cuda
+    if not O.ref_available():
+        pytest.skip("reference kernels not built")
+    for name in O.KERNELS:
+        FA.register_fekernel(name, O.kernel(name, "ref"))
+        assert FA.fekernel_name(O.kernel(name, "ref")) == name
+    ref = lambda n: O.kernel(n, "ref")  # noqa: E731
+    mesh = MESHES["tet4"]()
+    mat = elastic_setup(mesh, seed=51)
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig_lib = mat.create_integrator(dm)
+    ig_ref = FA.IntegratorDomain(dm)
+    for name, vals in (("density", mat.density), ("shear_modulus", mat.shear_modulus),
+                       ("bulk_modulus", mat.bulk_modulus)):
+        ig_ref.set_aux(name, FA.PER_CELL, vals[:, None])
+    ig_ref.set_kernels_residual([FA.ResidualKernels("displacement", FA.LHS, None, ref(F1_ILE))])
+    ig_ref.set_kernels_jacobian([FA.JacobianKernels("displacement", "displacement", FA.LHS, None, None, None,
+                                                    ref(JF3_ILE))])
+    u = dev(torch, np.random.default_rng(52).standard_normal(mesh.num_dof))
+    outs = []
+    for ig in (ig_lib, ig_ref):
+        r, jv = torch.empty_like(u), torch.empty_like(u)
+        ig.set_scatter(FA.SCATTER_DETERMINISTIC)
+        ig.compute_lhs_residual(0.0, 0.0, u, r)
+        ig.compute_lhs_jacobian_action(0.0, 0.0, 0.0, None, u, jv)
+        outs.append((r, jv))
+    ctx.synchronize()
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    # a fault with the reference's FaultCohesiveKin kernels
+    fmesh, fault = fault_setup()
+    fdm = FA.DeviceMesh(ctx, fmesh)
+    if_lib = fault.create_integrator(fdm)
+    if_ref = FA.IntegratorInterface(fdm)
+    if_ref.set_aux("slip", FA.PER_FAULT_NODE, fault.slip)
+    if_ref.set_constants(fault.constants)
+    if_ref.set_kernels_residual([
+        FA.InterfaceResidualKernels("displacement", FA.LHS, FA.FACE_NEGATIVE, ref("FaultCohesiveKin::f0u_neg"), None),
+        FA.InterfaceResidualKernels("displacement", FA.LHS, FA.FACE_POSITIVE, ref("FaultCohesiveKin::f0u_pos"), None),
+        FA.InterfaceResidualKernels("lagrange_multiplier_fault", FA.LHS, FA.FACE_FAULT,
+                                    ref("FaultCohesiveKin::f0l_slip"), None)])
+    fu = dev(torch, np.random.default_rng(53).standard_normal(fmesh.num_dof))
+    fr = [torch.zeros_like(fu), torch.zeros_like(fu)]
+    if_lib.compute_lhs_residual(0.0, 0.0, fu, fr[0])
+    if_ref.compute_lhs_residual(0.0, 0.0, fu, fr[1])
+    ctx.synchronize()
+    assert torch.equal(fr[0], fr[1])

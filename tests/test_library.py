@@ -133,3 +133,38 @@ def test_argument_validation_without_a_device(L):
     # destroying nothing is a no-op
     assert L.pl_integrator_destroy(null) == 0
     assert L.pl_matrix_destroy(null) == 0
+
+
+def test_registration_accepts_the_reference_build_and_refuses_other_functions():
+    """pl_fekernel_register runs a candidate on host probe inputs: the reference's kernels built
+    from its sources (oracle/_ref) are accepted under their names, and a function with the right
+    signature that computes something else is refused (PL_ERR_UNKNOWN_KERNEL), as is a name the
+    engine has no device implementation for."""
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+
+    import oracle as O  # tests/conftest.py puts oracle/ on the path
+
+    if O.ref_available():
+        for name in O.KERNELS:
+            FA.register_fekernel(name, O.kernel(name, "ref"))
+            assert FA.fekernel_name(O.kernel(name, "ref")) == name
+    D = ctypes.c_double
+    PI = ctypes.POINTER(ctypes.c_int)
+    PD = ctypes.POINTER(D)
+    POINT = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_int, ctypes.c_int, PI, PI, PD, PD, PD, PI, PI, PD, PD, PD,
+                             D, PD, ctypes.c_int, PD, PD)
+
+    def half_stress(dim, numS, numA, sOff, sOff_x, s, s_t, s_x, aOff, aOff_x, a, a_t, a_x, t, x, nc, c, f):
+        for i in range(9):
+            f[i] -= 0.5 * a[aOff[numA - 2]] * (s_x[i] + s_x[3 * (i % 3) + i // 3])
+
+    fn = POINT(half_stress)
+    addr = ctypes.cast(fn, ctypes.c_void_p).value
+    with pytest.raises(_lib.PylithB200Error) as e:
+        FA.register_fekernel("IsotropicLinearElasticity3D::f1v_infinitesimalStrain", addr)
+    assert e.value.code == -2
+    assert FA.fekernel_name(addr) is None
+    with pytest.raises(_lib.PylithB200Error) as e:
+        FA.register_fekernel("IsotropicLinearElasticity3D::f1v_infinitesimalStrain_refState", addr)
+    assert e.value.code == -2
