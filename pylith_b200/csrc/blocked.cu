@@ -752,17 +752,12 @@ static size_t blocked_smem(const BlockedLayout& b) {
     return (size_t)12 * kTetBlockCells * sizeof(double) + 2 * buf_bytes(b.max_local_nodes);
 }
 
-static int persistent_grid(int64_t nblocks) {
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    return (int)std::min<int64_t>(nblocks, (int64_t)nsm * PLB_TET_MIN_BLOCKS);
-}
+static int persistent_grid(int64_t nblocks) { return (int)std::min<int64_t>(nblocks, (int64_t)sm_count() * PLB_TET_MIN_BLOCKS); }
 
 template <int RHEO, bool BF, int OP, bool INSERT, bool DET>
 static void launch_one(const DomainParams& p, const BlockArrays& A, size_t smem, int grid, cudaStream_t s) {
     auto kern = k_tet_blocked<RHEO, BF, OP, INSERT, DET>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ensure_kernel_smem((const void*)kern, smem);
     kern<<<grid, kTetThreads, smem, s>>>(p, A);
     count_launch();
 }
@@ -803,7 +798,7 @@ static PipeArrays pipe_arrays_of(const BlockedLayout& b, double* partial) {
 template <bool PIPE, int RHEO, bool BF, int OP, bool INSERT, bool DET>
 static void launch_pipe_one(const DomainParams& p, const PipeArrays& A, size_t smem, int grid, cudaStream_t s) {
     auto kern = PIPE ? k_tet_pipe<RHEO, BF, OP, INSERT, DET> : k_tet_pad2<RHEO, BF, OP, INSERT, DET>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ensure_kernel_smem((const void*)kern, smem);
     kern<<<grid, kTetBlockCells, smem, s>>>(p, A);
     count_launch();
 }
@@ -812,10 +807,7 @@ template <bool PIPE, int RHEO, bool BF, int OP>
 static void launch_pipe_t(const DomainParams& p, const BlockedLayout& b, bool insert, double* partial, cudaStream_t s) {
     const PipeArrays A = pipe_arrays_of(b, partial);
     const size_t smem = PIPE ? pipe_smem_bytes(A.ld) : pad2_smem_bytes(A.ld);
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = (int)std::min<int64_t>(b.num_blocks, (int64_t)nsm * (PIPE ? PLB_PIPE_MIN_BLOCKS : PLB_PAD2_MIN_BLOCKS));
+    const int grid = (int)std::min<int64_t>(b.num_blocks, (int64_t)sm_count() * (PIPE ? PLB_PIPE_MIN_BLOCKS : PLB_PAD2_MIN_BLOCKS));
     const bool det = partial != nullptr;
     if (insert && det) launch_pipe_one<PIPE, RHEO, BF, OP, true, true>(p, A, smem, grid, s);
     else if (insert) launch_pipe_one<PIPE, RHEO, BF, OP, true, false>(p, A, smem, grid, s);
@@ -882,7 +874,7 @@ bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, i
     const size_t smem = (size_t)12 * kTetBlockCells * sizeof(float) +
                         (size_t)b.max_local_nodes * (3 * sizeof(double) + 3 * sizeof(float));
     if (smem > 200 * 1024) return false;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_tet_blocked_jv32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ensure_kernel_smem((const void*)k_tet_blocked_jv32, smem);
     // the output was zeroed by the caller (INSERT) or holds the partial sum (ADD)
     k_tet_blocked_jv32<<<persistent_grid(b.num_blocks), kTetBlockCells, smem, s>>>(p, arrays_of(b));
     count_launch();

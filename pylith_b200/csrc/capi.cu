@@ -23,6 +23,37 @@ unsigned long long state_epoch() { return g_epoch.load(); }
 
 void count_launch(int n) { g_launches += n; }
 
+void ensure_kernel_smem(const void* kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return;
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void*, int>, size_t>> set;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto& e : set)
+        if (e.first.first == kernel && e.first.second == dev) {
+            if (e.second >= bytes) return;
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            e.second = bytes;
+            return;
+        }
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    set.push_back({{kernel, dev}, bytes});
+}
+
+int sm_count() {
+    static int counts[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!counts[dev]) {
+        int n = 148;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        counts[dev] = n;
+    }
+    return counts[dev];
+}
+
 void set_error(const std::string& msg) { g_last_error = msg; }
 
 int fail(int code, const std::string& msg) {

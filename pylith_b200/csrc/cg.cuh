@@ -10,6 +10,12 @@ namespace plb {
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 296;  // 2 per SM
 
+// FP32 reliable-update PCG: an iterated residual this many times the last true residual counts
+// as a breakdown (the FP32 correction is dropped and the iteration restarts from the true
+// residual); a solve gives up after kMaxBreakdowns of them.
+constexpr double kBreakdownGrowth = 100.0;
+constexpr int kMaxBreakdowns = 20;
+
 enum Scalar { S_RZ = 0, S_RZ_OLD, S_PQ, S_RR, S_ALPHA, S_BETA, S_BB, S_COUNT };
 
 template <typename T>

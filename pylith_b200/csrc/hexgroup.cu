@@ -333,7 +333,7 @@ void launch_hex8_jv32_ragged(const DomainParams* ops, const int64_t* chunk0, con
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (smem > 48 * 1024) cudaFuncSetAttribute(k_hex8_jv32_ragged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        ensure_kernel_smem((const void*)k_hex8_jv32_ragged, smem);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hex8_jv32_ragged, H::WARPS * 32, smem);
         per_sm = std::max(per_sm, 1);
     }
@@ -864,11 +864,13 @@ template <int RHEO, bool BF, int OP>
 static void launch_lines_t(const DomainParams& p, cudaStream_t s) {
     auto kern = k_hex27_lines<RHEO, BF, OP>;
     const size_t smem = Lines::smem_bytes();
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Lines::WARPS * 32, smem);
+    ensure_kernel_smem((const void*)kern, smem);
+    const int nsm = sm_count();
+    static int per_sm = 0;  // occupancy of this instantiation (the same on every B200)
+    if (!per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Lines::WARPS * 32, smem);
+        per_sm = std::max(per_sm, 1);
+    }
     const int64_t blocks = (p.ncells + 3 * Lines::WARPS - 1) / (3 * Lines::WARPS);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)nsm * std::max(per_sm, 1)));
     kern<<<grid, Lines::WARPS * 32, smem, s>>>(p);
@@ -898,11 +900,13 @@ template <int RHEO, bool BF, int OP, typename T = double>
 static void launch_sumfact_t(const DomainParams& p, cudaStream_t s) {
     auto kern = k_hex27_sumfact<RHEO, BF, OP, T>;
     const size_t smem = SumFact::smem_bytes();
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SumFact::WARPS * 32, smem);
+    ensure_kernel_smem((const void*)kern, smem);
+    const int nsm = sm_count();
+    static int per_sm = 0;  // occupancy of this instantiation (the same on every B200)
+    if (!per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SumFact::WARPS * 32, smem);
+        per_sm = std::max(per_sm, 1);
+    }
     const int64_t blocks = (p.ncells + SumFact::WARPS - 1) / SumFact::WARPS;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)nsm * std::max(per_sm, 1)));
     kern<<<grid, SumFact::WARPS * 32, smem, s>>>(p);
@@ -914,11 +918,13 @@ static void launch_group_t(const DomainParams& p, cudaStream_t s) {
     using H = HexGroup<CELL, T>;
     auto kern = k_hex_group<CELL, RHEO, BF, OP, T>;
     const size_t smem = H::smem_bytes();
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, H::WARPS * 32, smem);
+    ensure_kernel_smem((const void*)kern, smem);
+    const int nsm = sm_count();
+    static int per_sm = 0;  // occupancy of this instantiation (the same on every B200)
+    if (!per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, H::WARPS * 32, smem);
+        per_sm = std::max(per_sm, 1);
+    }
     const int64_t groups = (p.ncells + H::WARPS * H::CPW - 1) / (H::WARPS * H::CPW);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(groups, (int64_t)nsm * std::max(per_sm, 1)));
     kern<<<grid, H::WARPS * 32, smem, s>>>(p);

@@ -18,6 +18,11 @@ struct BlockedLayout;
 
 // Counts kernel launches made by this library (reported by pl_kernel_launches).
 void count_launch(int n = 1);
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the current device; the
+// attribute is set once per (kernel, device, size) instead of on every launch.
+void ensure_kernel_smem(const void* kernel, size_t bytes);
+// Multiprocessor count of the current device (queried once per device).
+int sm_count();
 bool launch_tangent_lm32(const DomainParams& p, int rheo, float* out, cudaStream_t s);
 
 void launch_domain_apply_atomic(const DomainParams& p, int cell, int rheo, bool bf, int op,
@@ -60,7 +65,9 @@ void launch_hex8_jv32_ragged(const DomainParams* ops, const int64_t* chunk0, con
                              cudaStream_t s);
 // Step-by-step FP32 reliable-update PCG of one solver for an outside iteration loop (solver.cu).
 int solver32_begin(pl_solver_s* S, const double* b, double* x, double* b0);
-int solver32_replace(pl_solver_s* S, const double* b, double* x, bool restart, double* rt);
+int solver32_replace(pl_solver_s* S, const double* b, double* x, bool restart, bool keep_correction, double* rt);
+// P^T b for a solver with faults (in the solver's scratch vector), b otherwise.
+const double* solver_reduced_rhs(pl_solver_s* S, const double* b);
 
 // FP32 Jacobian action on the cell blocks (the output must be zeroed or hold the sum to add to).
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,

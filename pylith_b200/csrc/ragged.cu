@@ -211,7 +211,7 @@ struct Member {
     bool active = false;
     int status = PL_ERR_NOT_READY;  // PL_OK when converged, an error code on failure
     double b0 = 0.0, rref = 0.0, rt = 0.0, stop = 0.0;
-    int iterations = 0, replacements = 0;
+    int iterations = 0, replacements = 0, breakdowns = 0;
 };
 
 }  // namespace
@@ -390,9 +390,9 @@ int pl_ragged_add(pl_ragged R, pl_solver S, const double* b_dev, double* x_dev, 
     PLB_CUDA(cudaSetDevice(R->ctx->device));
     Member mb;
     mb.S = S;
-    mb.b = b_dev;
+    mb.b = solver_reduced_rhs(S, b_dev);  // with faults: P^T b in the solver's scratch vector
     mb.x = x_dev;
-    int rc = solver32_begin(S, b_dev, x_dev, &mb.b0);
+    int rc = solver32_begin(S, mb.b, x_dev, &mb.b0);
     if (rc) return rc;
     mb.rref = mb.rt = mb.b0;
     mb.stop = std::max(S->rtol * mb.b0, S->atol);
@@ -445,17 +445,19 @@ int pl_ragged_iterate(pl_ragged R, int* active_left) {
             mb.iterations += R->chunk;
             S->inner_iterations = mb.iterations;
             const double rn = std::sqrt(rr[i]);
-            if (!(rn == rn)) {
-                finish_member(R, mb, PL_ERR_NOT_CONVERGED);
+            // FP32 breakdown (see pcg32_reliable): drop the correction, restart from the true residual
+            const bool broke = !(rn == rn) || rn > kBreakdownGrowth * mb.rref;
+            if (!broke && rn > S->reliable_delta * mb.rref && rn > 0.5 * mb.stop) {
+                if (mb.iterations >= S->max_iter) finish_member(R, mb, PL_ERR_NOT_CONVERGED);
                 continue;
             }
-            if (rn > S->reliable_delta * mb.rref && rn > 0.5 * mb.stop) {
-                if (mb.iterations >= S->max_iter) finish_member(R, mb, PL_ERR_NOT_CONVERGED);
+            if (broke && ++mb.breakdowns > kMaxBreakdowns) {
+                finish_member(R, mb, PL_ERR_NOT_CONVERGED);
                 continue;
             }
             // residual replacement with this member's own FP64 launches
             double rt = 0.0;
-            if ((rc = solver32_replace(S, mb.b, mb.x, rn <= 0.5 * mb.stop, &rt)) != PL_OK) return rc;
+            if ((rc = solver32_replace(S, mb.b, mb.x, broke || rn <= 0.5 * mb.stop, !broke, &rt)) != PL_OK) return rc;
             mb.replacements++;
             mb.rt = rt;
             S->outer_iterations = mb.replacements;

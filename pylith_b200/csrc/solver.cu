@@ -491,6 +491,7 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
         return PL_OK;
     };
     double b0 = 0.0, rt = 0.0;
+    int breakdowns = 0;
     do {
         if (cudaMemsetAsync(x, 0, n * sizeof(double), cs) != cudaSuccess ||
             cudaMemsetAsync(S->f_x, 0, n * sizeof(float), cs) != cudaSuccess) {
@@ -523,13 +524,20 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
             }
             S->inner_iterations += chunk;
             const double rn = std::sqrt(h[S_RR]);
-            if (!(rn == rn)) {
-                rc = fail(PL_ERR_NOT_CONVERGED, "PCG diverged (NaN residual)");
+            // FP32 breakdown: the iterated residual is not a number, or has grown far above the
+            // last true residual (FP32 rounding of a nearly converged system can turn p.(A p) into
+            // noise). The FP32 correction since the last replacement is dropped and the iteration
+            // starts again from the true residual.
+            const bool broke = !(rn == rn) || rn > kBreakdownGrowth * rref;
+            if (!broke && rn > S->reliable_delta * rref && rn > 0.5 * stop) continue;
+            if (broke && ++breakdowns > kMaxBreakdowns) {
+                rc = fail(PL_ERR_NOT_CONVERGED, "FP32 PCG keeps breaking down");
                 break;
             }
-            if (rn > S->reliable_delta * rref && rn > 0.5 * stop) continue;
-            k_add_correction<<<vec_grid(n), 256, 0, cs>>>(x, S->f_x, S->d_mask, n);
-            count_launch();
+            if (!broke) {
+                k_add_correction<<<vec_grid(n), 256, 0, cs>>>(x, S->f_x, S->d_mask, n);
+                count_launch();
+            }
             if (cudaMemsetAsync(S->f_x, 0, n * sizeof(float), cs) != cudaSuccess) {
                 rc = fail(PL_ERR_CUDA, "memset");
                 break;
@@ -545,8 +553,8 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
             k_finish2<<<1, 1024, 0, cs>>>(S->d_partials, kRedBlocks, scal, S_RZ, -1);
             count_launch(2);
             // The FP32 iterations had run below the stopping threshold while the true residual had
-            // not: their search direction is rounding noise, so restart it from z.
-            if (rn <= 0.5 * stop &&
+            // not, or had broken down: their search direction is rounding noise, so restart it from z.
+            if ((broke || rn <= 0.5 * stop) &&
                 cudaMemcpyAsync(S->f_p, S->f_z, n * sizeof(float), cudaMemcpyDeviceToDevice, cs) != cudaSuccess) {
                 rc = fail(PL_ERR_CUDA, "search direction restart");
                 break;
@@ -563,6 +571,15 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
 }  // namespace
 
 namespace plb {
+
+// The reduced system's right-hand side P^T b (the two sides' equations of every fault node summed;
+// the solver's d_x holds it) when the mesh has faults, else b itself.
+const double* solver_reduced_rhs(pl_solver S, const double* b) {
+    if (S->npairs == 0) return b;
+    cudaMemcpyAsync(S->d_x, b, S->n * sizeof(double), cudaMemcpyDeviceToDevice, S->mesh->ctx->stream);
+    fault_fold(S, S->d_x);
+    return S->d_x;
+}
 
 // The FP32 reliable-update PCG of one solver, driven step by step by an outside loop (the ragged
 // batch runs the iterations of many solvers in shared launches). Both run on the context's
@@ -597,15 +614,18 @@ int solver32_begin(pl_solver S, const double* b, double* x, double* b0) {
     return PL_OK;
 }
 
-// Residual replacement: x += f_x, f_x = 0, r = b - A x in FP64 (*rt = |r|), r.z for the new r
-// (z = P r); with restart the search direction starts again from z; q = 0.
-int solver32_replace(pl_solver S, const double* b, double* x, bool restart, double* rt) {
+// Residual replacement: x += f_x (unless the correction is dropped after a breakdown), f_x = 0,
+// r = b - A x in FP64 (*rt = |r|), r.z for the new r (z = P r); with restart the search direction
+// starts again from z; q = 0.
+int solver32_replace(pl_solver S, const double* b, double* x, bool restart, bool keep_correction, double* rt) {
     pl_context c = S->mesh->ctx;
     cudaStream_t s = c->stream;
     const int64_t n = S->n;
     double h[S_COUNT];
-    k_add_correction<<<vec_grid(n), 256, 0, s>>>(x, S->f_x, S->d_mask, n);
-    count_launch();
+    if (keep_correction) {
+        k_add_correction<<<vec_grid(n), 256, 0, s>>>(x, S->f_x, S->d_mask, n);
+        count_launch();
+    }
     PLB_CUDA(cudaMemsetAsync(S->f_x, 0, n * sizeof(float), s));
     int rc = apply_J(S, x, S->d_q);
     if (rc) return rc;

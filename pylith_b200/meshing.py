@@ -212,6 +212,97 @@ def box_tet_delaunay(target_cells: int, seed: int = 0, lo=BOX_LO, hi=BOX_HI,
     return reorder_for_locality(mesh) if reorder else mesh
 
 
+def box_tet_delaunay_fault_x(target_cells: int, seed: int = 0, lo=BOX_LO, hi=BOX_HI, x0: float = 0.0,
+                             reorder: bool = True) -> Mesh:
+    """Delaunay P1 tetrahedra of a box symmetric about the plane x = x0, with a planar vertical
+    fault of cohesive cells on that plane.
+
+    The half box x >= x0 is triangulated as in `box_tet_delaunay` (seeded random interior points,
+    a grid on its faces jittered inside each face), and mirrored across x = x0, so the two halves'
+    triangulations of the plane are the same: the mesh is conforming across the fault. The plane's
+    nodes are split (the +x cells take new positive-side copies) and every cell of the plane's
+    face grid becomes a cohesive quadrilateral (negative side, positive side, Lagrange nodes; the
+    normal points from - to +), whose corners are the plane grid's points: the solver uses the
+    cohesive cells for their node pairs and the fault normal (libsrc/pylith/faults/TopologyOps.cc
+    inserts cohesive cells on the mesh's own faces; here the faces of the two halves coincide).
+    """
+    from scipy.spatial import Delaunay
+
+    lo = np.asarray(lo, dtype=np.float64)
+    hi = np.asarray(hi, dtype=np.float64)
+    if not np.isclose(x0 - lo[0], hi[0] - x0):
+        raise ValueError("the box must be symmetric about x = x0")
+    hlo = np.array([x0, lo[1], lo[2]])
+    ext = hi - hlo
+    npts = max(int(0.5 * target_cells / 6.3), 64)
+    h = (np.prod(ext) / npts) ** (1.0 / 3.0)
+    nb = np.maximum(np.round(ext / h).astype(int), 2)
+    axes = [np.linspace(hlo[d], hi[d], nb[d] + 1) for d in range(3)]
+    I, J, K = np.meshgrid(*[np.arange(n + 1) for n in nb], indexing="ij")
+    ijk = np.stack([I.ravel(), J.ravel(), K.ravel()], axis=1)
+    grid = np.stack([axes[d][ijk[:, d]] for d in range(3)], axis=1)
+    on_face = np.zeros(len(grid), dtype=bool)
+    for d in range(3):
+        on_face |= (ijk[:, d] == 0) | (ijk[:, d] == nb[d])
+    boundary, bijk = grid[on_face], ijk[on_face]
+    rng = np.random.default_rng(seed)
+    pinned = np.zeros_like(boundary, dtype=bool)
+    for d in range(3):
+        pinned[:, d] = (bijk[:, d] == 0) | (bijk[:, d] == nb[d])
+    step = ext / nb
+    boundary = np.where(pinned, boundary, boundary + rng.uniform(-0.3, 0.3, boundary.shape) * step)
+    nint = max(npts - len(boundary), 8)
+    margin = 0.25 * h
+    interior = hlo + margin + rng.random((nint, 3)) * (ext - 2 * margin)
+    pts = np.concatenate([boundary, interior], axis=0)
+    cells = Delaunay(pts).simplices.astype(np.int64)
+    vol = _tet_volumes(pts, cells)
+    keep = np.abs(vol) > 1e-9 * np.abs(vol).mean()
+    if not keep.all():
+        flat = pts[cells[~keep]]
+        same_face = np.zeros(len(flat), dtype=bool)
+        for d in range(3):
+            for v in (hlo[d], hi[d]):
+                same_face |= np.isclose(flat[:, :, d], v).all(axis=1)
+        if not same_face.all():
+            raise RuntimeError("Delaunay produced degenerate tetrahedra off the box faces")
+    cells, vol = cells[keep], vol[keep]
+    neg = vol < 0
+    cells[neg, 2], cells[neg, 3] = cells[neg, 3].copy(), cells[neg, 2].copy()
+    npt = len(pts)
+    # the fault plane's points (grid i == 0) and their (j, k) grid indices
+    plane = np.zeros(npt, dtype=bool)
+    plane[:len(boundary)] = bijk[:, 0] == 0
+    jk_of = np.full((nb[1] + 1, nb[2] + 1), -1, dtype=np.int64)
+    pidx = np.flatnonzero(plane)
+    jk_of[bijk[pidx, 1], bijk[pidx, 2]] = pidx
+    # nodes: the negative half (mirror; plane points shared), then the positive half's own points,
+    # then the positive-side copies of the plane points
+    off_pos = np.flatnonzero(~plane)
+    neg_id = np.arange(npt)                      # mirror: plane points keep their ids
+    mir = pts.copy()
+    mir[:, 0] = 2 * x0 - mir[:, 0]
+    pos_id = np.full(npt, -1, dtype=np.int64)
+    pos_id[off_pos] = npt + np.arange(len(off_pos))
+    pos_id[pidx] = npt + len(off_pos) + np.arange(len(pidx))
+    coords = np.concatenate([mir, pts[off_pos], pts[pidx]], axis=0)
+    neg_cells = neg_id[cells][:, [0, 1, 3, 2]]  # the mirror reverses orientation
+    pos_cells = pos_id[cells]
+    all_cells = np.concatenate([neg_cells, pos_cells], axis=0)
+    # cohesive quads of the plane grid, corners (j,k), (j+1,k), (j+1,k+1), (j,k+1): +y then +z
+    jj, kk = np.meshgrid(np.arange(nb[1]), np.arange(nb[2]), indexing="ij")
+    jj, kk = jj.ravel(), kk.ravel()
+    quad = np.stack([jk_of[jj, kk], jk_of[jj + 1, kk], jk_of[jj + 1, kk + 1], jk_of[jj, kk + 1]], axis=1)
+    lag_of = np.full(npt, -1, dtype=np.int64)
+    lag_of[pidx] = np.arange(len(pidx))
+    coh = np.concatenate([neg_id[quad], pos_id[quad], lag_of[quad]], axis=1).astype(np.int32)
+    used = np.unique(all_cells)
+    if len(used) != len(coords):
+        raise RuntimeError("unused nodes in the mirrored mesh")
+    mesh = Mesh(CELL_TET4, np.ascontiguousarray(coords), all_cells.astype(np.int32), coh, len(pidx))
+    return reorder_for_locality(mesh) if reorder else mesh
+
+
 def boundary_mask(mesh: Mesh, axis: int, side: str, lo=BOX_LO, hi=BOX_HI, tol: float = 1e-6):
     """Boolean mask of nodes on the box face x_axis = lo (side 'neg') or hi ('pos')."""
     val = lo[axis] if side == "neg" else hi[axis]
