@@ -721,13 +721,27 @@ def config_c2(args):
     dt = MAT.YEAR
     out = {"config": "c2", "cells": nc, "dof": mesh.num_dof, "steps": steps}
     from pylith_b200 import feassemble as FA
+    from pylith_b200 import multigrid as MG
 
     ctx = FA.Context(0)
+    levels = None
+    if nx % 4 == 0 and ny % 4 == 0 and nz % 4 == 0:
+        levels = MG.build_hierarchy(nx, ny, nz, fault_x=0.0,
+                                    constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))])
+        assert np.array_equal(levels[0].constrained, cons)
+        out["multigrid_levels"] = [list(lv.n) for lv in levels]
     sols = {}
-    for name, prec in (("fp64", FA.Solver.FP64), ("fp32_refined", FA.Solver.FP32_REFINED)):
+    variants = [("fp64", FA.Solver.FP64, None), ("fp32_refined", FA.Solver.FP32_REFINED, None)]
+    if levels is not None:
+        variants += [("fp64_multigrid", FA.Solver.FP64, FA.Solver.FP64),
+                     ("fp32_vcycle_multigrid", FA.Solver.FP64, FA.Solver.FP32_REFINED)]
+    for name, prec, mg_prec in variants:
         g = MAT.IsotropicLinearGenMaxwell(rho, mu, K, tau, ratio, z[0], z[1])
         prob = P.QuasistaticProblem(ctx, mesh, [(g, None)], cons, bc, faults=[MAT.FaultCohesiveKin(slip)],
                                     dt=dt, precision=prec, rtol=1e-10, inner_rtol=1e-4)
+        mg = None
+        if mg_prec is not None:
+            mg = MG.attach(ctx, prob.solver, levels, g, fault_x=0.0, dt=dt, precision=mg_prec)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         its = 0
@@ -738,10 +752,15 @@ def config_c2(args):
         el = time.perf_counter() - t0
         sols[name] = prob.u.cpu().numpy()
         out[name] = {"s_per_step": el / steps, "iterations_per_step": its / steps}
+        if mg is not None:
+            out[name]["lambda_max_per_level"] = mg.lambda_max()
+            mg.close()
     nd = 3 * mesh.num_nodes
-    out["rel_displacement_diff_fp32_vs_fp64"] = float(
-        np.linalg.norm(sols["fp32_refined"][:nd] - sols["fp64"][:nd]) / np.linalg.norm(sols["fp64"][:nd]))
-    out["speedup_fp32_refined"] = out["fp64"]["s_per_step"] / out["fp32_refined"]["s_per_step"]
+    ref = sols["fp64"][:nd]
+    for name in sols:
+        if name != "fp64":
+            out[f"rel_displacement_diff_{name}_vs_fp64"] = float(np.linalg.norm(sols[name][:nd] - ref) / np.linalg.norm(ref))
+            out[f"speedup_{name}"] = out["fp64"]["s_per_step"] / out[name]["s_per_step"]
     return out
 
 

@@ -349,6 +349,34 @@ int pl_solver_get_stats(pl_solver solver, int* iterations, int* inner_iterations
                         int* outer_iterations, double* rel_residual);
 int pl_solver_destroy(pl_solver solver);
 
+/* ---- geometric multigrid preconditioner (the class of preconditioner the reference configures:
+ *      PETSc GAMG, libsrc/pylith/materials/Elasticity.cc:298-330) ------------------------------ */
+/* A hierarchy of solvers on successively coarser meshes of the same domain (each with its own
+ * integrators, constraint mask and faults; all on one context), tied by prolongations from level
+ * l + 1 to level l given as host CSR node matrices: prolong_row_ptr[l] has (nodes of level l) + 1
+ * entries, prolong_col[l] holds level-(l+1) node indices and prolong_val[l] the weights (applied to
+ * each of the 3 components; positive-side fault nodes interpolate from their own side).
+ * pylith_b200/multigrid.py builds them for structured hexahedral boxes. */
+typedef struct pl_multigrid_s* pl_multigrid;
+int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
+                        const int32_t* const* prolong_row_ptr, const int32_t* const* prolong_col,
+                        const double* const* prolong_val, pl_multigrid* out);
+/* Smoother: Chebyshev polynomial of point-block Jacobi of `degree` on [lower_ratio b, b],
+ * b = 1.1 lambda_max(D^-1 A) estimated by power iterations at the first solve after each setup;
+ * the coarsest level takes degree coarse_degree on [coarse_lower_ratio b, b]. precision
+ * PL_SOLVER_FP32_REFINED runs the V-cycle in FP32 (the outer conjugate gradients stay FP64).
+ * Defaults: 2, 0.1, 40, 0.01, PL_SOLVER_FP64. */
+int pl_multigrid_set_smoother(pl_multigrid mg, int degree, double lower_ratio, int coarse_degree,
+                              double coarse_lower_ratio, int precision);
+/* Makes pl_solver_solve run flexible conjugate gradients in FP64 preconditioned by one V-cycle
+ * of `mg` (NULL: back to point-block Jacobi); pl_solver_setup then sets up every level. */
+int pl_solver_set_multigrid(pl_solver solver, pl_multigrid mg);
+/* Levels and each level's lambda_max(D^-1 A) estimate (0 before the first solve). */
+int pl_multigrid_get_levels(pl_multigrid mg, int* num_levels, double* lambda_max);
+/* Refused while the hierarchy is attached to its solver (pl_solver_set_multigrid(solver, NULL)
+ * or pl_solver_destroy detaches it). */
+int pl_multigrid_destroy(pl_multigrid mg);
+
 /* ---- batched right-hand sides (Green's functions; replaces the one-impulse-at-a-time
  *      SNES loop of libsrc/pylith/problems/GreensFns.cc:291-337) ------------------------------ */
 /* Solves A x_i = b_i for many right-hand sides with the operator, constraints, preconditioner and

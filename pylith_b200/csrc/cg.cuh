@@ -50,6 +50,40 @@ PL_D void block_sum2(double a, double b, double* partials) {
     }
 }
 
+// Sum the partials of the previous pass in a fixed order into scal[i0], scal[i1].
+static __global__ void k_finish2(const double* __restrict__ partials, int nblk, double* scal, int i0, int i1) {
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+        a += partials[2 * i];
+        b += partials[2 * i + 1];
+    }
+    __shared__ double sa[32], sb[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sa[w] = a;
+        sb[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = l < (int)(blockDim.x >> 5) ? sa[l] : 0.0;
+        b = l < (int)(blockDim.x >> 5) ? sb[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (l == 0) {
+            if (i0 >= 0) scal[i0] = a;
+            if (i1 >= 0) scal[i1] = b;
+        }
+    }
+}
+
 // z = P^{-1} r with point blocks; constrained entries of r are zero and P^{-1} is the identity
 // on them, so z stays zero there.
 template <typename T>

@@ -218,4 +218,13 @@ struct pl_solver_s {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_iters[2] = {0, 0};
     unsigned long long graph_epoch[2] = {0, 0};
+    // geometric multigrid preconditioner (pl_solver_set_multigrid): when set, pl_solver_solve runs
+    // multigrid-preconditioned flexible CG instead of point-block-Jacobi PCG
+    struct pl_multigrid_s* mg = nullptr;
 };
+
+namespace plb {
+int multigrid_setup(pl_multigrid_s* mg, double t, double dt);
+int multigrid_solve(pl_multigrid_s* mg, const double* b, double* x);
+void multigrid_detach(pl_multigrid_s* mg);
+}  // namespace plb

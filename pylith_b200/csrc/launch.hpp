@@ -66,6 +66,13 @@ void launch_hex8_jv32_ragged(const DomainParams* ops, const int64_t* chunk0, con
 // Step-by-step FP32 reliable-update PCG of one solver for an outside iteration loop (solver.cu).
 int solver32_begin(pl_solver_s* S, const double* b, double* x, double* b0);
 int solver32_replace(pl_solver_s* S, const double* b, double* x, bool restart, bool keep_correction, double* rt);
+// q = J v of a solver's integrators with its faults' unfold and fold; the unfold and fold alone.
+int solver_apply_J(pl_solver_s* S, const double* v, double* out);
+int solver_apply_J32(pl_solver_s* S, const float* v, float* out);
+void solver_unfold(pl_solver_s* S, double* v);
+void solver_unfold32(pl_solver_s* S, float* v);
+void solver_fold(pl_solver_s* S, double* v);
+void solver_fold32(pl_solver_s* S, float* v);
 // P^T b for a solver with faults (in the solver's scratch vector), b otherwise.
 const double* solver_reduced_rhs(pl_solver_s* S, const double* b);
 

@@ -23,40 +23,6 @@
 
 namespace plb {
 
-// Sum the partials of the previous pass in a fixed order into scal[i0], scal[i1].
-__global__ void k_finish2(const double* __restrict__ partials, int nblk, double* scal, int i0, int i1) {
-    double a = 0.0, b = 0.0;
-    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
-        a += partials[2 * i];
-        b += partials[2 * i + 1];
-    }
-    __shared__ double sa[32], sb[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        sa[w] = a;
-        sb[w] = b;
-    }
-    __syncthreads();
-    if (w == 0) {
-        a = l < (int)(blockDim.x >> 5) ? sa[l] : 0.0;
-        b = l < (int)(blockDim.x >> 5) ? sb[l] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xffffffffu, a, o);
-            b += __shfl_down_sync(0xffffffffu, b, o);
-        }
-        if (l == 0) {
-            if (i0 >= 0) scal[i0] = a;
-            if (i1 >= 0) scal[i1] = b;
-        }
-    }
-}
-
 // dots (a.b, c.d) over unconstrained DOFs.
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_dot2(const T* a, const T* b, const T* c, const T* d,
@@ -572,6 +538,15 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
 
 namespace plb {
 
+// Operator pieces for outside drivers (the multigrid hierarchy): q = J v with the fault's unfold
+// and fold (FP64, FP32), and the unfold / fold alone.
+int solver_apply_J(pl_solver S, const double* v, double* out) { return apply_J(S, v, out); }
+int solver_apply_J32(pl_solver S, const float* v, float* out) { return apply_J32(S, v, out); }
+void solver_unfold(pl_solver S, double* v) { fault_unfold(S, v); }
+void solver_unfold32(pl_solver S, float* v) { fault_unfold(S, v); }
+void solver_fold(pl_solver S, double* v) { fault_fold(S, v); }
+void solver_fold32(pl_solver S, float* v) { fault_fold(S, v); }
+
 // The reduced system's right-hand side P^T b (the two sides' equations of every fault node summed;
 // the solver's d_x holds it) when the mesh has faults, else b itself.
 const double* solver_reduced_rhs(pl_solver S, const double* b) {
@@ -790,6 +765,10 @@ int pl_solver_setup(pl_solver S, double t, double dt) {
     k_invert_blocks<<<vec_grid(S->nnodes), 256, 0, s>>>(S->d_diag, S->d_mask, S->nnodes, S->d_pinv, S->d_pinv32);
     count_launch();
     PLB_CUDA(cudaGetLastError());
+    if (S->mg) {
+        int rc = multigrid_setup(S->mg, t, dt);
+        if (rc) return rc;
+    }
     S->ready = true;
     return PL_OK;
 }
@@ -801,6 +780,7 @@ int pl_solver_solve(pl_solver S, const double* b, double* x) {
     cudaStream_t s = m->ctx->stream;
     PLB_CUDA(cudaSetDevice(m->ctx->device));
     S->iterations = S->inner_iterations = S->outer_iterations = 0;
+    if (S->mg) return multigrid_solve(S->mg, b, x);
     const int64_t n = S->n;
     if (S->npairs > 0) {  // right-hand side of the reduced system: P^T b
         PLB_CUDA(cudaMemcpyAsync(S->d_x, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -882,6 +862,7 @@ int pl_solver_get_stats(pl_solver S, int* iterations, int* inner_iterations, int
 }  // extern "C"
 
 static void solver_free(pl_solver S) {
+    if (S->mg) multigrid_detach(S->mg);
     cudaSetDevice(S->mesh->ctx->device);
     cudaStreamSynchronize(S->mesh->ctx->stream);
     for (cudaGraphExec_t g : S->graph)

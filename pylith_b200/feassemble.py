@@ -484,3 +484,45 @@ class RaggedBatch:
             self.close()
         except Exception:
             pass
+
+
+class Multigrid:
+    """Geometric multigrid preconditioner of a `Solver` (pl_multigrid_*): coarse-level solvers (set
+    up together with the fine one) and the prolongations between levels, as CSR node matrices
+    (row_ptr, col, val) from level l + 1 to level l. Attaching it makes the fine solver run
+    flexible CG preconditioned by V-cycles."""
+
+    def __init__(self, fine: Solver, coarse, prolongations, degree=2, lower=0.1, coarse_degree=40,
+                 coarse_lower=0.01, precision=C.PL_SOLVER_FP64):
+        self.fine = fine
+        self.coarse = list(coarse)
+        self._P = [tuple(np.ascontiguousarray(a, dtype=t) for a, t in zip(P, (np.int32, np.int32, np.float64)))
+                   for P in prolongations]
+        n = len(self.coarse)
+        solvers = (ctypes.c_void_p * n)(*[s.handle.value for s in self.coarse])
+        rows = (ctypes.c_void_p * n)(*[P[0].ctypes.data for P in self._P])
+        cols = (ctypes.c_void_p * n)(*[P[1].ctypes.data for P in self._P])
+        vals = (ctypes.c_void_p * n)(*[P[2].ctypes.data for P in self._P])
+        self.handle = ctypes.c_void_p()
+        check(C.lib().pl_multigrid_create(fine.handle, n, solvers, rows, cols, vals, ctypes.byref(self.handle)))
+        check(C.lib().pl_multigrid_set_smoother(self.handle, degree, lower, coarse_degree, coarse_lower, precision))
+        check(C.lib().pl_solver_set_multigrid(fine.handle, self.handle))
+
+    def lambda_max(self):
+        n = ctypes.c_int()
+        lam = (ctypes.c_double * (len(self.coarse) + 1))()
+        check(C.lib().pl_multigrid_get_levels(self.handle, ctypes.byref(n), lam))
+        return list(lam)[:n.value]
+
+    def close(self):
+        if self.handle:
+            if self.fine.handle:
+                C.lib().pl_solver_set_multigrid(self.fine.handle, None)
+            C.lib().pl_multigrid_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -14,6 +14,8 @@
 
 namespace plb {
 void count_launch(int) {}
+void ensure_kernel_smem(const void*, size_t) {}
+int sm_count() { return 148; }
 int cuda_fail(cudaError_t, const char*) { return PL_ERR_CUDA; }
 int fail(int code, const std::string&) { return code; }
 }  // namespace plb

@@ -1,0 +1,66 @@
+"""Geometric multigrid preconditioning of the device solver (pl_multigrid_*): on a Q1 box with a
+fault at x = 0, flexible CG with V-cycles (FP64, or FP32 V-cycles under FP64 CG) reaches the
+point-block-Jacobi PCG solution (relative displacement difference <= 1e-8 at rtol 1e-12) in at
+least five times fewer iterations, for isotropic elasticity and generalized Maxwell."""
+import numpy as np
+import pytest
+
+from pylith_b200 import materials as MAT
+from pylith_b200 import meshing as M
+from pylith_b200 import multigrid as MG
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from pylith_b200 import feassemble as FA
+
+    return FA.Context(0)
+
+
+@pytest.mark.parametrize("rheology", ["elastic", "genmaxwell"])
+def test_multigrid_matches_point_jacobi_in_fewer_iterations(ctx, rheology):
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import problems as P
+
+    levels = MG.build_hierarchy(16, 16, 12, fault_x=0.0, constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))])
+    assert len(levels) >= 3
+    mesh, cons = levels[0].mesh, levels[0].constrained
+    nc = mesh.num_cells
+    rho, mu, K = MAT.lognormal_elastic(nc, seed=3)
+    dt = MAT.YEAR if rheology == "genmaxwell" else 0.0
+    if rheology == "genmaxwell":
+        tau = MAT.genmaxwell_times(rho, np.sqrt(mu / rho), [1e18, 1e19, 1e20], [0.3, 0.3, 0.3])
+        mat = MAT.IsotropicLinearGenMaxwell(rho, mu, K, tau, np.tile([0.3, 0.3, 0.3], (nc, 1)),
+                                            np.zeros((nc, 8, 18)), np.zeros((nc, 8, 6)))
+    else:
+        mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    slip = np.zeros((mesh.num_lagrange, 3))
+    slip[: mesh.num_lagrange // 2, 1] = 2.0
+    bc = np.zeros(mesh.num_dof)
+
+    def run(precision=None):
+        prob = P.QuasistaticProblem(ctx, mesh, [(mat, None)], cons, bc, faults=[MAT.FaultCohesiveKin(slip)], dt=dt,
+                                    precision=FA.Solver.FP64, rtol=1e-12)
+        mg = None
+        if precision is not None:
+            mg = MG.attach(ctx, prob.solver, levels, mat, fault_x=0.0, dt=dt, precision=precision)
+        st = prob.step(dt)
+        u = prob.u.cpu().numpy()
+        lam = mg.lambda_max() if mg else None
+        if mg:
+            mg.close()
+        return u, st, lam
+
+    u_ref, st_ref, _ = run()
+    for precision in (FA.Solver.FP64, FA.Solver.FP32_REFINED):
+        u, st, lam = run(precision)
+        assert st.rel_residual <= 1e-12
+        assert np.linalg.norm(u - u_ref) <= 1e-8 * np.linalg.norm(u_ref), (precision, st)
+        assert 5 * st.iterations <= st_ref.iterations, (st.iterations, st_ref.iterations)
+        assert all(v > 0 for v in lam)

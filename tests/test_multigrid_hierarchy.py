@@ -1,0 +1,48 @@
+"""The host side of the geometric multigrid (pylith_b200/multigrid.py): level sizes, and the
+prolongation between levels -- trilinear, exact for fields that are linear on each side of the
+fault (with any jump across it), rows summing to one -- and the cell averaging of materials."""
+import numpy as np
+import scipy.sparse as sp
+
+from pylith_b200 import materials as MAT
+from pylith_b200 import multigrid as MG
+
+
+def _side_linear(mesh):
+    X = mesh.coords
+    f = 2.0 * X[:, 0] - 3.0 * X[:, 1] + 0.5 * X[:, 2]
+    plus = np.zeros(mesh.num_nodes, dtype=bool)
+    plus[np.unique(mesh.cells[mesh.coords[mesh.cells].mean(axis=1)[:, 0] > 0])] = True
+    return f + np.where(plus, 1000.0, 0.0)
+
+
+def test_levels_and_prolongation_with_a_fault():
+    levels = MG.build_hierarchy(16, 8, 12, fault_x=0.0, constrained_faces=[(0, "neg", (0,)), (2, "neg", (2,))])
+    assert [lv.n for lv in levels] == [(16, 8, 12), (8, 4, 6), (4, 2, 3)]
+    for (row, col, val), lf, lc in zip(MG.prolongations(levels, 0.0), levels[:-1], levels[1:]):
+        P = sp.csr_matrix((val, col, row), shape=(lf.mesh.num_nodes, lc.mesh.num_nodes))
+        np.testing.assert_allclose(np.asarray(P.sum(axis=1)).ravel(), 1.0)
+        np.testing.assert_allclose(P @ _side_linear(lc.mesh), _side_linear(lf.mesh), rtol=0, atol=1e-9)
+        # constrained faces line up: a coarse constrained DOF's node coincides with a constrained fine one
+        cf = lf.constrained[: 3 * lf.mesh.num_nodes].reshape(-1, 3)
+        cc = lc.constrained[: 3 * lc.mesh.num_nodes].reshape(-1, 3)
+        assert cc.sum() > 0 and cf.sum() > cc.sum()
+
+
+def test_prolongation_without_a_fault_reproduces_linear_fields():
+    levels = MG.build_hierarchy(8, 8, 8)
+    for (row, col, val), lf, lc in zip(MG.prolongations(levels, None), levels[:-1], levels[1:]):
+        P = sp.csr_matrix((val, col, row), shape=(lf.mesh.num_nodes, lc.mesh.num_nodes))
+        lin = lambda m: m.coords @ np.array([1.0, -2.0, 0.25])  # noqa: E731
+        np.testing.assert_allclose(P @ lin(lc.mesh), lin(lf.mesh), rtol=1e-12, atol=1e-9)
+
+
+def test_materials_are_averaged_over_child_cells():
+    levels = MG.build_hierarchy(4, 4, 4)
+    nc0 = levels[0].mesh.num_cells
+    rho, mu, K = MAT.lognormal_elastic(nc0, seed=1)
+    coarse = MG.coarsen_material(MAT.IsotropicLinearElasticity(rho, mu, K), levels[1].cell_parent)
+    assert coarse.shear_modulus.shape == (levels[1].mesh.num_cells,)
+    np.testing.assert_allclose(coarse.shear_modulus.sum() * 8, mu.sum())
+    # every fine cell is the child of exactly one coarse cell
+    assert np.array_equal(np.sort(levels[1].cell_parent.ravel()), np.arange(nc0))
