@@ -353,8 +353,9 @@ int pl_solver_destroy(pl_solver solver);
  *      PETSc GAMG, libsrc/pylith/materials/Elasticity.cc:298-330) ------------------------------ */
 /* A hierarchy of solvers on successively coarser meshes of the same domain (each with its own
  * integrators, constraint mask and faults; all on one context), tied by prolongations from level
- * l + 1 to level l given as host CSR node matrices: prolong_row_ptr[l] has (nodes of level l) + 1
- * entries, prolong_col[l] holds level-(l+1) node indices and prolong_val[l] the weights (applied to
+ * l + 1 to level l given as host CSR node matrices: prolong_row_ptr[l] has (mesh nodes of level l)
+ * + 1 entries, prolong_col[l] holds level-(l+1) mesh-node indices and prolong_val[l] the weights
+ * (Lagrange-multiplier nodes are eliminated by the solvers' reduced space; applied to
  * each of the 3 components; positive-side fault nodes interpolate from their own side).
  * pylith_b200/multigrid.py builds them for structured hexahedral boxes. */
 typedef struct pl_multigrid_s* pl_multigrid;

@@ -213,7 +213,8 @@ using namespace plb;
 
 struct MgLevel {
     pl_solver S = nullptr;
-    int64_t n = 0, nn = 0;
+    int64_t n = 0, nn = 0;  // DOFs and node rows of the solver (mesh nodes, then Lagrange nodes)
+    int64_t nmesh = 0;      // mesh nodes: the rows and columns of the prolongations
     // prolongation from the next coarser level into this one: fine-row CSR and its transpose
     int32_t *p_row = nullptr, *p_col = nullptr, *r_row = nullptr, *r_col = nullptr;
     double *p_val = nullptr, *r_val = nullptr;
@@ -292,7 +293,7 @@ int vcycle(pl_multigrid mg, int l) {
     MgLevel& C = mg->lv[l + 1];
     T* rc_ = f32 ? (T*)C.r32 : (T*)C.r;
     T* zc = f32 ? (T*)C.z32 : (T*)C.z;
-    k_mg_restrict<T><<<mg_grid(3 * C.nn), 256, 0, s>>>(t, L.r_row, L.r_col, L.r_val, C.nn, rc_);
+    k_mg_restrict<T><<<mg_grid(3 * C.nmesh), 256, 0, s>>>(t, L.r_row, L.r_col, L.r_val, C.nmesh, rc_);
     count_launch(2);
     if (f32) solver_fold32(C.S, (float*)rc_);
     else solver_fold(C.S, (double*)rc_);
@@ -301,7 +302,7 @@ int vcycle(pl_multigrid mg, int l) {
     if ((rc = vcycle<T>(mg, l + 1))) return rc;
     if (f32) solver_unfold32(C.S, (float*)zc);
     else solver_unfold(C.S, (double*)zc);
-    k_mg_prolong_add<T><<<mg_grid(3 * L.nn), 256, 0, s>>>(zc, L.p_row, L.p_col, L.p_val, L.S->d_mask, L.nn, z);
+    k_mg_prolong_add<T><<<mg_grid(3 * L.nmesh), 256, 0, s>>>(zc, L.p_row, L.p_col, L.p_val, L.S->d_mask, L.nmesh, z);
     count_launch();
     // post-smoothing on the new residual
     if ((rc = apply(z))) return rc;
@@ -534,6 +535,7 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
         L.S = levels[l];
         L.n = L.S->n;
         L.nn = L.S->nnodes;
+        L.nmesh = L.S->mesh->nnodes;
         A(&L.r, L.n); A(&L.z, L.n); A(&L.t, L.n); A(&L.d, L.n); A(&L.w, L.n); A(&L.q, L.n);
         A(&L.r32, L.n); A(&L.z32, L.n); A(&L.t32, L.n); A(&L.d32, L.n); A(&L.w32, L.n); A(&L.q32, L.n);
         mg->lv.push_back(L);
@@ -542,7 +544,7 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
         MgLevel& F = mg->lv[l];
         const MgLevel& C = mg->lv[l + 1];
         const int32_t* rp = prolong_row_ptr[l];
-        const int64_t nf = F.nn, nc = C.nn;
+        const int64_t nf = F.nmesh, nc = C.nmesh;
         const int64_t nnz = rp[nf];
         std::vector<int32_t> rrow(nc + 1, 0), rcol(nnz);
         std::vector<double> rval(nnz);
