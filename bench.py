@@ -24,6 +24,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -183,6 +184,21 @@ def issue_limiter(mesh, seconds_per_launch, sm_mhz):
             "source": "ncu warp-instruction counts of the same kernel (profiles/tet4_residual_traffic.json)"}
 
 
+def host_cpu():
+    """The host processor's model name and its logical cores (from /proc/cpuinfo)."""
+    model = platform.processor() or "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count() or 1,
+            "affinity_cores": len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else None}
+
+
 def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
     """Oracle cell loop on every host core: residual F(u) plus a second pass of the same loop
     standing in for J v (linear elasticity: F(u) = J u), repeated within a time budget."""
@@ -194,7 +210,7 @@ def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
     aux = O.AuxFields([(mat.density[:, None], "cell"), (mat.shear_modulus[:, None], "cell"),
                        (mat.bulk_modulus[:, None], "cell")])
     u = np.random.default_rng(0).standard_normal(mesh.num_nodes * 3)
-    cores = os.cpu_count() or 1
+    cores = host_cpu()["affinity_cores"] or os.cpu_count() or 1
     f1 = "IsotropicLinearElasticity3D::f1v_infinitesimalStrain"
     O.residual(mesh, u, aux, f1=f1, source=source, nthreads=cores)  # warm-up
     apps = 0
@@ -212,7 +228,7 @@ def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
         apps1 += 1
     dt1 = time.perf_counter() - t1
     return {"value": mesh.num_dof * apps / dt / 1e9, "unit": UNIT, "cores": cores,
-            "one_core_value": mesh.num_dof * apps1 / dt1 / 1e9,
+            "one_core_value": mesh.num_dof * apps1 / dt1 / 1e9, "cpu": host_cpu(),
             "kind": "reference" if source == "ref" else "port",
             "sample": (f"{apps} applications over the full {mesh.num_cells}-cell mesh in {dt:.1f} s; "
                        "oracle cell loop (restated PETSc DMPlexComputeResidual) calling "
@@ -793,7 +809,7 @@ def config_c3(args):
     # rtol 1e-11 for the batched and the FP64 solves: the Delaunay mesh's conditioning turns a 1e-10
     # residual into displacement differences just above 1e-8
     g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
-    usable = [imp for imp in g.impulses if len(patches[imp.patch]) > 0]  # coarse meshes leave some patches empty
+    usable = [imp for imp in g.impulses if len(patches[imp.patch]) > 0]  # every patch holds a node: all of them
     # the autotuner picks the tile size and the preconditioner (point-block Jacobi or Chebyshev-
     # Jacobi of degree 2-3) on a sample of 32 impulses
     step = max(1, len(usable) // 32)
@@ -828,9 +844,12 @@ def config_c3(args):
 
 def config_c4(args):
     """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
-    material, random rectangular left-lateral slip patch of 0.1-3 m. Server (continuous batching in
-    one ragged batch, FP32-refined, HBM-budget admission) vs the FP64 one-at-a-time path. The
-    requests' host-side meshes are built before the stream starts, for both."""
+    material, random rectangular left-lateral slip patch of 0.1-3 m. Server (HBM-budget admission;
+    small boxes in one ragged batch of FP32-refined solves, boxes of 32^3 and more with a multigrid
+    hierarchy solved beside it with FP32 V-cycles) vs the plain FP64 one-at-a-time path (point-block
+    Jacobi), and vs FP64 one at a time with FP64 multigrid. The requests' host-side meshes (and
+    multigrid hierarchies) are built before the stream starts, for all."""
+    from pylith_b200 import feassemble as FA
     from pylith_b200 import serving as SV
 
     count = max(8, int(40 * args.scale))
@@ -838,18 +857,24 @@ def config_c4(args):
     t0 = time.perf_counter()
     hps = [SV.prepare(r) for r in reqs]
     t_host = time.perf_counter() - t0
-    SV.Server(slots=64).run(hps[:2])  # warm-up: device code loading and the first graph capture
+    warm = [SV.prepare(SV.Request(0, n, 1, 0.0, 1.0, (0.2, 0.8, 0.2, 0.8))) for n in (8, 32)]
+    SV.Server(slots=64).run(warm)  # warm-up: device code loading and the first graph captures
     server = SV.Server(slots=64)
     served = server.run(hps)
     seq = SV.serve_sequential(hps)
-    a, b = SV.summarize(served), SV.summarize(seq)
-    mem = np.array([(p, m) for _, p, m in server.memory], dtype=float)
+    seq_mg = SV.serve_sequential(hps, multigrid=FA.Solver.FP64)
+    a, b, c = SV.summarize(served), SV.summarize(seq), SV.summarize(seq_mg)
+    mem = np.array([(p, m) for _, p, m in server.memory], dtype=float) if server.memory else np.zeros((1, 2))
+    routes = list(server.routes.values())
     return {"config": "c4", "requests": count, "server": a, "fp64_one_at_a_time": b,
             "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"],
+            "fp64_multigrid_one_at_a_time": c, "solves_per_s_ratio_vs_fp64_multigrid": a["solves_per_s"] / c["solves_per_s"],
+            "routes": {"ragged_batch": routes.count("batch"), "multigrid": routes.count("multigrid")},
             "host_mesh_build_s_excluded": t_host,
-            "admission_bytes": {"predicted_total": float(mem[:, 0].sum()), "measured_total": float(mem[:, 1].sum()),
-                                "how": "predicted: estimate_bytes(n) formula used for admission; measured: "
-                                       "free device memory before and after each request's build"}}
+            "admission_bytes": {"predicted_total_batch": float(mem[:, 0].sum()), "measured_total_batch": float(mem[:, 1].sum()),
+                                "how": "predicted: estimate_bytes(n) formula used for admission; measured: free device "
+                                       "memory before and after each batched request's build (approximate: the "
+                                       "multigrid worker allocates concurrently)"}}
 
 
 CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c4": config_c4}

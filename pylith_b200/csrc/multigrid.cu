@@ -141,18 +141,27 @@ __global__ void k_mg_power(const double* __restrict__ q, const double* __restric
     block_sum2(ww, 0.0, partials);
 }
 
-__global__ void k_mg_scale_seed(double* __restrict__ v, const uint8_t* __restrict__ mask, int64_t n, double s, int seeded) {
+// a fixed pseudo-random start vector on the free DOFs, and its partial squared norm
+__global__ void __launch_bounds__(kRedThreads) k_mg_seed(double* __restrict__ v, const uint8_t* __restrict__ mask, int64_t n,
+                                                         double* partials) {
+    double vv = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (!seeded) {
-            uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull;
-            h ^= h >> 29;
-            h *= 0xBF58476D1CE4E5B9ull;
-            h ^= h >> 32;
-            v[i] = mask[i] ? 0.0 : (double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5;
-        } else {
-            v[i] = mask[i] ? 0.0 : v[i] * s;
-        }
+        uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 32;
+        const double x = mask[i] ? 0.0 : (double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+        v[i] = x;
+        vv += x * x;
     }
+    block_sum2(vv, 0.0, partials);
+}
+
+// v = w / |w| with |w|^2 in scal[slot] (on the device: no host round trip per power iteration)
+__global__ void k_mg_normalize(double* __restrict__ v, const double* __restrict__ w, int64_t n, const double* scal, int slot) {
+    const double nrm = sqrt(scal[slot]);
+    const double s = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) v[i] = w[i] * s;
 }
 
 // ---- outer flexible PCG (FP64) ----------------------------------------------------------------
@@ -333,40 +342,27 @@ int precondition(pl_multigrid mg, const double* r, double* z) {
     return PL_OK;
 }
 
-// lambda_max(D^{-1} A) of every level by power iteration (FP64), after the levels' setup.
-int estimate_eigenvalues(pl_multigrid mg, int iters = 15) {
+// lambda_max(D^{-1} A) of every level by power iteration (FP64), after the levels' setup: the
+// iterates are normalised on the device and the host reads one number per level.
+int estimate_eigenvalues(pl_multigrid mg, int iters = 12) {
     cudaStream_t s = mg_stream(mg);
     for (MgLevel& L : mg->lv) {
-        k_mg_scale_seed<<<mg_grid(L.n), 256, 0, s>>>(L.t, L.S->d_mask, L.n, 1.0, 0);
-        count_launch();
-        double lam = 0.0, vv = 0.0;
-        {  // |v|
-            k_mg_pq<<<kMgRedBlocks, kRedThreads, 0, s>>>(L.t, L.t, L.S->d_mask, L.n, mg->partials);
-            k_finish2<<<1, 1024, 0, s>>>(mg->partials, kMgRedBlocks, mg->scal, M_RR, -1);
-            count_launch(2);
-            double h[M_COUNT];
-            PLB_CUDA(cudaMemcpyAsync(h, mg->scal, sizeof(h), cudaMemcpyDeviceToHost, s));
-            PLB_CUDA(cudaStreamSynchronize(s));
-            vv = std::sqrt(std::fabs(h[M_RR]));
-        }
+        k_mg_seed<<<kMgRedBlocks, kRedThreads, 0, s>>>(L.t, L.S->d_mask, L.n, mg->partials);
+        k_finish2<<<1, 1024, 0, s>>>(mg->partials, kMgRedBlocks, mg->scal, M_RR, -1);
+        k_mg_normalize<<<mg_grid(L.n), 256, 0, s>>>(L.t, L.t, L.n, mg->scal, M_RR);
+        count_launch(3);
         for (int it = 0; it < iters; ++it) {
             int rc = solver_apply_J(L.S, L.t, L.q);
             if (rc) return rc;
             k_mg_power<<<kMgRedBlocks, kRedThreads, 0, s>>>(L.q, L.S->d_pinv, L.S->d_mask, L.nn, L.w, mg->partials);
             k_finish2<<<1, 1024, 0, s>>>(mg->partials, kMgRedBlocks, mg->scal, M_RR, -1);
-            count_launch(2);
-            double h[M_COUNT];
-            PLB_CUDA(cudaMemcpyAsync(h, mg->scal, sizeof(h), cudaMemcpyDeviceToHost, s));
-            PLB_CUDA(cudaStreamSynchronize(s));
-            const double ww = std::sqrt(h[M_RR]);
-            lam = vv > 0.0 ? ww / vv : 0.0;
-            if (!(ww > 0.0)) break;
-            // v = w / |w|
-            PLB_CUDA(cudaMemcpyAsync(L.t, L.w, L.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-            k_mg_scale_seed<<<mg_grid(L.n), 256, 0, s>>>(L.t, L.S->d_mask, L.n, 1.0 / ww, 1);
-            count_launch();
-            vv = 1.0;
+            k_mg_normalize<<<mg_grid(L.n), 256, 0, s>>>(L.t, L.w, L.n, mg->scal, M_RR);
+            count_launch(3);
         }
+        double h[M_COUNT];
+        PLB_CUDA(cudaMemcpyAsync(h, mg->scal, sizeof(h), cudaMemcpyDeviceToHost, s));
+        PLB_CUDA(cudaStreamSynchronize(s));
+        const double lam = std::sqrt(h[M_RR]);  // |D^-1 A v| for the unit iterate v
         if (!(lam > 0.0) || !std::isfinite(lam)) return fail(PL_ERR_NOT_CONVERGED, "multigrid: no eigenvalue estimate");
         L.lmax = lam;
     }

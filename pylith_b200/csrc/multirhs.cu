@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -100,6 +101,43 @@ PL_D void red_vec(float* p, const float (&v)[W]) {
         red_add(p, v[0]);
 }
 
+// Warp sums of the KC per-lane values e[] of right-hand-side chunk ci (right-hand sides
+// ci * KC .. ci * KC + KC - 1), accumulated into one FP64 value per lane: for KC = 4 lane l
+// accumulates right-hand side (l & 7) * 4 + (l >> 3) (a reduce-scatter in 6 shuffles: halves
+// exchanged across lane bit 4, then bit 3, then a butterfly over bits 2..0); for KC < 4 lane l
+// accumulates right-hand side l. Every lane of the warp must take part.
+template <int KC>
+PL_D void warp_chunk_sum(const float (&e)[KC], int ci, double& acc) {
+    const int lane = threadIdx.x & 31;
+    if constexpr (KC == 4) {
+        const bool hi = lane & 16;
+        const float a0 = (hi ? e[2] : e[0]) + __shfl_xor_sync(0xffffffffu, hi ? e[0] : e[2], 16);
+        const float a1 = (hi ? e[3] : e[1]) + __shfl_xor_sync(0xffffffffu, hi ? e[1] : e[3], 16);
+        const bool b3 = lane & 8;
+        float c = (b3 ? a1 : a0) + __shfl_xor_sync(0xffffffffu, b3 ? a0 : a1, 8);
+        c += __shfl_xor_sync(0xffffffffu, c, 4);
+        c += __shfl_xor_sync(0xffffffffu, c, 2);
+        c += __shfl_xor_sync(0xffffffffu, c, 1);
+        if ((lane & 7) == ci) acc += c;
+    } else {
+#pragma unroll
+        for (int rr = 0; rr < KC; ++rr) {
+            float c = e[rr];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == ci * KC + rr) acc += c;
+        }
+    }
+}
+
+// The right-hand side whose sum lane l holds after warp_chunk_sum (-1: none).
+template <int K>
+PL_D int warp_chunk_rhs(int lane) {
+    constexpr int KC = MultiChunk<K>::value;
+    if constexpr (KC == 4) return (lane & 7) < K / KC ? (lane & 7) * KC + (lane >> 3) : -1;
+    else return lane < K ? lane : -1;
+}
+
 // v, out: [ndof][K] FP32 (ndof = 3 * nodes, node-major); out must be zeroed or hold the sum to add to.
 // Per cell block: the block's node coordinates (FP64, [3][ld]) and K field vectors (FP32, one row
 // of 3K values per node as in global memory, padded to MultiRow<K>) are staged in shared memory with the block's node ids
@@ -109,6 +147,61 @@ PL_D void red_vec(float* p, const float (&v)[W]) {
 // work item per (node, component) sums its incident corners over the block-local incidence list
 // in a fixed order, KC right-hand sides per vector, and adds the node into the output (one vector
 // reduction when the node is shared with other blocks).
+
+constexpr int kBThreads = 256;
+constexpr int kBBlocks = 1184;
+constexpr int kMaxTile = 16;  // right-hand sides per tile: 1, 2, 4, 8 or 16
+
+// Final sums fused into the kernel that produced the per-block partials: the last block to finish
+// (a ticket counter; the partials are fenced before the ticket is taken) sums partials[blk][K] in
+// block order, like k_b_finish, into out[k] (copying the old out[k] to prev[k] first when prev is
+// set). FinSpec::counter null: no fused sum (the caller launches k_b_finish).
+struct FinSpec {
+    unsigned int* counter = nullptr;
+    double* out_a = nullptr;   // sums of the first partial array
+    double* prev_a = nullptr;
+    double* out_b = nullptr;   // sums of the second partial array (kernels with two)
+};
+
+PL_D bool take_last_ticket(unsigned int* counter) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+        if (last) *counter = 0u;  // every other block has taken its ticket
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// sh: kBThreads / 32 * K doubles of shared memory.
+template <int K>
+PL_D void sum_partials_last_block_in(const double* partials, double* out, double* prev, double (*sh)[K]) {
+    const int k = threadIdx.x % K;
+    double s = 0.0;
+    for (int b = threadIdx.x / K; b < (int)gridDim.x; b += kBThreads / K) s += __ldcg(&partials[b * K + k]);
+#pragma unroll
+    for (int o = K; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l < K) sh[w][l] = s;
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < kBThreads / 32; ++i) t += sh[i][threadIdx.x];
+        if (prev) prev[threadIdx.x] = out[threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+template <int K>
+PL_D void sum_partials_last_block(const double* partials, double* out, double* prev) {
+    __shared__ double sh[kBThreads / 32][K];
+    sum_partials_last_block_in<K>(partials, out, prev, sh);
+}
 
 // Block metadata in shared memory (two buffers: the gather reads one while the next block's is
 // copied into the other): node ids [ld], incidence offsets [ld + 1], incidence list
@@ -140,16 +233,21 @@ PL_D MultiMeta multi_meta(char* base, int ld) {
 template <int K>
 PL_D void prefetch_multi(const DomainParams& p, const int32_t* __restrict__ slot_begin,
                          const uint32_t* __restrict__ slot_node, const uint32_t* __restrict__ inc_off,
-                         const uint16_t* __restrict__ inc, int64_t b, int ld, const float* __restrict__ v,
+                         const uint16_t* __restrict__ inc, const int32_t* __restrict__ pbeg,
+                         const double* __restrict__ pcoords, int64_t b, int ld, const float* __restrict__ v,
                          float* sV, double* sX, const MultiMeta& mm) {
     constexpr int CB = K % 4 == 0 ? 16 : (K % 2 == 0 ? 8 : 4);  // bytes per copy; rows are 12 K bytes
     const int s0 = slot_begin[b];
     const int ns = slot_begin[b + 1] - s0;
+    // coordinates: the block's [3][slots rounded up to 4] run of the padded layout, 16 bytes a copy
+    const int p0 = pbeg[b], np = pbeg[b + 1] - p0, half = np >> 1;
+    for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
+        const int d = t / half, j = t - d * half;
+        __pipeline_memcpy_async(&sX[d * ld + 2 * j], &pcoords[3 * (int64_t)p0 + (int64_t)d * np + 2 * j], 16);
+    }
     for (int i = threadIdx.x; i < ns; i += blockDim.x) {
         const uint32_t id = slot_node[s0 + i];
         const int64_t nd = id & ~kSharedBitM;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) __pipeline_memcpy_async(&sX[d * ld + i], &p.coords[3 * nd + d], sizeof(double));
         const float* vr = v + 3 * K * nd;
         float* sr = sV + MultiRow<K>::value * i;
 #pragma unroll
@@ -165,11 +263,29 @@ PL_D void prefetch_multi(const DomainParams& p, const int32_t* __restrict__ slot
 
 // store_owned: nodes owned by one block are stored (the output was zeroed and this is the first
 // integrator); otherwise they are added.
+// pq_part (optional, with fin.counter and pq_rz): the energies v.(A v) = -v.(J v) of the K
+// vectors, summed from the cells: a cell's share of v.(J v) is its element vector dotted with its
+// corner values, vol f1(grad v) : grad v = -vol (lambda tr(e)^2 + 2 mu e:e) with e = sym grad v, so
+// the sum over cells equals the sum over DOFs of v_i (J v)_i (the fault's fold adds each
+// positive-side row to its negative-side partner, whose value v carries, and constrained DOFs hold
+// v = 0). FP32 squares of small gradients would underflow (a residual of 1e-11 of a unit
+// right-hand side gives gradients near 1e-28), so each vector's gradient is scaled by
+// s_k = 1 / sqrt(pq_rz[k]) (its current r.z, of the order of its energy) before the products and
+// the FP64 sums are divided by s_k^2. Per-CTA FP64 partials [grid][K]; the last CTA forms the sums
+// in CTA order into fin.out_a.
 template <int K>
-__global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
+__global__ void __launch_bounds__(kMultiBlockCells, 3) k_tet_blocked_jv32_multi(
     DomainParams p, const int32_t* __restrict__ slot_begin, const uint32_t* __restrict__ slot_node,
     const ushort4* __restrict__ lconn, const uint32_t* __restrict__ inc_off, const uint16_t* __restrict__ inc,
-    int64_t nblocks, int ld, const float* __restrict__ v, float* out, bool store_owned) {
+    const int32_t* __restrict__ pbeg, const double* __restrict__ pcoords, int64_t nblocks, int ld,
+    const float* __restrict__ v, float* out, bool store_owned, double* pq_part, const double* __restrict__ pq_rz,
+    FinSpec fin) {
+    static_assert(kMultiBlockCells == kBThreads, "the fused sums assume kBThreads threads per CTA");
+    __shared__ float s_sig[K];  // energy scales (pq_part)
+    if (pq_part && threadIdx.x < K) {
+        const double rz = pq_rz[threadIdx.x];
+        s_sig[threadIdx.x] = (rz > 0.0 && rz < 1e300) ? (float)fmin(fmax(1.0 / sqrt(rz), 1e-30), 1e30) : 1.0f;
+    }
     constexpr int KC = MultiChunk<K>::value;
     using L = AuxLayout<RHEO_ILE, false>;
     extern __shared__ __align__(16) char smem_raw[];
@@ -184,15 +300,17 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
     const size_t mb = multi_meta_bytes(ld);
     int cur = 0;
     const int tc = threadIdx.x;
+    double pq_acc = 0.0;  // this lane's energy sum (warp_chunk_sum)
     if (blockIdx.x < nblocks)
-        prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, blockIdx.x, ld, v, sV, sX, multi_meta(metabase, ld));
+        prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, pbeg, pcoords, blockIdx.x, ld, v, sV, sX,
+                          multi_meta(metabase, ld));
     __pipeline_commit();
     for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int ns = slot_begin[b + 1] - slot_begin[b];
         const int64_t c = b * kMultiBlockCells + tc;
         const bool live = c < p.ncells;
         int ln[4] = {0, 0, 0, 0};
-        float inv[3][3], cf[3][3], lam = 0.f, mu = 0.f;
+        float inv[3][3], cf[3][3], lam = 0.f, mu = 0.f, vol = 0.f;
         // per-cell inputs from global memory first: their latency overlaps the staging copies
         if (live) {
             const ushort4 lc = lconn[c];
@@ -226,6 +344,7 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
             const double det = tet_cof_m(X, cof);
             if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
             const double rdet = 1.0 / det;
+            vol = (float)(det * (1.0 / 6.0));
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -236,6 +355,9 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
         }
 #pragma unroll 1
         for (int r0 = 0; r0 < K; r0 += KC) {
+            float en[KC];
+#pragma unroll
+            for (int rr = 0; rr < KC; ++rr) en[rr] = 0.f;
             if (live) {
                 // gradient of the KC fields: G[cc][k] = v_{k+1} - v_0 per component, then s_x = G inv
                 float s_x[KC][3][3];
@@ -253,13 +375,26 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                         for (int d = 0; d < 3; ++d) s_x[rr][cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
                     }
                 }
-                // flux f1 = -(lambda tr(e) I + 2 mu e), in place of s_x
+                // flux f1 = -(lambda tr(e) I + 2 mu e), in place of s_x (and, for pq_part, the
+                // energy vol (lambda tr(e)^2 + 2 mu e:e) first)
 #pragma unroll
                 for (int rr = 0; rr < KC; ++rr) {
-                    const float ltr = lam * (s_x[rr][0][0] + s_x[rr][1][1] + s_x[rr][2][2]);
-                    const float xy = -mu * (s_x[rr][0][1] + s_x[rr][1][0]);
-                    const float yz = -mu * (s_x[rr][1][2] + s_x[rr][2][1]);
-                    const float xz = -mu * (s_x[rr][0][2] + s_x[rr][2][0]);
+                    const float tr = s_x[rr][0][0] + s_x[rr][1][1] + s_x[rr][2][2];
+                    const float ltr = lam * tr;
+                    const float sxy = s_x[rr][0][1] + s_x[rr][1][0];
+                    const float syz = s_x[rr][1][2] + s_x[rr][2][1];
+                    const float sxz = s_x[rr][0][2] + s_x[rr][2][0];
+                    const float xy = -mu * sxy;
+                    const float yz = -mu * syz;
+                    const float xz = -mu * sxz;
+                    if (pq_part) {
+                        // scaled gradient; every product pairs a modulus-weighted factor with a bare one
+                        const float g = s_sig[r0 + rr];
+                        const float t = g * tr, a = g * s_x[rr][0][0], b = g * s_x[rr][1][1], c = g * s_x[rr][2][2];
+                        const float u = g * sxy, w = g * syz, z = g * sxz;
+                        en[rr] = vol * ((lam * t) * t + (2.0f * mu * a) * a + (2.0f * mu * b) * b +
+                                        (2.0f * mu * c) * c + (mu * u) * u + (mu * w) * w + (mu * z) * z);
+                    }
                     s_x[rr][0][0] = -(2.0f * mu * s_x[rr][0][0] + ltr);
                     s_x[rr][1][1] = -(2.0f * mu * s_x[rr][1][1] + ltr);
                     s_x[rr][2][2] = -(2.0f * mu * s_x[rr][2][2] + ltr);
@@ -285,10 +420,11 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
                     st_vec<KC>(sE + ((cc)*kMultiBlockCells + tc) * KC, e0);
                 }
             }
+            if (pq_part) warp_chunk_sum<KC>(en, r0 / KC, pq_acc);
             __syncthreads();
             // the node rows are no longer read in this block: copy the next block's while gathering
             if (r0 + KC >= K && b + gridDim.x < nblocks)
-                prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, b + gridDim.x, ld, v, sV, sX,
+                prefetch_multi<K>(p, slot_begin, slot_node, inc_off, inc, pbeg, pcoords, b + gridDim.x, ld, v, sV, sX,
                                   multi_meta(metabase + (cur ^ 1) * mb, ld));
             __pipeline_commit();
             // one work item per (node, component): a warp takes one component of 32 consecutive
@@ -329,6 +465,25 @@ __global__ void __launch_bounds__(kMultiBlockCells) k_tet_blocked_jv32_multi(
         cur ^= 1;
     }
     __pipeline_wait_prior(0);
+    if (pq_part) {
+        // the element-vector staging area is free after the loop's last barrier
+        double* sh = reinterpret_cast<double*>(smem_raw);  // [warps][K]
+        const int lane = tc & 31, wq = tc >> 5;
+        const int rhs = warp_chunk_rhs<K>(lane);
+        if (rhs >= 0) {
+            const double g = s_sig[rhs];
+            sh[wq * K + rhs] = pq_acc / (g * g);
+        }
+        __syncthreads();
+        if (tc < K) {
+            double t = 0.0;
+            for (int i = 0; i < kMultiBlockCells / 32; ++i) t += sh[i * K + tc];
+            pq_part[blockIdx.x * K + tc] = t;
+        }
+        if (fin.counter && take_last_ticket(fin.counter))
+            sum_partials_last_block_in<K>(pq_part, fin.out_a, fin.prev_a,
+                                          reinterpret_cast<double (*)[K]>(sh + kMultiBlockCells / 32 * K));
+    }
 }
 
 template <int K>
@@ -341,9 +496,6 @@ size_t multi_smem(int ld) {
 // ---- batched vector kernels, layout [n][K] -------------------------------------------------
 // Element e of an [n][K] array is DOF e / K of right-hand side e % K; every kernel below maps
 // consecutive threads to consecutive elements (thread index % K == right-hand side).
-constexpr int kBThreads = 256;
-constexpr int kBBlocks = 1184;
-constexpr int kMaxTile = 16;  // right-hand sides per tile: 1, 2, 4, 8 or 16
 
 // Per-block sums of one value per thread, by right-hand side (thread index % K), in a fixed
 // order -> partials[blk][K].
@@ -406,51 +558,6 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish(const double* __restrict
     }
 }
 
-// Final sums fused into the kernel that produced the per-block partials: the last block to finish
-// (a ticket counter; the partials are fenced before the ticket is taken) sums partials[blk][K] in
-// block order, like k_b_finish, into out[k] (copying the old out[k] to prev[k] first when prev is
-// set). FinSpec::counter null: no fused sum (the caller launches k_b_finish).
-struct FinSpec {
-    unsigned int* counter = nullptr;
-    double* out_a = nullptr;   // sums of the first partial array
-    double* prev_a = nullptr;
-    double* out_b = nullptr;   // sums of the second partial array (kernels with two)
-};
-
-PL_D bool take_last_ticket(unsigned int* counter) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        last = atomicAdd(counter, 1u) == gridDim.x - 1;
-        if (last) *counter = 0u;  // every other block has taken its ticket
-    }
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
-}
-
-template <int K>
-PL_D void sum_partials_last_block(const double* partials, double* out, double* prev) {
-    __shared__ double sh[kBThreads / 32][K];
-    const int k = threadIdx.x % K;
-    double s = 0.0;
-    for (int b = threadIdx.x / K; b < (int)gridDim.x; b += kBThreads / K) s += __ldcg(&partials[b * K + k]);
-#pragma unroll
-    for (int o = K; o < 32; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l < K) sh[w][l] = s;
-    __syncthreads();
-    if (threadIdx.x < K) {
-        double t = 0.0;
-#pragma unroll
-        for (int i = 0; i < kBThreads / 32; ++i) t += sh[i][threadIdx.x];
-        if (prev) prev[threadIdx.x] = out[threadIdx.x];
-        out[threadIdx.x] = t;
-    }
-    __syncthreads();
-}
-
 template <int K>
 PL_D void pinv_apply(const float* __restrict__ P, const float* r, int64_t node, int k, float z[3]) {
     const float* B = P + 9 * node;
@@ -499,9 +606,9 @@ __global__ void __launch_bounds__(kBThreads) k_b_pq(const float* p, const float*
     if (fin.counter && take_last_ticket(fin.counter)) sum_partials_last_block<K>(part, fin.out_a, fin.prev_a);
 }
 
-// alpha_k = active_k ? rz_k / pq_k : 0; r += alpha q; z = P r; partial rz, rr (x is updated by k_b_pupdate).
-// One thread per (node, rhs).
-template <int K>
+// alpha_k = active_k ? rz_k / pq_k : 0; r += alpha q; z = P r (stored when StoreZ); partial rz, rr
+// (x is updated by k_b_pupdate). One thread per (node, rhs).
+template <int K, bool StoreZ = true>
 __global__ void __launch_bounds__(kBThreads) k_b_update(float* r, const float* q, float* z,
                                                         const uint8_t* mask, const float* P, int64_t nnodes,
                                                         const double* rz, const double* pq, const int* active,
@@ -523,7 +630,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_update(float* r, const float* q
         for (int c = 0; c < 3; ++c) {
             const int64_t i = (3 * nd + c) * K + k;
             const float ri = r[i];
-            z[i] = zz[c];
+            if (StoreZ) z[i] = zz[c];
             srz += (double)ri * zz[c];
             srr += (double)ri * ri;
         }
@@ -550,6 +657,30 @@ __global__ void k_b_pupdate(float* x, float* p, const float* z, const uint8_t* m
         const float pe = p[e];
         if (!mask[e / K]) x[e] += alpha * pe;
         p[e] = z[e] + beta * pe;
+    }
+}
+
+// k_b_pupdate for the point-block Jacobi preconditioner, forming z = P r from r (one thread per
+// (node, rhs)) instead of reading a stored z.
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_b_pupdate_jacobi(float* x, float* p, const float* r,
+                                                                const uint8_t* mask, const float* P, int64_t nnodes,
+                                                                const double* rz, const double* rz_old,
+                                                                const double* pq, const int* active) {
+    const int k = threadIdx.x % K;  // blockDim and the grid stride are multiples of K
+    const float alpha = active[k] ? safe_step_f32(rz_old[k], pq[k]) : 0.0f;
+    const float beta = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        float zz[3];
+        pinv_apply<K>(P, r, nd, k, zz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const float pe = p[i];
+            if (!mask[3 * nd + c]) x[i] += alpha * pe;
+            p[i] = zz[c] + beta * pe;
+        }
     }
 }
 
@@ -803,11 +934,23 @@ constexpr int kMaxChebDegree = 8;
 
 namespace {
 
+// Whether a PCG iteration sums p.(A p) inside the operator launch (single-integrator operators;
+// PYLITH_B200_BATCH_FUSED_PQ=0 selects the separate reduction kernel instead).
+// Read when an iteration is recorded (graph capture), not per replay.
+bool fuses_energies(pl_batch_solver B) {
+    const char* e = std::getenv("PYLITH_B200_BATCH_FUSED_PQ");
+    return !(e && e[0] == '0') && B->base->ops.size() == 1;
+}
+
+// out = J v for the tile's K vectors; with pq (single-integrator operators only, see
+// fuses_energies), the energies v.(A v) are summed by the same launch into pq[K] (scaled by the
+// tile's current r.z, B->scal[0..K)).
 template <int K>
-int jv32_multi(pl_batch_solver B, const float* v, float* out) {
+int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullptr) {
     pl_solver S = B->base;
     pl_mesh m = S->mesh;
     cudaStream_t s = m->ctx->stream;
+    if (pq && S->ops.size() != 1) return fail(PL_ERR_UNSUPPORTED, "fused energies need a single integrator");
     if (S->npairs > 0) {
         k_b_unfold<K><<<bgrid(3 * K * S->npairs), 256, 0, s>>>(const_cast<float*>(v), S->d_pair_neg, S->d_pair_pos, S->npairs);
         count_launch();
@@ -828,18 +971,27 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out) {
         if (L.num_blocks == 0) return fail(PL_ERR_UNSUPPORTED, "no cell-block layout for this mesh");
         if (L.max_local_nodes > 2 * kMultiBlockCells)
             return fail(PL_ERR_UNSUPPORTED, "cell blocks too large for the batched kernel");
-        const size_t smem = multi_smem<K>(L.max_local_nodes);
+        const int ld = (L.max_local_nodes + 3) & ~3;  // 16-byte rows for the coordinate runs
+        const size_t smem = multi_smem<K>(ld);
         if (smem > 200 * 1024) return fail(PL_ERR_UNSUPPORTED, "cell blocks too large for the batched kernel");
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(k_tet_blocked_jv32_multi<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int dev = 0, nsm = 148, per_sm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tet_blocked_jv32_multi<K>, kMultiBlockCells, smem);
-        const int grid = (int)std::min<int64_t>(L.num_blocks, (int64_t)nsm * std::max(per_sm, 1));
+        ensure_kernel_smem((const void*)k_tet_blocked_jv32_multi<K>, smem);
+        static int per_sm = 0;  // occupancy of this instantiation for its shared memory
+        static size_t per_sm_smem = 0;
+        if (per_sm_smem != smem) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tet_blocked_jv32_multi<K>, kMultiBlockCells, smem);
+            per_sm = std::max(per_sm, 1);
+            per_sm_smem = smem;
+        }
+        const int grid = (int)std::min<int64_t>(L.num_blocks, (int64_t)sm_count() * per_sm);
+        FinSpec fin;
+        if (pq) {
+            fin.counter = B->ticket;
+            fin.out_a = pq;
+        }
         k_tet_blocked_jv32_multi<K><<<grid, kMultiBlockCells, smem, s>>>(
             pp, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
-            L.num_blocks, L.max_local_nodes, v, out, first);
+            L.d_pipe_begin, L.d_pipe_coords, L.num_blocks, ld, v, out, first, pq ? B->part_a : nullptr, B->scal,
+            fin);
         first = false;
         count_launch();
     }
@@ -884,13 +1036,17 @@ int pcg_iteration(pl_batch_solver B) {
     double* rz_old = B->scal + K;
     double* pq = B->scal + 2 * K;
     double* rr = B->scal + 3 * K;
-    int rc = jv32_multi<K>(B, B->p, B->q);
-    if (rc) return rc;
     // the final sums are formed by the last block of each reduction kernel (no k_b_finish launches)
-    FinSpec fpq;
-    fpq.counter = B->ticket;
-    fpq.out_a = pq;
-    k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a, fpq);
+    const bool fused = fuses_energies(B);
+    int rc = jv32_multi<K>(B, B->p, B->q, fused ? pq : nullptr);
+    if (rc) return rc;
+    if (!fused) {
+        FinSpec fpq;
+        fpq.counter = B->ticket;
+        fpq.out_a = pq;
+        k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a, fpq);
+        count_launch();
+    }
     if (B->cheb_degree >= 2) {
         FinSpec frr;
         frr.counter = B->ticket;
@@ -910,12 +1066,17 @@ int pcg_iteration(pl_batch_solver B) {
         fu.out_a = rz;
         fu.prev_a = rz_old;
         fu.out_b = rr;
-        k_b_update<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->q, B->z, S->d_mask, S->d_pinv32, B->nnodes, rz, pq,
-                                                     B->active, B->part_a, B->part_b, fu);
+        // z = P r is not stored: k_b_pupdate_jacobi forms it again from r
+        k_b_update<K, false><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->q, nullptr, S->d_mask, S->d_pinv32, B->nnodes, rz,
+                                                            pq, B->active, B->part_a, B->part_b, fu);
         count_launch();
+        k_b_pupdate_jacobi<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->p, B->r, S->d_mask, S->d_pinv32, B->nnodes, rz,
+                                                             rz_old, pq, B->active);
+        count_launch();
+        return PL_OK;
     }
     k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->p, B->z, S->d_mask, B->n, rz, rz_old, pq, B->active);
-    count_launch(2);
+    count_launch();
     return PL_OK;
 }
 

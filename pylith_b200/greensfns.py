@@ -23,7 +23,9 @@ COMPONENTS = {"opening": 0, "left_lateral": 1, "reverse": 2}
 
 
 def fault_patches(mesh, y_range, z_range, ny: int, nz: int):
-    """Fault-node index lists of an ny x nz grid of rectangular patches on the fault plane."""
+    """Fault-node index lists of an ny x nz grid of rectangular patches on the fault plane. A patch
+    that holds no fault node (an unstructured fault mesh coarser than the patch grid) takes the
+    fault node nearest its centre, so every patch carries an impulse."""
     lag_nodes = np.zeros(mesh.num_lagrange, dtype=np.int64)
     coh = mesh.cohesive
     lag_nodes[coh[:, 8:].ravel()] = coh[:, :4].ravel()  # negative-side node of each fault node
@@ -34,7 +36,12 @@ def fault_patches(mesh, y_range, z_range, ny: int, nz: int):
     patches = []
     for kz in range(nz):
         for ky in range(ny):
-            patches.append(np.nonzero(inside & (iy == ky) & (iz == kz))[0])
+            nodes = np.nonzero(inside & (iy == ky) & (iz == kz))[0]
+            if len(nodes) == 0 and len(yz):
+                cy = y_range[0] + (ky + 0.5) * (y_range[1] - y_range[0]) / ny
+                cz = z_range[0] + (kz + 0.5) * (z_range[1] - z_range[0]) / nz
+                nodes = np.array([int(np.argmin((yz[:, 0] - cy) ** 2 + (yz[:, 1] - cz) ** 2))])
+            patches.append(nodes)
     return patches
 
 

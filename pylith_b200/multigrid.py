@@ -5,10 +5,11 @@ x = x0 of cohesive cells), for the multigrid-preconditioned conjugate gradients 
 The reference preconditions its elasticity solves with algebraic multigrid (PETSc GAMG, fine-level
 smoother point-block Jacobi with faults; libsrc/pylith/materials/Elasticity.cc:298-330). The boxes
 of the configurations this build runs are structured, so the hierarchy here is geometric: every
-level is the same box with half the cells per direction (while the counts stay even), re-discretised
-with the registered pointwise kernels on cell-averaged aux fields; the levels are tied by trilinear
-prolongation, each side of the fault interpolating from its own side, and restriction is its
-transpose. In the solver's reduced space (positive-side fault DOFs follow the negative side), the
+level is the same box with about half the cells per direction (exactly half while that keeps the
+fault plane a grid plane; otherwise the nearest count that does, so the grids need not be nested),
+re-discretised with the registered pointwise kernels on cell-averaged aux fields; the levels are
+tied by trilinear interpolation (the prolongation), each side of the fault interpolating from its
+own side, and restriction is its transpose. In the solver's reduced space (positive-side fault DOFs follow the negative side), the
 device code unfolds the coarse vector before prolongation and folds the restricted one, so the
 reduced restriction is the transpose of the reduced prolongation and the V-cycle is symmetric.
 """
@@ -26,8 +27,9 @@ from . import meshing as M
 class Level:
     n: tuple                 # cells per direction
     mesh: M.Mesh
-    cell_parent: Optional[np.ndarray]  # for coarse levels: [8, ncells] fine cells of each coarse cell
+    cell_map: Optional[np.ndarray]  # for coarse levels: this level's cell holding each cell of the finer level
     constrained: np.ndarray  # bool [num_dof]
+    prolong: Optional[tuple] = None  # CSR (row_ptr, col, val) from the next coarser level to this one
 
 
 def _node_maps(nx, ny, nz, fault_i):
@@ -46,113 +48,160 @@ def _node_maps(nx, ny, nz, fault_i):
     return neg, pos
 
 
-def _weights_1d(nf):
-    """Fine index i = 0 .. nf -> two (coarse index, weight) pairs of 1-D linear interpolation
-    (nf even): (i/2, 1) and (i/2, 0) for even i, (i//2, 1/2) and (i//2 + 1, 1/2) for odd i."""
-    i = np.arange(nf + 1)
-    c0 = i // 2
-    odd = (i % 2).astype(bool)
-    return c0, np.where(odd, 0.5, 1.0), np.where(odd, c0 + 1, c0), np.where(odd, 0.5, 0.0)
+def _weights_1d(nf, nc):
+    """Fine index i = 0 .. nf of a uniform grid of nf cells -> two (coarse index, weight) pairs of
+    1-D linear interpolation from the grid of nc <= nf cells over the same interval: with
+    s = i nc / nf (exact integer arithmetic), (floor s, 1 - frac s) and (floor s + 1, frac s),
+    floor s capped at nc - 1."""
+    i = np.arange(nf + 1, dtype=np.int64)
+    c0 = np.minimum((i * nc) // nf, nc - 1)
+    w1 = (i * nc - c0 * nf) / nf
+    return c0, 1.0 - w1, c0 + 1, w1
 
 
 def prolongation(nf, fault_i_f, nc, fault_i_c, num_nodes_f, num_nodes_c):
-    """CSR (row_ptr, col, val) of the node prolongation from a coarse box (nc) to the fine box
-    nf = 2 nc: trilinear weights, fine nodes of the +x side (x > x0, and the plane's positive
-    copies) interpolating from the coarse +x side."""
+    """CSR (row_ptr, col, val) of the node prolongation from a coarse box (nc cells per direction)
+    to a fine box of the same extent (nf >= nc; nested or not): trilinear interpolation weights, fine nodes of the +x side (x > x0, and the plane's positive
+    copies) interpolating from the coarse +x side. Every fine node is one (side, lattice point)
+    pair, so the rows are laid out by scattering those pairs to their node ids; within a row the
+    entries are in increasing column order, zero weights left out."""
     negf, posf = _node_maps(*nf, fault_i_f)
     negc, posc = _node_maps(*nc, fault_i_c)
-    w = [_weights_1d(n) for n in nf]
+    w = [_weights_1d(a, b) for a, b in zip(nf, nc)]
     I, J, K = np.meshgrid(np.arange(nf[0] + 1), np.arange(nf[1] + 1), np.arange(nf[2] + 1), indexing="ij")
     I, J, K = I.ravel(), J.ravel(), K.ravel()
-    rows, cols, vals = [], [], []
-    sides = [("neg", negf, negc, I <= (fault_i_f if fault_i_f is not None else nf[0]))]
+    sides = [(negf, negc, I <= (fault_i_f if fault_i_f is not None else nf[0]))]
     if fault_i_f is not None:
-        sides.append(("pos", posf, posc, I >= fault_i_f))
-    for _, fmap, cmap, sel in sides:
+        sides.append((posf, posc, I >= fault_i_f))
+    cols = np.empty((num_nodes_f, 8), dtype=np.int64)
+    vals = np.empty((num_nodes_f, 8), dtype=np.float64)
+    seen = np.zeros(num_nodes_f, dtype=np.int32)
+    sc = (nc[1] + 1) * (nc[2] + 1), nc[2] + 1  # strides of a C-ordered (i, j, k) coarse lattice
+    for fmap, cmap, sel in sides:
         i, j, k = I[sel], J[sel], K[sel]
-        f = fmap[i, j, k]
+        f = fmap.ravel()[(i * (nf[1] + 1) + j) * (nf[2] + 1) + k]
+        cflat = cmap.ravel()
+        seen[f] += 1
+        C = np.empty((8, len(f)), dtype=np.int64)
+        W = np.empty((8, len(f)), dtype=np.float64)
+        e = 0
         for a in (0, 1):
             ci, wa = w[0][2 * a][i], w[0][2 * a + 1][i]
             for b in (0, 1):
                 cj, wb = w[1][2 * b][j], w[1][2 * b + 1][j]
                 for c in (0, 1):
                     ck, wc = w[2][2 * c][k], w[2][2 * c + 1][k]
-                    wt = wa * wb * wc
-                    keep = wt != 0.0
-                    rows.append(f[keep])
-                    cols.append(cmap[ci[keep], cj[keep], ck[keep]])
-                    vals.append(wt[keep])
-    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
-    order = np.lexsort((cols, rows))
-    rows, cols, vals = rows[order], cols[order], vals[order]
-    row_ptr = np.zeros(num_nodes_f + 1, dtype=np.int32)
-    np.add.at(row_ptr, rows + 1, 1)
-    return np.cumsum(row_ptr).astype(np.int32), cols.astype(np.int32), vals.astype(np.float64)
+                    C[e] = cflat[ci * sc[0] + cj * sc[1] + ck]
+                    W[e] = wa * wb * wc
+                    e += 1
+        cols[f] = C.T
+        vals[f] = W.T
+    if not np.all(seen == 1):
+        raise ValueError("prolongation: fine node ids do not match one (side, lattice point) each")
+    keep = vals != 0.0
+    order = np.argsort(np.where(keep, cols, np.iinfo(np.int64).max), axis=1, kind="stable")
+    cols = np.take_along_axis(cols, order, axis=1)
+    vals = np.take_along_axis(vals, order, axis=1)
+    keep = np.take_along_axis(keep, order, axis=1)
+    row_ptr = np.zeros(num_nodes_f + 1, dtype=np.int64)
+    np.cumsum(keep.sum(axis=1), out=row_ptr[1:])
+    return row_ptr.astype(np.int32), cols[keep].astype(np.int32), vals[keep]
+
+
+def _coarse_count(v: int, fault_i: Optional[int]) -> Optional[int]:
+    """Cells of the next coarser grid along an axis of v cells: v / 2 when v is even (and the fault
+    plane, at lattice index fault_i, stays a grid plane), else the count nearest v / 2 that keeps it
+    one; None when there is none."""
+    if fault_i is None:
+        return v // 2 if v % 2 == 0 else (v + 1) // 2
+    for m in sorted(range(max(1, v // 2 - 2), v // 2 + 3), key=lambda m: (abs(2 * m - v), m)):
+        if m < v and (fault_i * m) % v == 0:
+            return m
+    return None
+
+
+def _cell_map(nf, nc):
+    """The coarse cell (box_hex numbering, i fastest) holding each fine cell's centroid."""
+    ax = [((2 * np.arange(a) + 1) * b) // (2 * a) for a, b in zip(nf, nc)]
+    ci, cj, ck = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
+    ci, cj, ck = (x.ravel(order="F") for x in (ci, cj, ck))
+    return (ci + nc[0] * (cj + nc[1] * ck)).astype(np.int64)
 
 
 def build_hierarchy(nx, ny, nz, lo=M.BOX_LO, hi=M.BOX_HI, fault_x: Optional[float] = None,
                     constrained_faces=(), min_cells: int = 2, max_levels: int = 8) -> List[Level]:
     """Levels 0 (the fine box) .. L of a box_hex(nx, ny, nz) [+ insert_fault_x(fault_x)] with
     Dirichlet constraints on whole faces: constrained_faces = [(axis, side, components)], e.g.
-    (0, "neg", (0, 1, 2)). Coarsening stops when a count is odd or below 2 * min_cells."""
+    (0, "neg", (0, 1, 2)). Each coarser level has about half the cells per direction
+    (_coarse_count); coarsening stops when a count would drop below min_cells. Each level but the
+    coarsest carries the prolongation from the next coarser one (Level.prolong)."""
     levels = []
     n = (nx, ny, nz)
-    parent = None
+    cmap = None
+    fault_is = []
     while True:
         mesh = M.box_hex(*n, lo=lo, hi=hi)
         fault_i = None
         if fault_x is not None:
-            h = (hi[0] - lo[0]) / n[0]
-            fault_i = int(round((fault_x - lo[0]) / h))
+            t = (fault_x - lo[0]) / ((hi[0] - lo[0]) / n[0])
+            fault_i = int(round(t))
+            if abs(t - fault_i) > 1e-9 * max(1.0, abs(t)) or not 0 < fault_i < n[0]:
+                raise ValueError(f"fault plane x = {fault_x} is not an interior grid plane of {n[0]} cells")
             mesh = M.insert_fault_x(mesh, fault_x)
+        fault_is.append(fault_i)
         cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
         for axis, side, comps in constrained_faces:
             cons[np.ix_(M.boundary_mask(mesh, axis, side, lo, hi), list(comps))] = True
         cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
-        levels.append(Level(n, mesh, parent, cons))
-        if len(levels) >= max_levels or any(v % 2 or v < 2 * min_cells for v in n):
+        levels.append(Level(n, mesh, cmap, cons))
+        if len(levels) >= max_levels:
             break
-        if fault_x is not None and (fault_i % 2):
+        nc = (_coarse_count(n[0], fault_i), _coarse_count(n[1], None), _coarse_count(n[2], None))
+        if any(m is None or m < min_cells for m in nc):
             break
-        nc = tuple(v // 2 for v in n)
-        # the 8 fine cells of each coarse cell (box_hex orders cells with i fastest)
-        ci, cj, ck = np.meshgrid(np.arange(nc[0]), np.arange(nc[1]), np.arange(nc[2]), indexing="ij")
-        ci, cj, ck = (a.ravel(order="F") for a in (ci, cj, ck))
-        kids = []
-        for di in (0, 1):
-            for dj in (0, 1):
-                for dk in (0, 1):
-                    kids.append((2 * ci + di) + n[0] * ((2 * cj + dj) + n[1] * (2 * ck + dk)))
-        parent = np.stack(kids)
+        cmap = _cell_map(n, nc)
         n = nc
+    for l, (lf, lc) in enumerate(zip(levels[:-1], levels[1:])):
+        lf.prolong = prolongation(lf.n, fault_is[l], lc.n, fault_is[l + 1], lf.mesh.num_nodes, lc.mesh.num_nodes)
     return levels
 
 
-def coarsen_cells(values: np.ndarray, parent: np.ndarray) -> np.ndarray:
-    """Per-cell values of a coarse level: the mean over each coarse cell's 8 fine cells."""
-    return values[parent].mean(axis=0)
+def coarsen_cells(values: np.ndarray, cell_map: np.ndarray) -> np.ndarray:
+    """Per-cell values of a coarse level: the mean over the finer level's cells whose centroids lie
+    in each coarse cell (cell_map: the coarse cell of each fine cell)."""
+    nc = int(cell_map.max()) + 1
+    cnt = np.bincount(cell_map, minlength=nc).astype(np.float64)
+    v = np.asarray(values, dtype=np.float64)
+    flat = v.reshape(len(cell_map), -1)
+    out = np.stack([np.bincount(cell_map, weights=flat[:, j], minlength=nc) / cnt for j in range(flat.shape[1])], axis=1)
+    return out.reshape((nc,) + v.shape[1:])
 
 
 def prolongations(levels: List[Level], fault_x: Optional[float], lo=M.BOX_LO, hi=M.BOX_HI):
-    """[(row_ptr, col, val)] of the prolongation from level l + 1 to level l, l = 0 .. L - 1."""
+    """[(row_ptr, col, val)] of the prolongation from level l + 1 to level l, l = 0 .. L - 1 (the
+    ones build_hierarchy stored with the levels, else built here)."""
     out = []
     for lf, lc in zip(levels[:-1], levels[1:]):
+        if lf.prolong is not None:
+            out.append(lf.prolong)
+            continue
         fi = fc = None
         if fault_x is not None:
             fi = int(round((fault_x - lo[0]) / ((hi[0] - lo[0]) / lf.n[0])))
-            fc = fi // 2
+            fc = int(round((fault_x - lo[0]) / ((hi[0] - lo[0]) / lc.n[0])))
         out.append(prolongation(lf.n, fi, lc.n, fc, lf.mesh.num_nodes, lc.mesh.num_nodes))
     return out
 
 
-def coarsen_material(mat, parent):
-    """The material of a coarse level: every per-cell field averaged over the 8 fine cells of each
-    coarse cell; per-quadrature-point state starts at zero (the Jacobians read no state)."""
+def coarsen_material(mat, cell_map):
+    """The material of a coarse level: every per-cell field averaged over the finer level's cells
+    of each coarse cell (coarsen_cells); per-quadrature-point state starts at zero (the Jacobians
+    read no state)."""
     from . import materials as MAT
 
-    cc = lambda v: coarsen_cells(np.asarray(v), parent)  # noqa: E731
+    cc = lambda v: coarsen_cells(np.asarray(v), cell_map)  # noqa: E731
     if isinstance(mat, MAT.IsotropicLinearGenMaxwell):
-        nc = parent.shape[1]
+        nc = int(cell_map.max()) + 1
         return MAT.IsotropicLinearGenMaxwell(cc(mat.density), cc(mat.shear_modulus), cc(mat.bulk_modulus),
                                              cc(mat.maxwell_time), cc(mat.shear_modulus_ratio),
                                              np.zeros((nc, 8, 18)), np.zeros((nc, 8, 6)))
@@ -174,7 +223,7 @@ def attach(ctx, fine_solver, levels: List[Level], material, fault_x=None, dt=0.0
     coarse = []
     mat = material
     for lv in levels[1:]:
-        mat = coarsen_material(mat, lv.cell_parent)
+        mat = coarsen_material(mat, lv.cell_map)
         dm = FA.DeviceMesh(ctx, lv.mesh)
         ig = mat.create_integrator(dm, dt) if isinstance(mat, MAT.IsotropicLinearGenMaxwell) else mat.create_integrator(dm)
         s = FA.Solver(dm, lv.constrained, [ig])

@@ -1,13 +1,14 @@
 """Serving forward solves: a request loop with HBM-budget admission and continuous batching.
 
 Each request is a quasi-static forward solve (the same path as problems.QuasistaticProblem) on its
-own box mesh with a prescribed-slip fault. The server keeps one ragged batch (pl_ragged_*): a
-request is admitted when it has arrived, a slot is free and its estimated device memory fits the
-remaining HBM budget; its mesh, aux fields and solver are then built on the device, and its solve
-joins the batch at the next iteration boundary. Every PCG iteration of every admitted request
-shares the same launches (one operator launch over all their cells), each request converging on
-its own dot products; a request leaves the batch when its FP64 residual meets the tolerance, and
-its slot and memory go to the next arrival. Latency is measured from arrival to completion.
+own box mesh with a prescribed-slip fault. A request is admitted when it has arrived, a slot is free
+and its estimated device memory fits the remaining HBM budget; its mesh, aux fields and solver are
+then built on the device. Small boxes join one ragged batch (pl_ragged_*) at the next iteration
+boundary: every PCG iteration of every request in it shares the same launches (one operator launch
+over all their cells), each request converging on its own dot products, and a request leaves the
+batch when its FP64 residual meets the tolerance. Large boxes (with a multigrid hierarchy) are solved
+beside the batch, on a second stream, with FP32 V-cycles under FP64 conjugate gradients. A finished
+request's slot and memory go to the next arrival. Latency is measured from arrival to completion.
 
 Host mesh generation is not part of serving: the requests' host-side problem data (mesh, material
 fields, slip, constraints) is prepared before the request stream starts, for the server and the
@@ -88,11 +89,25 @@ class HostProblem:
     slip: np.ndarray
     constrained: np.ndarray
     bc: np.ndarray
+    levels: Optional[list] = None  # multigrid hierarchy (pylith_b200.multigrid) for large boxes
 
 
-def prepare(req: Request) -> HostProblem:
+MULTIGRID_MIN_N = 32
+
+
+def prepare(req: Request, multigrid_min_n: int = MULTIGRID_MIN_N) -> HostProblem:
+    """Host-side problem data; boxes of at least multigrid_min_n cells per side also get their
+    multigrid hierarchy (meshes, constraint masks and prolongations of every level)."""
+    from . import multigrid as MGH
+
     lo, hi = M.BOX_LO, M.BOX_HI
-    mesh = M.insert_fault_x(M.box_hex(req.n, req.n, req.n))
+    levels = None
+    if req.n >= multigrid_min_n:
+        levels = MGH.build_hierarchy(req.n, req.n, req.n, fault_x=0.0,
+                                     constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))])
+        if len(levels) < 3:
+            levels = None
+    mesh = levels[0].mesh if levels else M.insert_fault_x(M.box_hex(req.n, req.n, req.n))
     rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=req.seed)
     lag_nodes = np.zeros(mesh.num_lagrange, dtype=np.int64)
     lag_nodes[mesh.cohesive[:, 8:].ravel()] = mesh.cohesive[:, :4].ravel()
@@ -107,22 +122,39 @@ def prepare(req: Request) -> HostProblem:
     cons[M.boundary_mask(mesh, 0, "neg")] = True
     cons[M.boundary_mask(mesh, 0, "pos")] = True
     cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
-    return HostProblem(req, mesh, rho, mu, K, slip, cons, np.zeros(mesh.num_dof))
+    return HostProblem(req, mesh, rho, mu, K, slip, cons, np.zeros(mesh.num_dof), levels)
 
 
-def build_problem(ctx, hp: HostProblem, precision: int, rtol: float):
+def build_problem(ctx, hp: HostProblem, precision: int, rtol: float, multigrid: Optional[int] = None):
+    """The request's device problem; with `multigrid` (a precision) and a hierarchy, its solver is
+    preconditioned by V-cycles of that precision (the problem keeps the hierarchy alive)."""
+    from . import multigrid as MGH
     from . import problems as P
 
-    return P.QuasistaticProblem(ctx, hp.mesh, [(MAT.IsotropicLinearElasticity(hp.rho, hp.mu, hp.K), None)],
-                                hp.constrained, hp.bc, faults=[MAT.FaultCohesiveKin(hp.slip)], precision=precision,
-                                rtol=rtol)
+    mat = MAT.IsotropicLinearElasticity(hp.rho, hp.mu, hp.K)
+    prob = P.QuasistaticProblem(ctx, hp.mesh, [(mat, None)], hp.constrained, hp.bc,
+                                faults=[MAT.FaultCohesiveKin(hp.slip)], precision=precision, rtol=rtol)
+    prob.multigrid = None
+    if multigrid is not None and hp.levels is not None:
+        prob.multigrid = MGH.attach(ctx, prob.solver, hp.levels, mat, fault_x=0.0, precision=multigrid)
+    return prob
+
+
+def close_problem(prob) -> None:
+    if getattr(prob, "multigrid", None) is not None:
+        prob.multigrid.close()
+    prob.close()
 
 
 class Server:
-    """Continuous batching of FP32-refined solves in one ragged batch (single host thread)."""
+    """Serving loop: an admission thread (arrival times, slots, HBM budget) and two device workers,
+    each with its own stream: the batch worker keeps one ragged batch (pl_ragged_*) of FP32-refined
+    solves that requests join and leave between iteration chunks; the multigrid worker solves the
+    large boxes that have a multigrid hierarchy, one at a time, with FP32 V-cycles under FP64
+    conjugate gradients."""
 
     def __init__(self, device: int = 0, slots: int = 64, hbm_budget: Optional[int] = None, rtol: float = 1e-10,
-                 keep_solutions=False, chunk: int = 10):
+                 keep_solutions=False, chunk: int = 10, multigrid: bool = True):
         import torch
 
         self.device = device
@@ -132,61 +164,139 @@ class Server:
         self.rtol = rtol
         self.keep = keep_solutions
         self.chunk = chunk
+        self.multigrid = multigrid
         self.memory = []  # (request, predicted bytes, measured bytes)
+        self.routes = {}  # request -> "batch" or "multigrid"
 
     def run(self, problems: List[HostProblem]) -> List[Result]:
+        import queue
+        import threading
+
         import torch
 
-        torch.cuda.set_device(self.device)
-        ctx = FA.Context(self.device)
-        batch = FA.RaggedBatch(ctx, capacity=self.slots, chunk=self.chunk)
-        pending = deque(sorted(problems, key=lambda hp: hp.req.arrival))
+        pending = sorted(problems, key=lambda hp: hp.req.arrival)
         for hp in pending:
             if estimate_bytes(hp.req.n) > self.budget:
                 raise ValueError(f"request {hp.req.rid} ({hp.req.n}^3) exceeds the HBM budget")
-        active = {}
-        used = 0
+        lock = threading.Lock()
+        freed = threading.Condition(lock)
+        state = {"used": 0, "busy": 0}
         results: List[Result] = []
+        errors = []
         self.memory = []
+        q_batch, q_mg = queue.Queue(), queue.Queue()
         t0 = time.perf_counter()
-        while pending or active:
-            now = time.perf_counter() - t0
-            while (pending and pending[0].req.arrival <= now and len(active) < self.slots
-                   and used + estimate_bytes(pending[0].req.n) <= self.budget):
-                hp = pending.popleft()
-                start = time.perf_counter() - t0
-                predicted = estimate_bytes(hp.req.n)
-                free0 = torch.cuda.mem_get_info(self.device)[0]
-                prob = build_problem(ctx, hp, FA.Solver.FP32_REFINED, self.rtol)
-                F, du = prob.begin_step(0.0)
-                member = batch.add(prob.solver, F, du)
-                measured = free0 - torch.cuda.mem_get_info(self.device)[0]
-                self.memory.append((hp.req.rid, predicted, measured))
-                used += predicted
-                active[member] = (hp, prob, start, predicted)
-            if not active:
-                time.sleep(max(0.0, pending[0].req.arrival - (time.perf_counter() - t0)))
-                continue
-            batch.iterate()
-            for member in list(active):
-                st = batch.status(member)
-                if not st["done"]:
-                    continue
-                hp, prob, start, nbytes = active.pop(member)
-                if st["status"] != 0:
-                    raise RuntimeError(f"request {hp.req.rid} failed: {C_error(st['status'])}")
-                prob.end_step(0.0)
-                ctx.synchronize()
-                end = time.perf_counter() - t0
-                u = prob.u.cpu().numpy() if self.keep else None
-                results.append(Result(hp.req.rid, hp.req.n, prob.dmesh.num_dof, hp.req.arrival, start, end,
-                                      st["iterations"], u))
-                batch.remove(member)
-                prob.close()
-                used -= nbytes
-        batch.close()
-        ctx.close()
+
+        def finish(hp, prob, start, its, nbytes):
+            end = time.perf_counter() - t0
+            u = prob.u.cpu().numpy() if self.keep and prob.u is not None else None
+            with lock:
+                results.append(Result(hp.req.rid, hp.req.n, prob.dmesh.num_dof, hp.req.arrival, start, end, its, u))
+                state["used"] -= nbytes
+                state["busy"] -= 1
+                freed.notify_all()
+
+        def batch_worker():
+            torch.cuda.set_device(self.device)
+            stream = torch.cuda.Stream(device=self.device)
+            ctx = FA.Context(self.device, use_torch_stream=False)
+            ctx.set_stream(stream.cuda_stream)
+            batch = FA.RaggedBatch(ctx, capacity=self.slots, chunk=self.chunk)
+            active = {}
+            done = False
+            with torch.cuda.stream(stream):
+                while not done or active:
+                    while True:  # join the batch at this iteration boundary
+                        try:
+                            item = q_batch.get(block=not active and not done, timeout=0.05)
+                        except queue.Empty:
+                            break
+                        if item is None:
+                            done = True
+                            break
+                        hp, nbytes, start = item
+                        try:
+                            free0 = torch.cuda.mem_get_info(self.device)[0]
+                            prob = build_problem(ctx, hp, FA.Solver.FP32_REFINED, self.rtol)
+                            F, du = prob.begin_step(0.0)
+                            member = batch.add(prob.solver, F, du)
+                            self.memory.append((hp.req.rid, nbytes, free0 - torch.cuda.mem_get_info(self.device)[0]))
+                            active[member] = (hp, prob, start, nbytes)
+                        except Exception as e:
+                            errors.append((hp.req.rid, repr(e)))
+                            finish(hp, _Null(), start, 0, nbytes)
+                    if not active:
+                        continue
+                    batch.iterate()
+                    for member in list(active):
+                        st = batch.status(member)
+                        if not st["done"]:
+                            continue
+                        hp, prob, start, nbytes = active.pop(member)
+                        if st["status"] != 0:
+                            errors.append((hp.req.rid, C_error(st["status"])))
+                        prob.end_step(0.0)
+                        stream.synchronize()
+                        finish(hp, prob, start, st["iterations"], nbytes)
+                        batch.remove(member)
+                        close_problem(prob)
+            batch.close()
+            ctx.close()
+
+        def multigrid_worker():
+            torch.cuda.set_device(self.device)
+            stream = torch.cuda.Stream(device=self.device)
+            ctx = FA.Context(self.device, use_torch_stream=False)
+            ctx.set_stream(stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                while True:
+                    item = q_mg.get()
+                    if item is None:
+                        break
+                    hp, nbytes, start = item
+                    try:
+                        prob = build_problem(ctx, hp, FA.Solver.FP64, self.rtol, multigrid=FA.Solver.FP32_REFINED)
+                        st = prob.step(0.0)
+                        stream.synchronize()
+                        finish(hp, prob, start, st.iterations, nbytes)
+                        close_problem(prob)
+                    except Exception as e:
+                        errors.append((hp.req.rid, repr(e)))
+                        finish(hp, _Null(), start, 0, nbytes)
+            ctx.close()
+
+        workers = [threading.Thread(target=batch_worker, daemon=True), threading.Thread(target=multigrid_worker, daemon=True)]
+        for w in workers:
+            w.start()
+        for hp in pending:
+            nbytes = estimate_bytes(hp.req.n)
+            wait = hp.req.arrival - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            with lock:
+                while state["busy"] >= self.slots or state["used"] + nbytes > self.budget:
+                    freed.wait()
+                state["used"] += nbytes
+                state["busy"] += 1
+            start = time.perf_counter() - t0
+            route = "multigrid" if self.multigrid and hp.levels is not None else "batch"
+            self.routes[hp.req.rid] = route
+            (q_mg if route == "multigrid" else q_batch).put((hp, nbytes, start))
+        q_batch.put(None)
+        q_mg.put(None)
+        for w in workers:
+            w.join()
+        if errors:
+            raise RuntimeError(f"requests failed: {errors[:3]}")
         return sorted(results, key=lambda r: r.rid)
+
+
+class _Null:
+    """Stand-in for a problem that failed to build (its request is reported as an error)."""
+    u = None
+
+    class dmesh:
+        num_dof = 0
 
 
 def C_error(code: int) -> str:
@@ -196,8 +306,9 @@ def C_error(code: int) -> str:
 
 
 def serve_sequential(problems: List[HostProblem], device: int = 0, precision: int = FA.Solver.FP64,
-                     rtol: float = 1e-10, keep_solutions=False) -> List[Result]:
-    """The baseline: requests in arrival order, one at a time, each with its own solver."""
+                     rtol: float = 1e-10, keep_solutions=False, multigrid: Optional[int] = None) -> List[Result]:
+    """The baseline: requests in arrival order, one at a time, each with its own solver (point-block
+    Jacobi PCG; with `multigrid`, V-cycles of that precision where a hierarchy exists)."""
     import torch
 
     torch.cuda.set_device(device)
@@ -209,13 +320,13 @@ def serve_sequential(problems: List[HostProblem], device: int = 0, precision: in
         if wait > 0:
             time.sleep(wait)
         start = time.perf_counter() - t0
-        prob = build_problem(ctx, hp, precision, rtol)
+        prob = build_problem(ctx, hp, precision, rtol, multigrid=multigrid)
         st = prob.step(0.0)
         ctx.synchronize()
         u = prob.u.cpu().numpy() if keep_solutions else None
         out.append(Result(hp.req.rid, hp.req.n, prob.dmesh.num_dof, hp.req.arrival, start,
                           time.perf_counter() - t0, st.iterations + st.inner_iterations, u))
-        prob.close()
+        close_problem(prob)
     ctx.close()
     return out
 

@@ -1,7 +1,8 @@
 """Geometric multigrid preconditioning of the device solver (pl_multigrid_*): on a Q1 box with a
 fault at x = 0, flexible CG with V-cycles (FP64, or FP32 V-cycles under FP64 CG) reaches the
 point-block-Jacobi PCG solution (relative displacement difference <= 1e-8 at rtol 1e-12) in at
-least five times fewer iterations, for isotropic elasticity and generalized Maxwell."""
+least five times fewer iterations, for isotropic elasticity and generalized Maxwell, with nested
+levels and with levels whose grids are not nested."""
 import numpy as np
 import pytest
 
@@ -23,12 +24,13 @@ def ctx():
     return FA.Context(0)
 
 
-@pytest.mark.parametrize("rheology", ["elastic", "genmaxwell"])
-def test_multigrid_matches_point_jacobi_in_fewer_iterations(ctx, rheology):
+@pytest.mark.parametrize("rheology,dims", [("elastic", (16, 16, 12)), ("genmaxwell", (16, 16, 12)),
+                                           ("elastic", (18, 14, 11))])  # the last: non-nested levels
+def test_multigrid_matches_point_jacobi_in_fewer_iterations(ctx, rheology, dims):
     from pylith_b200 import feassemble as FA
     from pylith_b200 import problems as P
 
-    levels = MG.build_hierarchy(16, 16, 12, fault_x=0.0, constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))])
+    levels = MG.build_hierarchy(*dims, fault_x=0.0, constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))])
     assert len(levels) >= 3
     mesh, cons = levels[0].mesh, levels[0].constrained
     nc = mesh.num_cells

@@ -102,3 +102,21 @@ def test_admission_respects_the_hbm_budget(cuda):
         assert s1 >= e0 - 1e-3
     with pytest.raises(ValueError):
         SV.Server(slots=1, hbm_budget=budget // 4).run(hps)
+
+
+def test_large_boxes_take_the_multigrid_route(cuda):
+    """Boxes of 32^3 cells and more (with a multigrid hierarchy, nested or not: 34 coarsens to 16) are solved beside the ragged batch
+    with FP32 V-cycles under FP64 CG; their results, and the batched small ones', match the plain
+    FP64 one-at-a-time path."""
+    from pylith_b200 import serving as SV
+
+    reqs = [SV.Request(0, 32, 11, 0.0, 1.5, (0.1, 0.9, 0.2, 0.7)), SV.Request(1, 8, 12, 0.001, 0.7, (0.3, 0.6, 0.1, 0.9)),
+            SV.Request(2, 34, 13, 0.002, 2.0, (0.0, 0.5, 0.5, 1.0)), SV.Request(3, 10, 14, 0.003, 1.0, (0.2, 0.8, 0.2, 0.8))]
+    hps = [SV.prepare(r) for r in reqs]
+    assert [hp.levels is not None for hp in hps] == [True, False, True, False]
+    server = SV.Server(slots=4, keep_solutions=True, rtol=1e-12)
+    served = {r.rid: r for r in server.run(hps)}
+    assert server.routes == {0: "multigrid", 1: "batch", 2: "multigrid", 3: "batch"}
+    for s in SV.serve_sequential(hps, keep_solutions=True, rtol=1e-12):
+        m = served[s.rid]
+        assert np.linalg.norm(m.u - s.u) <= 1e-8 * np.linalg.norm(s.u), s.rid

@@ -423,6 +423,38 @@ def test_batched_reliable_updates_match_fp64_with_fewer_iterations(ctx):
     assert iters[True] <= iters[False], iters
 
 
+def test_batched_energy_sums_in_the_operator_launch_match_the_reduction_kernel(ctx, monkeypatch):
+    """The batched PCG sums p.(A p) inside the operator launch, from the cells' energies (on a
+    fault mesh: the reduced space's fold must not change the sum); the solutions and iteration
+    counts match those of the separate DOF-wise reduction kernel, and both match FP64 solves."""
+    from pylith_b200 import greensfns as GF
+
+    lo, hi = (-6000.0, -6000.0, -9000.0), (6000.0, 6000.0, 0.0)
+    mesh = M.box_tet_delaunay_fault_x(20000, seed=2, lo=lo, hi=hi)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=7)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg", lo, hi)] = True
+    cons[M.boundary_mask(mesh, 0, "pos", lo, hi)] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    patches = GF.fault_patches(mesh, (-6000.0, 6000.0), (-9000.0, 0.0), 4, 2)
+    out = {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("PYLITH_B200_BATCH_FUSED_PQ", fused)
+        g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
+        got, _ = g.solve(g.impulses[:8], batched=True)
+        out[fused] = ([x.cpu().numpy() for x in got], g.batch.stats())
+        if fused == "0":
+            ref, _ = g.solve(g.impulses[:8], batched=False)
+    for fused, (xs, st) in out.items():
+        assert st["max_rel_residual"] <= 1e-11
+        for a, b in zip(xs, ref):
+            b = b.cpu().numpy()
+            assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b), fused
+    i1, i0 = out["1"][1]["inner_iterations"], out["0"][1]["inner_iterations"]
+    assert abs(i1 - i0) <= 0.05 * i0 + 20, (i1, i0)
+
+
 def test_fp32_reliable_updates_and_restarted_refinement_match_the_oracle(ctx, oracle_lib):
     """The single-right-hand-side FP32 solver with reliable updates and with restarted iterative
     refinement both reach the FP64 tolerance on a heterogeneous tetrahedral problem and match

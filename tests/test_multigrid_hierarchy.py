@@ -41,8 +41,34 @@ def test_materials_are_averaged_over_child_cells():
     levels = MG.build_hierarchy(4, 4, 4)
     nc0 = levels[0].mesh.num_cells
     rho, mu, K = MAT.lognormal_elastic(nc0, seed=1)
-    coarse = MG.coarsen_material(MAT.IsotropicLinearElasticity(rho, mu, K), levels[1].cell_parent)
+    coarse = MG.coarsen_material(MAT.IsotropicLinearElasticity(rho, mu, K), levels[1].cell_map)
     assert coarse.shear_modulus.shape == (levels[1].mesh.num_cells,)
     np.testing.assert_allclose(coarse.shear_modulus.sum() * 8, mu.sum())
-    # every fine cell is the child of exactly one coarse cell
-    assert np.array_equal(np.sort(levels[1].cell_parent.ravel()), np.arange(nc0))
+    # nested levels: every coarse cell holds exactly 8 fine cells
+    assert levels[1].cell_map.shape == (nc0,)
+    assert np.array_equal(np.bincount(levels[1].cell_map), np.full(levels[1].mesh.num_cells, 8))
+
+
+def test_non_nested_levels_keep_the_fault_plane():
+    """Counts that are not powers of two (and halves that would move the fault plane off the grid)
+    coarsen to the nearest count that keeps the plane a grid plane; the interpolation between such
+    non-nested grids is still exact for fields linear on each side of the fault."""
+    levels = MG.build_hierarchy(30, 14, 9, fault_x=0.0, constrained_faces=[(0, "neg", (0, 1, 2))])
+    ns = [lv.n for lv in levels]
+    assert ns[0] == (30, 14, 9) and len(ns) >= 3
+    for (nx, ny, nz), (mx, my, mz) in zip(ns[:-1], ns[1:]):
+        assert mx % 2 == 0 and abs(2 * mx - nx) <= 4 and my == (ny + 1) // 2 and mz == (nz + 1) // 2
+    for (row, col, val), lf, lc in zip(MG.prolongations(levels, 0.0), levels[:-1], levels[1:]):
+        P = sp.csr_matrix((val, col, row), shape=(lf.mesh.num_nodes, lc.mesh.num_nodes))
+        np.testing.assert_allclose(np.asarray(P.sum(axis=1)).ravel(), 1.0)
+        assert val.min() > 0.0
+        np.testing.assert_allclose(P @ _side_linear(lc.mesh), _side_linear(lf.mesh), rtol=0, atol=1e-8)
+    # every coarse cell holds at least one finer cell, and a cell-wise constant averages to itself
+    for lf, lc in zip(levels[:-1], levels[1:]):
+        cnt = np.bincount(lc.cell_map, minlength=lc.mesh.num_cells)
+        assert cnt.min() >= 1
+        np.testing.assert_allclose(MG.coarsen_cells(np.full(lf.mesh.num_cells, 3.5), lc.cell_map), 3.5)
+        # cells stay on their side of the fault
+        xf = lf.mesh.coords[lf.mesh.cells].mean(axis=1)[:, 0]
+        xc = lc.mesh.coords[lc.mesh.cells].mean(axis=1)[:, 0]
+        assert np.all(np.sign(xf) == np.sign(xc[lc.cell_map]))
