@@ -386,12 +386,19 @@ def main():
     # pinned host memory, computes the residual and J v, and copies both results back. Copies in
     # and out run on their own streams and the device buffers alternate between steps, so one
     # step's transfers overlap the neighbouring steps' work (PCIe is full duplex).
-    hu = [torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(u.cpu()) for _ in range(2)]
-    hv = [torch.empty(n, dtype=torch.float64, pin_memory=True).copy_(v.cpu()) for _ in range(2)]
+    # a step's u and v sit side by side in one pinned buffer and one device buffer, so that they
+    # cross the link as one copy (fewer, larger copies run closer to the link's rate)
+    hin = [torch.empty(2, n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    for h in hin:
+        h[0].copy_(u.cpu())
+        h[1].copy_(v.cpu())
+    hu = [h[0] for h in hin]
+    hv = [h[1] for h in hin]
     hr = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
     hjv = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
-    du = [u, torch.empty_like(u)]
-    dv = [v, torch.empty_like(v)]
+    din = [torch.empty(2, n, dtype=torch.float64, device=u.device) for _ in range(2)]
+    du = [d[0] for d in din]
+    dv = [d[1] for d in din]
     dr = [r, torch.empty_like(r)]
     djv = [jv, torch.empty_like(jv)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
@@ -408,8 +415,7 @@ def main():
         i = k % 2
         s_in.wait_event(ev_done[i])  # inputs of step k - 2 consumed
         with torch.cuda.stream(s_in):
-            du[i].copy_(hu[i], non_blocking=True)
-            dv[i].copy_(hv[i], non_blocking=True)
+            din[i].copy_(hin[i], non_blocking=True)
             ev_in[i].record(s_in)
         comp.wait_event(ev_in[i])
         comp.wait_event(ev_out[i])  # results of step k - 2 copied out
@@ -468,22 +474,26 @@ def main():
     ctx.set_stream(stream.cuda_stream)
     e2e_value = 2 * global_dof * args.steps / t_e2e / 1e9
 
-    # the host link on this box: pinned copies of one step's input bytes, each direction alone and
-    # both directions at once (the bound of the overlapped end-to-end steps)
+    # the host link on this box: pinned copies of one step's bytes as the steps make them (inputs
+    # as one copy, the two results as two), each direction alone and both directions at once (the
+    # bound of the overlapped end-to-end steps)
     def link():
         out = {}
         reps = 5
-        for name, pairs in (("h2d", [(du, hu)]), ("d2h", [(hr, dr)]), ("duplex", [(du, hu), (hr, dr)])):
+        copy_in = [(din[0], hin[0])]
+        copy_out = [(hr[0], dr[0]), (hjv[0], djv[0])]
+        for name, plan in (("h2d", [(s_in, copy_in)]), ("d2h", [(s_out, copy_out)]),
+                           ("duplex", [(s_in, copy_in), (s_out, copy_out)])):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             s_in.wait_stream(stream)
             s_out.wait_stream(stream)
             for _ in range(reps):
-                for (dst, src), st in zip(pairs, (s_in, s_out)):
+                for st, copies in plan:
                     with torch.cuda.stream(st):
-                        dst[0].copy_(src[0], non_blocking=True)
-                        dst[1].copy_(src[1], non_blocking=True)
+                        for dst, src in copies:
+                            dst.copy_(src, non_blocking=True)
             stream.wait_stream(s_in)
             stream.wait_stream(s_out)
             e1.record(stream)
@@ -784,62 +794,92 @@ def config_c3(args):
     """Green's functions: 1.5 M-cell Delaunay P1 mesh of [-12,12]x[-15,15]x[-20,0] km (the config-1
     mesh construction, mirrored across x = 0 so that the plane carries a conforming fault of
     cohesive cells) with the config-1 material statistics; 40x25 unit-slip patches over y in
-    [-12,12] km, z in [-15,0] km, left-lateral then reverse: 2,000 impulses. All of them batched
-    (FP32 PCG with reliable updates, tile and preconditioner picked by the autotuner) against
-    one-at-a-time FP64 solves of a sample of at least 20 impulses."""
+    [-12,12] km, z in [-15,0] km, left-lateral then reverse: 2,000 impulses. Every impulse solved
+    (a) batched (FP32 PCG tiles with reliable updates, tile and preconditioner picked by the
+    autotuner) and (b) one at a time by FP64 CG with FP32 multigrid V-cycles over independent
+    coarser Delaunay meshes of the box; against one-at-a-time FP64 solves of a sample of at least
+    20 impulses with point-block Jacobi and with FP64 multigrid."""
     import torch
 
     from pylith_b200 import feassemble as FA
     from pylith_b200 import greensfns as GF
     from pylith_b200 import materials as MAT
     from pylith_b200 import meshing as M
+    from pylith_b200 import multigrid as MG
 
     lo, hi = (-12000.0, -15000.0, -20000.0), (12000.0, 15000.0, 0.0)
     t0 = time.perf_counter()
     mesh = M.box_tet_delaunay_fault_x(int(1_500_000 * args.scale), seed=0, lo=lo, hi=hi)
     t_mesh = time.perf_counter() - t0
+    faces = [(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))]
+    t0 = time.perf_counter()
+    levels = MG.build_tet_hierarchy(mesh, lambda n, l: M.box_tet_delaunay_fault_x(n, seed=l, lo=lo, hi=hi),
+                                    fault_x=0.0, lo=lo, hi=hi, constrained_faces=faces)
+    t_hier = time.perf_counter() - t0
     rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
     mat = MAT.IsotropicLinearElasticity(rho, mu, K)
-    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
-    for sd in ("neg", "pos"):
-        cons[M.boundary_mask(mesh, 0, sd, lo, hi)] = True
-    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    cons = levels[0].constrained
     patches = GF.fault_patches(mesh, (-12000.0, 12000.0), (-15000.0, 0.0), 40, 25)
     ctx = FA.Context(0)
-    # rtol 1e-11 for the batched and the FP64 solves: the Delaunay mesh's conditioning turns a 1e-10
-    # residual into displacement differences just above 1e-8
+    # rtol 1e-11 for every solve: the Delaunay mesh's conditioning turns a 1e-10 residual into
+    # displacement differences just above 1e-8
     g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
     usable = [imp for imp in g.impulses if len(patches[imp.patch]) > 0]  # every patch holds a node: all of them
     # the autotuner picks the tile size and the preconditioner (point-block Jacobi or Chebyshev-
     # Jacobi of degree 2-3) on a sample of 32 impulses
     step = max(1, len(usable) // 32)
     table = g.autotune(usable[step // 2::step][:32], tiles=(8, 16), degrees=(0, 2, 3))
+    mg32 = g.attach_multigrid(levels, mat, FA.Solver.FP32_REFINED)
+    mg64 = g.attach_multigrid(levels, mat, FA.Solver.FP64)
     g.solve(usable[:8], batched=True)  # warm-up
     g.solve(usable[:1], batched=False)
+    g.solve(usable[:2], batched=False, solver=mg32)
+    g.solve(usable[:2], batched=False, solver=mg64)
     ns = max(20, int(args.steps))
     sample_s = usable[::max(1, len(usable) // ns)][:ns]
     want = {id(imp) for imp in sample_s}
-    keep, t_b = {}, 0.0
+    keep_b, keep_m, t_b, t_m, its_m = {}, {}, 0.0, 0.0, []
     for c0 in range(0, len(usable), 400):  # 400 impulses' vectors at a time on the device
         part = usable[c0:c0 + 400]
         sols, dt_part = g.solve(part, batched=True)
         t_b += dt_part
-        keep.update({id(imp): x for imp, x in zip(part, sols) if id(imp) in want})
+        keep_b.update({id(imp): x for imp, x in zip(part, sols) if id(imp) in want})
+        del sols
+        sols, dt_part = g.solve(part, batched=False, solver=mg32)
+        t_m += dt_part
+        its_m.append(mg32.stats()["iterations"])
+        keep_m.update({id(imp): x for imp, x in zip(part, sols) if id(imp) in want})
         del sols
     st_b = g.batch.stats()
     sol_s, t_s = g.solve(sample_s, batched=False)
-    err = max(float(torch.linalg.norm(keep[id(imp)] - b) / torch.linalg.norm(b)) for imp, b in zip(sample_s, sol_s))
+    its_s = g.solver64.stats()["iterations"]
+    sol_g, t_g = g.solve(sample_s, batched=False, solver=mg64)
+    its_g = mg64.stats()["iterations"]
+
+    def err(keep, ref):
+        return max(float(torch.linalg.norm(keep[id(imp)] - b) / torch.linalg.norm(b)) for imp, b in zip(sample_s, ref))
+
+    rate_b, rate_m = len(usable) / t_b, len(usable) / t_m
+    rate_s, rate_g = len(sample_s) / t_s, len(sample_s) / t_g
     return {"config": "c3", "cells": mesh.num_cells, "dof": mesh.num_dof, "mesh": "Delaunay, mirrored across the fault",
             "mesh_build_s": t_mesh, "impulses_total": len(g.impulses), "impulses_solved": len(usable),
-            "batched": {"solves_per_s": len(usable) / t_b, "seconds": t_b, "tile": g.batch.tile,
+            "multigrid_levels": [lv.mesh.num_cells for lv in levels], "hierarchy_build_s": t_hier,
+            "batched": {"solves_per_s": rate_b, "seconds": t_b, "tile": g.batch.tile,
                         "chebyshev_degree": g.batch.degree, "lambda_max_estimate": g.batch.lambda_max,
                         "fp64_accuracy": "reliable updates (residual replacement, delta 0.01)",
                         "last_call_stats": st_b},
             "autotune": [{"tile": t, "chebyshev_degree": d, "solves_per_s": r} for t, d, r in table],
-            "fp64_one_at_a_time": {"sample": len(sample_s), "solves_per_s": len(sample_s) / t_s,
-                                   "iterations_last": g.solver64.stats()["iterations"]},
-            "speedup": (len(usable) / t_b) / (len(sample_s) / t_s),
-            "max_rel_displacement_error_vs_fp64": err}
+            "multigrid_fp32_vcycles": {"solves_per_s": rate_m, "seconds": t_m, "iterations_last": its_m[-1],
+                                       "how": "one impulse at a time: FP64 flexible CG, one FP32 V-cycle "
+                                              "(Chebyshev-Jacobi smoothing) per iteration"},
+            "fp64_one_at_a_time": {"sample": len(sample_s), "solves_per_s": rate_s, "iterations_last": its_s,
+                                   "preconditioner": "point-block Jacobi"},
+            "fp64_multigrid_one_at_a_time": {"sample": len(sample_s), "solves_per_s": rate_g, "iterations_last": its_g},
+            "speedup": rate_b / rate_s,
+            "speedup_multigrid_vs_fp64": rate_m / rate_s,
+            "speedup_multigrid_vs_fp64_multigrid": rate_m / rate_g,
+            "max_rel_displacement_error_vs_fp64": err(keep_b, sol_s),
+            "max_rel_displacement_error_multigrid_vs_fp64": err(keep_m, sol_s)}
 
 
 def config_c4(args):

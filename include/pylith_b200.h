@@ -363,8 +363,10 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
                         const int32_t* const* prolong_row_ptr, const int32_t* const* prolong_col,
                         const double* const* prolong_val, pl_multigrid* out);
 /* Smoother: Chebyshev polynomial of point-block Jacobi of `degree` on [lower_ratio b, b],
- * b = 1.1 lambda_max(D^-1 A) estimated by power iterations at the first solve after each setup;
- * the coarsest level takes degree coarse_degree on [coarse_lower_ratio b, b]. precision
+ * b = 1.1 lambda_max(D^-1 A) estimated by power iterations at the first solve after each setup.
+ * A coarsest level with at most 1536 unknowns is solved exactly (the inverse of its reduced matrix,
+ * assembled and inverted on the device at the first solve after each setup); a larger one takes
+ * degree coarse_degree on [coarse_lower_ratio b, b]. precision
  * PL_SOLVER_FP32_REFINED runs the V-cycle in FP32 (the outer conjugate gradients stay FP64).
  * Defaults: 2, 0.1, 40, 0.01, PL_SOLVER_FP64. */
 int pl_multigrid_set_smoother(pl_multigrid mg, int degree, double lower_ratio, int coarse_degree,
@@ -372,7 +374,8 @@ int pl_multigrid_set_smoother(pl_multigrid mg, int degree, double lower_ratio, i
 /* Makes pl_solver_solve run flexible conjugate gradients in FP64 preconditioned by one V-cycle
  * of `mg` (NULL: back to point-block Jacobi); pl_solver_setup then sets up every level. */
 int pl_solver_set_multigrid(pl_solver solver, pl_multigrid mg);
-/* Levels and each level's lambda_max(D^-1 A) estimate (0 before the first solve). */
+/* Levels and each level's lambda_max(D^-1 A) estimate (0 before the first solve, and for a
+ * coarsest level solved with its dense inverse). */
 int pl_multigrid_get_levels(pl_multigrid mg, int* num_levels, double* lambda_max);
 /* Refused while the hierarchy is attached to its solver (pl_solver_set_multigrid(solver, NULL)
  * or pl_solver_destroy detaches it). */

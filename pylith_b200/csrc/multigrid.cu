@@ -6,7 +6,10 @@
 // point-block Jacobi fine smoother on faults, libsrc/pylith/materials/Elasticity.cc:298-330). Here
 // each level smooths with a Chebyshev polynomial of point-block Jacobi (degree `degree`, interval
 // [lower b, b] with b = 1.1 lambda_max(D^-1 A) from power iterations at setup), the coarsest level
-// is approximated by a higher-degree Chebyshev polynomial over a wider interval, restriction is
+// is solved exactly with the inverse of its reduced matrix when it has at most kDenseMax unknowns
+// (assembled from the level's element Jacobians and inverted by Gauss-Jordan elimination on the
+// device at setup; one matrix-vector launch per V-cycle), else approximated by a higher-degree
+// Chebyshev polynomial over a wider interval, restriction is
 // the transpose of the prolongation (coarse vectors are unfolded before prolongation and the
 // restricted ones folded, so that both act in the solvers' reduced fault spaces), and the V-cycle
 // runs in FP64 or FP32 (FP32 operators with the cached per-cell tangent and FP32 vectors) while
@@ -29,6 +32,78 @@ namespace {
 constexpr int kMgRedBlocks = 296;
 
 enum MgScalar { M_RZ = 0, M_RZ_OLD, M_PQ, M_RR, M_ZROLD, M_COUNT };
+
+// Coarsest levels with at most this many unknowns are solved with their dense inverse.
+constexpr int kDenseMax = 1536;
+
+// dense[map[row dof]][map[col dof]] -= J block entry (A = -J; a fault node's two sides both land
+// on its negative-side unknown); one warp per block row of the mesh nodes (Lagrange rows are not
+// read), the entries' 9 components over the lanes.
+__global__ void k_dense_scatter(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const double* __restrict__ val, int64_t nmesh, const int32_t* __restrict__ map, int n,
+                                double* dense) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nmesh;
+         r += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t k0 = rp[r], k1 = rp[r + 1];
+        for (int64_t e = k0 * 9 + lane; e < k1 * 9; e += 32) {
+            const int64_t k = e / 9;
+            const int ab = (int)(e - 9 * k), a = ab / 3, b = ab - 3 * a;
+            const int64_t c = ci[k];
+            if (c >= nmesh) continue;
+            const int fi = map[3 * r + a], fj = map[3 * c + b];
+            if (fi >= 0 && fj >= 0) atomicAdd(&dense[(int64_t)fi * n + fj], -val[e]);
+        }
+    }
+}
+
+// Gauss-Jordan step k, part 1: row k and column k of the current matrix into row[], col[]; a
+// non-positive pivot (the reduced matrix is symmetric positive definite) sets *flag.
+__global__ void k_gj_take(const double* __restrict__ a, int n, int k, double* row, double* col, unsigned int* flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        row[i] = a[(int64_t)k * n + i];
+        col[i] = a[(int64_t)i * n + k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !(a[(int64_t)k * n + k] > 0.0)) atomicOr(flag, 1u);
+}
+
+// Gauss-Jordan step k, part 2 (in place, no pivoting): with p = a_kk, row k becomes row/p (its
+// diagonal 1/p) and every other row i becomes a_ij - a_ik a_kj / p (its column-k entry -a_ik / p).
+__global__ void k_gj_update(double* a, int n, int k, const double* __restrict__ row, const double* __restrict__ col) {
+    const double p = row[k];
+    const double inv = p != 0.0 ? 1.0 / p : 0.0;
+    const int64_t nn = (int64_t)n * n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / n), j = (int)(e - (int64_t)i * n);
+        const double rk = j == k ? 1.0 : row[j];
+        if (i == k) a[e] = rk * inv;
+        else a[e] = (j == k ? 0.0 : a[e]) - col[i] * rk * inv;
+    }
+}
+
+__global__ void k_dense_to_f32(const double* __restrict__ a, int64_t nn, float* out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = (float)a[e];
+}
+
+// z[idx[i]] = sum_j inv[i][j] r[idx[j]] (z zeroed before): each block stages the gathered right-
+// hand side in shared memory, one warp per row.
+template <typename T>
+__global__ void __launch_bounds__(256) k_dense_apply(const T* __restrict__ inv, const int32_t* __restrict__ idx, int n,
+                                                     const T* __restrict__ r, T* __restrict__ z) {
+    __shared__ T sr[kDenseMax];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) sr[j] = r[idx[j]];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int i = blockIdx.x * 8 + (threadIdx.x >> 5); i < n; i += gridDim.x * 8) {
+        const T* row = inv + (int64_t)i * n;
+        T acc = T(0);
+        for (int j = lane; j < n; j += 32) acc += row[j] * sr[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) z[idx[i]] = acc;
+    }
+}
 
 int mg_grid(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
@@ -248,6 +323,16 @@ struct pl_multigrid_s {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     unsigned long long graph_epoch = 0;
+    // dense solve of the coarsest level (dense_n: -1 not examined yet, 0 too large)
+    int dense_n = -1;
+    bool dense_ok = false;
+    int32_t* d_dense_idx = nullptr;  // [dense_n] DOF of each unknown
+    int32_t* d_dense_map = nullptr;  // [3 nmesh] unknown of each mesh DOF (-1: constrained)
+    double* d_dense = nullptr;       // [dense_n^2] matrix, inverted in place
+    float* d_dense32 = nullptr;
+    double* d_gj = nullptr;          // [2 dense_n] Gauss-Jordan row and column
+    unsigned int* d_flag = nullptr;
+    pl_matrix dense_A = nullptr;     // the coarsest level's assembled Jacobian
 };
 
 namespace {
@@ -292,7 +377,15 @@ int vcycle(pl_multigrid mg, int l) {
     T* w = f32 ? (T*)L.w32 : (T*)L.w;
     T* q = f32 ? (T*)L.q32 : (T*)L.q;
     const int last = (int)mg->lv.size() - 1;
-    if (l == last) return cheb<T>(mg, l, r, z, mg->coarse_degree, mg->coarse_lower);
+    if (l == last) {
+        if (!mg->dense_ok) return cheb<T>(mg, l, r, z, mg->coarse_degree, mg->coarse_lower);
+        PLB_CUDA(cudaMemsetAsync(z, 0, L.n * sizeof(T), s));
+        const T* inv = f32 ? (const T*)mg->d_dense32 : (const T*)mg->d_dense;
+        k_dense_apply<T><<<std::max(1, std::min((mg->dense_n + 7) / 8, 148)), 256, 0, s>>>(inv, mg->d_dense_idx,
+                                                                                             mg->dense_n, r, z);
+        count_launch();
+        return PL_OK;
+    }
     int rc = cheb<T>(mg, l, r, z, mg->degree, mg->lower);
     if (rc) return rc;
     auto apply = [&](T* v) { return f32 ? solver_apply_J32(L.S, (const float*)v, (float*)q) : solver_apply_J(L.S, (const double*)v, (double*)q); };
@@ -346,7 +439,9 @@ int precondition(pl_multigrid mg, const double* r, double* z) {
 // iterates are normalised on the device and the host reads one number per level.
 int estimate_eigenvalues(pl_multigrid mg, int iters = 12) {
     cudaStream_t s = mg_stream(mg);
-    for (MgLevel& L : mg->lv) {
+    for (size_t l = 0; l < mg->lv.size(); ++l) {
+        MgLevel& L = mg->lv[l];
+        if (l + 1 == mg->lv.size() && mg->dense_ok) break;  // solved exactly: no smoother
         k_mg_seed<<<kMgRedBlocks, kRedThreads, 0, s>>>(L.t, L.S->d_mask, L.n, mg->partials);
         k_finish2<<<1, 1024, 0, s>>>(mg->partials, kMgRedBlocks, mg->scal, M_RR, -1);
         k_mg_normalize<<<mg_grid(L.n), 256, 0, s>>>(L.t, L.t, L.n, mg->scal, M_RR);
@@ -367,6 +462,84 @@ int estimate_eigenvalues(pl_multigrid mg, int iters = 12) {
         L.lmax = lam;
     }
     mg->eig_valid = true;
+    return PL_OK;
+}
+
+// The coarsest level's dense inverse (after each setup): the unknowns' maps on first use, then the
+// reduced matrix from the level's assembled Jacobian and its Gauss-Jordan inverse. Levels with more
+// than kDenseMax unknowns, or a matrix that is not positive definite, keep the Chebyshev solve.
+int prepare_dense(pl_multigrid mg) {
+    MgLevel& L = mg->lv.back();
+    pl_solver S = L.S;
+    cudaStream_t s = mg_stream(mg);
+    mg->dense_ok = false;
+    if (mg->dense_n < 0) {
+        std::vector<uint8_t> mask(L.n);
+        std::vector<int32_t> pneg(S->npairs), ppos(S->npairs);
+        PLB_CUDA(cudaMemcpyAsync(mask.data(), S->d_mask, L.n, cudaMemcpyDeviceToHost, s));
+        if (S->npairs) {
+            PLB_CUDA(cudaMemcpyAsync(pneg.data(), S->d_pair_neg, S->npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            PLB_CUDA(cudaMemcpyAsync(ppos.data(), S->d_pair_pos, S->npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        }
+        PLB_CUDA(cudaStreamSynchronize(s));
+        std::vector<int32_t> fidx(L.n, -1), idx;
+        for (int64_t i = 0; i < L.n; ++i)
+            if (!mask[i]) {
+                fidx[i] = (int32_t)idx.size();
+                idx.push_back((int32_t)i);
+            }
+        if (idx.empty() || idx.size() > (size_t)kDenseMax) {
+            mg->dense_n = 0;
+            return PL_OK;
+        }
+        std::vector<int64_t> node_of(L.nmesh);
+        for (int64_t v = 0; v < L.nmesh; ++v) node_of[v] = v;
+        for (int64_t k = 0; k < S->npairs; ++k) node_of[ppos[k]] = pneg[k];
+        std::vector<int32_t> map(3 * L.nmesh);
+        for (int64_t i = 0; i < 3 * L.nmesh; ++i) map[i] = fidx[3 * node_of[i / 3] + i % 3];
+        const int n = (int)idx.size();
+        cudaError_t e = cudaMalloc((void**)&mg->d_dense_idx, n * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_dense_map, map.size() * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_dense, (size_t)n * n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_dense32, (size_t)n * n * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_gj, 2 * (size_t)n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_flag, sizeof(unsigned int));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(mg->d_dense_idx, idx.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(mg->d_dense_map, map.data(), map.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(e, "multigrid dense coarse solve");
+        int rc = pl_matrix_create(S->mesh, &mg->dense_A);
+        if (rc) return rc;
+        mg->dense_n = n;
+    }
+    if (mg->dense_n == 0) return PL_OK;
+    const int n = mg->dense_n;
+    int rc = pl_matrix_zero(mg->dense_A);
+    if (rc) return rc;
+    PLB_CUDA(cudaMemsetAsync(L.t, 0, L.n * sizeof(double), s));  // the state the Jacobian kernels read
+    for (pl_integrator ig : S->ops)
+        if ((rc = pl_compute_lhs_jacobian(ig, S->t, S->dt, 0.0, L.t, mg->dense_A)) != PL_OK) return rc;
+    PLB_CUDA(cudaMemsetAsync(mg->d_dense, 0, (size_t)n * n * sizeof(double), s));
+    PLB_CUDA(cudaMemsetAsync(mg->d_flag, 0, sizeof(unsigned int), s));
+    const pl_matrix_s& A = *mg->dense_A;
+    k_dense_scatter<<<mg_grid(32 * L.nmesh), 256, 0, s>>>(A.d_row_ptr, A.d_col, A.d_val, L.nmesh, mg->d_dense_map, n,
+                                                          mg->d_dense);
+    count_launch();
+    double* row = mg->d_gj;
+    double* col = mg->d_gj + n;
+    const int gt = std::max(1, std::min((n + 255) / 256, 8));
+    const int gu = mg_grid((int64_t)n * n);
+    for (int k = 0; k < n; ++k) {
+        k_gj_take<<<gt, 256, 0, s>>>(mg->d_dense, n, k, row, col, mg->d_flag);
+        k_gj_update<<<gu, 256, 0, s>>>(mg->d_dense, n, k, row, col);
+    }
+    count_launch(2 * n);
+    k_dense_to_f32<<<mg_grid((int64_t)n * n), 256, 0, s>>>(mg->d_dense, (int64_t)n * n, mg->d_dense32);
+    count_launch();
+    unsigned int flag = 0;
+    PLB_CUDA(cudaMemcpyAsync(&flag, mg->d_flag, sizeof(flag), cudaMemcpyDeviceToHost, s));
+    PLB_CUDA(cudaStreamSynchronize(s));
+    mg->dense_ok = flag == 0;
     return PL_OK;
 }
 
@@ -415,7 +588,7 @@ int multigrid_solve(pl_multigrid mg, const double* b, double* x) {
     cudaStream_t s0 = c->stream;
     const int64_t n = S->n;
     int rc;
-    if (!mg->eig_valid && (rc = estimate_eigenvalues(mg)) != PL_OK) return rc;
+    if (!mg->eig_valid && ((rc = prepare_dense(mg)) != PL_OK || (rc = estimate_eigenvalues(mg)) != PL_OK)) return rc;
     for (const MgLevel& L : mg->lv)
         for (pl_integrator ig : L.S->ops)
             if ((rc = prepare_jv32_tangent(ig, L.S->t, L.S->dt)) != PL_OK) return rc;
@@ -645,9 +818,11 @@ int pl_multigrid_destroy(pl_multigrid mg) {
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }
-    void* ptrs[] = {mg->x, mg->r, mg->r_old, mg->p, mg->q, mg->z, mg->scal, mg->partials};
+    void* ptrs[] = {mg->x, mg->r, mg->r_old, mg->p, mg->q, mg->z, mg->scal, mg->partials,
+                    mg->d_dense_idx, mg->d_dense_map, mg->d_dense, mg->d_dense32, mg->d_gj, mg->d_flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (mg->dense_A) pl_matrix_destroy(mg->dense_A);
     std::vector<pl_solver> coarse;
     for (size_t l = 1; l < mg->lv.size(); ++l) coarse.push_back(mg->lv[l].S);
     pl_context c = mg->ctx;

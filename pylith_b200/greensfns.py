@@ -66,6 +66,7 @@ class GreensFunctions:
         self.patches = patches
         self.impulses = [Impulse(p, c) for c in components for p in range(len(patches))]
         self.constrained = constrained
+        self.rtol = rtol
         self.solver64 = FA.Solver(self.dmesh, constrained, [self.domain], rtol=rtol)
         self.solver64.setup()
         self.solver32 = FA.Solver(self.dmesh, constrained, [self.domain], rtol=rtol,
@@ -75,6 +76,19 @@ class GreensFunctions:
         self.cheb_lower_ratio = cheb_lower_ratio
         if cheb_degree >= 2:
             self.batch.set_chebyshev(cheb_degree, cheb_lower_ratio)
+
+    def attach_multigrid(self, levels, material, precision=FA.Solver.FP32_REFINED, fault_x=0.0, rtol=None):
+        """A solver for one impulse at a time by FP64 flexible CG preconditioned with V-cycles (of
+        `precision`) over `levels` (pylith_b200.multigrid.build_tet_hierarchy of this mesh); returns
+        it (solve with method="multigrid" uses the last one attached)."""
+        from . import multigrid as MG
+
+        solver = FA.Solver(self.dmesh, self.constrained, [self.domain], rtol=rtol or self.rtol)
+        mg = MG.attach(self.ctx, solver, levels, material, fault_x=fault_x, precision=precision)
+        solver.setup()
+        self._mg_keep = getattr(self, "_mg_keep", []) + [(solver, mg)]
+        self.solver_mg = solver
+        return solver
 
     def impulse_rhs(self, imp: Impulse):
         """(u_slip, b): the displacement carrying unit slip on the patch, and b = F(u_slip)."""
@@ -122,8 +136,10 @@ class GreensFunctions:
         self.batch = best[3]
         return sorted(results, key=lambda r: -r[2])
 
-    def solve(self, impulses, batched=True):
-        """Solutions u = u_slip + du of the given impulses; returns (solutions, seconds)."""
+    def solve(self, impulses, batched=True, solver=None):
+        """Solutions u = u_slip + du of the given impulses; returns (solutions, seconds). batched:
+        the tiles of the batched FP32 solver; else one at a time with `solver` (default: the FP64
+        point-block Jacobi solver)."""
         import torch
 
         rhs = [self.impulse_rhs(imp) for imp in impulses]
@@ -133,8 +149,9 @@ class GreensFunctions:
         if batched:
             self.batch.solve([b for _, b in rhs], xs)
         else:
+            one = solver or self.solver64
             for (_, b), x in zip(rhs, xs):
-                self.solver64.solve(b, x)
+                one.solve(b, x)
         self.ctx.synchronize()
         dt = time.perf_counter() - t0
         return [u + x for (u, _), x in zip(rhs, xs)], dt

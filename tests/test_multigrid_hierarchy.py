@@ -17,7 +17,8 @@ def _side_linear(mesh):
 
 
 def test_levels_and_prolongation_with_a_fault():
-    levels = MG.build_hierarchy(16, 8, 12, fault_x=0.0, constrained_faces=[(0, "neg", (0,)), (2, "neg", (2,))])
+    levels = MG.build_hierarchy(16, 8, 12, fault_x=0.0, constrained_faces=[(0, "neg", (0,)), (2, "neg", (2,))],
+                                max_coarse_nodes=0)
     assert [lv.n for lv in levels] == [(16, 8, 12), (8, 4, 6), (4, 2, 3)]
     for (row, col, val), lf, lc in zip(MG.prolongations(levels, 0.0), levels[:-1], levels[1:]):
         P = sp.csr_matrix((val, col, row), shape=(lf.mesh.num_nodes, lc.mesh.num_nodes))
@@ -72,3 +73,37 @@ def test_non_nested_levels_keep_the_fault_plane():
         xf = lf.mesh.coords[lf.mesh.cells].mean(axis=1)[:, 0]
         xc = lc.mesh.coords[lc.mesh.cells].mean(axis=1)[:, 0]
         assert np.all(np.sign(xf) == np.sign(xc[lc.cell_map]))
+
+
+def test_tetrahedral_levels_interpolate_fields_linear_on_each_side():
+    """Unstructured P1 levels (independent Delaunay meshes of the same box and fault plane): the
+    interpolation at the fine nodes reproduces fields linear on each side of the fault with any
+    jump across it, uses non-negative weights summing to one, keeps box-face and fault-plane nodes
+    on their face's coarse nodes, and the cell averaging preserves constants."""
+    from pylith_b200 import meshing as M
+
+    lo, hi = (-6000.0, -6000.0, -9000.0), (6000.0, 6000.0, 0.0)
+    fine = M.box_tet_delaunay_fault_x(40000, seed=0, lo=lo, hi=hi)
+    levels = MG.build_tet_hierarchy(fine, lambda n, l: M.box_tet_delaunay_fault_x(n, seed=l, lo=lo, hi=hi),
+                                    fault_x=0.0, lo=lo, hi=hi, constrained_faces=[(0, "neg", (0, 1, 2))],
+                                    min_cells=100)
+    assert len(levels) >= 3
+    for (row, col, val), lf, lc in zip(MG.prolongations(levels, 0.0), levels[:-1], levels[1:]):
+        P = sp.csr_matrix((val, col, row), shape=(lf.mesh.num_nodes, lc.mesh.num_nodes))
+        np.testing.assert_allclose(np.asarray(P.sum(axis=1)).ravel(), 1.0, rtol=1e-12)
+        assert val.min() > 0.0
+        X = lf.mesh.coords
+        f = lambda m: (m.coords @ np.array([2.0, -3.0, 0.5])  # noqa: E731
+                       + np.where(MG.node_sides(m, 0.0) > 0, 1000.0, 0.0))
+        np.testing.assert_allclose(P @ f(lc.mesh), f(lf.mesh), rtol=0, atol=1e-7)
+        # nodes on the face x = lo take weights from coarse nodes on that face only
+        face_f = np.isclose(X[:, 0], lo[0])
+        face_c = np.isclose(lc.mesh.coords[:, 0], lo[0])
+        rows = np.repeat(np.arange(lf.mesh.num_nodes), np.diff(row))
+        assert face_c[col[face_f[rows]]].all()
+        # fault-plane copies interpolate from coarse copies of their own side
+        sf, sc = MG.node_sides(lf.mesh, 0.0), MG.node_sides(lc.mesh, 0.0)
+        assert np.array_equal(sf[rows], sc[col])
+        W = lc.cell_map
+        assert W.shape == (lc.mesh.num_cells, lf.mesh.num_cells)
+        np.testing.assert_allclose(MG.coarsen_cells(np.full(lf.mesh.num_cells, 2.5), W), 2.5)
