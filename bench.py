@@ -829,8 +829,13 @@ def config_c3(args):
     # Jacobi of degree 2-3) on a sample of 32 impulses
     step = max(1, len(usable) // 32)
     table = g.autotune(usable[step // 2::step][:32], tiles=(8, 16), degrees=(0, 2, 3))
-    mg32 = g.attach_multigrid(levels, mat, FA.Solver.FP32_REFINED)
     mg64 = g.attach_multigrid(levels, mat, FA.Solver.FP64)
+    mg64_h = g.mg
+    mg32 = g.attach_multigrid(levels, mat, FA.Solver.FP32_REFINED)
+    # the smoothing of the FP32 V-cycles, picked on a sample of 6 impulses (the FP64 multigrid
+    # baseline takes the same)
+    mg_table = g.tune_multigrid(usable[step // 2::step][:6])
+    mg64_h.set_smoother(g.mg.degree, g.mg.lower)
     g.solve(usable[:8], batched=True)  # warm-up
     g.solve(usable[:1], batched=False)
     g.solve(usable[:2], batched=False, solver=mg32)
@@ -870,6 +875,9 @@ def config_c3(args):
                         "last_call_stats": st_b},
             "autotune": [{"tile": t, "chebyshev_degree": d, "solves_per_s": r} for t, d, r in table],
             "multigrid_fp32_vcycles": {"solves_per_s": rate_m, "seconds": t_m, "iterations_last": its_m[-1],
+                                       "smoother": {"degree": g.mg.degree, "lower_ratio": g.mg.lower},
+                                       "smoother_tuning": [{"degree": d, "lower_ratio": lo, "solves_per_s": r,
+                                                            "iterations": it} for d, lo, r, it in mg_table],
                                        "how": "one impulse at a time: FP64 flexible CG, one FP32 V-cycle "
                                               "(Chebyshev-Jacobi smoothing) per iteration"},
             "fp64_one_at_a_time": {"sample": len(sample_s), "solves_per_s": rate_s, "iterations_last": its_s,
@@ -886,7 +894,7 @@ def config_c4(args):
     """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
     material, random rectangular left-lateral slip patch of 0.1-3 m. Server (HBM-budget admission;
     small boxes in one ragged batch of FP32-refined solves, boxes of 32^3 and more with a multigrid
-    hierarchy solved beside it with FP32 V-cycles) vs the plain FP64 one-at-a-time path (point-block
+    hierarchy solved beside it by two workers with FP32 V-cycles) vs the plain FP64 one-at-a-time path (point-block
     Jacobi), and vs FP64 one at a time with FP64 multigrid. The requests' host-side meshes (and
     multigrid hierarchies) are built before the stream starts, for all."""
     from pylith_b200 import feassemble as FA
@@ -899,7 +907,11 @@ def config_c4(args):
     t_host = time.perf_counter() - t0
     warm = [SV.prepare(SV.Request(0, n, 1, 0.0, 1.0, (0.2, 0.8, 0.2, 0.8))) for n in (8, 32)]
     SV.Server(slots=64).run(warm)  # warm-up: device code loading and the first graph captures
-    server = SV.Server(slots=64)
+    variants = {}
+    for k in (1, 3):
+        sv = SV.Server(slots=64, multigrid_workers=k)
+        variants[k] = SV.summarize(sv.run(hps))["solves_per_s"]
+    server = SV.Server(slots=64, multigrid_workers=2)
     served = server.run(hps)
     seq = SV.serve_sequential(hps)
     seq_mg = SV.serve_sequential(hps, multigrid=FA.Solver.FP64)
@@ -910,11 +922,14 @@ def config_c4(args):
             "solves_per_s_ratio": a["solves_per_s"] / b["solves_per_s"],
             "fp64_multigrid_one_at_a_time": c, "solves_per_s_ratio_vs_fp64_multigrid": a["solves_per_s"] / c["solves_per_s"],
             "routes": {"ragged_batch": routes.count("batch"), "multigrid": routes.count("multigrid")},
+            "multigrid_workers": server.multigrid_workers, "workers": server.workers,
+            "solves_per_s_with_multigrid_workers": {str(k): v for k, v in variants.items()},
             "host_mesh_build_s_excluded": t_host,
             "admission_bytes": {"predicted_total_batch": float(mem[:, 0].sum()), "measured_total_batch": float(mem[:, 1].sum()),
                                 "how": "predicted: estimate_bytes(n) formula used for admission; measured: free device "
                                        "memory before and after each batched request's build (approximate: the "
-                                       "multigrid worker allocates concurrently)"}}
+                                       "multigrid workers allocate concurrently, and the library's memory pool keeps "
+                                       "freed memory for reuse)"}}
 
 
 CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c4": config_c4}

@@ -1175,7 +1175,7 @@ static int build_blocked_layout(pl_mesh_s* m) {
     auto up = [&](auto** dst, const auto& v) {
         if (e != cudaSuccess || v.empty()) return;
         const size_t bytes = v.size() * sizeof(v[0]);
-        e = cudaMalloc((void**)dst, bytes);
+        e = dev_alloc((void**)dst, bytes);
         if (e == cudaSuccess) e = cudaMemcpyAsync(*dst, v.data(), bytes, cudaMemcpyHostToDevice, s);
         L->device_bytes += bytes;
     };
@@ -1194,7 +1194,7 @@ static int build_blocked_layout(pl_mesh_s* m) {
     up(&L->d_pipe_inc, pinc);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
-        free_blocked_layout(L);
+        free_blocked_layout(L, s);
         return cuda_fail(e, "blocked layout upload");
     }
     m->blocked = L;
@@ -1211,21 +1211,12 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     }
 }
 
-void free_blocked_layout(BlockedLayout* b) {
+void free_blocked_layout(BlockedLayout* b, cudaStream_t after) {
     if (!b) return;
-    cudaFree(b->d_block_node_begin);
-    cudaFree(b->d_slot_node);
-    cudaFree(b->d_local_cells);
-    cudaFree(b->d_inc_off);
-    cudaFree(b->d_inc);
-    cudaFree(b->d_fix_node);
-    cudaFree(b->d_fix_off);
-    cudaFree(b->d_fix_slot);
-    cudaFree(b->d_pipe_begin);
-    cudaFree(b->d_pipe_ids);
-    cudaFree(b->d_pipe_coords);
-    cudaFree(b->d_pipe_off);
-    cudaFree(b->d_pipe_inc);
+    void* ptrs[] = {b->d_block_node_begin, b->d_slot_node, b->d_local_cells, b->d_inc_off, b->d_inc,
+                    b->d_fix_node, b->d_fix_off, b->d_fix_slot, b->d_pipe_begin, b->d_pipe_ids,
+                    b->d_pipe_coords, b->d_pipe_off, b->d_pipe_inc};
+    for (void* p : ptrs) dev_free(p, after);
     delete b;
 }
 

@@ -61,22 +61,100 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+
+cudaMemPool_t device_pool(int dev) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+        // keep up to 4 GiB of freed memory for reuse; never make an allocation wait on another
+        // stream's frees (reuse only what is already free)
+        uint64_t keep = 4ull << 30;
+        int no = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+        g_pools[dev] = pool;
+    }
+    return g_pools[dev];
+}
+
+// The calling thread's allocation stream on `dev` (one per thread, so that one thread's pending
+// frees never hold up another thread's allocations).
+cudaStream_t thread_alloc_stream(int dev) {
+    thread_local cudaStream_t streams[kMaxDevices] = {};
+    if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    return streams[dev];
+}
+
+}  // namespace
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool = device_pool(dev);
+    cudaStream_t s = thread_alloc_stream(dev);
+    if (!pool || !s) return cudaErrorNotSupported;
+    e = cudaMallocFromPoolAsync(p, bytes, pool, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+}
+
+void dev_free(void* p, cudaStream_t after) {
+    if (!p) return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return;
+    cudaStream_t s = thread_alloc_stream(dev);
+    if (after) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(after, &cap);
+        if (cap != cudaStreamCaptureStatusNone) return;  // no ordering is possible during a capture: keep it
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(ev, after);
+            cudaStreamWaitEvent(s, ev, 0);
+            cudaEventDestroy(ev);
+        } else {
+            cudaStreamSynchronize(after);
+        }
+    }
+    cudaFreeAsync(p, s);
+}
+
+void dev_pool_trim(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (device >= 0 && device < kMaxDevices && g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
+}
+
 int cuda_fail(cudaError_t e, const char* what) {
     g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? PL_ERR_OUT_OF_MEMORY : PL_ERR_CUDA;
 }
 
 template <typename T>
-static int dev_alloc(T** p, size_t count) {
+static int alloc_n(T** p, size_t count) {
     *p = nullptr;
     if (count == 0) return PL_OK;
-    PLB_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
+    PLB_CUDA(dev_alloc(p, count));
     return PL_OK;
 }
 
 template <typename T>
 static int upload(T** p, const T* host, size_t count, cudaStream_t s) {
-    int rc = dev_alloc(p, count);
+    int rc = alloc_n(p, count);
     if (rc) return rc;
     if (count) PLB_CUDA(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
     return PL_OK;
@@ -218,12 +296,13 @@ int pl_context_create(int device, pl_context* out) {
         return cuda_fail(e, "cudaStreamCreate");
     }
     c->stream = c->own_stream;
-    e = cudaMalloc((void**)&c->d_err, sizeof(unsigned int));
-    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(unsigned int));
+    e = dev_alloc(&c->d_err, 1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_err, 0, sizeof(unsigned int), c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
         cudaStreamDestroy(c->own_stream);
         delete c;
-        return cuda_fail(e, "cudaMalloc(error word)");
+        return cuda_fail(e, "device memory for the error word");
     }
     *out = c;
     return PL_OK;
@@ -232,10 +311,11 @@ int pl_context_create(int device, pl_context* out) {
 static void context_free(pl_context c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    if (c->d_err) cudaFree(c->d_err);
-    if (c->d_stage) cudaFree(c->d_stage);
+    dev_free(c->d_err, c->stream);
+    dev_free(c->d_stage, c->stream);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    dev_pool_trim(c->device);
     delete c;
 }
 
@@ -324,7 +404,7 @@ int pl_mesh_set_cohesive(pl_mesh m, int64_t ncoh, const int32_t* coh, int64_t nl
             if (v < 0 || v >= lim) return fail(PL_ERR_INVALID_ARG, "cohesive cell index out of range");
         }
     PLB_CUDA(cudaSetDevice(m->ctx->device));
-    if (m->d_coh) cudaFree(m->d_coh);
+    dev_free(m->d_coh, m->ctx->stream);
     m->d_coh = nullptr;
     m->ncoh = ncoh;
     m->nlag = nlag;
@@ -340,10 +420,10 @@ static void mesh_free(pl_mesh m) {
     pl_context c = m->ctx;
     cudaSetDevice(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
-    if (m->d_cells) cudaFree(m->d_cells);
-    if (m->d_coords) cudaFree(m->d_coords);
-    if (m->d_coh) cudaFree(m->d_coh);
-    if (m->blocked) free_blocked_layout(m->blocked);
+    dev_free(m->d_cells, m->ctx->stream);
+    dev_free(m->d_coords, m->ctx->stream);
+    dev_free(m->d_coh, m->ctx->stream);
+    if (m->blocked) free_blocked_layout(m->blocked, m->ctx->stream);
     delete m;
     if (--c->refs == 0 && c->destroy_requested) context_free(c);
 }
@@ -558,7 +638,7 @@ int pl_integrator_set_aux(pl_integrator ig, const char* name, int storage, int n
     for (AuxField& a : ig->aux)
         if (a.name == name) f = &a;
     if (f && (f->ncomp != ncomp || f->storage != storage)) {
-        cudaFree(f->d);
+        dev_free(f->d, m->ctx->stream);
         f->d = nullptr;
     }
     if (!f) {
@@ -569,7 +649,7 @@ int pl_integrator_set_aux(pl_integrator ig, const char* name, int storage, int n
     f->storage = storage;
     f->ncomp = ncomp;
     if (!f->d) {
-        int rc = dev_alloc(&f->d, count);
+        int rc = alloc_n(&f->d, count);
         if (rc) return rc;
     }
     PLB_CUDA(cudaMemcpyAsync(f->d, dev.data(), count * sizeof(double), cudaMemcpyHostToDevice, m->ctx->stream));
@@ -619,11 +699,11 @@ int pl_integrator_set_scatter(pl_integrator ig, int scatter) {
 static void integrator_free(pl_integrator ig) {
     cudaSetDevice(ig->mesh->ctx->device);
     cudaStreamSynchronize(ig->mesh->ctx->stream);
-    for (AuxField& f : ig->aux)
-        if (f.d) cudaFree(f.d);
-    if (ig->d_cell_ids) cudaFree(ig->d_cell_ids);
-    if (ig->d_block_partial) cudaFree(ig->d_block_partial);
-    if (ig->d_lm32) cudaFree(ig->d_lm32);
+    cudaStream_t s = ig->mesh->ctx->stream;
+    for (AuxField& f : ig->aux) dev_free(f.d, s);
+    dev_free(ig->d_cell_ids, s);
+    dev_free(ig->d_block_partial, s);
+    dev_free(ig->d_lm32, s);
     pl_mesh m = ig->mesh;
     delete ig;
     mesh_release(m);
@@ -661,7 +741,7 @@ int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt) {
     if (rc) return rc;
     p.t = t;
     p.dt = dt;
-    if (!ig->d_lm32 && ig->ncells > 0) PLB_CUDA(cudaMalloc((void**)&ig->d_lm32, 2 * ig->ncells * sizeof(float)));
+    if (!ig->d_lm32 && ig->ncells > 0) PLB_CUDA(dev_alloc(&ig->d_lm32, 2 * ig->ncells));
     launch_tangent_lm32(p, rheo, ig->d_lm32, m->ctx->stream);
     PLB_CUDA(cudaGetLastError());
     ig->lm32_valid = true;
@@ -675,7 +755,7 @@ int prepare_blocked(pl_integrator_s* ig) {
     int rc = ensure_blocked_layout(m);
     if (rc) return rc;
     if (ig->scatter == PL_SCATTER_DETERMINISTIC && !ig->d_block_partial && m->blocked->num_slots > 0)
-        PLB_CUDA(cudaMalloc((void**)&ig->d_block_partial, 3 * m->blocked->num_slots * sizeof(double)));
+        PLB_CUDA(dev_alloc(&ig->d_block_partial, 3 * m->blocked->num_slots));
     return PL_OK;
 }
 }  // namespace plb
@@ -831,10 +911,10 @@ int pl_compute_lhs_residual_host(pl_integrator ig, double t, double dt, const do
     const size_t bytes = 2 * n * sizeof(double);
     PLB_CUDA(cudaSetDevice(c->device));
     if (c->d_stage_bytes < bytes) {
-        if (c->d_stage) cudaFree(c->d_stage);
+        dev_free(c->d_stage, c->stream);
         c->d_stage = nullptr;
         c->d_stage_bytes = 0;
-        PLB_CUDA(cudaMalloc((void**)&c->d_stage, bytes));
+        PLB_CUDA(dev_alloc((void**)&c->d_stage, bytes));
         c->d_stage_bytes = bytes;
     }
     double* du = c->d_stage;

@@ -92,7 +92,7 @@ int pl_halo_create(pl_context ctx, int npeers, const int64_t* counts, const int3
     cudaError_t e = cudaSetDevice(ctx->device);
     auto up = [&](int32_t** dst, const int32_t* src, size_t n) {
         if (e != cudaSuccess || n == 0) return;
-        e = cudaMalloc((void**)dst, n * sizeof(int32_t));
+        e = dev_alloc(dst, n);
         if (e == cudaSuccess) e = cudaMemcpy(*dst, src, n * sizeof(int32_t), cudaMemcpyHostToDevice);
     };
     up(&h->d_nodes, nodes_host, (size_t)total);
@@ -100,10 +100,7 @@ int pl_halo_create(pl_context ctx, int npeers, const int64_t* counts, const int3
     up(&h->d_off, off.data(), off.size());
     up(&h->d_pos, pos.data(), pos.size());
     if (e != cudaSuccess) {
-        cudaFree(h->d_nodes);
-        cudaFree(h->d_unique);
-        cudaFree(h->d_off);
-        cudaFree(h->d_pos);
+        for (void* p : {(void*)h->d_nodes, (void*)h->d_unique, (void*)h->d_off, (void*)h->d_pos}) dev_free(p, nullptr);
         delete h;
         return cuda_fail(e, "pl_halo_create");
     }
@@ -160,10 +157,7 @@ int pl_halo_destroy(pl_halo h) {
     if (!h) return PL_OK;
     cudaSetDevice(h->ctx->device);
     cudaStreamSynchronize(h->ctx->stream);
-    cudaFree(h->d_nodes);
-    cudaFree(h->d_unique);
-    cudaFree(h->d_off);
-    cudaFree(h->d_pos);
+    for (void* p : {(void*)h->d_nodes, (void*)h->d_unique, (void*)h->d_off, (void*)h->d_pos}) dev_free(p, h->ctx->stream);
     pl_context c = h->ctx;
     delete h;
     context_release(c);

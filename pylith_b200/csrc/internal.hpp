@@ -42,6 +42,22 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
+// Device memory of the library's objects comes from a stream-ordered pool per device: creating
+// and destroying meshes, integrators and solvers then neither maps memory nor synchronises the
+// device (cudaMalloc and cudaFree do both), which matters when one process builds and drops
+// problems on several streams at once. dev_alloc returns memory ready for use on any stream;
+// dev_free returns p to the pool once the work enqueued on `after` so far has completed (pass the
+// object's context stream: a call's work on private streams is joined into it before the call
+// returns), without blocking the host.
+cudaError_t dev_alloc(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t dev_alloc(T** p, size_t count) {
+    return dev_alloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+void dev_free(void* p, cudaStream_t after);
+// Releases the pool memory of `device` that no allocation holds.
+void dev_pool_trim(int device);
+
 #define PLB_CUDA(call)                                             \
     do {                                                           \
         cudaError_t _e = (call);                                   \

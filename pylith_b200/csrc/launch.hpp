@@ -46,7 +46,7 @@ struct DerivedSpec {
 void launch_domain_derived(const DomainParams& p, int cell, int rheo, const DerivedSpec& spec, cudaStream_t s);
 // Builds (once per mesh) the cell-block layout used by the blocked scatter.
 int ensure_blocked_layout(pl_mesh_s* m);
-void free_blocked_layout(BlockedLayout* b);
+void free_blocked_layout(BlockedLayout* b, cudaStream_t after);
 // Cell-block (shared-memory, deterministic) residual / Jacobian action; returns false when the
 // layout does not support the configuration.
 bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell,

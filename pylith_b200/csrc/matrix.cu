@@ -117,11 +117,11 @@ int pl_matrix_create(pl_mesh m, pl_matrix* out) {
     A->nrows = nrows;
     A->nnzb = (int64_t)ci.size();
     cudaStream_t s = m->ctx->stream;
-    cudaError_t e = cudaMalloc((void**)&A->d_row_ptr, rp.size() * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&A->d_col, ci.size() * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&A->d_val, ci.size() * 9 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&A->d_cell_pos, cpos.size() * sizeof(int32_t));
-    if (e == cudaSuccess && !hpos.empty()) e = cudaMalloc((void**)&A->d_coh_pos, hpos.size() * sizeof(int32_t));
+    cudaError_t e = dev_alloc(&A->d_row_ptr, rp.size());
+    if (e == cudaSuccess) e = dev_alloc(&A->d_col, ci.size());
+    if (e == cudaSuccess) e = dev_alloc(&A->d_val, ci.size() * 9);
+    if (e == cudaSuccess) e = dev_alloc(&A->d_cell_pos, cpos.size());
+    if (e == cudaSuccess && !hpos.empty()) e = dev_alloc(&A->d_coh_pos, hpos.size());
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->d_row_ptr, rp.data(), rp.size() * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->d_col, ci.data(), ci.size() * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(A->d_cell_pos, cpos.data(), cpos.size() * 4, cudaMemcpyHostToDevice, s);
@@ -216,11 +216,9 @@ int pl_matrix_destroy(pl_matrix A) {
     if (!A) return PL_OK;
     cudaSetDevice(A->mesh->ctx->device);
     cudaStreamSynchronize(A->mesh->ctx->stream);
-    if (A->d_row_ptr) cudaFree(A->d_row_ptr);
-    if (A->d_col) cudaFree(A->d_col);
-    if (A->d_val) cudaFree(A->d_val);
-    if (A->d_cell_pos) cudaFree(A->d_cell_pos);
-    if (A->d_coh_pos) cudaFree(A->d_coh_pos);
+    cudaStream_t s = A->mesh->ctx->stream;
+    for (void* p : {(void*)A->d_row_ptr, (void*)A->d_col, (void*)A->d_val, (void*)A->d_cell_pos, (void*)A->d_coh_pos})
+        dev_free(p, s);
     pl_mesh m = A->mesh;
     delete A;
     mesh_release(m);

@@ -290,6 +290,68 @@ __global__ void k_mg_pupdate(double* __restrict__ p, const double* __restrict__ 
 
 __global__ void k_mg_copy_scalar(double* scal, int from, int to) { scal[to] = scal[from]; }
 
+// ---- restriction = transpose of the prolongation, built on the device -------------------------
+// Entries per coarse node (cnt zeroed before).
+__global__ void k_tr_count(const int32_t* __restrict__ col, int64_t nnz, int32_t* cnt) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnz; j += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[col[j]], 1);
+}
+
+// out[0] = 0, out[i + 1] = cnt[0] + .. + cnt[i] (one block of 1024 threads, each summing a
+// contiguous run).
+__global__ void __launch_bounds__(1024) k_tr_scan(const int32_t* __restrict__ cnt, int64_t n, int32_t* out) {
+    __shared__ int32_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t per = (n + 1023) / 1024, a = t * per, b = std::min<int64_t>(n, a + per);
+    int32_t sum = 0;
+    for (int64_t i = a; i < b; ++i) sum += cnt[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int32_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int32_t run = t > 0 ? part[t - 1] : 0;
+    if (t == 0) out[0] = 0;
+    for (int64_t i = a; i < b; ++i) {
+        run += cnt[i];
+        out[i + 1] = run;
+    }
+}
+
+// Scatter of every prolongation entry (fine row f, coarse col c) into coarse row c (fill zeroed).
+__global__ void k_tr_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ col, const double* __restrict__ val,
+                          int64_t nf, const int32_t* __restrict__ rrow, int32_t* fill, int32_t* rcol, double* rval) {
+    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nf; f += (int64_t)gridDim.x * blockDim.x)
+        for (int32_t j = rp[f]; j < rp[f + 1]; ++j) {
+            const int32_t c = col[j];
+            const int32_t pos = rrow[c] + atomicAdd(&fill[c], 1);
+            rcol[pos] = (int32_t)f;
+            rval[pos] = val[j];
+        }
+}
+
+// Each coarse row's entries in increasing fine row (the order the atomics left is arbitrary).
+__global__ void k_tr_sort(const int32_t* __restrict__ rrow, int64_t nc, int32_t* rcol, double* rval) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t a = rrow[c], b = rrow[c + 1];
+        for (int32_t i = a + 1; i < b; ++i) {
+            const int32_t k = rcol[i];
+            const double v = rval[i];
+            int32_t j = i - 1;
+            while (j >= a && rcol[j] > k) {
+                rcol[j + 1] = rcol[j];
+                rval[j + 1] = rval[j];
+                --j;
+            }
+            rcol[j + 1] = k;
+            rval[j + 1] = v;
+        }
+    }
+}
+
 }  // namespace
 }  // namespace plb
 
@@ -498,12 +560,12 @@ int prepare_dense(pl_multigrid mg) {
         std::vector<int32_t> map(3 * L.nmesh);
         for (int64_t i = 0; i < 3 * L.nmesh; ++i) map[i] = fidx[3 * node_of[i / 3] + i % 3];
         const int n = (int)idx.size();
-        cudaError_t e = cudaMalloc((void**)&mg->d_dense_idx, n * sizeof(int32_t));
-        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_dense_map, map.size() * sizeof(int32_t));
-        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_dense, (size_t)n * n * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_dense32, (size_t)n * n * sizeof(float));
-        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_gj, 2 * (size_t)n * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc((void**)&mg->d_flag, sizeof(unsigned int));
+        cudaError_t e = dev_alloc(&mg->d_dense_idx, n);
+        if (e == cudaSuccess) e = dev_alloc(&mg->d_dense_map, map.size());
+        if (e == cudaSuccess) e = dev_alloc(&mg->d_dense, (size_t)n * n);
+        if (e == cudaSuccess) e = dev_alloc(&mg->d_dense32, (size_t)n * n);
+        if (e == cudaSuccess) e = dev_alloc(&mg->d_gj, 2 * (size_t)n);
+        if (e == cudaSuccess) e = dev_alloc(&mg->d_flag, 1);
         if (e == cudaSuccess) e = cudaMemcpyAsync(mg->d_dense_idx, idx.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(mg->d_dense_map, map.data(), map.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
@@ -693,11 +755,12 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
     pl_multigrid mg = new pl_multigrid_s();
     cudaError_t e = cudaSuccess;
     auto A = [&](auto** p, size_t cnt) {
-        if (e == cudaSuccess && cnt) e = cudaMalloc((void**)p, cnt * sizeof(**p));
+        if (e == cudaSuccess && cnt) e = dev_alloc(p, cnt);
     };
     auto up = [&](auto** p, const auto* src, size_t cnt) {
         A(p, cnt);
-        if (e == cudaSuccess && cnt) e = cudaMemcpy(*p, src, cnt * sizeof(*src), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && cnt)
+            e = cudaMemcpyAsync(*p, src, cnt * sizeof(*src), cudaMemcpyHostToDevice, fine->mesh->ctx->stream);
     };
     for (size_t l = 0; l < levels.size(); ++l) {
         MgLevel L;
@@ -709,44 +772,48 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
         A(&L.r32, L.n); A(&L.z32, L.n); A(&L.t32, L.n); A(&L.d32, L.n); A(&L.w32, L.n); A(&L.q32, L.n);
         mg->lv.push_back(L);
     }
+    cudaStream_t s = fine->mesh->ctx->stream;
+    int32_t* d_tmp = nullptr;  // per coarse node: counts, then fill positions
     for (int l = 0; l < num_coarse && e == cudaSuccess; ++l) {
         MgLevel& F = mg->lv[l];
         const MgLevel& C = mg->lv[l + 1];
         const int32_t* rp = prolong_row_ptr[l];
         const int64_t nf = F.nmesh, nc = C.nmesh;
         const int64_t nnz = rp[nf];
-        std::vector<int32_t> rrow(nc + 1, 0), rcol(nnz);
-        std::vector<double> rval(nnz);
-        bool ok = rp[0] == 0;
-        for (int64_t f = 0; f < nf && ok; ++f)
-            for (int32_t j = rp[f]; j < rp[f + 1]; ++j) {
-                const int32_t cc = prolong_col[l][j];
-                if (cc < 0 || cc >= nc) ok = false;
-                else rrow[cc + 1]++;
-            }
+        bool ok = rp[0] == 0 && nnz >= 0;
+        for (int64_t f = 0; f < nf && ok; ++f) ok = rp[f + 1] >= rp[f];
+        for (int64_t j = 0; j < nnz && ok; ++j) ok = prolong_col[l][j] >= 0 && prolong_col[l][j] < nc;
         if (!ok) {
             for (MgLevel& L : mg->lv) {
                 void* ptrs[] = {L.r, L.z, L.t, L.d, L.w, L.q, L.r32, L.z32, L.t32, L.d32, L.w32, L.q32, L.p_row, L.p_col, L.p_val,
                                 L.r_row, L.r_col, L.r_val};
-                for (void* p : ptrs) cudaFree(p);
+                for (void* p : ptrs) dev_free(p, nullptr);
             }
             delete mg;
             return fail(PL_ERR_INVALID_ARG, "prolongation column outside the coarse level");
         }
-        for (int64_t cc = 0; cc < nc; ++cc) rrow[cc + 1] += rrow[cc];
-        std::vector<int32_t> pos(rrow.begin(), rrow.end() - 1);
-        for (int64_t f = 0; f < nf; ++f)
-            for (int32_t j = rp[f]; j < rp[f + 1]; ++j) {
-                const int32_t cc = prolong_col[l][j];
-                rcol[pos[cc]] = (int32_t)f;
-                rval[pos[cc]++] = prolong_val[l][j];
-            }
         up(&F.p_row, rp, (size_t)nf + 1);
         up(&F.p_col, prolong_col[l], (size_t)nnz);
         up(&F.p_val, prolong_val[l], (size_t)nnz);
-        up(&F.r_row, rrow.data(), rrow.size());
-        up(&F.r_col, rcol.data(), rcol.size());
-        up(&F.r_val, rval.data(), rval.size());
+        // the restriction P^T, its rows in increasing fine index
+        A(&F.r_row, (size_t)nc + 1);
+        A(&F.r_col, (size_t)nnz);
+        A(&F.r_val, (size_t)nnz);
+        if (e == cudaSuccess) e = dev_alloc(&d_tmp, (size_t)nc);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_tmp, 0, nc * sizeof(int32_t), s);
+        if (e == cudaSuccess && nnz > 0) {
+            k_tr_count<<<mg_grid(nnz), 256, 0, s>>>(F.p_col, nnz, d_tmp);
+            k_tr_scan<<<1, 1024, 0, s>>>(d_tmp, nc, F.r_row);
+            e = cudaMemsetAsync(d_tmp, 0, nc * sizeof(int32_t), s);
+            k_tr_fill<<<mg_grid(nf), 256, 0, s>>>(F.p_row, F.p_col, F.p_val, nf, F.r_row, d_tmp, F.r_col, F.r_val);
+            k_tr_sort<<<mg_grid(nc), 256, 0, s>>>(F.r_row, nc, F.r_col, F.r_val);
+            count_launch(4);
+        } else if (e == cudaSuccess) {
+            e = cudaMemsetAsync(F.r_row, 0, (nc + 1) * sizeof(int32_t), s);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        dev_free(d_tmp, s);
+        d_tmp = nullptr;
     }
     const int64_t n = fine->n;
     A(&mg->x, n); A(&mg->r, n); A(&mg->r_old, n); A(&mg->p, n); A(&mg->q, n); A(&mg->z, n);
@@ -756,10 +823,10 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
         for (MgLevel& L : mg->lv) {
             void* ptrs[] = {L.r, L.z, L.t, L.d, L.w, L.q, L.r32, L.z32, L.t32, L.d32, L.w32, L.q32, L.p_row, L.p_col, L.p_val,
                             L.r_row, L.r_col, L.r_val};
-            for (void* p : ptrs) cudaFree(p);
+            for (void* p : ptrs) dev_free(p, s);
         }
         void* ptrs[] = {mg->x, mg->r, mg->r_old, mg->p, mg->q, mg->z, mg->scal, mg->partials};
-        for (void* p : ptrs) cudaFree(p);
+        for (void* p : ptrs) dev_free(p, s);
         delete mg;
         return cuda_fail(e, "pl_multigrid_create");
     }
@@ -815,13 +882,11 @@ int pl_multigrid_destroy(pl_multigrid mg) {
     for (MgLevel& L : mg->lv) {
         void* ptrs[] = {L.r, L.z, L.t, L.d, L.w, L.q, L.r32, L.z32, L.t32, L.d32, L.w32, L.q32, L.p_row, L.p_col, L.p_val,
                         L.r_row, L.r_col, L.r_val};
-        for (void* p : ptrs)
-            if (p) cudaFree(p);
+        for (void* p : ptrs) dev_free(p, mg->ctx ? mg->ctx->stream : nullptr);
     }
     void* ptrs[] = {mg->x, mg->r, mg->r_old, mg->p, mg->q, mg->z, mg->scal, mg->partials,
                     mg->d_dense_idx, mg->d_dense_map, mg->d_dense, mg->d_dense32, mg->d_gj, mg->d_flag};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (void* p : ptrs) dev_free(p, mg->ctx ? mg->ctx->stream : nullptr);
     if (mg->dense_A) pl_matrix_destroy(mg->dense_A);
     std::vector<pl_solver> coarse;
     for (size_t l = 1; l < mg->lv.size(); ++l) coarse.push_back(mg->lv[l].S);

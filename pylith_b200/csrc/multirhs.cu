@@ -1475,7 +1475,7 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     solver_retain(base);
     cudaError_t e = cudaSuccess;
     auto A = [&](auto** p, size_t cnt) {
-        if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(**p));
+        if (e == cudaSuccess) e = dev_alloc(p, cnt);
     };
     const size_t nk = (size_t)B->n * tile;
     A(&B->r, nk); A(&B->z, nk); A(&B->p, nk); A(&B->q, nk); A(&B->x, nk);
@@ -1561,10 +1561,10 @@ int pl_batch_solver_set_chebyshev(pl_batch_solver B, int degree, double lower_ra
     PLB_CUDA(cudaSetDevice(B->base->mesh->ctx->device));
     if (degree >= 2 && !B->res) {
         const size_t nk = (size_t)B->n * B->K;
-        PLB_CUDA(cudaMalloc((void**)&B->res, nk * sizeof(float)));
-        cudaError_t e = cudaMalloc((void**)&B->d, nk * sizeof(float));
+        PLB_CUDA(dev_alloc(&B->res, nk));
+        cudaError_t e = dev_alloc(&B->d, nk);
         if (e != cudaSuccess) {
-            cudaFree(B->res);
+            dev_free(B->res, nullptr);
             B->res = nullptr;
             return cuda_fail(e, "pl_batch_solver_set_chebyshev");
         }
@@ -1612,8 +1612,7 @@ int pl_batch_solver_destroy(pl_batch_solver B) {
     if (B->ev_out) cudaEventDestroy(B->ev_out);
     if (B->stream) cudaStreamDestroy(B->stream);
     void* ptrs[] = {B->r, B->z, B->p, B->q, B->x, B->scal, B->active, B->part_a, B->part_b, B->r64, B->jx64, B->res, B->d, B->ticket};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (void* p : ptrs) dev_free(p, m->ctx->stream);
     pl_solver base = B->base;
     delete B;
     mesh_release(m);

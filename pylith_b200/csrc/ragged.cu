@@ -279,10 +279,10 @@ int upload_tables(pl_ragged R) {
     }
     cudaStream_t s = R->ctx->stream;
     if (node0[M] > R->partials_cap) {
-        if (R->d_partials) cudaFree(R->d_partials);
+        dev_free(R->d_partials, R->cs);
         R->d_partials = nullptr;
         R->partials_cap = std::max<int64_t>(node0[M], 2 * R->partials_cap);
-        PLB_CUDA(cudaMalloc((void**)&R->d_partials, 2 * R->partials_cap * sizeof(double)));
+        PLB_CUDA(dev_alloc(&R->d_partials, 2 * R->partials_cap));
         // the captured graph holds the old partials buffer
         if (R->graph) cudaGraphExecDestroy(R->graph);
         R->graph = nullptr;
@@ -353,7 +353,7 @@ int pl_ragged_create(pl_context ctx, int capacity, pl_ragged* out) {
     R->capacity = capacity;
     cudaError_t e = cudaSuccess;
     auto A = [&](auto** p, size_t cnt) {
-        if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(**p));
+        if (e == cudaSuccess) e = dev_alloc(p, cnt);
     };
     A(&R->d_ops, capacity);
     A(&R->d_cell_chunk0, capacity + 1);
@@ -514,8 +514,7 @@ int pl_ragged_destroy(pl_ragged R) {
     if (R->cs) cudaStreamDestroy(R->cs);
     void* ptrs[] = {R->d_ops, R->d_cell_chunk0, R->d_vec, R->d_node_chunk0, R->d_pair0, R->d_active, R->d_nmembers,
                     R->d_partials, R->d_rr};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (void* p : ptrs) dev_free(p, R->ctx->stream);
     pl_context c = R->ctx;
     delete R;
     context_release(c);

@@ -661,7 +661,7 @@ int pl_solver_create(pl_mesh m, const uint8_t* constrained, pl_solver* out) {
     const int64_t n = S->n;
     cudaError_t e = cudaSuccess;
     auto A = [&](auto** p, size_t cnt) {
-        if (e == cudaSuccess) e = cudaMalloc((void**)p, cnt * sizeof(**p));
+        if (e == cudaSuccess) e = dev_alloc(p, cnt);
     };
     A(&S->d_mask, n);
     A(&S->d_diag, 9 * S->nnodes);
@@ -874,8 +874,7 @@ static void solver_free(pl_solver S) {
     void* ptrs[] = {S->d_mask, S->d_diag, S->d_pinv, S->d_pinv32, S->d_r, S->d_p, S->d_q, S->d_z, S->d_x,
                     S->d_xs, S->f_r, S->f_p, S->f_q, S->f_z, S->f_x, S->d_scal, S->d_partials,
                     S->d_pair_neg, S->d_pair_pos, S->d_pair_normal};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (void* p : ptrs) dev_free(p, S->mesh->ctx->stream);
     std::vector<pl_integrator> ops;
     ops.swap(S->ops);
     pl_mesh m = S->mesh;

@@ -505,8 +505,14 @@ class Multigrid:
         vals = (ctypes.c_void_p * n)(*[P[2].ctypes.data for P in self._P])
         self.handle = ctypes.c_void_p()
         check(C.lib().pl_multigrid_create(fine.handle, n, solvers, rows, cols, vals, ctypes.byref(self.handle)))
-        check(C.lib().pl_multigrid_set_smoother(self.handle, degree, lower, coarse_degree, coarse_lower, precision))
+        self.precision = precision
+        self.set_smoother(degree, lower, coarse_degree, coarse_lower)
         check(C.lib().pl_solver_set_multigrid(fine.handle, self.handle))
+
+    def set_smoother(self, degree, lower, coarse_degree=40, coarse_lower=0.01):
+        """Chebyshev-Jacobi smoothing of `degree` on [lower b, b] (pl_multigrid_set_smoother)."""
+        check(C.lib().pl_multigrid_set_smoother(self.handle, degree, lower, coarse_degree, coarse_lower, self.precision))
+        self.degree, self.lower = degree, lower
 
     def lambda_max(self):
         n = ctypes.c_int()

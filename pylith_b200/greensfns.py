@@ -88,7 +88,31 @@ class GreensFunctions:
         solver.setup()
         self._mg_keep = getattr(self, "_mg_keep", []) + [(solver, mg)]
         self.solver_mg = solver
+        self.mg = mg
         return solver
+
+    def tune_multigrid(self, impulses, degrees=(2, 3, 4), lowers=(0.1, 0.3)):
+        """Picks the Chebyshev smoothing (degree, lower ratio) of the last attached multigrid with
+        the highest solves/s on `impulses` (each setting solves them once to warm up and once timed)
+        and keeps it. Returns [(degree, lower, solves_per_s, iterations)], best first."""
+        rhs = [self.impulse_rhs(imp)[1] for imp in impulses]
+        import torch
+
+        out = []
+        for d in degrees:
+            for lo in lowers:
+                self.mg.set_smoother(d, lo)
+                xs = [torch.zeros_like(b) for b in rhs]
+                self.solver_mg.solve(rhs[0], xs[0])  # graph capture
+                self.ctx.synchronize()
+                t0 = time.perf_counter()
+                for b, x in zip(rhs, xs):
+                    self.solver_mg.solve(b, x)
+                self.ctx.synchronize()
+                out.append((d, lo, len(rhs) / (time.perf_counter() - t0), self.solver_mg.stats()["iterations"]))
+        best = max(out, key=lambda r: r[2])
+        self.mg.set_smoother(best[0], best[1])
+        return sorted(out, key=lambda r: -r[2])
 
     def impulse_rhs(self, imp: Impulse):
         """(u_slip, b): the displacement carrying unit slip on the patch, and b = F(u_slip)."""

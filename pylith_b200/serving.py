@@ -147,14 +147,14 @@ def close_problem(prob) -> None:
 
 
 class Server:
-    """Serving loop: an admission thread (arrival times, slots, HBM budget) and two device workers,
-    each with its own stream: the batch worker keeps one ragged batch (pl_ragged_*) of FP32-refined
-    solves that requests join and leave between iteration chunks; the multigrid worker solves the
-    large boxes that have a multigrid hierarchy, one at a time, with FP32 V-cycles under FP64
-    conjugate gradients."""
+    """Serving loop: an admission thread (arrival times, slots, HBM budget) and device workers, each
+    with its own stream: the batch worker keeps one ragged batch (pl_ragged_*) of FP32-refined
+    solves that requests join and leave between iteration chunks; multigrid_workers workers take
+    the large boxes that have a multigrid hierarchy from one queue and solve each with FP32
+    V-cycles under FP64 conjugate gradients (their solves overlap on the device)."""
 
     def __init__(self, device: int = 0, slots: int = 64, hbm_budget: Optional[int] = None, rtol: float = 1e-10,
-                 keep_solutions=False, chunk: int = 10, multigrid: bool = True):
+                 keep_solutions=False, chunk: int = 10, multigrid: bool = True, multigrid_workers: int = 2):
         import torch
 
         self.device = device
@@ -165,8 +165,10 @@ class Server:
         self.keep = keep_solutions
         self.chunk = chunk
         self.multigrid = multigrid
+        self.multigrid_workers = max(1, multigrid_workers)
         self.memory = []  # (request, predicted bytes, measured bytes)
         self.routes = {}  # request -> "batch" or "multigrid"
+        self.workers = {}  # worker -> {"requests", "busy_s", "last_end_s"}
 
     def run(self, problems: List[HostProblem]) -> List[Result]:
         import queue
@@ -174,6 +176,7 @@ class Server:
 
         import torch
 
+        self.workers = {}
         pending = sorted(problems, key=lambda hp: hp.req.arrival)
         for hp in pending:
             if estimate_bytes(hp.req.n) > self.budget:
@@ -186,6 +189,14 @@ class Server:
         self.memory = []
         q_batch, q_mg = queue.Queue(), queue.Queue()
         t0 = time.perf_counter()
+
+        def account(worker, t_begin):
+            now = time.perf_counter() - t0
+            with lock:
+                w = self.workers.setdefault(worker, {"requests": 0, "busy_s": 0.0, "last_end_s": 0.0})
+                w["requests"] += 1
+                w["busy_s"] += now - t_begin
+                w["last_end_s"] = max(w["last_end_s"], now)
 
         def finish(hp, prob, start, its, nbytes):
             end = time.perf_counter() - t0
@@ -240,10 +251,11 @@ class Server:
                         finish(hp, prob, start, st["iterations"], nbytes)
                         batch.remove(member)
                         close_problem(prob)
+                        account("batch", start)
             batch.close()
             ctx.close()
 
-        def multigrid_worker():
+        def multigrid_worker(name):
             torch.cuda.set_device(self.device)
             stream = torch.cuda.Stream(device=self.device)
             ctx = FA.Context(self.device, use_torch_stream=False)
@@ -254,6 +266,7 @@ class Server:
                     if item is None:
                         break
                     hp, nbytes, start = item
+                    t_begin = time.perf_counter() - t0
                     try:
                         prob = build_problem(ctx, hp, FA.Solver.FP64, self.rtol, multigrid=FA.Solver.FP32_REFINED)
                         st = prob.step(0.0)
@@ -263,9 +276,12 @@ class Server:
                     except Exception as e:
                         errors.append((hp.req.rid, repr(e)))
                         finish(hp, _Null(), start, 0, nbytes)
+                    account(name, t_begin)
             ctx.close()
 
-        workers = [threading.Thread(target=batch_worker, daemon=True), threading.Thread(target=multigrid_worker, daemon=True)]
+        mg_names = [f"multigrid{i}" for i in range(self.multigrid_workers)]
+        workers = [threading.Thread(target=batch_worker, daemon=True)]
+        workers += [threading.Thread(target=multigrid_worker, args=(nm,), daemon=True) for nm in mg_names]
         for w in workers:
             w.start()
         for hp in pending:
@@ -283,7 +299,8 @@ class Server:
             self.routes[hp.req.rid] = route
             (q_mg if route == "multigrid" else q_batch).put((hp, nbytes, start))
         q_batch.put(None)
-        q_mg.put(None)
+        for _ in mg_names:
+            q_mg.put(None)
         for w in workers:
             w.join()
         if errors:

@@ -18,6 +18,8 @@ void ensure_kernel_smem(const void*, size_t) {}
 int sm_count() { return 148; }
 int cuda_fail(cudaError_t, const char*) { return PL_ERR_CUDA; }
 int fail(int code, const std::string&) { return code; }
+cudaError_t dev_alloc(void**, size_t) { return cudaErrorNotSupported; }
+void dev_free(void*, cudaStream_t) {}
 }  // namespace plb
 
 using namespace plb;
