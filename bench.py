@@ -10,7 +10,7 @@ The L2 cache (126 MB) is flushed (256 MiB write) before every application, becau
 application's working set (~53 MB) would otherwise stay cached between applications.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pylith_b200|reference]
-  python bench.py --config c0|c1q2|c2|c3|c4     (the other configurations, one JSON line each)
+  python bench.py --config c0|c1q2|c2|c3|c3tile|c4  (the other configurations, one JSON line each)
 
 Under torchrun (N > 1) the ranks share one mesh of N x 1.2 M cells (the same Delaunay box
 stretched N times along x, so every rank's part is the single-GPU workload: weak scaling), cut into
@@ -266,7 +266,7 @@ def main():
     ap.add_argument("--impl", default="pylith_b200")
     ap.add_argument("--cells", type=int, default=TARGET_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1q2", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1q2", "c2", "c3", "c3tile", "c4"])
     ap.add_argument("--scale", type=float, default=1.0, help="size factor for the --config runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -890,6 +890,29 @@ def config_c3(args):
             "max_rel_displacement_error_multigrid_vs_fp64": err(keep_m, sol_s)}
 
 
+def config_c3tile(args):
+    """One batched tile of the C3 Green's functions (8 impulses, FP32 PCG with reliable updates) on
+    the 1.5 M-cell mirrored Delaunay mesh: the profiling case of the batched operator kernel."""
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import greensfns as GF
+    from pylith_b200 import materials as MAT
+    from pylith_b200 import meshing as M
+
+    lo, hi = (-12000.0, -15000.0, -20000.0), (12000.0, 15000.0, 0.0)
+    mesh = M.box_tet_delaunay_fault_x(int(1_500_000 * args.scale), seed=0, lo=lo, hi=hi)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    for sd in ("neg", "pos"):
+        cons[M.boundary_mask(mesh, 0, sd, lo, hi)] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    patches = GF.fault_patches(mesh, (-12000.0, 12000.0), (-15000.0, 0.0), 40, 25)
+    ctx = FA.Context(0)
+    g = GF.GreensFunctions(ctx, mesh, mat, cons, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
+    _, dt = g.solve(g.impulses[:8], batched=True)
+    return {"config": "c3tile", "cells": mesh.num_cells, "dof": mesh.num_dof, "seconds": dt, "stats": g.batch.stats()}
+
+
 def config_c4(args):
     """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
     material, random rectangular left-lateral slip patch of 0.1-3 m. Server (HBM-budget admission;
@@ -932,7 +955,8 @@ def config_c4(args):
                                        "freed memory for reuse)"}}
 
 
-CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c4": config_c4}
+CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c3tile": config_c3tile,
+           "c4": config_c4}
 
 
 if __name__ == "__main__":
