@@ -199,6 +199,100 @@ def host_cpu():
             "affinity_cores": len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else None}
 
 
+def cudart():
+    """The CUDA runtime library this process already uses (torch's), through ctypes."""
+    import ctypes
+
+    path = None
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                if "libcudart.so" in ln:
+                    path = ln.split()[-1]
+                    break
+    except OSError:
+        pass
+    lib = ctypes.CDLL(path or "libcudart.so.12")
+    P, I, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    lib.cudaMemcpyAsync.argtypes = [P, P, S, I, P]
+    lib.cudaEventRecord.argtypes = [P, P]
+    lib.cudaStreamWaitEvent.argtypes = [P, P, ctypes.c_uint]
+    lib.cudaEventCreateWithFlags.argtypes = [ctypes.POINTER(P), ctypes.c_uint]
+    lib.cudaEventDestroy.argtypes = [P]
+    return lib
+
+
+def native_e2e_steps(ig, hin, din, dr, djv, hr, hjv, s_in, s_comp, s_out, n, s_main):
+    """run(k): k end-to-end steps through the C ABI with host buffers, double-buffered like the
+    torch version: per step one pinned H2D copy of u and v, the residual and J v calls on the
+    library's stream, and D2H copies of r (after the residual) and J v; events order the three
+    streams, which start after the work on s_main and which s_main waits for at the end. The
+    context's stream must be s_comp."""
+    import ctypes
+
+    from pylith_b200 import _lib as C
+
+    rt = cudart()
+    lib = C.lib()
+    res, jac = lib.pl_compute_lhs_residual, lib.pl_compute_lhs_jacobian_action
+    h = ig.handle
+    P = ctypes.c_void_p
+    si, sc, so = P(s_in.cuda_stream), P(s_comp.cuda_stream), P(s_out.cuda_stream)
+    sm = P(s_main.cuda_stream)
+
+    def events():
+        out = []
+        for _ in range(2):
+            e = P()
+            if rt.cudaEventCreateWithFlags(ctypes.byref(e), 2) != 0:  # cudaEventDisableTiming
+                raise RuntimeError("cudaEventCreateWithFlags failed")
+            out.append(e)
+        return out
+
+    ev_in, ev_res, ev_done, ev_out = events(), events(), events(), events()
+    ev_edge = events()
+    hin_p = [P(x.data_ptr()) for x in hin]
+    din_p = [P(x.data_ptr()) for x in din]
+    du_p = [P(x.data_ptr()) for x in din]
+    dv_p = [P(x.data_ptr() + 8 * n) for x in din]
+    dr_p, djv_p = [P(x.data_ptr()) for x in dr], [P(x.data_ptr()) for x in djv]
+    hr_p, hjv_p = [P(x.data_ptr()) for x in hr], [P(x.data_ptr()) for x in hjv]
+    bin_, bout = ctypes.c_size_t(16 * n), ctypes.c_size_t(8 * n)
+    H2D, D2H = 1, 2
+    for i in range(2):  # every buffer starts free
+        rt.cudaEventRecord(ev_done[i], sc)
+        rt.cudaEventRecord(ev_out[i], sc)
+
+    def run(steps):
+        rt.cudaEventRecord(ev_edge[0], sm)
+        for st in (si, sc, so):
+            rt.cudaStreamWaitEvent(st, ev_edge[0], 0)
+        for k in range(steps):
+            i = k & 1
+            rt.cudaStreamWaitEvent(si, ev_done[i], 0)
+            rt.cudaMemcpyAsync(din_p[i], hin_p[i], bin_, H2D, si)
+            rt.cudaEventRecord(ev_in[i], si)
+            rt.cudaStreamWaitEvent(sc, ev_in[i], 0)
+            rt.cudaStreamWaitEvent(sc, ev_out[i], 0)
+            rc = res(h, 0.0, 0.0, du_p[i], None, dr_p[i], 0)
+            rt.cudaEventRecord(ev_res[i], sc)
+            rc |= jac(h, 0.0, 0.0, 0.0, du_p[i], dv_p[i], djv_p[i], 0)
+            rt.cudaEventRecord(ev_done[i], sc)
+            rt.cudaStreamWaitEvent(so, ev_res[i], 0)
+            rt.cudaMemcpyAsync(hr_p[i], dr_p[i], bout, D2H, so)
+            rt.cudaStreamWaitEvent(so, ev_done[i], 0)
+            rt.cudaMemcpyAsync(hjv_p[i], djv_p[i], bout, D2H, so)
+            rt.cudaEventRecord(ev_out[i], so)
+            if rc:
+                raise RuntimeError(f"library call failed ({rc})")
+        for i in range(2):  # s_main waits for the last copies out
+            rt.cudaStreamWaitEvent(sc, ev_out[i], 0)
+        rt.cudaEventRecord(ev_edge[1], sc)
+        rt.cudaStreamWaitEvent(sm, ev_edge[1], 0)
+
+    return run
+
+
 def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
     """Oracle cell loop on every host core: residual F(u) plus a second pass of the same loop
     standing in for J v (linear elasticity: F(u) = J u), repeated within a time budget."""
@@ -470,7 +564,16 @@ def main():
     for k in range(args.warmup):
         e2e_step(k, comp_stream)
     torch.cuda.synchronize()
-    t_e2e = timed(eager)
+    if world == 1:
+        # the same steps issued as a C caller would: the C ABI and the CUDA runtime through ctypes,
+        # every pointer and handle bound once (the torch calls above cost tens of microseconds of
+        # host time each, more than a step's device time)
+        eager_native = native_e2e_steps(ig, hin, din, dr, djv, hr, hjv, s_in, comp_stream, s_out, n, stream)
+        eager_native(args.warmup)
+        torch.cuda.synchronize()
+        t_e2e = timed(lambda: eager_native(args.steps))
+    else:
+        t_e2e = timed(eager)
     ctx.set_stream(stream.cuda_stream)
     e2e_value = 2 * global_dof * args.steps / t_e2e / 1e9
 
@@ -568,8 +671,10 @@ def main():
                     "d2h_bytes_per_step": 2 * n * 8,
                     "overlap": "copies in and out on their own streams, device buffers alternating between steps",
                     "graph_replay_value": e2e_graph,
-                    "method": "per step: pinned H2D of u and v, residual and J v through the public API, D2H of r and J v; "
-                              "value: eager per-call steps; graph_replay_value: the same steps captured once in a CUDA graph",
+                    "method": "per step: one pinned H2D copy of u and v, residual and J v through the C ABI "
+                              "(pl_compute_lhs_residual, pl_compute_lhs_jacobian_action), D2H of r and J v; value: "
+                              "eager per-call steps issued through ctypes as a C caller would (one GPU; torch calls "
+                              "under torchrun); graph_replay_value: the same steps captured once in a CUDA graph",
                     "host_link": {**link_gbs, "bound_gdof_s": link_bound,
                                   "note": "pinned copies of one step's inputs (h2d), outputs (d2h) and both at once"}},
             "gpu_launches": int(launches),

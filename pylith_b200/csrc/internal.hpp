@@ -69,6 +69,7 @@ struct BlockedLayout {
     int cells_per_block = 0;
     int64_t num_blocks = 0;
     int max_local_nodes = 0;
+    int32_t* d_cell_begin = nullptr;        // [num_blocks + 1] first cell of each block
     int32_t* d_block_node_begin = nullptr;  // [num_blocks + 1] into slot_node
     uint32_t* d_slot_node = nullptr;        // global node of each block-local slot (sorted per block),
                                             // high bit set if other blocks also touch the node

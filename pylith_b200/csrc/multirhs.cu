@@ -275,11 +275,11 @@ PL_D void prefetch_multi(const DomainParams& p, const int32_t* __restrict__ slot
 // in CTA order into fin.out_a.
 template <int K>
 __global__ void __launch_bounds__(kMultiBlockCells, 3) k_tet_blocked_jv32_multi(
-    DomainParams p, const int32_t* __restrict__ slot_begin, const uint32_t* __restrict__ slot_node,
-    const ushort4* __restrict__ lconn, const uint32_t* __restrict__ inc_off, const uint16_t* __restrict__ inc,
-    const int32_t* __restrict__ pbeg, const double* __restrict__ pcoords, int64_t nblocks, int ld,
-    const float* __restrict__ v, float* out, bool store_owned, double* pq_part, const double* __restrict__ pq_rz,
-    FinSpec fin) {
+    DomainParams p, const int32_t* __restrict__ cell_begin, const int32_t* __restrict__ slot_begin,
+    const uint32_t* __restrict__ slot_node, const ushort4* __restrict__ lconn, const uint32_t* __restrict__ inc_off,
+    const uint16_t* __restrict__ inc, const int32_t* __restrict__ pbeg, const double* __restrict__ pcoords,
+    int64_t nblocks, int ld, const float* __restrict__ v, float* out, bool store_owned, double* pq_part,
+    const double* __restrict__ pq_rz, FinSpec fin) {
     static_assert(kMultiBlockCells == kBThreads, "the fused sums assume kBThreads threads per CTA");
     __shared__ float s_sig[K];  // energy scales (pq_part)
     if (pq_part && threadIdx.x < K) {
@@ -307,8 +307,8 @@ __global__ void __launch_bounds__(kMultiBlockCells, 3) k_tet_blocked_jv32_multi(
     __pipeline_commit();
     for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int ns = slot_begin[b + 1] - slot_begin[b];
-        const int64_t c = b * kMultiBlockCells + tc;
-        const bool live = c < p.ncells;
+        const int64_t c = cell_begin[b] + tc;
+        const bool live = c < cell_begin[b + 1];
         int ln[4] = {0, 0, 0, 0};
         float inv[3][3], cf[3][3], lam = 0.f, mu = 0.f, vol = 0.f;
         // per-cell inputs from global memory first: their latency overlaps the staging copies
@@ -989,7 +989,7 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullp
             fin.out_a = pq;
         }
         k_tet_blocked_jv32_multi<K><<<grid, kMultiBlockCells, smem, s>>>(
-            pp, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
+            pp, L.d_cell_begin, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
             L.d_pipe_begin, L.d_pipe_coords, L.num_blocks, ld, v, out, first, pq ? B->part_a : nullptr, B->scal,
             fin);
         first = false;
