@@ -611,6 +611,191 @@ __global__ void __launch_bounds__(kTetBlockCells, PLB_PAD2_MIN_BLOCKS) k_tet_pad
     __pipeline_wait_prior(0);
 }
 
+// ---- FP32 Jacobian action over the padded layout ---------------------------------------------
+// Shared memory of k_tet_pad_jv32: element vectors (FP32) [12][kTetBlockCells], then two node
+// buffers of [3][ld] FP64 coordinates and [3][ld] FP32 field values, then two metadata buffers.
+PL_HD size_t padjv_node_bytes(int ld) { return round16(3 * (size_t)ld * sizeof(double) + 3 * (size_t)ld * sizeof(float)); }
+
+PL_HD size_t padjv_smem_bytes(int ld) {
+    return 12 * (size_t)kTetBlockCells * sizeof(float) + 2 * padjv_node_bytes(ld) + 2 * pipe_meta_bytes(ld);
+}
+
+// Asynchronous copies of block b for k_tet_pad_jv32: coordinates, ids, offsets and incidences as
+// 16-byte runs (as pipe_stage), the FP32 field of its nodes as 4-byte gathers.
+PL_D void padjv_stage(const float* __restrict__ v32, const PipeArrays& A, int64_t b,
+                      const uint32_t nd[kMaxSlotsPerThread], char* buf, const PipeMeta& M, int ld) {
+    double* X = reinterpret_cast<double*>(buf);
+    float* V = reinterpret_cast<float*>(buf + 3 * (size_t)ld * sizeof(double));
+    const int p0 = A.pbeg[b];
+    const int np = A.pbeg[b + 1] - p0;
+    const int ns = A.slot_begin[b + 1] - A.slot_begin[b];
+    const int half = np >> 1;
+    for (int t = threadIdx.x; t < 3 * half; t += blockDim.x) {
+        const int d = t / half, j = t - d * half;
+        __pipeline_memcpy_async(&X[d * ld + 2 * j], &A.coords[3 * (int64_t)p0 + (int64_t)d * np + 2 * j], 16);
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxSlotsPerThread; ++k) {
+        const int i = threadIdx.x + k * blockDim.x;
+        if (i < ns) {
+            const int64_t n = nd[k] & ~kSharedBit;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) __pipeline_memcpy_async(&V[d * ld + i], &v32[3 * n + d], sizeof(float));
+        }
+    }
+    const int q = np >> 2;
+    for (int t = threadIdx.x; t < q; t += blockDim.x) __pipeline_memcpy_async(&M.ids[4 * t], &A.ids[p0 + 4 * t], 16);
+    for (int t = threadIdx.x; t <= q; t += blockDim.x)
+        __pipeline_memcpy_async(&M.off[4 * t], &A.off[(int64_t)p0 + 4 * b + 4 * t], 16);
+    for (int t = threadIdx.x; t < kTetBlockCells / 2; t += blockDim.x)
+        __pipeline_memcpy_async(&M.inc[8 * t], &A.inc[b * 4 * kTetBlockCells + 8 * t], 16);
+}
+
+// FP32 Jacobian action of an isotropic tangent on the padded cell-block layout, in the shape of
+// k_tet_pad2: block b + G is staged with cp.async while block b is computed, geometry (cofactors,
+// 1/det) in FP64 per cell, field, gradient, flux, element vectors and node sums in FP32. The
+// tangent's (lambda, mu) per cell come from the solver's cache (p.lm32; CACHED) or from the
+// registered Jacobian kernel. The output holds zero (INSERT) or the sum to add to: owned nodes are
+// added, shared ones reduced.
+template <bool CACHED>
+__global__ void __launch_bounds__(kTetBlockCells, 4) k_tet_pad_jv32(DomainParams p, PipeArrays A) {
+    using L = AuxLayout<RHEO_ILE, false>;
+    extern __shared__ __align__(16) char smem_raw[];
+    const AuxOffsets<RHEO_ILE, false> aoff;
+    const int ld = A.ld;
+    float* sE = reinterpret_cast<float*>(smem_raw);  // [12][kTetBlockCells]
+    char* nodeb = smem_raw + 12 * kTetBlockCells * sizeof(float);
+    const size_t nbytes = padjv_node_bytes(ld);
+    char* metab = nodeb + 2 * nbytes;
+    const size_t mb = pipe_meta_bytes(ld);
+    const int64_t G = gridDim.x;
+    const int tc = threadIdx.x;
+    int64_t b = blockIdx.x;
+    if (b >= A.nblocks) return;
+    uint32_t nd_next[kMaxSlotsPerThread];
+    {
+        uint32_t nd0[kMaxSlotsPerThread];
+        pipe_load_ids(A, b, nd0);
+        padjv_stage(p.v32, A, b, nd0, nodeb, pipe_meta(metab, ld), ld);
+        __pipeline_commit();
+        pipe_load_ids(A, b + G, nd_next);
+    }
+    for (int it = 0; b < A.nblocks; b += G, ++it) {
+        const int64_t c = A.cell_begin[b] + tc;
+        const bool live = c < A.cell_begin[b + 1];
+        ushort4 lc = make_ushort4(0, 0, 0, 0);
+        float lam = 0.f, mu = 0.f;
+        if (live) {
+            lc = A.lconn[c];
+            if (CACHED) {
+                const float2 lm = reinterpret_cast<const float2*>(p.lm32)[c];
+                lam = lm.x;
+                mu = lm.y;
+            } else {
+                double a[L::size];
+                L::load_cell(p, c, a);
+                double x[3] = {0, 0, 0}, Jf3[81];
+#pragma unroll
+                for (int i = 0; i < 81; ++i) Jf3[i] = 0.0;
+                call_jf3<RHEO_ILE>(L::numA, aoff.v, a, p, x, Jf3);
+                lam = (float)(-Jf3[((0 * 3 + 1) * 3 + 0) * 3 + 1]);
+                mu = (float)(-Jf3[((0 * 3 + 1) * 3 + 1) * 3 + 0]);
+            }
+        }
+        uint32_t nd_after[kMaxSlotsPerThread];
+        pipe_load_ids(A, b + 2 * G, nd_after);
+        __pipeline_wait_prior(0);
+        // block b's copies have landed; every thread has finished the node sums of the previous
+        // block (its buffers are free for block b + G)
+        __syncthreads();
+        if (b + G < A.nblocks) {
+            padjv_stage(p.v32, A, b + G, nd_next, nodeb + ((it + 1) & 1) * nbytes, pipe_meta(metab + ((it + 1) & 1) * mb, ld),
+                        ld);
+            const int64_t cn = A.cell_begin[b + G] + tc;
+            if (cn < A.cell_begin[b + G + 1]) {
+                prefetch_l2(&A.lconn[cn]);
+                if (CACHED) prefetch_l2(&p.lm32[2 * cn]);
+            }
+        }
+        __pipeline_commit();
+#pragma unroll
+        for (int k = 0; k < kMaxSlotsPerThread; ++k) nd_next[k] = nd_after[k];
+        const double* X = reinterpret_cast<const double*>(nodeb + (it & 1) * nbytes);
+        const float* V = reinterpret_cast<const float*>(nodeb + (it & 1) * nbytes + 3 * (size_t)ld * sizeof(double));
+        if (live) {
+            const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
+            double Xc[4][3];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Xc[k][d] = X[d * ld + ln[k]];
+            double cof[3][3];
+            const double det = tet_cofactors(Xc, cof);
+            if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+            const double rdet = 1.0 / det;
+            float inv[3][3], cf[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    inv[i][j] = (float)(cof[i][j] * rdet);
+                    cf[i][j] = (float)(cof[i][j] * (1.0 / 6.0));
+                }
+            float s[3][3];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                const float v0 = V[cc * ld + ln[0]];
+                const float g0 = V[cc * ld + ln[1]] - v0, g1 = V[cc * ld + ln[2]] - v0, g2 = V[cc * ld + ln[3]] - v0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) s[cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
+            }
+            // flux f1 = -(lambda tr(e) I + 2 mu e), e = sym grad v
+            const float ltr = lam * (s[0][0] + s[1][1] + s[2][2]);
+            const float xy = -mu * (s[0][1] + s[1][0]), yz = -mu * (s[1][2] + s[2][1]), xz = -mu * (s[0][2] + s[2][0]);
+            const float f[3][3] = {{-(2.0f * mu * s[0][0] + ltr), xy, xz},
+                                   {xy, -(2.0f * mu * s[1][1] + ltr), yz},
+                                   {xz, yz, -(2.0f * mu * s[2][2] + ltr)}};
+            float e0[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    const float v = f[cc][0] * cf[k][0] + f[cc][1] * cf[k][1] + f[cc][2] * cf[k][2];
+                    e0[cc] -= v;
+                    sE[((k + 1) * 3 + cc) * kTetBlockCells + tc] = v;
+                }
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + tc] = e0[cc];
+        }
+        __syncthreads();
+        const PipeMeta M = pipe_meta(metab + (it & 1) * mb, ld);
+        const int ns = A.slot_begin[b + 1] - A.slot_begin[b];
+        for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+            const int j0 = M.off[k], j1 = M.off[k + 1];
+            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+#pragma unroll 4
+            for (int j = j0; j < j1; ++j) {
+                const int e = M.inc[j];
+                r0 += sE[e];
+                r1 += sE[e + kTetBlockCells];
+                r2 += sE[e + 2 * kTetBlockCells];
+            }
+            const uint32_t id = M.ids[k];
+            float* o = p.out32 + 3 * (int64_t)(id & ~kSharedBit);
+            if (id & kSharedBit) {
+                red_add(o, r0);
+                red_add(o + 1, r1);
+                red_add(o + 2, r2);
+            } else {
+                o[0] += r0;
+                o[1] += r1;
+                o[2] += r2;
+            }
+        }
+    }
+    __pipeline_wait_prior(0);
+}
+
 // FP32 Jacobian action of isotropic linear elasticity on the cell blocks: geometry (cofactors,
 // 1/det) and the elastic tangent in FP64 per cell, the field, gradient, flux and element vectors
 // in FP32. Used by the inner iterations of the mixed-precision solver.
@@ -877,7 +1062,21 @@ bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, 
 
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,
                                 cudaStream_t s) {
-    if (cell != TET4 || rheo != RHEO_ILE || !blocked_usable(b)) return false;
+    if (cell != TET4 || !blocked_usable(b)) return false;
+    // the padded-layout kernel (default); with the solver's cached tangent any isotropic rheology
+    const int ld = (b.max_local_nodes + 3) & ~3;
+    if (tet_kernel_choice() != TK_TWOPHASE && b.d_pipe_begin && padjv_smem_bytes(ld) <= 48 * 1024 &&
+        (p.lm32 || rheo == RHEO_ILE)) {
+        const size_t smem = padjv_smem_bytes(ld);
+        const void* kern = p.lm32 ? (const void*)k_tet_pad_jv32<true> : (const void*)k_tet_pad_jv32<false>;
+        ensure_kernel_smem(kern, smem);
+        const int grid = (int)std::min<int64_t>(b.num_blocks, (int64_t)sm_count() * 4);
+        if (p.lm32) k_tet_pad_jv32<true><<<grid, kTetBlockCells, smem, s>>>(p, pipe_arrays_of(b, nullptr));
+        else k_tet_pad_jv32<false><<<grid, kTetBlockCells, smem, s>>>(p, pipe_arrays_of(b, nullptr));
+        count_launch();
+        return true;
+    }
+    if (rheo != RHEO_ILE) return false;
     const size_t smem = (size_t)12 * kTetBlockCells * sizeof(float) +
                         (size_t)b.max_local_nodes * (3 * sizeof(double) + 3 * sizeof(float));
     if (smem > 200 * 1024) return false;

@@ -732,7 +732,8 @@ void integrator_release(pl_integrator_s* ig) {
 
 int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt) {
     pl_mesh m = ig->mesh;
-    if (ig->is_interface || m->cell_type != PL_CELL_HEX8 || ig->j3 == K_NONE) return PL_OK;
+    if (ig->is_interface || (m->cell_type != PL_CELL_HEX8 && m->cell_type != PL_CELL_TET4) || ig->j3 == K_NONE)
+        return PL_OK;
     const Rheology rheo = rheology_of(ig, true);
     if (rheo != RHEO_ILE && rheo != RHEO_GENMAXWELL) return PL_OK;
     if (ig->lm32_valid && ig->lm32_t == t && ig->lm32_dt == dt) return PL_OK;
@@ -890,7 +891,9 @@ int pl_compute_lhs_jacobian_action_f32(pl_integrator ig, double t, double dt, co
     p.out32 = jv;
     p.t = t;
     p.dt = dt;
-    if (m->cell_type == PL_CELL_HEX8 && ig->lm32_valid && ig->lm32_t == t && ig->lm32_dt == dt) p.lm32 = ig->d_lm32;
+    if ((m->cell_type == PL_CELL_HEX8 || m->cell_type == PL_CELL_TET4) && ig->lm32_valid && ig->lm32_t == t &&
+        ig->lm32_dt == dt)
+        p.lm32 = ig->d_lm32;
     if (use_blocked(ig) && (rc = ensure_blocked_layout(m)) == PL_OK &&
         launch_domain_jv32_blocked(p, *m->blocked, m->cell_type, rheo, m->nnodes, s)) {
         PLB_CUDA(cudaGetLastError());

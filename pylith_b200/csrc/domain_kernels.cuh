@@ -38,7 +38,7 @@ struct DomainParams {
     int num_constants;
     double constants[8];
     unsigned int* err;
-    const float* lm32;  // FP32 Jacobian action of hexahedra: per-cell (lambda, mu) of the
+    const float* lm32;  // FP32 Jacobian action (hexahedra, tetrahedra): per-cell (lambda, mu) of the
                         // isotropic tangent at (t, dt), or NULL to evaluate the tangent per point
 };
 

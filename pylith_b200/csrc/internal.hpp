@@ -178,7 +178,7 @@ struct pl_integrator_s {
     std::vector<plb::AuxField> aux;
     std::vector<double> constants;
     int scatter = PL_SCATTER_AUTO;
-    // per-cell (lambda, mu) for the FP32 Jacobian action of hexahedra, valid for (lm32_t,
+    // per-cell (lambda, mu) for the FP32 Jacobian action (hexahedra, tetrahedra), valid for (lm32_t,
     // lm32_dt) until the aux fields or constants change
     float* d_lm32 = nullptr;
     bool lm32_valid = false;

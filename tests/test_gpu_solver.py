@@ -590,3 +590,51 @@ def test_fp32_hex_jacobian_action_uses_the_tangent_cached_by_solver_setup(ctx):
     assert close(jv(), elastic)
     for S in (S1, S2, S3, S4):
         S.close()
+
+
+@pytest.mark.parametrize("rheology", ["elastic", "genmaxwell"])
+def test_fp32_tet_jacobian_action_with_the_cached_tangent(ctx, rheology):
+    """P1 tetrahedra: after a FP32 solver's setup has cached each cell's (lambda, mu), the FP32
+    Jacobian action (the padded cell-block kernel) reads them; it matches the action that
+    evaluates the registered tangent per cell (<= 1e-6) and the FP64 action (<= 1e-5), for
+    isotropic elasticity and for generalized Maxwell (whose per-cell tangent the cache makes
+    available to the cell-block kernel)."""
+    import torch
+    from pylith_b200 import feassemble as FA
+
+    mesh = M.box_tet_delaunay(60000, seed=6)
+    nc = mesh.num_cells
+    rng = np.random.default_rng(8)
+    rho, mu, K = MAT.lognormal_elastic(nc, seed=9)
+    dt = 0.0
+    if rheology == "genmaxwell":
+        mu_g, K_g, lam_g, tau = KA.genmaxwell_params()
+        mat = MAT.IsotropicLinearGenMaxwell(
+            np.full(nc, KA.GM_DENSITY), mu_g * rng.uniform(0.5, 1.5, nc), np.full(nc, K_g), np.tile(tau, (nc, 1)),
+            np.tile(KA.GM_RATIO, (nc, 1)), np.zeros((nc, 1, 18)), np.zeros((nc, 1, 6)))
+        dt = KA.GM_DT
+    else:
+        mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    dm = FA.DeviceMesh(ctx, mesh)
+    ig = mat.create_integrator(dm, dt) if rheology == "genmaxwell" else mat.create_integrator(dm)
+    v64 = torch.from_numpy(rng.standard_normal(dm.num_dof)).cuda()
+    v = v64.float()
+
+    def jv32():
+        out = torch.zeros_like(v)
+        ig.compute_lhs_jacobian_action_f32(0.0, dt, v, out)
+        torch.cuda.synchronize()
+        return out.double()
+
+    per_cell = jv32()
+    ref = torch.zeros_like(v64)
+    ig.compute_lhs_jacobian_action(0.0, dt, 0.0, None, v.double(), ref)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 2, "neg")] = True
+    S = FA.Solver(dm, cons.ravel(), [ig], precision=FA.Solver.FP32_REFINED)
+    S.setup(0.0, dt)
+    cached = jv32()
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))  # noqa: E731
+    assert rel(cached, per_cell) <= 1e-6
+    assert rel(cached, ref) <= 1e-5
+    S.close()
