@@ -971,12 +971,12 @@ static void launch_t(const DomainParams& p, const BlockedLayout& b, bool insert,
     }
 }
 
-static PipeArrays pipe_arrays_of(const BlockedLayout& b, double* partial) {
+static PipeArrays pipe_arrays_of(const BlockedLayout& b, double* partial, bool reduced = false) {
     PipeArrays A;
     A.cell_begin = b.d_cell_begin;
     A.slot_begin = b.d_block_node_begin;
     A.pbeg = b.d_pipe_begin;
-    A.ids = b.d_pipe_ids;
+    A.ids = reduced ? b.d_pipe_ids_red : b.d_pipe_ids;
     A.coords = b.d_pipe_coords;
     A.off = b.d_pipe_off;
     A.inc = b.d_pipe_inc;
@@ -996,8 +996,9 @@ static void launch_pipe_one(const DomainParams& p, const PipeArrays& A, size_t s
 }
 
 template <bool PIPE, int RHEO, bool BF, int OP>
-static void launch_pipe_t(const DomainParams& p, const BlockedLayout& b, bool insert, double* partial, cudaStream_t s) {
-    const PipeArrays A = pipe_arrays_of(b, partial);
+static void launch_pipe_t(const DomainParams& p, const BlockedLayout& b, bool insert, double* partial, cudaStream_t s,
+                          bool reduced = false) {
+    const PipeArrays A = pipe_arrays_of(b, partial, reduced);
     const size_t smem = PIPE ? pipe_smem_bytes(A.ld) : pad2_smem_bytes(A.ld);
     const int grid = (int)std::min<int64_t>(b.num_blocks, (int64_t)sm_count() * (PIPE ? PLB_PIPE_MIN_BLOCKS : PLB_PAD2_MIN_BLOCKS));
     const bool det = partial != nullptr;
@@ -1033,8 +1034,28 @@ static bool blocked_usable(const BlockedLayout& b) {
 }
 
 bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, bool bf,
-                                 int op, bool insert, int64_t nnodes, double* partial, cudaStream_t s) {
+                                 int op, bool insert, int64_t nnodes, double* partial, cudaStream_t s, bool reduced) {
     if (cell != TET4 || rheo != RHEO_ILE || !blocked_usable(b)) return false;
+    if (reduced) {
+        // padded-layout kernels with the reduced slot ids; the caller zeroed the output
+        const int ld = (b.max_local_nodes + 3) & ~3;
+        const TetKernel kr = tet_kernel_choice();
+        if (partial || insert || !b.d_pipe_ids_red || kr == TK_TWOPHASE ||
+            (kr == TK_PIPE && pipe_smem_bytes(ld) > 75 * 1024) || (kr == TK_PAD2 && pad2_smem_bytes(ld) > 56 * 1024))
+            return false;
+        const bool pipe = kr == TK_PIPE;
+        if (op == OP_RESIDUAL) {
+            if (pipe && bf) launch_pipe_t<true, RHEO_ILE, true, OP_RESIDUAL>(p, b, false, nullptr, s, true);
+            else if (pipe) launch_pipe_t<true, RHEO_ILE, false, OP_RESIDUAL>(p, b, false, nullptr, s, true);
+            else if (bf) launch_pipe_t<false, RHEO_ILE, true, OP_RESIDUAL>(p, b, false, nullptr, s, true);
+            else launch_pipe_t<false, RHEO_ILE, false, OP_RESIDUAL>(p, b, false, nullptr, s, true);
+        } else if (pipe) {
+            launch_pipe_t<true, RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, false, nullptr, s, true);
+        } else {
+            launch_pipe_t<false, RHEO_ILE, false, OP_JACOBIAN_ACTION>(p, b, false, nullptr, s, true);
+        }
+        return true;
+    }
     // Nodes owned by one block are stored (INSERT) or added (ADD) by their block. With a
     // partial-sum buffer (deterministic mode) the fixup pass then writes or adds every other
     // node, so no output zeroing and no atomics are needed and the sums are the same every run.
@@ -1061,8 +1082,9 @@ bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, 
 }
 
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,
-                                cudaStream_t s) {
+                                cudaStream_t s, bool reduced) {
     if (cell != TET4 || !blocked_usable(b)) return false;
+    if (reduced && !b.d_pipe_ids_red) return false;
     // the padded-layout kernel (default); with the solver's cached tangent any isotropic rheology
     const int ld = (b.max_local_nodes + 3) & ~3;
     if (tet_kernel_choice() != TK_TWOPHASE && b.d_pipe_begin && padjv_smem_bytes(ld) <= 48 * 1024 &&
@@ -1071,12 +1093,12 @@ bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, i
         const void* kern = p.lm32 ? (const void*)k_tet_pad_jv32<true> : (const void*)k_tet_pad_jv32<false>;
         ensure_kernel_smem(kern, smem);
         const int grid = (int)std::min<int64_t>(b.num_blocks, (int64_t)sm_count() * 4);
-        if (p.lm32) k_tet_pad_jv32<true><<<grid, kTetBlockCells, smem, s>>>(p, pipe_arrays_of(b, nullptr));
-        else k_tet_pad_jv32<false><<<grid, kTetBlockCells, smem, s>>>(p, pipe_arrays_of(b, nullptr));
+        if (p.lm32) k_tet_pad_jv32<true><<<grid, kTetBlockCells, smem, s>>>(p, pipe_arrays_of(b, nullptr, reduced));
+        else k_tet_pad_jv32<false><<<grid, kTetBlockCells, smem, s>>>(p, pipe_arrays_of(b, nullptr, reduced));
         count_launch();
         return true;
     }
-    if (rheo != RHEO_ILE) return false;
+    if (rheo != RHEO_ILE || reduced) return false;
     const size_t smem = (size_t)12 * kTetBlockCells * sizeof(float) +
                         (size_t)b.max_local_nodes * (3 * sizeof(double) + 3 * sizeof(float));
     if (smem > 200 * 1024) return false;
@@ -1403,6 +1425,9 @@ static int build_blocked_layout(pl_mesh_s* m) {
     up(&L->d_fix_slot, fix_slot);
     up(&L->d_pipe_begin, pbeg);
     up(&L->d_pipe_ids, pids);
+    L->h_pipe_ids = pids;
+    L->h_pipe_begin = pbeg;
+    L->h_block_node_begin = begin;
     up(&L->d_pipe_coords, pcoords);
     up(&L->d_pipe_off, poff);
     up(&L->d_pipe_inc, pinc);
@@ -1425,8 +1450,38 @@ int ensure_blocked_layout(pl_mesh_s* m) {
     }
 }
 
+int ensure_reduced_ids(pl_mesh_s* m) {
+    BlockedLayout* L = m->blocked;
+    if (!L || L->num_blocks == 0) return fail(PL_ERR_UNSUPPORTED, "no cell-block layout");
+    if (L->d_pipe_ids_red) return PL_OK;
+    if (m->h_node_red.size() != (size_t)m->nnodes) return fail(PL_ERR_UNSUPPORTED, "no reduced fault space");
+    // a node of the reduced space is owned by its block only if it has one slot in all blocks
+    std::vector<uint32_t> ids(L->h_pipe_ids.size(), 0u);
+    std::vector<int32_t> slots(m->nnodes, 0);
+    for (int64_t b = 0; b < L->num_blocks; ++b) {
+        const int p0 = L->h_pipe_begin[b], ns = L->h_block_node_begin[b + 1] - L->h_block_node_begin[b];
+        for (int i = 0; i < ns; ++i) {
+            const uint32_t r = (uint32_t)m->h_node_red[L->h_pipe_ids[p0 + i] & ~kSharedBit];
+            ids[p0 + i] = r;
+            slots[r]++;
+        }
+    }
+    for (int64_t b = 0; b < L->num_blocks; ++b) {
+        const int p0 = L->h_pipe_begin[b], ns = L->h_block_node_begin[b + 1] - L->h_block_node_begin[b];
+        for (int i = 0; i < ns; ++i)
+            if (slots[ids[p0 + i]] > 1) ids[p0 + i] |= kSharedBit;
+    }
+    uint32_t* d = nullptr;
+    PLB_CUDA(dev_alloc(&d, ids.size()));
+    PLB_CUDA(cudaMemcpyAsync(d, ids.data(), ids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, m->ctx->stream));
+    PLB_CUDA(cudaStreamSynchronize(m->ctx->stream));
+    L->d_pipe_ids_red = d;
+    return PL_OK;
+}
+
 void free_blocked_layout(BlockedLayout* b, cudaStream_t after) {
     if (!b) return;
+    dev_free(b->d_pipe_ids_red, after);
     void* ptrs[] = {b->d_cell_begin, b->d_block_node_begin, b->d_slot_node, b->d_local_cells, b->d_inc_off, b->d_inc,
                     b->d_fix_node, b->d_fix_off, b->d_fix_slot, b->d_pipe_begin, b->d_pipe_ids,
                     b->d_pipe_coords, b->d_pipe_off, b->d_pipe_inc};

@@ -406,6 +406,14 @@ int pl_mesh_set_cohesive(pl_mesh m, int64_t ncoh, const int32_t* coh, int64_t nl
     PLB_CUDA(cudaSetDevice(m->ctx->device));
     dev_free(m->d_coh, m->ctx->stream);
     m->d_coh = nullptr;
+    dev_free(m->d_cells_red, m->ctx->stream);
+    m->d_cells_red = nullptr;
+    m->h_node_red.clear();
+    if (m->blocked) {
+        dev_free(m->blocked->d_pipe_ids_red, m->ctx->stream);
+        m->blocked->d_pipe_ids_red = nullptr;
+    }
+    bump_state_epoch();  // captured solver graphs hold the reduced connectivity
     m->ncoh = ncoh;
     m->nlag = nlag;
     m->h_coh.assign(coh, coh + 12 * ncoh);
@@ -423,6 +431,7 @@ static void mesh_free(pl_mesh m) {
     dev_free(m->d_cells, m->ctx->stream);
     dev_free(m->d_coords, m->ctx->stream);
     dev_free(m->d_coh, m->ctx->stream);
+    dev_free(m->d_cells_red, m->ctx->stream);
     if (m->blocked) free_blocked_layout(m->blocked, m->ctx->stream);
     delete m;
     if (--c->refs == 0 && c->destroy_requested) context_free(c);
@@ -751,6 +760,112 @@ int prepare_jv32_tangent(pl_integrator_s* ig, double t, double dt) {
     return PL_OK;
 }
 
+static bool use_blocked(pl_integrator ig) {
+    pl_mesh m = ig->mesh;
+    if (ig->scatter == PL_SCATTER_ATOMIC) return false;
+    if (ig->subset) return false;  // the blocked layout covers whole meshes
+    return m->cell_type == PL_CELL_TET4 || ig->scatter == PL_SCATTER_BLOCKED || ig->scatter == PL_SCATTER_DETERMINISTIC;
+}
+
+// The reduced fault space's connectivity (each positive-side node replaced by its negative-side
+// partner) and node map. Refused (PL_ERR_UNSUPPORTED) when a pair's two nodes do not coincide:
+// the kernels then read the partner's coordinates in place of the node's own.
+int ensure_reduced_cells(pl_mesh_s* m) {
+    if (m->d_cells_red) return PL_OK;
+    if (m->ncoh == 0) return PL_ERR_UNSUPPORTED;
+    std::vector<int32_t> red(m->nnodes);
+    for (int64_t v = 0; v < m->nnodes; ++v) red[v] = (int32_t)v;
+    double scale = 0.0;
+    for (double x : m->h_coords) scale = std::max(scale, std::fabs(x));
+    for (int64_t c = 0; c < m->ncoh; ++c)
+        for (int a = 0; a < 4; ++a) {
+            const int32_t neg = m->h_coh[12 * c + a], pos = m->h_coh[12 * c + 4 + a];
+            for (int d = 0; d < 3; ++d)
+                if (std::fabs(m->h_coords[3 * (size_t)neg + d] - m->h_coords[3 * (size_t)pos + d]) > 1e-12 * scale)
+                    return PL_ERR_UNSUPPORTED;
+            red[pos] = neg;
+        }
+    std::vector<int32_t> cells(m->h_cells.size());
+    for (size_t i = 0; i < cells.size(); ++i) cells[i] = red[m->h_cells[i]];
+    int32_t* d = nullptr;
+    PLB_CUDA(dev_alloc(&d, cells.size()));
+    PLB_CUDA(cudaMemcpyAsync(d, cells.data(), cells.size() * sizeof(int32_t), cudaMemcpyHostToDevice, m->ctx->stream));
+    PLB_CUDA(cudaStreamSynchronize(m->ctx->stream));
+    m->d_cells_red = d;
+    m->h_node_red.swap(red);
+    return PL_OK;
+}
+
+// Whether jacobian_action_reduced(_f32) serves this integrator (domain cells of a mesh with
+// faults whose node pairs coincide, not the deterministic scatter, and for cell blocks a padded
+// layout kernel).
+bool jacobian_action_reduced_supported(pl_integrator_s* ig) {
+    if (!ig || ig->is_interface || ig->j3 == K_NONE || ig->scatter == PL_SCATTER_DETERMINISTIC) return false;
+    pl_mesh m = ig->mesh;
+    if (ensure_reduced_cells(m) != PL_OK) return false;
+    // the cell-block path of tetrahedra needs the reduced slot ids (built here, outside capture)
+    if (use_blocked(ig) && m->cell_type == PL_CELL_TET4)
+        return prepare_blocked(ig) == PL_OK && ensure_reduced_ids(m) == PL_OK;
+    return true;
+}
+
+// J v of the solvers' reduced fault space without unfolding v or folding the result: every
+// positive-side node is read as, and adds into, its negative-side partner (v's positive-side
+// entries are not read; the result's are zero after INSERT).
+int jacobian_action_reduced(pl_integrator_s* ig, double t, double dt, const double* v, double* jv, int mode) {
+    pl_mesh m = ig->mesh;
+    cudaStream_t s = m->ctx->stream;
+    int rc = ensure_reduced_cells(m);
+    if (rc) return rc;
+    const Rheology rheo = rheology_of(ig, true);
+    DomainParams p;
+    if ((rc = bind_domain(ig, rheo, false, &p)) != PL_OK) return rc;
+    p.cells = m->d_cells_red;
+    p.v = v;
+    p.out = jv;
+    p.t = t;
+    p.dt = dt;
+    if (mode == PL_INSERT) PLB_CUDA(cudaMemsetAsync(jv, 0, pl_mesh_num_dof(m) * sizeof(double), s));
+    if (use_blocked(ig) && m->cell_type == PL_CELL_TET4) {
+        if ((rc = prepare_blocked(ig)) != PL_OK || (rc = ensure_reduced_ids(m)) != PL_OK) return rc;
+        if (!launch_domain_apply_blocked(p, *m->blocked, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, false, m->nnodes,
+                                         nullptr, s, true))
+            return PL_ERR_UNSUPPORTED;
+    } else if (ig->scatter == PL_SCATTER_ATOMIC ||
+               !launch_domain_apply_hexgroup(p, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, s)) {
+        launch_domain_apply_atomic(p, m->cell_type, rheo, false, OP_JACOBIAN_ACTION, s);
+    }
+    PLB_CUDA(cudaGetLastError());
+    return PL_OK;
+}
+
+int jacobian_action_reduced_f32(pl_integrator_s* ig, double t, double dt, const float* v, float* jv, int mode) {
+    pl_mesh m = ig->mesh;
+    cudaStream_t s = m->ctx->stream;
+    int rc = ensure_reduced_cells(m);
+    if (rc) return rc;
+    const Rheology rheo = rheology_of(ig, true);
+    DomainParams p;
+    if ((rc = bind_domain(ig, rheo, false, &p)) != PL_OK) return rc;
+    p.cells = m->d_cells_red;
+    p.v32 = v;
+    p.out32 = jv;
+    p.t = t;
+    p.dt = dt;
+    if ((m->cell_type == PL_CELL_HEX8 || m->cell_type == PL_CELL_TET4) && ig->lm32_valid && ig->lm32_t == t &&
+        ig->lm32_dt == dt)
+        p.lm32 = ig->d_lm32;
+    if (mode == PL_INSERT) PLB_CUDA(cudaMemsetAsync(jv, 0, pl_mesh_num_dof(m) * sizeof(float), s));
+    if (use_blocked(ig) && m->cell_type == PL_CELL_TET4) {
+        if ((rc = ensure_blocked_layout(m)) != PL_OK || (rc = ensure_reduced_ids(m)) != PL_OK) return rc;
+        if (!launch_domain_jv32_blocked(p, *m->blocked, m->cell_type, rheo, m->nnodes, s, true)) return PL_ERR_UNSUPPORTED;
+    } else if (ig->scatter == PL_SCATTER_ATOMIC || !launch_domain_jv32_hexgroup(p, m->cell_type, rheo, s)) {
+        launch_domain_jv_f32_atomic(p, m->cell_type, rheo, s);
+    }
+    PLB_CUDA(cudaGetLastError());
+    return PL_OK;
+}
+
 int prepare_blocked(pl_integrator_s* ig) {
     pl_mesh m = ig->mesh;
     int rc = ensure_blocked_layout(m);
@@ -762,12 +877,6 @@ int prepare_blocked(pl_integrator_s* ig) {
 }  // namespace plb
 }
 
-static bool use_blocked(pl_integrator ig) {
-    pl_mesh m = ig->mesh;
-    if (ig->scatter == PL_SCATTER_ATOMIC) return false;
-    if (ig->subset) return false;  // the blocked layout covers whole meshes
-    return m->cell_type == PL_CELL_TET4 || ig->scatter == PL_SCATTER_BLOCKED || ig->scatter == PL_SCATTER_DETERMINISTIC;
-}
 
 int pl_compute_lhs_residual(pl_integrator ig, double t, double dt, const double* u, const double* u_t,
                             double* r, int mode) {

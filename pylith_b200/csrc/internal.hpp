@@ -91,10 +91,16 @@ struct BlockedLayout {
     uint32_t* d_pipe_ids = nullptr;         // node id | shared bit, per padded slot
     double* d_pipe_coords = nullptr;        // per block [3][padded slots] coordinates
     uint32_t* d_pipe_off = nullptr;         // per block, at d_pipe_begin[b] + 4 b: ns + 1 offsets
+    uint32_t* d_pipe_ids_red = nullptr;     // as d_pipe_ids in the reduced fault space (node of the
+                                            // reduced space | shared bit: the node has more than one
+                                            // slot), built on first use
     uint16_t* d_pipe_inc = nullptr;         // [num_blocks][4 * cells_per_block] staging offsets
                                             // corner * 3 * cells_per_block + cell, node groups of
                                             // the pipelined kernel
     size_t device_bytes = 0;
+    // host copies for the reduced slot ids
+    std::vector<uint32_t> h_pipe_ids;
+    std::vector<int32_t> h_pipe_begin, h_block_node_begin;
 };
 
 void context_retain(pl_context_s* c);
@@ -144,6 +150,11 @@ struct pl_mesh_s {
     int32_t* d_coh = nullptr;
     std::vector<int32_t> h_coh;
     plb::BlockedLayout* blocked = nullptr;
+    // The solvers' reduced fault space (each fault node's positive side follows its negative
+    // side): the connectivity with every positive-side node replaced by its negative-side
+    // partner, built on first use, and dropped when the cohesive cells change.
+    int32_t* d_cells_red = nullptr;
+    std::vector<int32_t> h_node_red;  // node -> node of the reduced space
 };
 
 namespace plb {
@@ -203,6 +214,7 @@ struct pl_solver_s {
     bool destroy_requested = false;
     pl_mesh mesh = nullptr;
     std::vector<pl_integrator> ops;
+    bool reduced = false;  // the operator runs in the reduced fault space directly (set up by pl_solver_setup)
     int64_t n = 0;       // DOFs (3 per node)
     int64_t nnodes = 0;  // node rows
     uint8_t* d_mask = nullptr;

@@ -48,10 +48,22 @@ void launch_domain_derived(const DomainParams& p, int cell, int rheo, const Deri
 int ensure_blocked_layout(pl_mesh_s* m);
 void free_blocked_layout(BlockedLayout* b, cudaStream_t after);
 // Cell-block (shared-memory, deterministic) residual / Jacobian action; returns false when the
-// layout does not support the configuration.
+// layout does not support the configuration. reduced: the solvers' reduced fault space (slot ids
+// of d_pipe_ids_red; padded-layout kernels only, no partial-sum buffer, output zeroed or holding
+// the sum to add to).
 bool launch_domain_apply_blocked(const DomainParams& p, const BlockedLayout& b, int cell,
                                  int rheo, bool bf, int op, bool insert, int64_t nnodes, double* partial,
-                                 cudaStream_t s);
+                                 cudaStream_t s, bool reduced = false);
+// The padded layout's slot ids in the reduced fault space (mesh with faults, after
+// ensure_reduced_cells); call outside stream capture.
+int ensure_reduced_ids(pl_mesh_s* m);
+// The reduced fault space of a mesh with faults (csrc/capi.cu): connectivity and node map.
+int ensure_reduced_cells(pl_mesh_s* m);
+// J v in the solvers' reduced fault space without unfold and fold (csrc/capi.cu); supported: see
+// jacobian_action_reduced_supported.
+bool jacobian_action_reduced_supported(pl_integrator_s* ig);
+int jacobian_action_reduced(pl_integrator_s* ig, double t, double dt, const double* v, double* jv, int mode);
+int jacobian_action_reduced_f32(pl_integrator_s* ig, double t, double dt, const float* v, float* jv, int mode);
 // The cell-block layout of the integrator's mesh and the integrator's partial-sum buffer
 // (allocations: call outside stream capture).
 int prepare_blocked(pl_integrator_s* ig);
@@ -78,7 +90,7 @@ const double* solver_reduced_rhs(pl_solver_s* S, const double* b);
 
 // FP32 Jacobian action on the cell blocks (the output must be zeroed or hold the sum to add to).
 bool launch_domain_jv32_blocked(const DomainParams& p, const BlockedLayout& b, int cell, int rheo, int64_t nnodes,
-                                cudaStream_t s);
+                                cudaStream_t s, bool reduced = false);
 
 struct CohesiveParams {
     const int32_t* coh;      // [ncoh][12]

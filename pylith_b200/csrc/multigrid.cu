@@ -152,17 +152,53 @@ __global__ void k_mg_residual(const T* __restrict__ in, const T* __restrict__ q,
         t[i] = mask[i] ? T(0) : (T)(in[i] + q[i]);
 }
 
-// coarse[c] = sum_j R[c][j] fine[col_j] (R = P^T in coarse rows), node by node, 3 components.
+// coarse[c] = sum_j R[c][j] fine[col_j] (R = P^T in coarse rows) for the 3 components, 0 on the
+// coarse level's masked DOFs: one warp per coarse node, its lanes over the row's entries, a fixed
+// shuffle tree for the sums.
 template <typename T>
 __global__ void k_mg_restrict(const T* __restrict__ fine, const int32_t* __restrict__ row, const int32_t* __restrict__ col,
-                              const double* __restrict__ val, int64_t nc, T* __restrict__ coarse) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * nc; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = i / 3;
-        const int k = (int)(i % 3);
-        double s = 0.0;
-        for (int32_t j = row[c]; j < row[c + 1]; ++j) s += val[j] * (double)fine[3 * (int64_t)col[j] + k];
-        coarse[i] = (T)s;
+                              const double* __restrict__ val, const uint8_t* __restrict__ cmask, int64_t nc,
+                              T* __restrict__ coarse) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < nc;
+         c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int32_t j = row[c] + lane; j < row[c + 1]; j += 32) {
+            const double w = val[j];
+            const int64_t f = 3 * (int64_t)col[j];
+            s0 += w * (double)fine[f];
+            s1 += w * (double)fine[f + 1];
+            s2 += w * (double)fine[f + 2];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        }
+        if (lane < 3) {
+            const int64_t i = 3 * c + lane;
+            coarse[i] = cmask[i] ? T(0) : (T)(lane == 0 ? s0 : (lane == 1 ? s1 : s2));
+        }
     }
+}
+
+// Prolongation columns in the coarse level's reduced space: a positive-side fault node's column
+// becomes its negative-side partner's (map: node -> node of the reduced space).
+__global__ void k_mg_map_cols(int32_t* col, int64_t nnz, const int32_t* __restrict__ map) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnz; j += (int64_t)gridDim.x * blockDim.x)
+        col[j] = map[col[j]];
+}
+
+__global__ void k_mg_iota(int32_t* map, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        map[i] = (int32_t)i;
+}
+
+__global__ void k_mg_pair_map2(int32_t* map, const int32_t* __restrict__ neg, const int32_t* __restrict__ pos,
+                               int64_t npairs) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < npairs; k += (int64_t)gridDim.x * blockDim.x)
+        map[pos[k]] = neg[k];
 }
 
 // fine[f] += sum_j P[f][j] coarse[col_j] on free DOFs (P in fine rows).
@@ -457,15 +493,13 @@ int vcycle(pl_multigrid mg, int l) {
     MgLevel& C = mg->lv[l + 1];
     T* rc_ = f32 ? (T*)C.r32 : (T*)C.r;
     T* zc = f32 ? (T*)C.z32 : (T*)C.z;
-    k_mg_restrict<T><<<mg_grid(3 * C.nmesh), 256, 0, s>>>(t, L.r_row, L.r_col, L.r_val, C.nmesh, rc_);
+    // the restriction's rows are the coarse level's reduced space (its prolongation columns were
+    // mapped onto it): no fold; the Lagrange rows of the coarse vector stay zero
+    if (C.n > 3 * C.nmesh) PLB_CUDA(cudaMemsetAsync(rc_ + 3 * C.nmesh, 0, (C.n - 3 * C.nmesh) * sizeof(T), s));
+    k_mg_restrict<T><<<mg_grid(32 * C.nmesh), 256, 0, s>>>(t, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, rc_);
     count_launch(2);
-    if (f32) solver_fold32(C.S, (float*)rc_);
-    else solver_fold(C.S, (double*)rc_);
-    k_mg_mask<T><<<mg_grid(C.n), 256, 0, s>>>(rc_, C.S->d_mask, C.n);
-    count_launch();
     if ((rc = vcycle<T>(mg, l + 1))) return rc;
-    if (f32) solver_unfold32(C.S, (float*)zc);
-    else solver_unfold(C.S, (double*)zc);
+    // ... and the prolongation reads the coarse correction there: no unfold
     k_mg_prolong_add<T><<<mg_grid(3 * L.nmesh), 256, 0, s>>>(zc, L.p_row, L.p_col, L.p_val, L.S->d_mask, L.nmesh, z);
     count_launch();
     // post-smoothing on the new residual
@@ -795,6 +829,17 @@ int pl_multigrid_create(pl_solver fine, int num_coarse, const pl_solver* coarse,
         up(&F.p_row, rp, (size_t)nf + 1);
         up(&F.p_col, prolong_col[l], (size_t)nnz);
         up(&F.p_val, prolong_val[l], (size_t)nnz);
+        if (e == cudaSuccess && C.S->npairs > 0 && nnz > 0) {
+            int32_t* d_map = nullptr;
+            e = dev_alloc(&d_map, (size_t)nc);
+            if (e == cudaSuccess) {
+                k_mg_iota<<<mg_grid(nc), 256, 0, s>>>(d_map, nc);
+                k_mg_pair_map2<<<mg_grid(C.S->npairs), 256, 0, s>>>(d_map, C.S->d_pair_neg, C.S->d_pair_pos, C.S->npairs);
+                k_mg_map_cols<<<mg_grid(nnz), 256, 0, s>>>(F.p_col, nnz, d_map);
+                count_launch(3);
+                dev_free(d_map, s);
+            }
+        }
         // the restriction P^T, its rows in increasing fine index
         A(&F.r_row, (size_t)nc + 1);
         A(&F.r_col, (size_t)nnz);

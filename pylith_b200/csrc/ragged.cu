@@ -338,6 +338,7 @@ void finish_member(pl_ragged R, Member& mb, int status) {
     mb.active = false;
     mb.status = status;
     R->dirty = true;
+    if (mb.S && mb.x) solver_unfold(mb.S, mb.x);  // the positive side of every fault node follows its negative side
 }
 
 }  // namespace

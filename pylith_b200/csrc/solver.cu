@@ -12,6 +12,7 @@
 //     products, inside FP64 iterative refinement (outer residual b - A x in FP64).
 // Reductions are two-pass and deterministic (per-CTA partials, then one CTA in fixed order).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -301,8 +302,17 @@ void fault_fold(pl_solver S, T* v) {
     count_launch();
 }
 
-// out = P^T J P v (the unfold writes the positive-side entries of v in place).
+// out = P^T J P v: with S->reduced by the kernels' reduced fault space (every positive-side node
+// read as, and added into, its negative-side partner), else by unfolding v in place (its
+// positive-side entries are written) and folding the result.
 int apply_J(pl_solver S, const double* v, double* out) {
+    if (S->reduced) {
+        for (size_t i = 0; i < S->ops.size(); ++i) {
+            int rc = jacobian_action_reduced(S->ops[i], S->t, S->dt, v, out, i == 0 ? PL_INSERT : PL_ADD);
+            if (rc) return rc;
+        }
+        return PL_OK;
+    }
     fault_unfold(S, const_cast<double*>(v));
     for (size_t i = 0; i < S->ops.size(); ++i) {
         int rc = pl_compute_lhs_jacobian_action(S->ops[i], S->t, S->dt, 0.0, nullptr, v, out, i == 0 ? PL_INSERT : PL_ADD);
@@ -313,6 +323,13 @@ int apply_J(pl_solver S, const double* v, double* out) {
 }
 
 int apply_J32(pl_solver S, const float* v, float* out) {
+    if (S->reduced) {
+        for (size_t i = 0; i < S->ops.size(); ++i) {
+            int rc = jacobian_action_reduced_f32(S->ops[i], S->t, S->dt, v, out, i == 0 ? PL_INSERT : PL_ADD);
+            if (rc) return rc;
+        }
+        return PL_OK;
+    }
     fault_unfold(S, const_cast<float*>(v));
     for (size_t i = 0; i < S->ops.size(); ++i) {
         int rc = pl_compute_lhs_jacobian_action_f32(S->ops[i], S->t, S->dt, v, out, i == 0 ? PL_INSERT : PL_ADD);
@@ -531,6 +548,7 @@ int pcg32_reliable(pl_solver S, const double* b, double* x) {
     c->stream = s;
     cudaEventRecord(S->ev_out, cs);
     cudaStreamWaitEvent(s, S->ev_out, 0);
+    fault_unfold(S, x);  // the positive side of every fault node follows its negative side
     return rc;
 }
 
@@ -762,6 +780,15 @@ int pl_solver_setup(pl_solver S, double t, double dt) {
         k_fault_fold_blocks<<<vec_grid(9 * S->npairs), 256, 0, s>>>(S->d_diag, S->d_pair_neg, S->d_pair_pos, S->npairs);
         count_launch();
     }
+    // the operator in the reduced fault space without unfold and fold launches, when every
+    // integrator supports it (PYLITH_B200_REDUCED_KERNELS=0: always unfold and fold)
+    S->reduced = false;
+    if (S->npairs > 0) {
+        const char* env = std::getenv("PYLITH_B200_REDUCED_KERNELS");
+        bool ok = !(env && env[0] == '0');
+        for (pl_integrator ig : S->ops) ok = ok && jacobian_action_reduced_supported(ig);
+        S->reduced = ok;
+    }
     k_invert_blocks<<<vec_grid(S->nnodes), 256, 0, s>>>(S->d_diag, S->d_mask, S->nnodes, S->d_pinv, S->d_pinv32);
     count_launch();
     PLB_CUDA(cudaGetLastError());
@@ -799,7 +826,7 @@ int pl_solver_solve(pl_solver S, const double* b, double* x) {
         return rc;
     }
     if (S->reliable) return pcg32_reliable(S, b, x);
-    // FP64 iterative refinement around FP32 PCG (apply_J unfolds x on every outer pass).
+    // FP64 iterative refinement around FP32 PCG (x unfolded before it is returned).
     PLB_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
     double h[S_COUNT];
     double b0 = -1.0;
@@ -815,7 +842,10 @@ int pl_solver_solve(pl_solver S, const double* b, double* x) {
         if (b0 < 0.0) b0 = rn;
         S->rel_residual = b0 > 0.0 ? rn / b0 : 0.0;
         S->outer_iterations = outer;
-        if (rn <= std::max(S->rtol * b0, S->atol) || b0 == 0.0) return PL_OK;
+        if (rn <= std::max(S->rtol * b0, S->atol) || b0 == 0.0) {
+            fault_unfold(S, x);
+            return PL_OK;
+        }
         int it = 0;
         double rel = 0.0;
         // Inner solve A d = r in FP32 (d in f_x).

@@ -638,3 +638,41 @@ def test_fp32_tet_jacobian_action_with_the_cached_tangent(ctx, rheology):
     assert rel(cached, per_cell) <= 1e-6
     assert rel(cached, ref) <= 1e-5
     S.close()
+
+
+@pytest.mark.parametrize("kind", ["tet", "hex"])
+def test_reduced_fault_space_operator_matches_unfold_and_fold(ctx, monkeypatch, kind):
+    """With faults, the solvers apply their operator in the reduced fault space directly (every
+    positive-side node read as, and added into, its negative-side partner: no unfold and fold
+    launches). FP64 and FP32-refined solves match the unfold-and-fold operator's to <= 1e-10 in
+    about the same number of iterations."""
+    from pylith_b200 import problems as P
+    from pylith_b200 import feassemble as FA
+
+    if kind == "tet":
+        lo, hi = (-6000.0, -6000.0, -9000.0), (6000.0, 6000.0, 0.0)
+        mesh = M.box_tet_delaunay_fault_x(40000, seed=5, lo=lo, hi=hi)
+    else:
+        lo, hi = M.BOX_LO, M.BOX_HI
+        mesh = M.insert_fault_x(M.box_hex(12, 10, 8))
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=11)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    cons[M.boundary_mask(mesh, 0, "neg", lo, hi)] = True
+    cons[M.boundary_mask(mesh, 0, "pos", lo, hi)] = True
+    cons = np.concatenate([cons.ravel(), np.zeros(3 * mesh.num_lagrange, dtype=bool)])
+    slip = np.zeros((mesh.num_lagrange, 3))
+    slip[: mesh.num_lagrange // 2, 1] = 1.0
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("PYLITH_B200_REDUCED_KERNELS", flag)
+        for prec in (FA.Solver.FP64, FA.Solver.FP32_REFINED):
+            prob = P.QuasistaticProblem(ctx, mesh, [(mat, None)], cons, np.zeros(mesh.num_dof),
+                                        faults=[MAT.FaultCohesiveKin(slip)], precision=prec, rtol=1e-12)
+            st = prob.step(0.0)
+            out[(flag, prec)] = (prob.u.cpu().numpy(), st.iterations + st.inner_iterations)
+            prob.close()
+    for prec in (FA.Solver.FP64, FA.Solver.FP32_REFINED):
+        (u1, i1), (u0, i0) = out[("1", prec)], out[("0", prec)]
+        assert np.linalg.norm(u1 - u0) <= 1e-10 * np.linalg.norm(u0), prec
+        assert abs(i1 - i0) <= 0.05 * i0 + 10, (prec, i1, i0)
