@@ -1049,7 +1049,7 @@ def config_c4(args):
     """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
     material, random rectangular left-lateral slip patch of 0.1-3 m. Server (HBM-budget admission;
     small boxes in one ragged batch of FP32-refined solves, boxes of 32^3 and more with a multigrid
-    hierarchy solved beside it by two workers with FP32 V-cycles) vs the plain FP64 one-at-a-time path (point-block
+    hierarchy solved beside it by three workers with FP32 V-cycles) vs the plain FP64 one-at-a-time path (point-block
     Jacobi), and vs FP64 one at a time with FP64 multigrid. The requests' host-side meshes (and
     multigrid hierarchies) are built before the stream starts, for all."""
     from pylith_b200 import feassemble as FA
@@ -1063,10 +1063,10 @@ def config_c4(args):
     warm = [SV.prepare(SV.Request(0, n, 1, 0.0, 1.0, (0.2, 0.8, 0.2, 0.8))) for n in (8, 32)]
     SV.Server(slots=64).run(warm)  # warm-up: device code loading and the first graph captures
     variants = {}
-    for k in (1, 3):
+    for k in (1, 2, 4):
         sv = SV.Server(slots=64, multigrid_workers=k)
         variants[k] = SV.summarize(sv.run(hps))["solves_per_s"]
-    server = SV.Server(slots=64, multigrid_workers=2)
+    server = SV.Server(slots=64, multigrid_workers=3)
     served = server.run(hps)
     seq = SV.serve_sequential(hps)
     seq_mg = SV.serve_sequential(hps, multigrid=FA.Solver.FP64)

@@ -154,7 +154,7 @@ class Server:
     V-cycles under FP64 conjugate gradients (their solves overlap on the device)."""
 
     def __init__(self, device: int = 0, slots: int = 64, hbm_budget: Optional[int] = None, rtol: float = 1e-10,
-                 keep_solutions=False, chunk: int = 10, multigrid: bool = True, multigrid_workers: int = 2):
+                 keep_solutions=False, chunk: int = 10, multigrid: bool = True, multigrid_workers: int = 3):
         import torch
 
         self.device = device
