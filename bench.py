@@ -901,9 +901,10 @@ def config_c3(args):
     cohesive cells) with the config-1 material statistics; 40x25 unit-slip patches over y in
     [-12,12] km, z in [-15,0] km, left-lateral then reverse: 2,000 impulses. Every impulse solved
     (a) batched (FP32 PCG tiles with reliable updates, tile and preconditioner picked by the
-    autotuner) and (b) one at a time by FP64 CG with FP32 multigrid V-cycles over independent
-    coarser Delaunay meshes of the box; against one-at-a-time FP64 solves of a sample of at least
-    20 impulses with point-block Jacobi and with FP64 multigrid."""
+    autotuner), (b) one at a time by FP64 CG with FP32 multigrid V-cycles over independent
+    coarser Delaunay meshes of the box, and (c) batched with one FP32 V-cycle on all 8 vectors of a
+    tile per iteration; against one-at-a-time FP64 solves of a sample of at least 20 impulses with
+    point-block Jacobi and with FP64 multigrid."""
     import torch
 
     from pylith_b200 import feassemble as FA
@@ -941,6 +942,8 @@ def config_c3(args):
     # baseline takes the same)
     mg_table = g.tune_multigrid(usable[step // 2::step][:6])
     mg64_h.set_smoother(g.mg.degree, g.mg.lower)
+    bmg = g.batched_multigrid(8)  # (c) tiles of 8 impulses, one V-cycle on all 8 per iteration
+    g.solve(usable[:8], batched=True, batch=bmg)  # warm-up: graph capture
     g.solve(usable[:8], batched=True)  # warm-up
     g.solve(usable[:1], batched=False)
     g.solve(usable[:2], batched=False, solver=mg32)
@@ -948,12 +951,16 @@ def config_c3(args):
     ns = max(20, int(args.steps))
     sample_s = usable[::max(1, len(usable) // ns)][:ns]
     want = {id(imp) for imp in sample_s}
-    keep_b, keep_m, t_b, t_m, its_m = {}, {}, 0.0, 0.0, []
+    keep_b, keep_m, keep_bm, t_b, t_m, t_bm, its_m = {}, {}, {}, 0.0, 0.0, 0.0, []
     for c0 in range(0, len(usable), 400):  # 400 impulses' vectors at a time on the device
         part = usable[c0:c0 + 400]
         sols, dt_part = g.solve(part, batched=True)
         t_b += dt_part
         keep_b.update({id(imp): x for imp, x in zip(part, sols) if id(imp) in want})
+        del sols
+        sols, dt_part = g.solve(part, batched=True, batch=bmg)
+        t_bm += dt_part
+        keep_bm.update({id(imp): x for imp, x in zip(part, sols) if id(imp) in want})
         del sols
         sols, dt_part = g.solve(part, batched=False, solver=mg32)
         t_m += dt_part
@@ -969,7 +976,8 @@ def config_c3(args):
     def err(keep, ref):
         return max(float(torch.linalg.norm(keep[id(imp)] - b) / torch.linalg.norm(b)) for imp, b in zip(sample_s, ref))
 
-    rate_b, rate_m = len(usable) / t_b, len(usable) / t_m
+    rate_b, rate_m, rate_bm = len(usable) / t_b, len(usable) / t_m, len(usable) / t_bm
+    st_bm = bmg.stats()
     rate_s, rate_g = len(sample_s) / t_s, len(sample_s) / t_g
     return {"config": "c3", "cells": mesh.num_cells, "dof": mesh.num_dof, "mesh": "Delaunay, mirrored across the fault",
             "mesh_build_s": t_mesh, "impulses_total": len(g.impulses), "impulses_solved": len(usable),
@@ -985,12 +993,18 @@ def config_c3(args):
                                                             "iterations": it} for d, lo, r, it in mg_table],
                                        "how": "one impulse at a time: FP64 flexible CG, one FP32 V-cycle "
                                               "(Chebyshev-Jacobi smoothing) per iteration"},
+            "batched_multigrid": {"solves_per_s": rate_bm, "seconds": t_bm, "tile": 8, "last_call_stats": st_bm,
+                                  "how": "tiles of 8 impulses: FP32 PCG with reliable updates, one FP32 V-cycle "
+                                         "on all 8 vectors per iteration (batched cell-block operator on every level)"},
             "fp64_one_at_a_time": {"sample": len(sample_s), "solves_per_s": rate_s, "iterations_last": its_s,
                                    "preconditioner": "point-block Jacobi"},
             "fp64_multigrid_one_at_a_time": {"sample": len(sample_s), "solves_per_s": rate_g, "iterations_last": its_g},
             "speedup": rate_b / rate_s,
             "speedup_multigrid_vs_fp64": rate_m / rate_s,
             "speedup_multigrid_vs_fp64_multigrid": rate_m / rate_g,
+            "speedup_batched_multigrid_vs_fp64": rate_bm / rate_s,
+            "speedup_batched_multigrid_vs_fp64_multigrid": rate_bm / rate_g,
+            "max_rel_displacement_error_batched_multigrid_vs_fp64": err(keep_bm, sol_s),
             "max_rel_displacement_error_vs_fp64": err(keep_b, sol_s),
             "max_rel_displacement_error_multigrid_vs_fp64": err(keep_m, sol_s)}
 

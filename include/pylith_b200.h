@@ -410,6 +410,14 @@ int pl_batch_solver_set_chebyshev(pl_batch_solver solver, int degree, double low
  * dropped by the base solver's inner_rtol. pl_batch_solver_get_stats counts FP64 true residuals
  * after the first as outer iterations with reliable updates, refinement passes without. */
 int pl_batch_solver_set_reliable(pl_batch_solver solver, int enable, double delta);
+/* Preconditions the tile's FP32 PCG with one V-cycle of `mg` per iteration on all K vectors at
+ * once (NULL: back to the Chebyshev or point-block Jacobi setting): the hierarchy's smoothing,
+ * transfers and dense coarsest inverse, with the batched cell-block operator on every level (P1
+ * tetrahedra, isotropic linear elasticity; tiles of at most 8). The hierarchy's fine level must be
+ * the base solver's mesh, and its fine solver set up at the same (t, dt); the eigenvalue estimates
+ * come from the hierarchy (made at the next solve if not yet). pl_multigrid_destroy is refused while
+ * a batched solver uses the hierarchy. */
+int pl_batch_solver_set_multigrid(pl_batch_solver solver, pl_multigrid mg);
 int pl_batch_solver_get_chebyshev(pl_batch_solver solver, double* lambda_max);
 int pl_batch_solver_get_stats(pl_batch_solver solver, int64_t* solves, int64_t* inner_iterations,
                               int64_t* outer_iterations, double* max_rel_residual);

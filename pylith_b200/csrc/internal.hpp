@@ -256,4 +256,29 @@ namespace plb {
 int multigrid_setup(pl_multigrid_s* mg, double t, double dt);
 int multigrid_solve(pl_multigrid_s* mg, const double* b, double* x);
 void multigrid_detach(pl_multigrid_s* mg);
+// A hierarchy as the batched solver's V-cycles read it (csrc/multirhs.cu): per level its solver,
+// sizes, transfer operators (prolongation columns and restriction rows in the coarse level's
+// reduced fault space) and lambda_max(D^-1 A); the smoothing; the coarsest level's dense FP32
+// inverse (dense_n 0: none). multigrid_prepare makes the eigenvalue estimates and the dense
+// inverse current (outside stream capture).
+struct MgLevelView {
+    pl_solver_s* S;
+    int64_t n, nn, nmesh;
+    const int32_t *p_row, *p_col, *r_row, *r_col;
+    const double *p_val, *r_val;
+    double lmax;
+};
+struct MgView {
+    std::vector<MgLevelView> levels;
+    int degree;
+    double lower;
+    int coarse_degree;
+    double coarse_lower;
+    const float* dense_inv32;
+    const int32_t* dense_idx;
+    int dense_n;
+};
+int multigrid_prepare(pl_multigrid_s* mg);
+MgView multigrid_view(const pl_multigrid_s* mg);
+void multigrid_batch_use(pl_multigrid_s* mg, int delta);
 }  // namespace plb

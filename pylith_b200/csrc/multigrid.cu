@@ -414,6 +414,7 @@ struct pl_multigrid_s {
     bool fp32 = false;
     bool eig_valid = false;
     pl_solver attached = nullptr;
+    int batch_users = 0;  // batched solvers preconditioned by this hierarchy
     // outer PCG state
     double *x = nullptr, *r = nullptr, *r_old = nullptr, *p = nullptr, *q = nullptr, *z = nullptr;
     double* scal = nullptr;
@@ -769,6 +770,29 @@ int multigrid_solve(pl_multigrid mg, const double* b, double* x) {
 
 void multigrid_detach(pl_multigrid mg) { mg->attached = nullptr; }
 
+int multigrid_prepare(pl_multigrid mg) {
+    if (mg->eig_valid) return PL_OK;
+    int rc = prepare_dense(mg);
+    if (rc == PL_OK) rc = estimate_eigenvalues(mg);
+    return rc;
+}
+
+MgView multigrid_view(const pl_multigrid_s* mg) {
+    MgView v;
+    for (const MgLevel& L : mg->lv)
+        v.levels.push_back({L.S, L.n, L.nn, L.nmesh, L.p_row, L.p_col, L.r_row, L.r_col, L.p_val, L.r_val, L.lmax});
+    v.degree = mg->degree;
+    v.lower = mg->lower;
+    v.coarse_degree = mg->coarse_degree;
+    v.coarse_lower = mg->coarse_lower;
+    v.dense_inv32 = mg->dense_ok ? mg->d_dense32 : nullptr;
+    v.dense_idx = mg->dense_ok ? mg->d_dense_idx : nullptr;
+    v.dense_n = mg->dense_ok ? mg->dense_n : 0;
+    return v;
+}
+
+void multigrid_batch_use(pl_multigrid mg, int delta) { mg->batch_users += delta; }
+
 }  // namespace plb
 
 extern "C" {
@@ -919,6 +943,7 @@ int pl_multigrid_get_levels(pl_multigrid mg, int* num_levels, double* lambda_max
 int pl_multigrid_destroy(pl_multigrid mg) {
     if (!mg) return PL_OK;
     if (mg->attached) return fail(PL_ERR_INVALID_ARG, "the hierarchy is still attached to its solver");
+    if (mg->batch_users > 0) return fail(PL_ERR_INVALID_ARG, "the hierarchy still preconditions a batched solver");
     if (mg->ctx) {
         cudaSetDevice(mg->ctx->device);
         cudaStreamSynchronize(mg->ctx->stream);

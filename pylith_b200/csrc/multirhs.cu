@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 
+#include "cg.cuh"
 #include "domain_kernels.cuh"
 #include "internal.hpp"
 #include "launch.hpp"
@@ -649,10 +650,19 @@ __global__ void __launch_bounds__(kBThreads) k_b_update(float* r, const float* q
 // pass that reads p anyway.
 template <int K>
 __global__ void k_b_pupdate(float* x, float* p, const float* z, const uint8_t* mask, int64_t n, const double* rz,
-                            const double* rz_old, const double* pq, const int* active) {
+                            const double* rz_old, const double* pq, const int* active, const double* zq = nullptr) {
     const int k = threadIdx.x % K;
     const float alpha = active[k] ? safe_step_f32(rz_old[k], pq[k]) : 0.0f;
-    const float beta = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
+    // zq (a preconditioner that is not exactly fixed, the FP32 V-cycle): the flexible step
+    // beta = max(0, z.(r - r_old) / rz_old) = max(0, z.q / p.(A p)) with r - r_old = alpha q
+    float beta;
+    if (zq) {
+        const double bz = pq[k] > 0.0 ? zq[k] / pq[k] : 0.0;
+        beta = (active[k] && isfinite(bz) && bz > 0.0) ? (float)bz : 0.0f;
+    } else {
+        beta = (active[k] && rz_old[k] != 0.0) ? (float)(rz[k] / rz_old[k]) : 0.0f;
+    }
+    if (!isfinite(beta)) beta = 0.0f;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x) {
         const float pe = p[e];
         if (!mask[e / K]) x[e] += alpha * pe;
@@ -926,6 +936,14 @@ struct pl_batch_solver_s {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int64_t solves = 0, inner_iterations = 0, outer_iterations = 0;
     double max_rel_residual = 0.0;
+    // Multigrid preconditioner (pl_batch_solver_set_multigrid): one V-cycle of the hierarchy on
+    // the tile's K vectors per iteration, [n_l][K] work vectors per level.
+    struct BmgLevel {
+        float *r = nullptr, *z = nullptr, *t = nullptr, *d = nullptr, *q = nullptr, *w = nullptr;
+    };
+    pl_multigrid mg = nullptr;
+    std::vector<BmgLevel> bmg;
+    plb::MgView mgv;
 };
 
 namespace plb {
@@ -946,8 +964,8 @@ bool fuses_energies(pl_batch_solver B) {
 // fuses_energies), the energies v.(A v) are summed by the same launch into pq[K] (scaled by the
 // tile's current r.z, B->scal[0..K)).
 template <int K>
-int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullptr) {
-    pl_solver S = B->base;
+int jv32_multi_on(pl_solver S, int64_t n, const float* v, float* out, double* pq, unsigned int* ticket, double* part,
+                  const double* scal) {
     pl_mesh m = S->mesh;
     cudaStream_t s = m->ctx->stream;
     if (pq && S->ops.size() != 1) return fail(PL_ERR_UNSUPPORTED, "fused energies need a single integrator");
@@ -955,7 +973,7 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullp
         k_b_unfold<K><<<bgrid(3 * K * S->npairs), 256, 0, s>>>(const_cast<float*>(v), S->d_pair_neg, S->d_pair_pos, S->npairs);
         count_launch();
     }
-    PLB_CUDA(cudaMemsetAsync(out, 0, B->n * K * sizeof(float), s));
+    PLB_CUDA(cudaMemsetAsync(out, 0, n * K * sizeof(float), s));
     bool first = true;
     for (pl_integrator ig : S->ops) {
         DomainParams pp;
@@ -985,13 +1003,12 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullp
         const int grid = (int)std::min<int64_t>(L.num_blocks, (int64_t)sm_count() * per_sm);
         FinSpec fin;
         if (pq) {
-            fin.counter = B->ticket;
+            fin.counter = ticket;
             fin.out_a = pq;
         }
         k_tet_blocked_jv32_multi<K><<<grid, kMultiBlockCells, smem, s>>>(
             pp, L.d_cell_begin, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
-            L.d_pipe_begin, L.d_pipe_coords, L.num_blocks, ld, v, out, first, pq ? B->part_a : nullptr, B->scal,
-            fin);
+            L.d_pipe_begin, L.d_pipe_coords, L.num_blocks, ld, v, out, first, pq ? part : nullptr, scal, fin);
         first = false;
         count_launch();
     }
@@ -1000,6 +1017,11 @@ int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullp
         count_launch();
     }
     return PL_OK;
+}
+
+template <int K>
+int jv32_multi(pl_batch_solver B, const float* v, float* out, double* pq = nullptr) {
+    return jv32_multi_on<K>(B->base, B->n, v, out, pq, B->ticket, B->part_a, B->scal);
 }
 
 // z = q(P A) P r with the Chebyshev coefficients of the solver; partial r.z into part_a (and,
@@ -1027,6 +1049,248 @@ int cheb_apply(pl_batch_solver B, FinSpec fin = FinSpec()) {
     return PL_OK;
 }
 
+// ---- multigrid V-cycles on the tile's K vectors ([n][K], one thread per (DOF or node, rhs)) ----
+// The same cycle as the single-vector multigrid (csrc/multigrid.cu): Chebyshev-Jacobi pre- and
+// post-smoothing, restriction and prolongation in the coarse levels' reduced fault spaces, the
+// coarsest level by its dense inverse; the level operators are the batched cell-block kernel.
+
+// out = D^{-1} in / theta; d = out
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_cheb_first(const float* __restrict__ in, const float* __restrict__ P,
+                                                              int64_t nnodes, float inv_theta, float* __restrict__ d,
+                                                              float* __restrict__ out) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        const int k = (int)(t % K);
+        float z[3];
+        pinv_apply<K>(P, in, nd, k, z);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const float v = z[c] * inv_theta;
+            d[i] = v;
+            out[i] = v;
+        }
+    }
+}
+
+// res = in - A out (= in + q on free DOFs), d = c1 d + c2 D^{-1} res, out += d
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_cheb_next(const float* __restrict__ in, const float* __restrict__ q,
+                                                             const float* __restrict__ P, const uint8_t* __restrict__ mask,
+                                                             int64_t nnodes, float c1, float c2, float* __restrict__ d,
+                                                             float* __restrict__ out) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnodes * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t nd = t / K;
+        const int k = (int)(t % K);
+        float res[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            res[c] = mask[3 * nd + c] ? 0.0f : in[i] + q[i];
+        }
+        const float* Bk = P + 9 * nd;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = (3 * nd + c) * K + k;
+            const float zr = Bk[3 * c] * res[0] + Bk[3 * c + 1] * res[1] + Bk[3 * c + 2] * res[2];
+            const float dv = c1 * d[i] + c2 * zr;
+            d[i] = dv;
+            out[i] += dv;
+        }
+    }
+}
+
+// t = in + q on free DOFs (in - A z), 0 elsewhere
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_residual(const float* __restrict__ in, const float* __restrict__ q,
+                                                            const uint8_t* __restrict__ mask, int64_t n,
+                                                            float* __restrict__ t) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
+        t[e] = mask[e / K] ? 0.0f : in[e] + q[e];
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_axpy(float* __restrict__ y, const float* __restrict__ x, int64_t n) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] += x[e];
+}
+
+// coarse[(3c + comp)][k] = sum_j R[c][j] fine[(3 col_j + comp)][k], 0 on the coarse level's masked
+// DOFs (R = P^T in coarse rows, in the coarse reduced space)
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_restrict(const float* __restrict__ fine, const int32_t* __restrict__ row,
+                                                            const int32_t* __restrict__ col, const double* __restrict__ val,
+                                                            const uint8_t* __restrict__ cmask, int64_t nc,
+                                                            float* __restrict__ coarse) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3 * nc * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t ck = t / K;  // coarse DOF
+        const int k = (int)(t % K);
+        const int64_t c = ck / 3;
+        const int comp = (int)(ck % 3);
+        double sum = 0.0;
+        if (!cmask[ck])
+            for (int32_t j = row[c]; j < row[c + 1]; ++j) sum += val[j] * (double)fine[(3 * (int64_t)col[j] + comp) * K + k];
+        coarse[t] = (float)sum;
+    }
+}
+
+// fine[(3f + comp)][k] += sum_j P[f][j] coarse[(3 col_j + comp)][k] on free fine DOFs
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_prolong_add(const float* __restrict__ coarse, const int32_t* __restrict__ row,
+                                                               const int32_t* __restrict__ col, const double* __restrict__ val,
+                                                               const uint8_t* __restrict__ mask, int64_t nf,
+                                                               float* __restrict__ fine) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3 * nf * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t fk = t / K;
+        if (mask[fk]) continue;
+        const int k = (int)(t % K);
+        const int64_t f = fk / 3;
+        const int comp = (int)(fk % 3);
+        double sum = 0.0;
+        for (int32_t j = row[f]; j < row[f + 1]; ++j) sum += val[j] * (double)coarse[(3 * (int64_t)col[j] + comp) * K + k];
+        fine[t] += (float)sum;
+    }
+}
+
+// z[idx[i]][k] = sum_j inv[i][j] r[idx[j]][k] (z zeroed before): each block stages the gathered
+// right-hand sides ([n][K] floats of dynamic shared memory), one thread per (row, rhs).
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_bmg_dense(const float* __restrict__ inv, const int32_t* __restrict__ idx, int n,
+                                                         const float* __restrict__ r, float* __restrict__ z) {
+    extern __shared__ float sr[];
+    for (int t = threadIdx.x; t < n * K; t += blockDim.x) sr[t] = r[(int64_t)idx[t / K] * K + t % K];
+    __syncthreads();
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * K; t += gridDim.x * blockDim.x) {
+        const int i = t / K, k = t % K;
+        const float* row = inv + (int64_t)i * n;
+        float acc = 0.0f;
+        for (int j = 0; j < n; ++j) acc += row[j] * sr[j * K + k];
+        z[(int64_t)idx[i] * K + k] = acc;
+    }
+}
+
+// partials of r.z (part) and, with q, of z.q (part_q) over free DOFs by right-hand side (and, with
+// fin.counter, the final sums: r.z into fin.out_a, z.q into fin.out_b)
+template <int K>
+__global__ void __launch_bounds__(kBThreads) k_b_rz(const float* __restrict__ r, const float* __restrict__ z,
+                                                    const float* __restrict__ q, const uint8_t* __restrict__ mask,
+                                                    int64_t n, double* part, double* part_q, FinSpec fin) {
+    double acc = 0.0, accq = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * K; e += (int64_t)gridDim.x * blockDim.x)
+        if (!mask[e / K]) {
+            acc += (double)r[e] * z[e];
+            if (q) accq += (double)z[e] * q[e];
+        }
+    block_sum_by_rhs<K>(acc, part);
+    if (q) {
+        __syncthreads();
+        block_sum_by_rhs<K>(accq, part_q);
+    }
+    if (fin.counter && take_last_ticket(fin.counter)) {
+        sum_partials_last_block<K>(part, fin.out_a, fin.prev_a);
+        if (q && fin.out_b) sum_partials_last_block<K>(part_q, fin.out_b, nullptr);
+    }
+}
+
+// Level l's operator on K vectors: the batched cell-block kernel of its solver (level 0: the
+// tile's own solver) with its faults' unfold and fold.
+template <int K>
+int bmg_jv(pl_batch_solver B, int l, const float* v, float* out) {
+    pl_solver S = l == 0 ? B->base : B->mgv.levels[l].S;
+    return jv32_multi_on<K>(S, S->n, v, out, nullptr, B->ticket, B->part_a, B->scal);
+}
+
+// Chebyshev-Jacobi polynomial of level l on K vectors from a zero guess (as the single-vector
+// multigrid's cheb()).
+template <int K>
+int bmg_cheb(pl_batch_solver B, int l, const float* in, float* out, int degree, double lower) {
+    const MgLevelView& L = B->mgv.levels[l];
+    pl_solver S = l == 0 ? B->base : L.S;
+    const pl_batch_solver_s::BmgLevel& W = B->bmg[l];
+    cudaStream_t s = S->mesh->ctx->stream;
+    const double b = 1.1 * L.lmax, a = lower * b;
+    const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+    k_bmg_cheb_first<K><<<kBBlocks, kBThreads, 0, s>>>(in, S->d_pinv32, S->nnodes, (float)(1.0 / theta), W.d, out);
+    count_launch();
+    double rho_old = 1.0 / sigma;
+    for (int i = 1; i < degree; ++i) {
+        int rc = bmg_jv<K>(B, l, out, W.q);
+        if (rc) return rc;
+        const double rho = 1.0 / (2.0 * sigma - rho_old);
+        k_bmg_cheb_next<K><<<kBBlocks, kBThreads, 0, s>>>(in, W.q, S->d_pinv32, S->d_mask, S->nnodes, (float)(rho * rho_old),
+                                                          (float)(2.0 * rho / delta), W.d, out);
+        count_launch();
+        rho_old = rho;
+    }
+    return PL_OK;
+}
+
+// z = V(r) on level l (K vectors)
+template <int K>
+int bmg_vcycle(pl_batch_solver B, int l, const float* r, float* z) {
+    const MgView& V = B->mgv;
+    const MgLevelView& L = V.levels[l];
+    pl_solver S = l == 0 ? B->base : L.S;
+    const pl_batch_solver_s::BmgLevel& W = B->bmg[l];
+    cudaStream_t s = S->mesh->ctx->stream;
+    const int last = (int)V.levels.size() - 1;
+    if (l == last) {
+        if (V.dense_n > 0) {
+            PLB_CUDA(cudaMemsetAsync(z, 0, S->n * K * sizeof(float), s));
+            const size_t smem = (size_t)V.dense_n * K * sizeof(float);
+            ensure_kernel_smem((const void*)k_bmg_dense<K>, smem);
+            const int grid = std::max(1, std::min((V.dense_n * K + kBThreads - 1) / kBThreads, 148));
+            k_bmg_dense<K><<<grid, kBThreads, smem, s>>>(V.dense_inv32, V.dense_idx, V.dense_n, r, z);
+            count_launch();
+            return PL_OK;
+        }
+        return bmg_cheb<K>(B, l, r, z, V.coarse_degree, V.coarse_lower);
+    }
+    int rc = bmg_cheb<K>(B, l, r, z, V.degree, V.lower);
+    if (rc) return rc;
+    if ((rc = bmg_jv<K>(B, l, z, W.q))) return rc;
+    k_bmg_residual<K><<<kBBlocks, kBThreads, 0, s>>>(r, W.q, S->d_mask, S->n, W.t);
+    const MgLevelView& C = V.levels[l + 1];
+    const pl_batch_solver_s::BmgLevel& Wc = B->bmg[l + 1];
+    if (C.n > 3 * C.nmesh) PLB_CUDA(cudaMemsetAsync(Wc.r + 3 * C.nmesh * K, 0, (C.n - 3 * C.nmesh) * K * sizeof(float), s));
+    k_bmg_restrict<K><<<kBBlocks, kBThreads, 0, s>>>(W.t, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, Wc.r);
+    count_launch(2);
+    if ((rc = bmg_vcycle<K>(B, l + 1, Wc.r, Wc.z))) return rc;
+    k_bmg_prolong_add<K><<<kBBlocks, kBThreads, 0, s>>>(Wc.z, L.p_row, L.p_col, L.p_val, S->d_mask, L.nmesh, z);
+    count_launch();
+    if ((rc = bmg_jv<K>(B, l, z, W.q))) return rc;
+    k_bmg_residual<K><<<kBBlocks, kBThreads, 0, s>>>(r, W.q, S->d_mask, S->n, W.t);
+    count_launch();
+    if ((rc = bmg_cheb<K>(B, l, W.t, W.w, V.degree, V.lower))) return rc;
+    k_bmg_axpy<K><<<kBBlocks, kBThreads, 0, s>>>(z, W.w, S->n);
+    count_launch();
+    return PL_OK;
+}
+
+// z = V(r) for the tile; partial r.z into part_a (and with fin.counter the final sums).
+template <int K>
+int bmg_apply(pl_batch_solver B, FinSpec fin = FinSpec()) {
+    pl_solver S = B->base;
+    cudaStream_t s = S->mesh->ctx->stream;
+    int rc = bmg_vcycle<K>(B, 0, B->r, B->z);
+    if (rc) return rc;
+    // inside an iteration (fin.out_b set) also z.q for the flexible step (q = J p of this iteration)
+    k_b_rz<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, fin.out_b ? B->q : nullptr, S->d_mask, B->n, B->part_a,
+                                             B->part_b, fin);
+    count_launch();
+    return PL_OK;
+}
+
+// The polynomial or multigrid preconditioner of the tile (point-block Jacobi runs inside the
+// update kernels instead).
+bool tile_preconditioned(pl_batch_solver B) { return B->mg || B->cheb_degree >= 2; }
+
+template <int K>
+int precond_apply(pl_batch_solver B, FinSpec fin = FinSpec()) {
+    return B->mg ? bmg_apply<K>(B, fin) : cheb_apply<K>(B, fin);
+}
+
 // One PCG iteration for all K vectors of the tile (capturable: kernels and memsets only).
 template <int K>
 int pcg_iteration(pl_batch_solver B) {
@@ -1047,7 +1311,7 @@ int pcg_iteration(pl_batch_solver B) {
         k_b_pq<K><<<kBBlocks, kBThreads, 0, s>>>(B->p, B->q, S->d_mask, B->n, B->part_a, fpq);
         count_launch();
     }
-    if (B->cheb_degree >= 2) {
+    if (tile_preconditioned(B)) {
         FinSpec frr;
         frr.counter = B->ticket;
         frr.out_a = rr;
@@ -1058,7 +1322,8 @@ int pcg_iteration(pl_batch_solver B) {
         frz.counter = B->ticket;
         frz.out_a = rz;
         frz.prev_a = rz_old;
-        rc = cheb_apply<K>(B, frz);
+        if (B->mg) frz.out_b = B->scal + 5 * kMaxTile;  // z.q of the flexible step
+        rc = precond_apply<K>(B, frz);
         if (rc) return rc;
     } else {
         FinSpec fu;
@@ -1075,7 +1340,8 @@ int pcg_iteration(pl_batch_solver B) {
         count_launch();
         return PL_OK;
     }
-    k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->p, B->z, S->d_mask, B->n, rz, rz_old, pq, B->active);
+    k_b_pupdate<K><<<kBBlocks, kBThreads, 0, s>>>(B->x, B->p, B->z, S->d_mask, B->n, rz, rz_old, pq, B->active,
+                                                  B->mg ? B->scal + 5 * kMaxTile : nullptr);
     count_launch();
     return PL_OK;
 }
@@ -1167,9 +1433,9 @@ int tile_pcg(pl_batch_solver B, int nact, double rtol, int max_iter, int* iters)
     count_launch(3);
     double h[4 * kMaxTile];
     int act[kMaxTile];
-    if (B->cheb_degree >= 2) {
-        // z = q(P A) P r, p = z, rz = r.z
-        int rc = cheb_apply<K>(B);
+    if (tile_preconditioned(B)) {
+        // z = q(P A) P r or V(r), p = z, rz = r.z
+        int rc = precond_apply<K>(B);
         if (rc) return rc;
         k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
         count_launch();
@@ -1279,7 +1545,7 @@ int solve_reliable(pl_batch_solver B, int nrhs, const double* const* bs, double*
     cudaStream_t s = S->mesh->ctx->stream;
     const int64_t n = B->n;
     double bnorm[kMaxTile] = {0}, rref[kMaxTile] = {0};
-    int act[kMaxTile] = {0}, slot[kMaxTile], iters[kMaxTile] = {0};
+    int act[kMaxTile] = {0}, slot[kMaxTile], iters[kMaxTile] = {0}, breakdowns[kMaxTile] = {0};
     bool fresh[kMaxTile] = {false}, replaced[kMaxTile] = {false};
     for (int k = 0; k < K; ++k) slot[k] = -1;
     int next = 0;
@@ -1324,8 +1590,8 @@ int solve_reliable(pl_batch_solver B, int nrhs, const double* const* bs, double*
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
     k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_b, kBBlocks, B->scal + 3 * K, nullptr);
     count_launch(3);
-    if (B->cheb_degree >= 2) {
-        if ((rc = cheb_apply<K>(B)) != PL_OK) return rc;
+    if (tile_preconditioned(B)) {
+        if ((rc = precond_apply<K>(B)) != PL_OK) return rc;
         k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
         count_launch();
         PLB_CUDA(cudaMemcpyAsync(B->p, B->z, n * K * sizeof(float), cudaMemcpyDeviceToDevice, s));
@@ -1348,7 +1614,21 @@ int solve_reliable(pl_batch_solver B, int nrhs, const double* const* bs, double*
             iters[k] += chunk;
             if (iters[k] > S->max_iter) return fail(PL_ERR_NOT_CONVERGED, "batched PCG reached the iteration limit");
             const double rn = std::sqrt(h[3 * K + k]);
-            if (!(rn == rn)) return fail(PL_ERR_NOT_CONVERGED, "batched PCG diverged (NaN residual)");
+            // FP32 breakdown (the iterated residual not a number or far above the last true one):
+            // drop the column's FP32 correction and restart it from its FP64 true residual
+            const bool broke = !(rn == rn) || rn > kBreakdownGrowth * rref[k];
+            if (broke) {
+                if (++breakdowns[k] > kMaxBreakdowns)
+                    return fail(PL_ERR_NOT_CONVERGED, "batched PCG broke down repeatedly");
+                k_b_col_zero<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k);
+                count_launch();
+                double rt = 0.0;
+                if ((rc = col_true_residual(B, K, k, bs[slot[k]], xs[slot[k]], &rt)) != PL_OK) return rc;
+                B->outer_iterations++;
+                rref[k] = rt;
+                fresh[k] = update_z = true;  // p = z again
+                continue;
+            }
             if (rn > B->reliable_delta * rref[k] && rn > 0.5 * S->rtol * bnorm[k]) continue;
             const int j = slot[k];
             k_b_unpack_add<<<bgrid(n), 256, 0, s>>>(B->x, n, K, k, S->d_mask, xs[j]);
@@ -1370,10 +1650,10 @@ int solve_reliable(pl_batch_solver B, int nrhs, const double* const* bs, double*
             replaced[k] = update_z = true;
         }
         if (update_z) {
-            if (B->cheb_degree >= 2) {
-                // z = q(P A) P r with the same polynomial for the whole tile (the other columns get
-                // their own z and r.z again), so the preconditioner stays fixed
-                if ((rc = cheb_apply<K>(B)) != PL_OK) return rc;
+            if (tile_preconditioned(B)) {
+                // z = q(P A) P r (or V(r)) with the same operator for the whole tile (the other
+                // columns get their own z and r.z again), so the preconditioner stays fixed
+                if ((rc = precond_apply<K>(B)) != PL_OK) return rc;
                 k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
                 count_launch();
             } else {
@@ -1479,7 +1759,7 @@ int pl_batch_solver_create(pl_solver base, int tile, pl_batch_solver* out) {
     };
     const size_t nk = (size_t)B->n * tile;
     A(&B->r, nk); A(&B->z, nk); A(&B->p, nk); A(&B->q, nk); A(&B->x, nk);
-    A(&B->scal, 4 * kMaxTile + 1);
+    A(&B->scal, 6 * kMaxTile);  // rz, rz_old, pq, rr; the outer residual; z.q (flexible step)
     A(&B->active, kMaxTile);
     A(&B->part_a, (size_t)kBBlocks * kMaxTile);
     A(&B->part_b, (size_t)kBBlocks * kMaxTile);
@@ -1519,7 +1799,21 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
     PLB_CUDA(cudaStreamWaitEvent(B->stream, B->ev_in, 0));
     c->stream = B->stream;
     int rc = PL_OK;
-    if (nrhs > 0 && B->cheb_degree >= 2 && (B->cheb_version == 0 || B->cheb_epoch != state_epoch())) {
+    if (nrhs > 0 && B->mg) {
+        // the hierarchy's eigenvalue estimates and dense coarsest inverse (made by its first solve
+        // after a setup, or here)
+        rc = multigrid_prepare(B->mg);
+        if (rc == PL_OK) {
+            const MgView v = multigrid_view(B->mg);
+            bool changed = v.levels.size() != B->mgv.levels.size() || v.dense_inv32 != B->mgv.dense_inv32 ||
+                           v.degree != B->mgv.degree || v.lower != B->mgv.lower;
+            for (size_t l = 0; !changed && l < v.levels.size(); ++l) changed = v.levels[l].lmax != B->mgv.levels[l].lmax;
+            B->mgv = v;
+            if (changed) B->cheb_version++;  // the captured iterations hold the coefficients
+        }
+    }
+    if (rc == PL_OK && nrhs > 0 && !B->mg && B->cheb_degree >= 2 &&
+        (B->cheb_version == 0 || B->cheb_epoch != state_epoch())) {
         switch (B->K) {
             case 1: rc = cheb_setup<1>(B); break;
             case 2: rc = cheb_setup<2>(B); break;
@@ -1601,11 +1895,63 @@ int pl_batch_solver_get_stats(pl_batch_solver B, int64_t* solves, int64_t* inner
     return PL_OK;
 }
 
+static void bmg_release(pl_batch_solver B) {
+    cudaStream_t s = B->base->mesh->ctx->stream;
+    for (auto& W : B->bmg)
+        for (float* p : {W.r, W.z, W.t, W.d, W.q, W.w}) dev_free(p, s);
+    B->bmg.clear();
+    if (B->mg) multigrid_batch_use(B->mg, -1);
+    B->mg = nullptr;
+    B->mgv = MgView();
+}
+
+int pl_batch_solver_set_multigrid(pl_batch_solver B, pl_multigrid mg) {
+    if (!B) return fail(PL_ERR_INVALID_ARG, "null batched solver");
+    pl_solver S = B->base;
+    PLB_CUDA(cudaSetDevice(S->mesh->ctx->device));
+    PLB_CUDA(cudaStreamSynchronize(S->mesh->ctx->stream));
+    if (B->stream) PLB_CUDA(cudaStreamSynchronize(B->stream));
+    bmg_release(B);
+    B->cheb_version++;  // the captured iterations change
+    if (!mg) return PL_OK;
+    const MgView v = multigrid_view(mg);
+    if (v.levels.empty() || v.levels[0].S->mesh != S->mesh || v.levels[0].n != S->n)
+        return fail(PL_ERR_INVALID_ARG, "the hierarchy's fine level is not the batched solver's mesh");
+    if (B->K > 8) return fail(PL_ERR_UNSUPPORTED, "multigrid tiles of at most 8 right-hand sides");
+    // every level's operator is the batched cell-block kernel: its layout is built now, outside
+    // any stream capture
+    for (const MgLevelView& L : v.levels) {
+        pl_mesh lm = L.S->mesh;
+        if (lm->cell_type != PL_CELL_TET4) return fail(PL_ERR_UNSUPPORTED, "batched multigrid needs P1 tetrahedral levels");
+        int rc = ensure_blocked_layout(lm);
+        if (rc) return rc;
+    }
+    B->bmg.resize(v.levels.size());
+    cudaError_t e = cudaSuccess;
+    for (size_t l = 0; l < v.levels.size() && e == cudaSuccess; ++l) {
+        const size_t nk = (size_t)v.levels[l].n * B->K;
+        auto& W = B->bmg[l];
+        for (float** p : {&W.r, &W.z, &W.t, &W.d, &W.q, &W.w})
+            if (e == cudaSuccess) e = dev_alloc(p, nk);
+        if (e == cudaSuccess) e = cudaMemsetAsync(W.r, 0, nk * sizeof(float), S->mesh->ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->mesh->ctx->stream);
+    if (e != cudaSuccess) {
+        bmg_release(B);
+        return cuda_fail(e, "pl_batch_solver_set_multigrid");
+    }
+    B->mg = mg;
+    multigrid_batch_use(mg, +1);
+    B->mgv = v;
+    return PL_OK;
+}
+
 int pl_batch_solver_destroy(pl_batch_solver B) {
     if (!B) return PL_OK;
     pl_mesh m = B->base->mesh;
     cudaSetDevice(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
+    bmg_release(B);
     if (B->graph) cudaGraphExecDestroy(B->graph);
     if (B->stream) cudaStreamSynchronize(B->stream);
     if (B->ev_in) cudaEventDestroy(B->ev_in);

@@ -404,6 +404,12 @@ class BatchSolver:
         check(C.lib().pl_batch_solver_set_chebyshev(self.handle, int(degree), float(lower_ratio), int(eig_iters)))
         self.degree = int(degree)
 
+    def set_multigrid(self, mg: Optional["Multigrid"]) -> None:
+        """One V-cycle of `mg` on all the tile's vectors per PCG iteration (None: back to
+        Chebyshev or point-block Jacobi); keeps `mg` alive while set."""
+        check(C.lib().pl_batch_solver_set_multigrid(self.handle, mg.handle if mg is not None else None))
+        self._mg = mg
+
     def set_reliable(self, enable: bool = True, delta: float = 0.01) -> None:
         """FP64 accuracy of the FP32 tile PCG: reliable updates (residual replacement whenever the
         iterated residual has dropped by `delta`; the default, with delta 0.01) or restarted

@@ -91,6 +91,15 @@ class GreensFunctions:
         self.mg = mg
         return solver
 
+    def batched_multigrid(self, tile=8):
+        """A batched solver (tiles of `tile` impulses, FP32 PCG with reliable updates on the
+        single-impulse solvers' FP32 operator) preconditioned by one V-cycle of the last attached
+        hierarchy on all the tile's vectors per iteration; solve(..., batch=it) uses it."""
+        bs = FA.BatchSolver(self.solver32, tile)
+        bs.set_multigrid(self.mg)
+        self._mg_keep = getattr(self, "_mg_keep", []) + [(bs, None)]
+        return bs
+
     def tune_multigrid(self, impulses, degrees=(2, 3, 4), lowers=(0.1, 0.3)):
         """Picks the Chebyshev smoothing (degree, lower ratio) of the last attached multigrid with
         the highest solves/s on `impulses` (each setting solves them once to warm up and once timed)
@@ -160,10 +169,10 @@ class GreensFunctions:
         self.batch = best[3]
         return sorted(results, key=lambda r: -r[2])
 
-    def solve(self, impulses, batched=True, solver=None):
+    def solve(self, impulses, batched=True, solver=None, batch=None):
         """Solutions u = u_slip + du of the given impulses; returns (solutions, seconds). batched:
-        the tiles of the batched FP32 solver; else one at a time with `solver` (default: the FP64
-        point-block Jacobi solver)."""
+        the tiles of `batch` (default: the autotuned batched FP32 solver); else one at a time with
+        `solver` (default: the FP64 point-block Jacobi solver)."""
         import torch
 
         rhs = [self.impulse_rhs(imp) for imp in impulses]
@@ -171,7 +180,7 @@ class GreensFunctions:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         if batched:
-            self.batch.solve([b for _, b in rhs], xs)
+            (batch or self.batch).solve([b for _, b in rhs], xs)
         else:
             one = solver or self.solver64
             for (_, b), x in zip(rhs, xs):

@@ -107,3 +107,34 @@ def test_multigrid_on_unstructured_tetrahedra_with_a_fault(ctx):
         assert st.rel_residual <= 1e-12
         assert np.linalg.norm(u - u_ref) <= 1e-8 * np.linalg.norm(u_ref), (precision, st)
         assert 5 * st.iterations <= st_ref.iterations, (st.iterations, st_ref.iterations)
+
+
+def test_batched_multigrid_green_functions(ctx):
+    """Green's functions on a Delaunay fault mesh, batched: tiles of 8 impulses whose FP32 PCG is
+    preconditioned by one V-cycle of the tet hierarchy on all 8 vectors at once. The solutions match
+    one-at-a-time FP64 solves to <= 1e-8 with far fewer iterations than the point-Jacobi tiles."""
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import greensfns as GF
+
+    lo, hi = (-6000.0, -6000.0, -9000.0), (6000.0, 6000.0, 0.0)
+    mesh = M.box_tet_delaunay_fault_x(120000, seed=3, lo=lo, hi=hi)
+    levels = MG.build_tet_hierarchy(mesh, lambda n, l: M.box_tet_delaunay_fault_x(n, seed=20 + l, lo=lo, hi=hi),
+                                    fault_x=0.0, lo=lo, hi=hi,
+                                    constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))], min_cells=500)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=6)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    patches = GF.fault_patches(mesh, (-6000.0, 6000.0), (-9000.0, 0.0), 4, 3)
+    g = GF.GreensFunctions(ctx, mesh, mat, levels[0].constrained, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
+    g.attach_multigrid(levels, mat, FA.Solver.FP32_REFINED)
+    bmg = g.batched_multigrid(8)
+    imps = g.impulses[:8]
+    ref, _ = g.solve(imps, batched=False)
+    got, _ = g.solve(imps, batched=True, batch=bmg)
+    st_mg = bmg.stats()
+    _, _ = g.solve(imps, batched=True)
+    st_j = g.batch.stats()
+    for a, b in zip(got, ref):
+        a, b = a.cpu().numpy(), b.cpu().numpy()
+        assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b)
+    assert st_mg["max_rel_residual"] <= 1e-11
+    assert 5 * st_mg["inner_iterations"] <= st_j["inner_iterations"], (st_mg, st_j)
