@@ -10,7 +10,7 @@ The L2 cache (126 MB) is flushed (256 MiB write) before every application, becau
 application's working set (~53 MB) would otherwise stay cached between applications.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pylith_b200|reference]
-  python bench.py --config c0|c1q2|c2|c3|c3tile|c3mg|c4  (the other configurations, one JSON line each)
+  python bench.py --config c0|c1q2|c2|c3|c3tile|c3mg|c3bmg|c4  (the other configurations, one JSON line each)
 
 Under torchrun (N > 1) the ranks share one mesh of N x 1.2 M cells (the same Delaunay box
 stretched N times along x, so every rank's part is the single-GPU workload: weak scaling), cut into
@@ -360,7 +360,7 @@ def main():
     ap.add_argument("--impl", default="pylith_b200")
     ap.add_argument("--cells", type=int, default=TARGET_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1q2", "c2", "c3", "c3tile", "c3mg", "c4"])
+    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1q2", "c2", "c3", "c3tile", "c3mg", "c3bmg", "c4"])
     ap.add_argument("--scale", type=float, default=1.0, help="size factor for the --config runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -1059,6 +1059,33 @@ def config_c3mg(args):
             "seconds_per_solve": dt / 4, "iterations": solver.stats()["iterations"]}
 
 
+def config_c3bmg(args):
+    """Sixteen Green's-function impulses on the C3 mesh in tiles of 8, the tile's FP32 PCG
+    preconditioned by one V-cycle on all 8 vectors per iteration: the profiling case of the
+    batched multigrid path."""
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import greensfns as GF
+    from pylith_b200 import materials as MAT
+    from pylith_b200 import meshing as M
+    from pylith_b200 import multigrid as MG
+
+    lo, hi = (-12000.0, -15000.0, -20000.0), (12000.0, 15000.0, 0.0)
+    mesh = M.box_tet_delaunay_fault_x(int(1_500_000 * args.scale), seed=0, lo=lo, hi=hi)
+    levels = MG.build_tet_hierarchy(mesh, lambda n, l: M.box_tet_delaunay_fault_x(n, seed=l, lo=lo, hi=hi),
+                                    fault_x=0.0, lo=lo, hi=hi, constrained_faces=[(0, "neg", (0, 1, 2)), (0, "pos", (0, 1, 2))])
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+    mat = MAT.IsotropicLinearElasticity(rho, mu, K)
+    patches = GF.fault_patches(mesh, (-12000.0, 12000.0), (-15000.0, 0.0), 40, 25)
+    ctx = FA.Context(0)
+    g = GF.GreensFunctions(ctx, mesh, mat, levels[0].constrained, patches, rtol=1e-11, inner_rtol=1e-4, tile=8)
+    g.attach_multigrid(levels, mat, FA.Solver.FP32_REFINED)
+    g.mg.set_smoother(3, 0.1)
+    bmg = g.batched_multigrid(8)
+    g.solve(g.impulses[:8], batched=True, batch=bmg)  # eigenvalue estimates, graph capture
+    _, dt = g.solve(g.impulses[8:24], batched=True, batch=bmg)
+    return {"config": "c3bmg", "cells": mesh.num_cells, "seconds_per_solve": dt / 16, "stats": bmg.stats()}
+
+
 def config_c4(args):
     """Serving: Poisson requests (200 req/s), box meshes n^3 with n log-uniform in [8, 96], log-normal
     material, random rectangular left-lateral slip patch of 0.1-3 m. Server (HBM-budget admission;
@@ -1102,7 +1129,7 @@ def config_c4(args):
 
 
 CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c3tile": config_c3tile,
-           "c3mg": config_c3mg, "c4": config_c4}
+           "c3mg": config_c3mg, "c3bmg": config_c3bmg, "c4": config_c4}
 
 
 if __name__ == "__main__":

@@ -1649,7 +1649,23 @@ int solve_reliable(pl_batch_solver B, int nrhs, const double* const* bs, double*
             rref[k] = rt;
             replaced[k] = update_z = true;
         }
-        if (update_z) {
+        if (update_z && B->mg) {
+            // multigrid (flexible steps): no V-cycle of the whole tile here, which would cost as
+            // much as an iteration. A replaced residual keeps its column's z, the V-cycle of the
+            // residual it replaces (they differ by the FP32 drift, which the flexible step
+            // absorbs); a new (or restarted) column starts from point-block Jacobi, z = P r, and
+            // meets the V-cycle at its next iteration. Then r.z of every column again.
+            for (int k = 0; k < K; ++k)
+                if (fresh[k]) {
+                    k_b_col_prec<<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, S->d_mask, S->d_pinv32, B->nnodes, K, k,
+                                                                B->part_a);
+                    k_b_col_copy<<<bgrid(n), 256, 0, s>>>(B->p, B->z, n, K, k);
+                    count_launch(2);
+                }
+            k_b_rz<K><<<kBBlocks, kBThreads, 0, s>>>(B->r, B->z, nullptr, S->d_mask, B->n, B->part_a, B->part_b, FinSpec());
+            k_b_finish<K><<<K, kBThreads, 0, s>>>(B->part_a, kBBlocks, B->scal, nullptr);
+            count_launch(2);
+        } else if (update_z) {
             if (tile_preconditioned(B)) {
                 // z = q(P A) P r (or V(r)) with the same operator for the whole tile (the other
                 // columns get their own z and r.z again), so the preconditioner stays fixed
