@@ -1471,17 +1471,32 @@ int ensure_reduced_ids(pl_mesh_s* m) {
         for (int i = 0; i < ns; ++i)
             if (slots[ids[p0 + i]] > 1) ids[p0 + i] |= kSharedBit;
     }
-    uint32_t* d = nullptr;
+    // the same ids without the padding, for the batched kernel's slot order
+    std::vector<uint32_t> slot_ids((size_t)L->h_block_node_begin[L->num_blocks], 0u);
+    for (int64_t b = 0; b < L->num_blocks; ++b) {
+        const int p0 = L->h_pipe_begin[b], s0 = L->h_block_node_begin[b], ns = L->h_block_node_begin[b + 1] - s0;
+        for (int i = 0; i < ns; ++i) slot_ids[s0 + i] = ids[p0 + i];
+    }
+    uint32_t *d = nullptr, *d2 = nullptr;
     PLB_CUDA(dev_alloc(&d, ids.size()));
+    cudaError_t e = dev_alloc(&d2, slot_ids.size());
+    if (e != cudaSuccess) {
+        dev_free(d, nullptr);
+        return cuda_fail(e, "reduced slot ids");
+    }
     PLB_CUDA(cudaMemcpyAsync(d, ids.data(), ids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, m->ctx->stream));
+    PLB_CUDA(cudaMemcpyAsync(d2, slot_ids.data(), slot_ids.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             m->ctx->stream));
     PLB_CUDA(cudaStreamSynchronize(m->ctx->stream));
     L->d_pipe_ids_red = d;
+    L->d_slot_node_red = d2;
     return PL_OK;
 }
 
 void free_blocked_layout(BlockedLayout* b, cudaStream_t after) {
     if (!b) return;
     dev_free(b->d_pipe_ids_red, after);
+    dev_free(b->d_slot_node_red, after);
     void* ptrs[] = {b->d_cell_begin, b->d_block_node_begin, b->d_slot_node, b->d_local_cells, b->d_inc_off, b->d_inc,
                     b->d_fix_node, b->d_fix_off, b->d_fix_slot, b->d_pipe_begin, b->d_pipe_ids,
                     b->d_pipe_coords, b->d_pipe_off, b->d_pipe_inc};

@@ -412,6 +412,8 @@ int pl_mesh_set_cohesive(pl_mesh m, int64_t ncoh, const int32_t* coh, int64_t nl
     if (m->blocked) {
         dev_free(m->blocked->d_pipe_ids_red, m->ctx->stream);
         m->blocked->d_pipe_ids_red = nullptr;
+        dev_free(m->blocked->d_slot_node_red, m->ctx->stream);
+        m->blocked->d_slot_node_red = nullptr;
     }
     bump_state_epoch();  // captured solver graphs hold the reduced connectivity
     m->ncoh = ncoh;

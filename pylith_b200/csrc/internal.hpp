@@ -94,6 +94,7 @@ struct BlockedLayout {
     uint32_t* d_pipe_ids_red = nullptr;     // as d_pipe_ids in the reduced fault space (node of the
                                             // reduced space | shared bit: the node has more than one
                                             // slot), built on first use
+    uint32_t* d_slot_node_red = nullptr;    // as d_slot_node in the reduced fault space (same build)
     uint16_t* d_pipe_inc = nullptr;         // [num_blocks][4 * cells_per_block] staging offsets
                                             // corner * 3 * cells_per_block + cell, node groups of
                                             // the pipelined kernel

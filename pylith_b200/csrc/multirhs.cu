@@ -969,7 +969,9 @@ int jv32_multi_on(pl_solver S, int64_t n, const float* v, float* out, double* pq
     pl_mesh m = S->mesh;
     cudaStream_t s = m->ctx->stream;
     if (pq && S->ops.size() != 1) return fail(PL_ERR_UNSUPPORTED, "fused energies need a single integrator");
-    if (S->npairs > 0) {
+    // the solver's reduced fault space directly (slot ids of the reduced space: no unfold or fold)
+    const bool reduced = S->npairs > 0 && S->reduced && m->blocked && m->blocked->d_slot_node_red;
+    if (S->npairs > 0 && !reduced) {
         k_b_unfold<K><<<bgrid(3 * K * S->npairs), 256, 0, s>>>(const_cast<float*>(v), S->d_pair_neg, S->d_pair_pos, S->npairs);
         count_launch();
     }
@@ -1007,12 +1009,13 @@ int jv32_multi_on(pl_solver S, int64_t n, const float* v, float* out, double* pq
             fin.out_a = pq;
         }
         k_tet_blocked_jv32_multi<K><<<grid, kMultiBlockCells, smem, s>>>(
-            pp, L.d_cell_begin, L.d_block_node_begin, L.d_slot_node, (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
+            pp, L.d_cell_begin, L.d_block_node_begin, reduced ? L.d_slot_node_red : L.d_slot_node,
+            (const ushort4*)L.d_local_cells, L.d_inc_off, L.d_inc,
             L.d_pipe_begin, L.d_pipe_coords, L.num_blocks, ld, v, out, first, pq ? part : nullptr, scal, fin);
         first = false;
         count_launch();
     }
-    if (S->npairs > 0) {
+    if (S->npairs > 0 && !reduced) {
         k_b_fold<K><<<bgrid(3 * K * S->npairs), 256, 0, s>>>(out, S->d_pair_neg, S->d_pair_pos, S->npairs);
         count_launch();
     }
@@ -1117,21 +1120,37 @@ __global__ void __launch_bounds__(kBThreads) k_bmg_axpy(float* __restrict__ y, c
 }
 
 // coarse[(3c + comp)][k] = sum_j R[c][j] fine[(3 col_j + comp)][k], 0 on the coarse level's masked
-// DOFs (R = P^T in coarse rows, in the coarse reduced space)
+// DOFs (R = P^T in coarse rows, in the coarse reduced space): one warp per coarse node, its lanes
+// (32 / K row entries at a time) x (K right-hand sides); the entry groups' sums meet in a fixed
+// shuffle tree.
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_bmg_restrict(const float* __restrict__ fine, const int32_t* __restrict__ row,
                                                             const int32_t* __restrict__ col, const double* __restrict__ val,
                                                             const uint8_t* __restrict__ cmask, int64_t nc,
                                                             float* __restrict__ coarse) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3 * nc * K; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t ck = t / K;  // coarse DOF
-        const int k = (int)(t % K);
-        const int64_t c = ck / 3;
-        const int comp = (int)(ck % 3);
-        double sum = 0.0;
-        if (!cmask[ck])
-            for (int32_t j = row[c]; j < row[c + 1]; ++j) sum += val[j] * (double)fine[(3 * (int64_t)col[j] + comp) * K + k];
-        coarse[t] = (float)sum;
+    constexpr int G = 32 / K;  // entries per step
+    const int lane = threadIdx.x & 31, k = lane % K, g = lane / K;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < nc;
+         c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int32_t j = row[c] + g; j < row[c + 1]; j += G) {
+            const double w = val[j];
+            const float* f = fine + 3 * (int64_t)col[j] * K + k;
+            s0 += w * (double)f[0];
+            s1 += w * (double)f[K];
+            s2 += w * (double)f[2 * K];
+        }
+#pragma unroll
+        for (int o = K; o < 32; o <<= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        }
+        if (g == 0) {
+            coarse[(3 * c + 0) * K + k] = cmask[3 * c + 0] ? 0.0f : (float)s0;
+            coarse[(3 * c + 1) * K + k] = cmask[3 * c + 1] ? 0.0f : (float)s1;
+            coarse[(3 * c + 2) * K + k] = cmask[3 * c + 2] ? 0.0f : (float)s2;
+        }
     }
 }
 
@@ -1154,19 +1173,36 @@ __global__ void __launch_bounds__(kBThreads) k_bmg_prolong_add(const float* __re
 }
 
 // z[idx[i]][k] = sum_j inv[i][j] r[idx[j]][k] (z zeroed before): each block stages the gathered
-// right-hand sides ([n][K] floats of dynamic shared memory), one thread per (row, rhs).
+// right-hand sides ([n][K] floats of dynamic shared memory); one warp per row, its lanes over the
+// row's columns with K sums each, reduced across the warp.
 template <int K>
 __global__ void __launch_bounds__(kBThreads) k_bmg_dense(const float* __restrict__ inv, const int32_t* __restrict__ idx, int n,
                                                          const float* __restrict__ r, float* __restrict__ z) {
     extern __shared__ float sr[];
     for (int t = threadIdx.x; t < n * K; t += blockDim.x) sr[t] = r[(int64_t)idx[t / K] * K + t % K];
     __syncthreads();
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * K; t += gridDim.x * blockDim.x) {
-        const int i = t / K, k = t % K;
+    const int lane = threadIdx.x & 31;
+    for (int i = blockIdx.x * (kBThreads / 32) + (threadIdx.x >> 5); i < n; i += gridDim.x * (kBThreads / 32)) {
         const float* row = inv + (int64_t)i * n;
-        float acc = 0.0f;
-        for (int j = 0; j < n; ++j) acc += row[j] * sr[j * K + k];
-        z[(int64_t)idx[i] * K + k] = acc;
+        float acc[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[k] = 0.0f;
+        for (int j = lane; j < n; j += 32) {
+            const float a = row[j];
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] += a * sr[j * K + k];
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+        if (lane < K) {
+            float v = acc[0];
+#pragma unroll
+            for (int k = 1; k < K; ++k)
+                if (lane == k) v = acc[k];
+            z[(int64_t)idx[i] * K + lane] = v;
+        }
     }
 }
 
@@ -1240,7 +1276,7 @@ int bmg_vcycle(pl_batch_solver B, int l, const float* r, float* z) {
             PLB_CUDA(cudaMemsetAsync(z, 0, S->n * K * sizeof(float), s));
             const size_t smem = (size_t)V.dense_n * K * sizeof(float);
             ensure_kernel_smem((const void*)k_bmg_dense<K>, smem);
-            const int grid = std::max(1, std::min((V.dense_n * K + kBThreads - 1) / kBThreads, 148));
+            const int grid = std::max(1, std::min((V.dense_n + kBThreads / 32 - 1) / (kBThreads / 32), 4 * 148));
             k_bmg_dense<K><<<grid, kBThreads, smem, s>>>(V.dense_inv32, V.dense_idx, V.dense_n, r, z);
             count_launch();
             return PL_OK;
@@ -1254,7 +1290,8 @@ int bmg_vcycle(pl_batch_solver B, int l, const float* r, float* z) {
     const MgLevelView& C = V.levels[l + 1];
     const pl_batch_solver_s::BmgLevel& Wc = B->bmg[l + 1];
     if (C.n > 3 * C.nmesh) PLB_CUDA(cudaMemsetAsync(Wc.r + 3 * C.nmesh * K, 0, (C.n - 3 * C.nmesh) * K * sizeof(float), s));
-    k_bmg_restrict<K><<<kBBlocks, kBThreads, 0, s>>>(W.t, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, Wc.r);
+    k_bmg_restrict<K><<<(int)std::max<int64_t>(1, std::min<int64_t>((C.nmesh + 7) / 8, kBBlocks)), kBThreads, 0, s>>>(
+        W.t, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, Wc.r);
     count_launch(2);
     if ((rc = bmg_vcycle<K>(B, l + 1, Wc.r, Wc.z))) return rc;
     k_bmg_prolong_add<K><<<kBBlocks, kBThreads, 0, s>>>(Wc.z, L.p_row, L.p_col, L.p_val, S->d_mask, L.nmesh, z);
