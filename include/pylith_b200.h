@@ -374,6 +374,10 @@ int pl_multigrid_set_smoother(pl_multigrid mg, int degree, double lower_ratio, i
 /* Makes pl_solver_solve run flexible conjugate gradients in FP64 preconditioned by one V-cycle
  * of `mg` (NULL: back to point-block Jacobi); pl_solver_setup then sets up every level. */
 int pl_solver_set_multigrid(pl_solver solver, pl_multigrid mg);
+/* The cycle: pre- and post-smoothing on (1) or off (0) on every level but the coarsest (default
+ * both). Without pre-smoothing the residual is restricted as it is and the V-cycle is no longer
+ * symmetric, which the flexible conjugate gradients accept. */
+int pl_multigrid_set_cycle(pl_multigrid mg, int pre_smooth, int post_smooth);
 /* Levels and each level's lambda_max(D^-1 A) estimate (0 before the first solve, and for a
  * coarsest level solved with its dense inverse). */
 int pl_multigrid_get_levels(pl_multigrid mg, int* num_levels, double* lambda_max);

@@ -128,6 +128,7 @@ SIGNATURES = {
     "pl_batch_solver_get_chebyshev": (_I, [_P, ctypes.POINTER(_D)]),
     "pl_batch_solver_set_reliable": (_I, [_P, _I, _D]),
     "pl_batch_solver_set_multigrid": (_I, [_P, _P]),
+    "pl_multigrid_set_cycle": (_I, [_P, _I, _I]),
     "pl_multigrid_create": (_I, [_P, _I, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     "pl_multigrid_set_smoother": (_I, [_P, _I, _D, _I, _D, _I]),
     "pl_solver_set_multigrid": (_I, [_P, _P]),

@@ -275,6 +275,7 @@ struct MgView {
     double lower;
     int coarse_degree;
     double coarse_lower;
+    bool pre_smooth, post_smooth;
     const float* dense_inv32;
     const int32_t* dense_idx;
     int dense_n;

@@ -410,6 +410,7 @@ struct pl_multigrid_s {
     pl_context ctx = nullptr;  // retained: the levels' context (the fine solver may go first)
     std::vector<MgLevel> lv;
     int degree = 2, coarse_degree = 40;
+    bool pre_smooth = true, post_smooth = true;  // pl_multigrid_set_cycle
     double lower = 0.1, coarse_lower = 0.01;
     bool fp32 = false;
     bool eig_valid = false;
@@ -485,11 +486,17 @@ int vcycle(pl_multigrid mg, int l) {
         count_launch();
         return PL_OK;
     }
-    int rc = cheb<T>(mg, l, r, z, mg->degree, mg->lower);
-    if (rc) return rc;
     auto apply = [&](T* v) { return f32 ? solver_apply_J32(L.S, (const float*)v, (float*)q) : solver_apply_J(L.S, (const double*)v, (double*)q); };
-    if ((rc = apply(z))) return rc;
-    k_mg_residual<T><<<mg_grid(L.n), 256, 0, s>>>(r, q, L.S->d_mask, L.n, t);
+    int rc = PL_OK;
+    const T* tr = r;  // the residual to restrict
+    if (mg->pre_smooth) {
+        if ((rc = cheb<T>(mg, l, r, z, mg->degree, mg->lower))) return rc;
+        if ((rc = apply(z))) return rc;
+        k_mg_residual<T><<<mg_grid(L.n), 256, 0, s>>>(r, q, L.S->d_mask, L.n, t);
+        tr = t;
+    } else {
+        PLB_CUDA(cudaMemsetAsync(z, 0, L.n * sizeof(T), s));
+    }
     // restriction into the coarse level's r, folded and masked
     MgLevel& C = mg->lv[l + 1];
     T* rc_ = f32 ? (T*)C.r32 : (T*)C.r;
@@ -497,13 +504,14 @@ int vcycle(pl_multigrid mg, int l) {
     // the restriction's rows are the coarse level's reduced space (its prolongation columns were
     // mapped onto it): no fold; the Lagrange rows of the coarse vector stay zero
     if (C.n > 3 * C.nmesh) PLB_CUDA(cudaMemsetAsync(rc_ + 3 * C.nmesh, 0, (C.n - 3 * C.nmesh) * sizeof(T), s));
-    k_mg_restrict<T><<<mg_grid(32 * C.nmesh), 256, 0, s>>>(t, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, rc_);
+    k_mg_restrict<T><<<mg_grid(32 * C.nmesh), 256, 0, s>>>(tr, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, rc_);
     count_launch(2);
     if ((rc = vcycle<T>(mg, l + 1))) return rc;
     // ... and the prolongation reads the coarse correction there: no unfold
     k_mg_prolong_add<T><<<mg_grid(3 * L.nmesh), 256, 0, s>>>(zc, L.p_row, L.p_col, L.p_val, L.S->d_mask, L.nmesh, z);
     count_launch();
     // post-smoothing on the new residual
+    if (!mg->post_smooth) return PL_OK;
     if ((rc = apply(z))) return rc;
     k_mg_residual<T><<<mg_grid(L.n), 256, 0, s>>>(r, q, L.S->d_mask, L.n, t);
     count_launch();
@@ -784,6 +792,8 @@ MgView multigrid_view(const pl_multigrid_s* mg) {
     v.degree = mg->degree;
     v.lower = mg->lower;
     v.coarse_degree = mg->coarse_degree;
+    v.pre_smooth = mg->pre_smooth;
+    v.post_smooth = mg->post_smooth;
     v.coarse_lower = mg->coarse_lower;
     v.dense_inv32 = mg->dense_ok ? mg->d_dense32 : nullptr;
     v.dense_idx = mg->dense_ok ? mg->d_dense_idx : nullptr;
@@ -929,6 +939,15 @@ int pl_solver_set_multigrid(pl_solver S, pl_multigrid mg) {
     S->mg = mg;
     if (mg) mg->attached = S;
     S->ready = false;  // the coarse levels are set up with the next pl_solver_setup
+    return PL_OK;
+}
+
+int pl_multigrid_set_cycle(pl_multigrid mg, int pre_smooth, int post_smooth) {
+    if (!mg || (!pre_smooth && !post_smooth)) return fail(PL_ERR_INVALID_ARG, "a V-cycle smooths at least once");
+    mg->pre_smooth = pre_smooth != 0;
+    mg->post_smooth = post_smooth != 0;
+    if (mg->graph) cudaGraphExecDestroy(mg->graph);
+    mg->graph = nullptr;
     return PL_OK;
 }
 

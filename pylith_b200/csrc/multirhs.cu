@@ -1283,19 +1283,27 @@ int bmg_vcycle(pl_batch_solver B, int l, const float* r, float* z) {
         }
         return bmg_cheb<K>(B, l, r, z, V.coarse_degree, V.coarse_lower);
     }
-    int rc = bmg_cheb<K>(B, l, r, z, V.degree, V.lower);
-    if (rc) return rc;
-    if ((rc = bmg_jv<K>(B, l, z, W.q))) return rc;
-    k_bmg_residual<K><<<kBBlocks, kBThreads, 0, s>>>(r, W.q, S->d_mask, S->n, W.t);
+    int rc = PL_OK;
+    const float* tr = r;  // the residual to restrict
+    if (V.pre_smooth) {
+        if ((rc = bmg_cheb<K>(B, l, r, z, V.degree, V.lower))) return rc;
+        if ((rc = bmg_jv<K>(B, l, z, W.q))) return rc;
+        k_bmg_residual<K><<<kBBlocks, kBThreads, 0, s>>>(r, W.q, S->d_mask, S->n, W.t);
+        count_launch();
+        tr = W.t;
+    } else {
+        PLB_CUDA(cudaMemsetAsync(z, 0, S->n * K * sizeof(float), s));
+    }
     const MgLevelView& C = V.levels[l + 1];
     const pl_batch_solver_s::BmgLevel& Wc = B->bmg[l + 1];
     if (C.n > 3 * C.nmesh) PLB_CUDA(cudaMemsetAsync(Wc.r + 3 * C.nmesh * K, 0, (C.n - 3 * C.nmesh) * K * sizeof(float), s));
     k_bmg_restrict<K><<<(int)std::max<int64_t>(1, std::min<int64_t>((C.nmesh + 7) / 8, kBBlocks)), kBThreads, 0, s>>>(
-        W.t, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, Wc.r);
-    count_launch(2);
+        tr, L.r_row, L.r_col, L.r_val, C.S->d_mask, C.nmesh, Wc.r);
+    count_launch();
     if ((rc = bmg_vcycle<K>(B, l + 1, Wc.r, Wc.z))) return rc;
     k_bmg_prolong_add<K><<<kBBlocks, kBThreads, 0, s>>>(Wc.z, L.p_row, L.p_col, L.p_val, S->d_mask, L.nmesh, z);
     count_launch();
+    if (!V.post_smooth) return PL_OK;
     if ((rc = bmg_jv<K>(B, l, z, W.q))) return rc;
     k_bmg_residual<K><<<kBBlocks, kBThreads, 0, s>>>(r, W.q, S->d_mask, S->n, W.t);
     count_launch();
@@ -1859,7 +1867,8 @@ int pl_batch_solver_solve(pl_batch_solver B, int nrhs, const double* const* b_de
         if (rc == PL_OK) {
             const MgView v = multigrid_view(B->mg);
             bool changed = v.levels.size() != B->mgv.levels.size() || v.dense_inv32 != B->mgv.dense_inv32 ||
-                           v.degree != B->mgv.degree || v.lower != B->mgv.lower;
+                           v.degree != B->mgv.degree || v.lower != B->mgv.lower ||
+                           v.pre_smooth != B->mgv.pre_smooth || v.post_smooth != B->mgv.post_smooth;
             for (size_t l = 0; !changed && l < v.levels.size(); ++l) changed = v.levels[l].lmax != B->mgv.levels[l].lmax;
             B->mgv = v;
             if (changed) B->cheb_version++;  // the captured iterations hold the coefficients

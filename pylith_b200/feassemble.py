@@ -515,6 +515,11 @@ class Multigrid:
         self.set_smoother(degree, lower, coarse_degree, coarse_lower)
         check(C.lib().pl_solver_set_multigrid(fine.handle, self.handle))
 
+    def set_cycle(self, pre_smooth: bool = True, post_smooth: bool = True):
+        """Pre- and post-smoothing on or off (pl_multigrid_set_cycle)."""
+        check(C.lib().pl_multigrid_set_cycle(self.handle, 1 if pre_smooth else 0, 1 if post_smooth else 0))
+        self.pre_smooth, self.post_smooth = pre_smooth, post_smooth
+
     def set_smoother(self, degree, lower, coarse_degree=40, coarse_lower=0.01):
         """Chebyshev-Jacobi smoothing of `degree` on [lower b, b] (pl_multigrid_set_smoother)."""
         check(C.lib().pl_multigrid_set_smoother(self.handle, degree, lower, coarse_degree, coarse_lower, self.precision))
