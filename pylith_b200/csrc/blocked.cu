@@ -254,8 +254,8 @@ __global__ void __launch_bounds__(kTetThreads, PLB_TET_MIN_BLOCKS) k_tet_blocked
         // per-cell inputs and the slot ids two blocks ahead: issued before the wait
         ushort4 lc[kTetCellsPerThread];
         double a[kTetCellsPerThread][L::size];
-#pragma unroll
         const int64_t cb0 = A.cell_begin[b], cb1 = A.cell_begin[b + 1];
+#pragma unroll
         for (int j = 0; j < kTetCellsPerThread; ++j) {
             const int64_t c = cb0 + tc + j * kTetThreads;
             lc[j] = make_ushort4(0, 0, 0, 0);
