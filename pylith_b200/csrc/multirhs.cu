@@ -59,6 +59,8 @@ PL_D double tet_cof_m(const double X[4][3], double cof[3][3]) {
 template <int K>
 struct MultiChunk {
     static constexpr int value = K < 4 ? K : 4;
+    // ld_vec / st_vec / red_vec move 1, 2 or 4 floats at a time.
+    static_assert(value == 1 || value == 2 || value == 4, "tile sizes are 1, 2, 4, 8 or 16");
 };
 
 // Floats per staged node row in shared memory: the 3K field values, padded so that for K a
