@@ -482,14 +482,19 @@ def main():
     # step's transfers overlap the neighbouring steps' work (PCIe is full duplex).
     # a step's u and v sit side by side in one pinned buffer and one device buffer, so that they
     # cross the link as one copy (fewer, larger copies run closer to the link's rate)
-    hin = [torch.empty(2, n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    # host buffers: page-locked memory on the GPU's NUMA node (pl_host_alloc), so that the
+    # host-to-device reads do not cross the inter-socket link of a two-socket host
+    def host(*shape):
+        return torch.from_numpy(ctx.host_empty(shape))
+
+    hin = [host(2, n) for _ in range(2)]
     for h in hin:
         h[0].copy_(u.cpu())
         h[1].copy_(v.cpu())
     hu = [h[0] for h in hin]
     hv = [h[1] for h in hin]
-    hr = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
-    hjv = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    hr = [host(n) for _ in range(2)]
+    hjv = [host(n) for _ in range(2)]
     din = [torch.empty(2, n, dtype=torch.float64, device=u.device) for _ in range(2)]
     du = [d[0] for d in din]
     dv = [d[1] for d in din]
@@ -675,6 +680,7 @@ def main():
                               "(pl_compute_lhs_residual, pl_compute_lhs_jacobian_action), D2H of r and J v; value: "
                               "eager per-call steps issued through ctypes as a C caller would (one GPU; torch calls "
                               "under torchrun); graph_replay_value: the same steps captured once in a CUDA graph",
+                    "host_buffers": f"pl_host_alloc: page-locked, GPU NUMA node {ctx.numa_node}",
                     "host_link": {**link_gbs, "bound_gdof_s": link_bound,
                                   "note": "pinned copies of one step's inputs (h2d), outputs (d2h) and both at once"}},
             "gpu_launches": int(launches),

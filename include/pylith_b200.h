@@ -194,6 +194,21 @@ int pl_context_use_own_stream(pl_context ctx);
 void* pl_context_get_stream(pl_context ctx);
 int pl_context_synchronize(pl_context ctx);
 
+/* ---- host memory ---------------------------------------------------------------------- */
+/* No counterpart in the reference (PETSc keeps its Vecs in pageable host memory). Page-locked
+ * host memory for the host buffers of calls that copy between host and device (the
+ * pl_compute_*_host entry points, or a caller's own copies around the device entry points):
+ * anonymous pages, advised as transparent huge pages from 2 MiB up, preferring the NUMA node
+ * the host reports for the context's GPU (so that on a two-socket host the device's reads do
+ * not cross the inter-socket link), faulted in and registered with CUDA. The node is a
+ * preference: with no NUMA information (one-node hosts) or no free memory on that node the
+ * pages land where the kernel puts them. *out is page-aligned and zero-filled; release it with
+ * pl_host_free (not cudaFreeHost). Thread-safe. */
+int pl_host_alloc(pl_context ctx, size_t bytes, void** out);
+int pl_host_free(void* ptr);
+/* NUMA node the host reports for the context's GPU; -1 when it reports none. */
+int pl_context_numa_node(pl_context ctx, int* node);
+
 /* ---- mesh ----------------------------------------------------------------------------- */
 /* Uploads cells [num_cells][nodes_per_cell] (int32) and coordinates [num_nodes][3] (FP64).
  * Replaces the mesh/closure data PETSc keeps in the DMPlex (topology/Field.cc:276-440,

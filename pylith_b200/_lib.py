@@ -74,6 +74,9 @@ SIGNATURES = {
     "pl_context_use_own_stream": (_I, [_P]),
     "pl_context_get_stream": (_P, [_P]),
     "pl_context_synchronize": (_I, [_P]),
+    "pl_host_alloc": (_I, [_P, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "pl_host_free": (_I, [_P]),
+    "pl_context_numa_node": (_I, [_P, ctypes.POINTER(_I)]),
     "pl_mesh_create": (_I, [_P, _I, _I64, _P, _I64, _P, ctypes.POINTER(_P)]),
     "pl_mesh_set_cohesive": (_I, [_P, _I64, _P, _I64]),
     "pl_mesh_destroy": (_I, [_P]),

@@ -111,6 +111,25 @@ class InterfaceJacobianKernels:
     j3: Optional[int] = None
 
 
+class _HostBuffer:
+    """Owner of one pl_host_alloc allocation, exposed to numpy through the array interface (the
+    array keeps this object alive as its base; the memory is freed with it)."""
+
+    def __init__(self, ctx, nbytes: int, shape, dtype):
+        self.ptr = ctypes.c_void_p()
+        check(C.lib().pl_host_alloc(ctx.handle, nbytes, ctypes.byref(self.ptr)))
+        self.__array_interface__ = {"shape": shape, "typestr": dtype.str, "data": (self.ptr.value, False),
+                                    "version": 3}
+
+    def __del__(self):
+        ptr, self.ptr = getattr(self, "ptr", None), None
+        if ptr:
+            try:
+                C.lib().pl_host_free(ptr)
+            except Exception:
+                pass
+
+
 class Context:
     """One CUDA device and the stream all work is enqueued on (torch's current stream)."""
 
@@ -128,6 +147,22 @@ class Context:
 
     def synchronize(self) -> None:
         check(C.lib().pl_context_synchronize(self.handle))
+
+    @property
+    def numa_node(self) -> int:
+        """NUMA node the host reports for this context's GPU (-1: none reported)."""
+        node = ctypes.c_int(-1)
+        check(C.lib().pl_context_numa_node(self.handle, ctypes.byref(node)))
+        return node.value
+
+    def host_empty(self, shape, dtype=np.float64) -> np.ndarray:
+        """A zero-filled numpy array in page-locked host memory on the NUMA node of this
+        context's GPU (pl_host_alloc), for the host side of copies to and from the device; the
+        memory is released with the last array that views it."""
+        dtype = np.dtype(dtype)
+        shape = (shape,) if np.isscalar(shape) else tuple(shape)
+        nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+        return np.asarray(_HostBuffer(self, max(nbytes, 1), shape, dtype))
 
     def close(self):
         if self.handle:

@@ -287,6 +287,62 @@ def test_host_buffer_entry_point(oracle_lib, torch_cuda, ctx):
     r = np.zeros_like(u)
     ig.compute_lhs_residual_host(0.0, 0.0, u, r)
     assert rel_l2(r, r_ref) <= TOL64
+    # the same call with both host buffers from pl_host_alloc
+    hu, hr = ctx.host_empty(u.shape), ctx.host_empty(u.shape)
+    hu[:] = u
+    ig.compute_lhs_residual_host(0.0, 0.0, hu, hr)
+    assert rel_l2(hr, r_ref) <= TOL64
+
+
+def _page_nodes(ptr: int, nbytes: int):
+    """NUMA node of every 64th page of [ptr, ptr + nbytes) (move_pages query; x86-64 / arm64)."""
+    import ctypes
+    import platform
+
+    nr = {"x86_64": 279, "aarch64": 239}.get(platform.machine())
+    if nr is None:
+        return None
+    libc = ctypes.CDLL(None, use_errno=True)
+    addrs = list(range(ptr, ptr + nbytes, 64 * 4096))
+    pages = (ctypes.c_void_p * len(addrs))(*addrs)
+    status = (ctypes.c_int * len(addrs))()
+    if libc.syscall(nr, 0, ctypes.c_ulong(len(addrs)), pages, None, status, 0) != 0:
+        return None
+    return list(status)
+
+
+def test_numa_local_host_buffers(torch_cuda, ctx):
+    """pl_host_alloc: page-aligned, zero-filled, page-locked (CUDA sees it as pinned host memory)
+    and, where the host reports the GPU's NUMA node and lets the process use that node's memory,
+    placed there; a round trip through the device returns the same bytes."""
+    torch = torch_cuda
+    n = 3 << 20
+    a = ctx.host_empty((2, n))
+    assert a.shape == (2, n) and a.dtype == np.float64
+    assert a.ctypes.data % 4096 == 0
+    assert not a.any()
+    t = torch.from_numpy(a)
+    assert t.is_pinned()
+    a[0] = np.arange(n, dtype=np.float64)
+    a[1] = -a[0]
+    d = t.to("cuda", non_blocking=True)
+    back = ctx.host_empty((2, n))
+    torch.from_numpy(back).copy_(d * 2.0, non_blocking=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(back, 2.0 * a)
+    node = ctx.numa_node
+    allowed = ""
+    with open("/proc/self/status") as f:
+        for ln in f:
+            if ln.startswith("Mems_allowed_list:"):
+                allowed = ln.split(":", 1)[1].strip()
+    mems = set()
+    for part in filter(None, allowed.split(",")):
+        lo, _, hi = part.partition("-")
+        mems |= set(range(int(lo), int(hi or lo) + 1))
+    nodes = _page_nodes(a.ctypes.data, a.nbytes)
+    if node >= 0 and node in mems and len(mems) > 1 and nodes is not None:
+        assert sum(x == node for x in nodes) >= 0.9 * len(nodes), (node, nodes[:16])
 
 
 def test_unknown_kernel_is_rejected(torch_cuda, ctx):

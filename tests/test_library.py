@@ -63,6 +63,15 @@ def test_error_strings(L):
     assert L.pl_error_string(0) == b"ok"
 
 
+def test_host_free_accepts_only_its_own_buffers(L):
+    """pl_host_free: NULL is a no-op, a pointer pl_host_alloc did not return is refused (the
+    check runs before any CUDA call)."""
+    assert L.pl_host_free(None) == 0
+    buf = ctypes.create_string_buffer(64)
+    assert L.pl_host_free(ctypes.addressof(buf)) == -1
+    assert L.pl_host_alloc(None, 64, ctypes.byref(ctypes.c_void_p())) == -1
+
+
 @pytest.mark.parametrize("name", KERNEL_NAMES)
 def test_host_pointwise_matches_reference_golden(L, name):
     """The exported pylith::fekernels::* host functions run the same pointwise code the device
