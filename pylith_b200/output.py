@@ -241,3 +241,128 @@ class DataWriterVTK:
 
     def close(self) -> None:
         self._mesh = None
+
+
+# ---------------------------------------------------------------------------------------------
+# HDF5 output
+# ---------------------------------------------------------------------------------------------
+
+VECTOR_FIELD_TYPES = ("scalar", "vector", "tensor", "other", "multi_scalar", "multi_vector", "multi_tensor",
+                      "multi_other")  # FieldBase::vectorFieldString (topology/FieldBase.cc:34-56)
+
+
+def _vector_field_type(ncomp: int) -> str:
+    return {1: "scalar", 3: "vector", 6: "tensor"}.get(ncomp, "other")
+
+
+@dataclass
+class DataWriterHDF5:
+    """The reference's DataWriterHDF5 (libsrc/pylith/meshio/DataWriterHDF5.hh) over
+    pylith_b200.hdf5.H5Writer, with the layout PETSc's HDF5 viewer gives that writer's files
+    (the reference's golden files tests/libtests/meshio/data/*.h5 pin it):
+
+      * /geometry/vertices: float64 [nvertices][3], coordinates times the length scale
+        (DataWriter.cc:235-237);
+      * /viz/topology/cells: int32 [ncells][ncorners] with int32 attributes cell_corners and
+        cell_dim; cohesive cells in /viz/topology_1/cells (negative-side then positive-side face
+        vertices);
+      * /cell_fields/partition_rank: float64 [ncells][1] (the MPI rank of every cell, 0 here),
+        attributes vector_field_type "scalar" and componentName0 "0";
+      * /time: float64 [nsteps][1][1], t times the time scale, one entry per output step
+        (DataWriterHDF5.cc:441-463); attribute timestepping = 1 (uint8);
+      * /vertex_fields/<name>, /cell_fields/<name>: float64 [nsteps][npoints][ncomp], attributes
+        timestepping = 1 and vector_field_type (FieldBase::vectorFieldString);
+      * /stations: fixed-length strings (longest name + 1 bytes) from write_point_names.
+
+    The file is written as the calls come: after every call it is complete and readable
+    (datasets grow one step at a time). Steps follow the reference's rule: the k-th write of a
+    field is its step k, and the first field written at a new step adds that step's time."""
+
+    filename: str = "output.h5"
+    time_scale: float = 1.0
+    length_scale: float = 1.0
+    is_info: bool = False
+    _h5: Optional[object] = None
+    _mesh: Optional[M.Mesh] = None
+    _steps: dict = field(default_factory=dict)
+    _tstamp_index: int = 0
+
+    def hdf5_filename(self) -> str:
+        """DataWriterHDF5::hdf5Filename (DataWriterHDF5.cc:422-435)."""
+        if self.is_info:
+            i = self.filename.find(".h5")
+            return (self.filename[:i] if i >= 0 else self.filename[:-1]) + "_info.h5"
+        return self.filename
+
+    def open(self, mesh: M.Mesh, is_info: Optional[bool] = None) -> None:
+        """DataWriterHDF5::open (DataWriterHDF5.cc:82-117): a new file with the mesh."""
+        from . import hdf5 as H5
+
+        if is_info is not None:
+            self.is_info = is_info
+        self.close()
+        self._mesh = mesh
+        self._steps, self._tstamp_index = {}, 0
+        w = H5.H5Writer(self.hdf5_filename())
+        w.create_dataset("/geometry/vertices", np.asarray(mesh.coords, dtype=np.float64) * self.length_scale)
+        corners = vtk_cells(mesh)[0].astype(np.int32)
+        w.create_dataset("/viz/topology/cells", corners,
+                         {"cell_corners": np.int32(corners.shape[1]), "cell_dim": np.int32(3)})
+        if mesh.cohesive is not None and len(mesh.cohesive):
+            coh = np.ascontiguousarray(mesh.cohesive[:, :8], dtype=np.int32)
+            w.create_dataset("/viz/topology_1/cells", coh, {"cell_corners": np.int32(8), "cell_dim": np.int32(3)})
+        w.create_dataset("/cell_fields/partition_rank", np.zeros((mesh.num_cells, 1)),
+                         {"vector_field_type": "scalar", "componentName0": "0"})
+        self._h5 = w
+
+    def _write_time(self, t: float) -> None:
+        w = self._h5
+        if "/time" not in w.series:
+            w.create_series("/time", (1, 1), attrs={"timestepping": np.uint8(1)})
+        w.append("/time", [[t * self.time_scale]])
+        self._tstamp_index += 1
+
+    def _write_field(self, group: str, t: float, name: str, values, npoints: int, vector_field_type) -> None:
+        v = np.asarray(values, dtype=np.float64)
+        if v.shape[0] != npoints:
+            raise ValueError(f"field '{name}' has {v.shape[0]} points, the mesh {npoints}")
+        v = v.reshape(npoints, -1)
+        vtype = vector_field_type or _vector_field_type(v.shape[1])
+        if vtype not in VECTOR_FIELD_TYPES:
+            raise ValueError(f"unknown vector field type '{vtype}'")
+        key = f"{group}/{name}"
+        istep = self._steps[key] = self._steps.get(key, -1) + 1
+        if self._tstamp_index == istep:
+            self._write_time(t)
+        w = self._h5
+        if istep == 0:
+            w.create_series(key, v.shape, attrs={"timestepping": np.uint8(1), "vector_field_type": vtype})
+        w.append(key, v)
+
+    def write_vertex_field(self, t: float, name: str, values, vector_field_type: Optional[str] = None) -> None:
+        """DataWriterHDF5::writeVertexField (DataWriterHDF5.cc:162-216): values [nvertices] or
+        [nvertices][ncomp]; the vector field type defaults from the component count (1 scalar,
+        3 vector, 6 tensor, else other)."""
+        if self._h5 is None:
+            raise RuntimeError("open() the writer with a mesh first")
+        self._write_field("/vertex_fields", t, name, values, self._mesh.num_nodes, vector_field_type)
+
+    def write_cell_field(self, t: float, name: str, values, vector_field_type: Optional[str] = None) -> None:
+        """DataWriterHDF5::writeCellField (DataWriterHDF5.cc:222-276): values [ncells] or
+        [ncells][ncomp] over the domain cells (e.g. the derived cauchy_stress)."""
+        if self._h5 is None:
+            raise RuntimeError("open() the writer with a mesh first")
+        self._write_field("/cell_fields", t, name, values, self._mesh.num_cells, vector_field_type)
+
+    def write_point_names(self, names: Sequence[str]) -> None:
+        """DataWriterHDF5::writePointNames (DataWriterHDF5.cc:282-416): /stations as
+        null-padded fixed-length strings of the longest name plus one byte."""
+        if self._h5 is None:
+            raise RuntimeError("open() the writer with a mesh first")
+        width = max([len(n) for n in names] + [0]) + 1
+        self._h5.create_dataset("/stations", np.array([n.encode() for n in names], dtype=f"S{width}"))
+
+    def close(self) -> None:
+        if self._h5 is not None:
+            self._h5.close()
+            self._h5 = None

@@ -419,9 +419,10 @@ def test_destroy_in_any_order(torch_cuda):
 
 
 @pytest.mark.parametrize("kind", ["tet4", "hex8", "hex27"])
-def test_derived_fields_match_oracle(oracle_lib, torch_cuda, ctx, kind):
+def test_derived_fields_match_oracle(oracle_lib, torch_cuda, ctx, kind, tmp_path):
     """pl_compute_derived_field (cauchy_stress, cauchy_strain of basis order 0 at the cell
-    centroids, IntegratorDomain.cc:596-630) against the oracle's centroid projection."""
+    centroids, IntegratorDomain.cc:596-630) against the oracle's centroid projection; the fields
+    and the solution written through DataWriterHDF5 read back unchanged."""
     from pylith_b200 import feassemble as FA
 
     O, torch = oracle_lib, torch_cuda
@@ -439,6 +440,20 @@ def test_derived_fields_match_oracle(oracle_lib, torch_cuda, ctx, kind):
     got = out.cpu().numpy()
     assert rel_l2(got[:, :6], ref_s) <= TOL64
     assert rel_l2(got[:, 6:], ref_e) <= TOL64
+    from pylith_b200 import hdf5 as H5
+    from pylith_b200 import output as OUT
+
+    w = OUT.DataWriterHDF5(filename=str(tmp_path / "out.h5"))
+    w.open(mesh)
+    w.write_vertex_field(1.0, "displacement", u[:3 * mesh.num_nodes].reshape(-1, 3))
+    w.write_cell_field(1.0, "cauchy_stress", got[:, :6])
+    w.write_cell_field(1.0, "cauchy_strain", got[:, 6:])
+    w.close()
+    f = H5.H5File(str(tmp_path / "out.h5"))
+    assert np.array_equal(f.dataset("/vertex_fields/displacement")[0], u[:3 * mesh.num_nodes].reshape(-1, 3))
+    assert np.array_equal(f.dataset("/cell_fields/cauchy_stress")[0], got[:, :6])
+    assert np.array_equal(f.dataset("/cell_fields/cauchy_strain")[0], got[:, 6:])
+    assert f.attrs("/cell_fields/cauchy_stress")["vector_field_type"] == "tensor"
 
 
 def test_derived_genmaxwell_stress(oracle_lib, torch_cuda, ctx):
