@@ -76,9 +76,11 @@ class H5File:
     strings as a list of str), `attrs(path)` the attributes of a group or dataset."""
 
     def __init__(self, path_or_bytes):
+        self.path = None
         if isinstance(path_or_bytes, (bytes, bytearray)):
             self.buf = bytes(path_or_bytes)
         else:
+            self.path = str(path_or_bytes)
             with open(path_or_bytes, "rb") as f:
                 self.buf = f.read()
         self._objects: Dict[int, _Object] = {}
@@ -367,9 +369,42 @@ class H5File:
         arr = np.frombuffer(raw[:count * dt.size], dtype=dt.dtype).reshape(shape)
         return arr.astype(arr.dtype.newbyteorder("=")) if dt.dtype.byteorder == ">" else arr.copy()
 
+    def _external(self, efl: bytes, nbytes: int, path: str) -> bytes:
+        """Data of a dataset kept in external raw files (External Data Files message): the
+        slots' byte ranges, concatenated. A relative file name is looked up from the current
+        directory (the HDF5 library's default) and then beside this file."""
+        import os
+
+        if efl[0] != 1:
+            raise H5FormatError(f"external data files message version {efl[0]} in {path}")
+        used = self._u_bytes(efl, 6, 2)
+        heap = self._local_heap(self._u_bytes(efl, 8, self.so))
+        out = bytearray()
+        p = 8 + self.so
+        for _ in range(used):
+            name_off, offset, size = (self._u_bytes(efl, p + i * self.sl, self.sl) for i in range(3))
+            p += 3 * self.sl
+            name = heap[name_off:heap.index(b"\0", name_off)].decode()
+            cands = [name] + ([os.path.join(os.path.dirname(self.path), name)] if self.path else [])
+            fn = next((c for c in cands if os.path.isfile(c)), None)
+            if fn is None:
+                raise H5FormatError(f"external file '{name}' of {path} not found")
+            with open(fn, "rb") as fh:
+                fh.seek(offset)
+                want = nbytes - len(out)
+                out += fh.read(want if size == UNDEF else min(want, size))
+            if len(out) >= nbytes:
+                break
+        if len(out) < nbytes:
+            raise H5FormatError(f"external files of {path} hold {len(out)} of {nbytes} bytes")
+        return bytes(out)
+
     def _raw(self, ob: _Object, layout: bytes, shape, esize: int, path: str) -> bytes:
         v = layout[0]
         nbytes = int(np.prod(shape, dtype=np.int64)) * esize
+        efl = ob.first(MSG_EXTERNAL)
+        if efl is not None:
+            return self._external(efl, nbytes, path)
         if v == 3:
             cls = layout[1]
             if cls == 0:
@@ -544,6 +579,7 @@ def _datatype_message(dtype) -> bytes:
     """Datatype message (version 1) for little-endian IEEE floats, two's-complement and
     unsigned integers and null-terminated fixed-length ASCII strings."""
     dt = np.dtype(dtype)
+    big = dt.byteorder == ">"
     if dt.kind == "f":
         size = dt.itemsize
         if size == 8:
@@ -552,10 +588,10 @@ def _datatype_message(dtype) -> bytes:
             exp_loc, exp_size, mant_size, bias, sign = 23, 8, 23, 127, 31
         else:
             raise ValueError(f"float size {size}")
-        return struct.pack("<BBBBI", 0x11, 0x20, sign, 0, size) + struct.pack(
+        return struct.pack("<BBBBI", 0x11, 0x20 | int(big), sign, 0, size) + struct.pack(
             "<HHBBBBI", 0, 8 * size, exp_loc, exp_size, 0, mant_size, bias)
     if dt.kind in "iu":
-        bits = 0x08 if dt.kind == "i" else 0
+        bits = (0x08 if dt.kind == "i" else 0) | int(big)
         return struct.pack("<BBBBI", 0x10, bits, 0, 0, dt.itemsize) + struct.pack("<HH", 0, 8 * dt.itemsize)
     if dt.kind == "S":
         return struct.pack("<BBBBI", 0x13, 0, 0, 0, dt.itemsize)
@@ -616,6 +652,7 @@ class _Series:
     def __init__(self, header: int, dims_at: int, layout_at: int, tail, dtype):
         self.header, self.dims_at, self.layout_at = header, dims_at, layout_at
         self.tail, self.dtype = tuple(int(t) for t in tail), np.dtype(dtype)
+        self.step_bytes = int(np.prod(self.tail, dtype=np.int64)) * self.dtype.itemsize
         self.chunks: List[Tuple[int, int]] = []  # (address, bytes) per step
         self.nodes: Dict[Tuple[int, int], int] = {}  # (level, index) -> address
         self.root = UNDEF
@@ -775,6 +812,41 @@ class H5Writer:
         layout_at = h.addr + 16 + len(msgs[0]) + len(msgs[1]) + len(msgs[2]) + 8 + 3
         self.series["/" + path.strip("/")] = _Series(h.addr, dims_at, layout_at, tail, dt)
         self._link(self._split(path)[0], name, h.addr)
+        self._superblock()
+
+    def create_external(self, path: str, filename: str, tail, dtype=">f8", max_steps: Optional[int] = None,
+                        attrs: Optional[Dict[str, object]] = None) -> None:
+        """A dataset of shape (1,) + tail whose data live in the raw file `filename` (External Data
+        Files message, one slot from offset 0 of unlimited size), as H5Pset_external gives it;
+        `extend` sets its number of steps as the caller appends raw steps to that file.
+        max_steps None makes the first dimension unlimited."""
+        name = self._ensure_parent(path)
+        tail = tuple(int(t) for t in tail)
+        dt = np.dtype(dtype)
+        fname = filename.encode() + b"\0"
+        heap_data = bytes(8) + fname + bytes(_pad8(len(fname)) - len(fname))
+        heap_at = self._alloc(32 + len(heap_data))
+        self._write(heap_at, b"HEAP" + bytes(4) + _u8(len(heap_data)) + _u8(UNDEF) + _u8(heap_at + 32) + heap_data)
+        efl = struct.pack("<B3xHH", 1, 1, 1) + _u8(heap_at) + _u8(8) + _u8(0) + _u8(UNDEF)
+        nbytes = int(np.prod(tail, dtype=np.int64)) * dt.itemsize
+        space = _dataspace_message((1,) + tail, (max_steps,) + tail)
+        layout = struct.pack("<BB", 3, 1) + _u8(UNDEF) + _u8(nbytes)
+        msgs = [_msg(MSG_DATASPACE, space), _msg(MSG_DATATYPE, _datatype_message(dt)),
+                _msg(MSG_FILL, _fill_message(False)), _msg(MSG_LAYOUT, layout), _msg(MSG_EXTERNAL, efl)]
+        msgs += [_msg(MSG_ATTRIBUTE, _attribute_message(k, v)) for k, v in (attrs or {}).items()]
+        h = self._object_header(msgs)
+        dims_at = h.addr + 16 + 8 + 8
+        size_at = h.addr + 16 + len(msgs[0]) + len(msgs[1]) + len(msgs[2]) + 8 + 2 + _SO
+        s = _Series(h.addr, dims_at, size_at, tail, dt)
+        self.series["/" + path.strip("/")] = s
+        self._link(self._split(path)[0], name, h.addr)
+        self._superblock()
+
+    def extend(self, path: str, steps: int) -> None:
+        """Sets the number of steps of an external dataset (its dataspace and layout size)."""
+        s = self.series["/" + path.strip("/")]
+        self._write(s.dims_at, _u8(steps))
+        self._write(s.layout_at, _u8(steps * s.step_bytes))
         self._superblock()
 
     def append(self, path: str, data) -> int:

@@ -334,10 +334,13 @@ class DataWriterHDF5:
         istep = self._steps[key] = self._steps.get(key, -1) + 1
         if self._tstamp_index == istep:
             self._write_time(t)
-        w = self._h5
+        self._store(key, name, v, vtype, istep)
+
+    def _store(self, key: str, name: str, v: np.ndarray, vtype: str, istep: int) -> None:
+        """One step of a field: a chunk of the dataset (created at the field's first step)."""
         if istep == 0:
-            w.create_series(key, v.shape, attrs={"timestepping": np.uint8(1), "vector_field_type": vtype})
-        w.append(key, v)
+            self._h5.create_series(key, v.shape, attrs={"timestepping": np.uint8(1), "vector_field_type": vtype})
+        self._h5.append(key, v)
 
     def write_vertex_field(self, t: float, name: str, values, vector_field_type: Optional[str] = None) -> None:
         """DataWriterHDF5::writeVertexField (DataWriterHDF5.cc:162-216): values [nvertices] or
@@ -363,6 +366,212 @@ class DataWriterHDF5:
         self._h5.create_dataset("/stations", np.array([n.encode() for n in names], dtype=f"S{width}"))
 
     def close(self) -> None:
+        """DataWriterHDF5::close (DataWriterHDF5.cc:137-160): closes the file and writes its Xdmf
+        description next to it (write_xdmf)."""
+        if self._h5 is not None:
+            self._h5.close()
+            self._h5 = None
+            write_xdmf(self.hdf5_filename())
+
+
+# ---------------------------------------------------------------------------------------------
+# Xdmf metadata for HDF5 output
+# ---------------------------------------------------------------------------------------------
+
+_XDMF_CELL_TYPES = {(0, 1): "Polyvertex", (1, 2): "Polyline", (2, 3): "Triangle", (2, 4): "Quadrilateral",
+                    (3, 4): "Tetrahedron", (3, 8): "Hexahedron"}
+_XDMF_VECTOR_TYPES = {"scalar": "Scalar", "vector": "Vector", "tensor": "Tensor6"}
+_XDMF_TENSOR_SUFFIXES = {2: ("_xx", "_yy", "_xy"), 3: ("_xx", "_yy", "_zz", "_xy", "_yz", "_xz")}
+_HEAVY = "&HeavyData;:"
+
+
+class _XdmfLines:
+    """Lines of an Xdmf document, each indented by two spaces per depth."""
+
+    def __init__(self):
+        self.lines: List[str] = []
+
+    def __call__(self, depth: int, text: str) -> None:
+        self.lines.append("  " * depth + text)
+
+    def item(self, depth: int, attrs: str, body: str) -> None:
+        """<DataItem attrs> body </DataItem>, the body one level deeper."""
+        self(depth, f"<DataItem {attrs}>")
+        self(depth + 1, body)
+        self(depth, "</DataItem>")
+
+    def text(self) -> str:
+        return "\n".join(self.lines) + "\n"
+
+
+def _xdmf_field(f, group: str, name: str):
+    """(name, Xdmf type, center, HDF5 path, steps, points, components) of one field dataset."""
+    path = f"/{group}/{name}"
+    shape = f.dataset(path).shape
+    vtype = f.attrs(path).get("vector_field_type")
+    if vtype is not None:
+        xtype = _XDMF_VECTOR_TYPES.get(str(vtype).lower(), "Matrix")
+    else:  # no attribute: guess from the component count
+        xtype = {1: "Scalar", 3: "Vector"}.get(shape[-1], "Matrix") if len(shape) in (2, 3) else "Matrix"
+    if len(shape) == 2:
+        steps, points, comps = 1, shape[0], shape[1]
+    elif len(shape) == 3:
+        steps, points, comps = shape
+    else:
+        raise ValueError(f"unexpected shape {shape} of dataset '{path}'")
+    center = "Node" if group == "vertex_fields" else "Cell"
+    return name, xtype, center, path, steps, points, comps
+
+
+def write_xdmf(filename_h5: str, filename_xdmf: Optional[str] = None) -> Optional[str]:
+    """Writes the Xdmf file describing an HDF5 output file for visualization tools, as the
+    reference's Xdmf writer does (pylith/meshio/Xdmf.py, called from DataWriterHDF5::close,
+    meshio/DataWriterHDF5.cc:146-157); its golden files tests/pytests/meshio/data/*.xmf pin the
+    text line for line. Returns the path written, or None for a 1-D mesh (Xdmf has no 1-D grids).
+
+    The document references the HDF5 datasets by path: the cells and vertices once in the domain
+    (a 2-D mesh gets a zero z coordinate through a JOIN function), then one uniform grid per time
+    stamp of /time (in a temporal collection) or one grid without time, each with the fields of
+    /vertex_fields and /cell_fields in name order. Scalars and vectors are one attribute per
+    field (2-D vectors joined with a zero z); tensors become one scalar attribute per component
+    (_xx, _yy, _zz, _xy, _yz, _xz; _xx, _yy, _xy in 2-D) and other fields one per component
+    (_0, _1, ...)."""
+    from . import hdf5 as H5
+
+    f = H5.H5File(filename_h5)
+    out_path = filename_xdmf or filename_h5.replace(".h5", ".xmf")
+    verts = f.dataset("/geometry/vertices")
+    cells = f.dataset("/viz/topology/cells")
+    nv, dim = verts.shape
+    if dim == 1:
+        return None
+    nc, ncorners = cells.shape
+    cell_dim = int(f.attrs("/viz/topology/cells").get("cell_dim", dim))
+    cell_type = _XDMF_CELL_TYPES.get((cell_dim, ncorners), "Unknown")
+    times = f.dataset("/time").ravel() if f.has("/time") else None
+    fields = [_xdmf_field(f, g, k) for g in ("vertex_fields", "cell_fields") if f.has("/" + g) for k in f.keys("/" + g)]
+
+    x = _XdmfLines()
+    x(0, '<?xml version="1.0" ?>')
+    x(0, '<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" [')
+    x(0, f'<!ENTITY HeavyData "{os.path.basename(filename_h5)}">')
+    x(0, "]>")
+    x(0, "")
+    x(0, "<Xdmf>")
+    x(1, '<Domain Name="domain">')
+    x.item(2, f'Name="cells" ItemType="Uniform" Format="HDF" NumberType="Float" Precision="8" '
+              f'Dimensions="{nc} {ncorners}"', _HEAVY + "/viz/topology/cells")
+    if dim == 3:
+        x.item(2, f'Name="vertices" ItemType="Uniform" Format="HDF" Dimensions="{nv} {dim}"',
+               _HEAVY + "/geometry/vertices")
+    elif dim == 2:
+        x(2, f'<DataItem Name="vertices" ItemType="Function" Dimensions="{nv} 3" Function="JOIN($0, $1, $2)">')
+        for axis, comp in (("X", 0), ("Y", 1)):
+            x(3, f'<DataItem Name="vertices{axis}" ItemType="Hyperslab" Type="HyperSlab" Dimensions="{nv} 1">')
+            x.item(4, 'Dimensions="3 2" Format="XML"', f"0 {comp}   1 1   {nv} 1")
+            x.item(4, f'Dimensions="{nv} 1" Format="HDF"', _HEAVY + "/geometry/vertices")
+            x(3, "</DataItem>")
+        x(3, f'<DataItem Name="verticesZ" ItemType="Function" Dimensions="{nv} 1" Function="0*$0">')
+        x.item(4, 'Reference="XML"', '/Xdmf/Domain/DataItem[@Name="vertices"]/DataItem[@Name="verticesX"]')
+        x(3, "</DataItem>")
+        x(2, "</DataItem>")
+    else:
+        raise ValueError(f"unexpected spatial dimension {dim} of the domain vertices")
+
+    def grid(step: Optional[int]) -> None:
+        x(3, '<Grid Name="domain" GridType="Uniform">')
+        x(4, f'<Topology TopologyType="{cell_type}" NumberOfElements="{nc}">')
+        x.item(5, 'Reference="XML"', '/Xdmf/Domain/DataItem[@Name="cells"]')
+        x(4, "</Topology>")
+        x(4, '<Geometry GeometryType="XYZ">')
+        x.item(5, 'Reference="XML"', '/Xdmf/Domain/DataItem[@Name="vertices"]')
+        x(4, "</Geometry>")
+        at = 0 if step is None else step
+        for name, xtype, center, path, steps, points, comps in fields:
+            hdf = f'DataType="Float" Precision="8" Dimensions="{steps} {points} {comps}" Format="HDF"'
+            if xtype in ("Tensor6", "Matrix"):
+                suffixes = (_XDMF_TENSOR_SUFFIXES[dim] if xtype == "Tensor6" else
+                            tuple(f"_{i}" for i in range(comps)))
+                for i in range(comps):
+                    x(4, f'<Attribute Name="{name}{suffixes[i]}" Type="Scalar" Center="{center}">')
+                    x(5, f'<DataItem ItemType="HyperSlab" Dimensions="1 {points} 1" Type="HyperSlab">')
+                    x.item(6, 'Dimensions="3 3" Format="XML"', f"{at} 0 {i}    1 1 1    1 {points} 1")
+                    x.item(6, hdf, _HEAVY + path)
+                    x(5, "</DataItem>")
+                    x(4, "</Attribute>")
+                continue
+            x(4, f'<Attribute Name="{name}" Type="{xtype}" Center="{center}">')
+            if dim == 2 and xtype == "Vector":
+                x(5, f'<DataItem ItemType="Function" Dimensions="{points} 3" Function="JOIN($0, $1, $2)">')
+                for comp in (0, 1):
+                    x(6, f'<DataItem ItemType="HyperSlab" Dimensions="{points} 1" Type="HyperSlab">')
+                    x.item(7, 'Dimensions="3 3" Format="XML"', f"{at} 0 {comp}    1 1 1    1 {points} 1")
+                    x.item(7, hdf, _HEAVY + path)
+                    x(6, "</DataItem>")
+                grid_ref = "/Xdmf/Domain/Grid" if step is None else "/Xdmf/Domain/Grid/Grid[1]"
+                x(6, f'<DataItem ItemType="Function" Dimensions="{points} 1" Function="0*$0">')
+                x.item(7, 'Reference="XML"', f'{grid_ref}/Attribute[@Name="{name}"]/DataItem[1]/DataItem[1]')
+                x(6, "</DataItem>")
+                x(5, "</DataItem>")
+            else:
+                x(5, f'<DataItem ItemType="HyperSlab" Dimensions="1 {points} {comps}" Type="HyperSlab">')
+                x.item(6, 'Dimensions="3 3" Format="XML"', f"{at} 0 0    1 1 1    1 {points} {comps}")
+                x.item(6, hdf, _HEAVY + path)
+                x(5, "</DataItem>")
+            x(4, "</Attribute>")
+        x(3, "</Grid>")
+
+    if times is not None:
+        x(2, '<Grid Name="TimeSeries" GridType="Collection" CollectionType="Temporal">')
+        x(3, '<Time TimeType="List">')
+        x(4, f'<DataItem Format="XML" NumberType="Float" Dimensions="{len(times)}">')
+        x(4, "".join("  %16.8e" % t for t in times))
+        x(4, "</DataItem>")
+        x(3, "</Time>")
+        for step in range(len(times)):
+            grid(step)
+        x(2, "</Grid>")
+    else:
+        grid(None)
+    x(1, "</Domain>")
+    x(0, "</Xdmf>")
+    with open(out_path, "w") as fh:
+        fh.write(x.text())
+    return out_path
+
+
+@dataclass
+class DataWriterHDF5Ext(DataWriterHDF5):
+    """The reference's DataWriterHDF5Ext (libsrc/pylith/meshio/DataWriterHDF5Ext.hh): the HDF5
+    file holds the mesh and /time as DataWriterHDF5 writes them, while every field's values go
+    to a raw file of big-endian FP64 values, <file base>_<field>.dat (_datasetFilename,
+    DataWriterHDF5Ext.cc:518-529), one step after another; the field's dataset in the HDF5 file
+    refers to that file (an external dataset, HDF5::createDatasetRawExternal) with dimensions
+    steps x points x components (at most one step for an info file) and carries the attribute
+    vector_field_type. No Xdmf file is written (DataWriterHDF5Ext::close)."""
+
+    _raw: dict = field(default_factory=dict)
+
+    def dataset_filename(self, name: str) -> str:
+        base = self.hdf5_filename()
+        i = base.find(".h5")
+        return (base[:i] if i >= 0 else base) + f"_{name}.dat"
+
+    def _store(self, key: str, name: str, v: np.ndarray, vtype: str, istep: int) -> None:
+        if istep == 0:
+            fn = self.dataset_filename(name)
+            self._raw[key] = open(fn, "wb")
+            self._h5.create_external(key, fn, v.shape, ">f8", 1 if self.is_info else None,
+                                     attrs={"vector_field_type": vtype})
+        fh = self._raw[key]
+        fh.write(v.astype(">f8").tobytes())
+        fh.flush()
+        self._h5.extend(key, istep + 1)
+
+    def close(self) -> None:
+        for fh in self._raw.values():
+            fh.close()
+        self._raw = {}
         if self._h5 is not None:
             self._h5.close()
             self._h5 = None

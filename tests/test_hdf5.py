@@ -153,3 +153,91 @@ def test_reader_pins_on_the_reference_files():
         f = H5.H5File(raw)
         for p, v in meta[name]["datasets"].items():
             assert np.array_equal(f.dataset(p), d[v["key"]])
+
+
+XDMF_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "xdmf_golden.json")
+
+
+def _xdmf_cases():
+    with open(XDMF_GOLDEN) as fh:
+        return json.load(fh)
+
+
+@pytest.mark.parametrize("name", sorted(_xdmf_cases()))
+def test_xdmf_is_byte_identical_to_the_reference(tmp_path, name):
+    """write_xdmf against the reference's golden .xmf files (tests/pytests/meshio/data, compared
+    line for line by its TestXdmf.py). The HDF5 file is rebuilt from the golden metadata (dataset
+    shapes and types, cell_dim, vector_field_type, time stamps; values are irrelevant to Xdmf)."""
+    import hashlib
+
+    case = _xdmf_cases()[name]
+    path = str(tmp_path / name)
+    with H5.H5Writer(path) as w:
+        for p, d in case["datasets"].items():
+            data = np.asarray(d["values"]).reshape(d["shape"]) if "values" in d else np.zeros(d["shape"], d["dtype"])
+            w.create_dataset(p, data.astype(d["dtype"]), attrs={k: (np.int32(v) if k == "cell_dim" else v)
+                                                                for k, v in d["attrs"].items()})
+    out = OUT.write_xdmf(path)
+    assert out == path.replace(".h5", ".xmf")
+    assert hashlib.sha256(open(out, "rb").read()).hexdigest() == case["xmf_sha256"]
+
+
+def test_data_writer_hdf5_writes_its_xdmf(tmp_path):
+    mesh = M.box_hex(2, 1, 1)
+    w = OUT.DataWriterHDF5(filename=str(tmp_path / "soln.h5"))
+    w.open(mesh)
+    for t in (0.0, 1.0):
+        w.write_vertex_field(t, "displacement", np.zeros((mesh.num_nodes, 3)))
+        w.write_cell_field(t, "cauchy_stress", np.zeros((mesh.num_cells, 6)))
+    w.close()
+    text = open(tmp_path / "soln.xmf").read()
+    assert '<!ENTITY HeavyData "soln.h5">' in text
+    assert text.count('<Grid Name="domain" GridType="Uniform">') == 2
+    assert '<Attribute Name="cauchy_stress_xz" Type="Scalar" Center="Cell">' in text
+    assert '<Topology TopologyType="Hexahedron" NumberOfElements="2">' in text
+
+
+@pytest.mark.parametrize("name", ["tet4_vertex.h5", "hex8_cell.h5"])
+def test_external_writer_reproduces_the_reference_datasets(tmp_path, name):
+    """DataWriterHDF5Ext: the reference's HDF5Ext tests compare against the same golden files as
+    the HDF5 ones (TestDataWriterHDF5ExtMesh_Cases.cc), reading fields through the external raw
+    files; values, shapes and vector_field_type must match."""
+    ds, _ = _golden(name)
+    kind, where = name[:-3].split("_")
+    cohesive = None
+    if kind == "hex8":
+        prisms = ds["/viz/topology_1/cells"][0]
+        cohesive = np.concatenate([prisms, np.zeros((len(prisms), 4), dtype=np.int32)], axis=1)
+    mesh = M.Mesh(M.CELL_TET4 if kind == "tet4" else M.CELL_HEX8, ds["/geometry/vertices"][0],
+                  ds["/viz/topology/cells"][0].astype(np.int32), cohesive)
+    w = OUT.DataWriterHDF5Ext(filename=str(tmp_path / name))
+    w.open(mesh)
+    group = f"/{where}_fields"
+    fields = {p: (v, a) for p, (v, a) in ds.items() if p.startswith(group + "/") and "timestepping" in a}
+    for p, (v, a) in fields.items():
+        add = w.write_vertex_field if where == "vertex" else w.write_cell_field
+        add(1.0, p.rsplit("/", 1)[1], v[0], vector_field_type=a["vector_field_type"])
+    w.close()
+    f = H5.H5File(str(tmp_path / name))
+    assert np.array_equal(f.dataset("/time"), ds["/time"][0])
+    assert np.array_equal(f.dataset("/geometry/vertices"), ds["/geometry/vertices"][0])
+    for p, (v, a) in fields.items():
+        assert np.array_equal(f.dataset(p), v), p
+        assert f.attrs(p) == {"vector_field_type": a["vector_field_type"]}
+        raw = np.fromfile(w.dataset_filename(p.rsplit("/", 1)[1]), dtype=">f8")
+        assert np.array_equal(raw, v.ravel())
+
+
+def test_external_writer_steps(tmp_path):
+    mesh = M.box_hex(2, 1, 1)
+    w = OUT.DataWriterHDF5Ext(filename=str(tmp_path / "soln.h5"), time_scale=10.0)
+    w.open(mesh)
+    disp = [np.random.default_rng(k).standard_normal((mesh.num_nodes, 3)) for k in range(5)]
+    for k, d in enumerate(disp):
+        w.write_vertex_field(float(k), "displacement", d)
+        f = H5.H5File(str(tmp_path / "soln.h5"))
+        assert np.array_equal(f.dataset("/vertex_fields/displacement"), np.array(disp[:k + 1]))
+        assert np.array_equal(f.dataset("/time")[:, 0, 0], 10.0 * np.arange(k + 1))
+    w.close()
+    assert not (tmp_path / "soln.xmf").exists()
+    assert (tmp_path / "soln_displacement.dat").stat().st_size == 5 * mesh.num_nodes * 3 * 8
