@@ -198,12 +198,13 @@ int pl_context_synchronize(pl_context ctx);
 /* No counterpart in the reference (PETSc keeps its Vecs in pageable host memory). Page-locked
  * host memory for the host buffers of calls that copy between host and device (the
  * pl_compute_*_host entry points, or a caller's own copies around the device entry points):
- * anonymous pages, advised as transparent huge pages from 2 MiB up, preferring the NUMA node
- * the host reports for the context's GPU (so that on a two-socket host the device's reads do
- * not cross the inter-socket link), faulted in and registered with CUDA. The node is a
- * preference: with no NUMA information (one-node hosts) or no free memory on that node the
- * pages land where the kernel puts them. *out is page-aligned and zero-filled; release it with
- * pl_host_free (not cudaFreeHost). Thread-safe. */
+ * the CUDA driver's page-locked allocation (cudaHostAlloc, portable), made while the calling
+ * thread prefers the NUMA node the host reports for the context's GPU, so that on a two-socket
+ * host the device's reads do not cross the inter-socket link. Copy engines read such buffers at
+ * the link's rate, where page-locked ranges of scattered small pages can cap host-to-device
+ * copies far below it. The node is a preference: with no NUMA information (one-node hosts) or
+ * no free memory on that node the pages land where the kernel puts them. *out is zero-filled
+ * and at least 256-byte aligned; release it with pl_host_free (not cudaFreeHost). Thread-safe. */
 int pl_host_alloc(pl_context ctx, size_t bytes, void** out);
 int pl_host_free(void* ptr);
 /* NUMA node the host reports for the context's GPU; -1 when it reports none. */

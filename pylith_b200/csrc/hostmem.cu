@@ -1,14 +1,13 @@
 // Page-locked host memory for the host side of host <-> device copies (pl_host_alloc).
 //
-// A host-to-device DMA copy reads host memory with non-posted PCIe reads, so its rate depends
-// on where the pages are: on a two-socket host, pages on the other socket make every read cross
-// the inter-socket link, and page-locked buffers from cudaHostAlloc land wherever the
-// allocating thread happens to run. pl_host_alloc maps anonymous memory, prefers the GPU's
-// node (a node without free memory still yields a buffer), advises transparent huge pages for
-// buffers of 2 MiB and more, faults every page in under that policy and registers the range
-// with CUDA.
+// The buffers come from the CUDA driver (cudaHostAlloc), whose page-locked allocations the copy
+// engines read at the link's rate; page-locked ranges made of scattered small pages (as some
+// general-purpose pinned-memory caches hand out) can cap host-to-device DMA at a fraction of it.
+// A host-to-device copy also reads host memory across the PCIe link with non-posted reads, so on
+// a two-socket host pages on the far socket add the inter-socket link to every read: for the
+// duration of the allocation the calling thread prefers the GPU's NUMA node (its previous policy
+// is restored afterwards).
 #include <cuda_runtime.h>
-#include <sys/mman.h>
 #include <sys/syscall.h>
 #include <unistd.h>
 
@@ -59,28 +58,27 @@ int pl_context_numa_node(pl_context c, int* node) {
 int pl_host_alloc(pl_context c, size_t bytes, void** out) {
     if (!c || !out || bytes == 0) return fail(PL_ERR_INVALID_ARG, "bad arguments");
     *out = nullptr;
-    const size_t page = (size_t)sysconf(_SC_PAGESIZE);
-    const size_t len = (bytes + page - 1) / page * page;
-    void* p = mmap(nullptr, len, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
-    if (p == MAP_FAILED) return fail(PL_ERR_OUT_OF_MEMORY, "mmap of host buffer failed");
+    PLB_CUDA(cudaSetDevice(c->device));
     const int node = gpu_numa_node(c->device);
-    if (node >= 0 && node < 64) {
+    // the calling thread's memory policy, restored after the allocation
+    int old_mode = 0;
+    unsigned long old_mask[16] = {0};
+    bool policy = false;
+    if (node >= 0 && node < 64 &&
+        syscall(SYS_get_mempolicy, &old_mode, old_mask, 16ul * 64ul, nullptr, 0ul) == 0) {
         unsigned long mask = 1ul << node;
-        // a refused policy (no NUMA support in the kernel, the node outside the process's
-        // cpuset) leaves the default placement, which still works
-        syscall(SYS_mbind, p, len, kMpolPreferred, &mask, 64ul, 0u);
+        // a refused policy (no NUMA support, the node outside the process's cpuset) leaves the
+        // default placement, which still works
+        policy = syscall(SYS_set_mempolicy, kMpolPreferred, &mask, 64ul) == 0;
     }
-    if (len >= (2u << 20)) madvise(p, len, MADV_HUGEPAGE);
-    std::memset(p, 0, len);  // fault the pages in under the node policy
-    cudaError_t e = cudaSetDevice(c->device);
-    if (e == cudaSuccess) e = cudaHostRegister(p, len, cudaHostRegisterPortable);
-    if (e != cudaSuccess) {
-        munmap(p, len);
-        return cuda_fail(e, "cudaHostRegister");
-    }
+    void* p = nullptr;
+    const cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+    if (policy) syscall(SYS_set_mempolicy, old_mode, old_mask, 16ul * 64ul);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    std::memset(p, 0, bytes);
     {
         std::lock_guard<std::mutex> lk(g_host_mu);
-        g_host_maps[p] = len;
+        g_host_maps[p] = bytes;
     }
     *out = p;
     return PL_OK;
@@ -88,17 +86,13 @@ int pl_host_alloc(pl_context c, size_t bytes, void** out) {
 
 int pl_host_free(void* ptr) {
     if (!ptr) return PL_OK;
-    size_t len = 0;
     {
         std::lock_guard<std::mutex> lk(g_host_mu);
         auto it = g_host_maps.find(ptr);
         if (it == g_host_maps.end()) return fail(PL_ERR_INVALID_ARG, "pointer not from pl_host_alloc");
-        len = it->second;
         g_host_maps.erase(it);
     }
-    cudaError_t e = cudaHostUnregister(ptr);
-    munmap(ptr, len);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaHostUnregister");
+    PLB_CUDA(cudaFreeHost(ptr));
     return PL_OK;
 }
 
