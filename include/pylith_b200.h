@@ -358,6 +358,11 @@ int pl_solver_set_reliable(pl_solver solver, int enable, double delta);
  * change; call it again after such a change or a new time step. */
 int pl_solver_setup(pl_solver solver, double t, double dt);
 int pl_solver_solve(pl_solver solver, const double* b_dev, double* x_dev);
+/* The Dirichlet values into a solution vector: u[i] = values[i] at every DOF marked in the
+ * constrained mask given to pl_solver_create, every other entry untouched (fault DOFs included); values is a full local vector whose
+ * constrained entries hold the boundary values (ConstraintSpatialDB::setSolution,
+ * feassemble/ConstraintSpatialDB.cc:116-159, DMPlexInsertBoundaryValuesEssentialBdField). */
+int pl_solver_insert_constrained(pl_solver solver, const double* values_dev, double* u_dev);
 /* Sets the positive side of every fault node to u+ = u- + d from the interface integrator's
  * slip and reference directions (planar faults: one normal per fault node). */
 int pl_solver_apply_fault_slip(pl_solver solver, pl_integrator iface, double* u_dev);

@@ -120,6 +120,7 @@ SIGNATURES = {
     "pl_solver_solve": (_I, [_P, _P, _P]),
     "pl_solver_get_stats": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                                  ctypes.POINTER(_D)]),
+    "pl_solver_insert_constrained": (_I, [_P, _P, _P]),
     "pl_solver_apply_fault_slip": (_I, [_P, _P, _P]),
     "pl_solver_destroy": (_I, [_P]),
     "pl_batch_solver_create": (_I, [_P, _I, ctypes.POINTER(_P)]),

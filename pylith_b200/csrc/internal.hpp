@@ -219,6 +219,7 @@ struct pl_solver_s {
     int64_t n = 0;       // DOFs (3 per node)
     int64_t nnodes = 0;  // node rows
     uint8_t* d_mask = nullptr;
+    uint8_t* d_dirichlet = nullptr;  // the caller's constrained DOFs alone (boundary-value insertion)
     double* d_diag = nullptr;
     double* d_pinv = nullptr;
     float* d_pinv32 = nullptr;

@@ -263,6 +263,15 @@ __global__ void k_fault_fold_blocks(double* diag, const int32_t* __restrict__ ne
     }
 }
 
+// Dirichlet values into the solution: u[i] = values[i] at every DOF the caller constrained (not
+// the DOFs the reduced fault formulation eliminates), the other entries untouched (ConstraintSpatialDB::setSolution,
+// feassemble/ConstraintSpatialDB.cc:116-159, through DMPlexInsertBoundaryValuesEssentialBdField).
+__global__ void k_insert_constrained(double* __restrict__ u, const double* __restrict__ values,
+                                     const uint8_t* __restrict__ mask, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (mask[i]) u[i] = values[i];
+}
+
 // u+ = u- + d, d = n slip[0] + t1 slip[1] + t2 slip[2] with the fault's tangential directions
 // (BoundaryDirections::tangential_directions, the same construction f0l_slip uses).
 __global__ void k_fault_apply_slip(double* u, const int32_t* __restrict__ neg, const int32_t* __restrict__ pos,
@@ -682,6 +691,7 @@ int pl_solver_create(pl_mesh m, const uint8_t* constrained, pl_solver* out) {
         if (e == cudaSuccess) e = dev_alloc(p, cnt);
     };
     A(&S->d_mask, n);
+    A(&S->d_dirichlet, n);
     A(&S->d_diag, 9 * S->nnodes);
     A(&S->d_pinv, 9 * S->nnodes);
     A(&S->d_pinv32, 9 * S->nnodes);
@@ -699,6 +709,8 @@ int pl_solver_create(pl_mesh m, const uint8_t* constrained, pl_solver* out) {
     // the Lagrange-multiplier DOFs (eliminated by the reduced formulation).
     std::vector<uint8_t> mask(n, 0);
     if (constrained) std::memcpy(mask.data(), constrained, n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S->d_dirichlet, mask.data(), n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host mask is modified below
     for (int64_t l = 0; l < S->npairs; ++l)
         for (int d = 0; d < 3; ++d) {
             mask[3 * (int64_t)ppos[l] + d] = 1;
@@ -861,6 +873,16 @@ int pl_solver_solve(pl_solver S, const double* b, double* x) {
     return fail(PL_ERR_NOT_CONVERGED, "iterative refinement did not converge");
 }
 
+int pl_solver_insert_constrained(pl_solver S, const double* values, double* u) {
+    if (!S || !values || !u) return fail(PL_ERR_INVALID_ARG, "bad arguments");
+    PLB_CUDA(cudaSetDevice(S->mesh->ctx->device));
+    const int64_t n = S->n;
+    k_insert_constrained<<<vec_grid(n), 256, 0, S->mesh->ctx->stream>>>(u, values, S->d_dirichlet, n);
+    count_launch();
+    PLB_CUDA(cudaGetLastError());
+    return PL_OK;
+}
+
 int pl_solver_apply_fault_slip(pl_solver S, pl_integrator iface, double* u) {
     if (!S || !iface || !u || !iface->is_interface || iface->mesh != S->mesh)
         return fail(PL_ERR_INVALID_ARG, "bad arguments");
@@ -901,7 +923,7 @@ static void solver_free(pl_solver S) {
     if (S->ev_in) cudaEventDestroy(S->ev_in);
     if (S->ev_out) cudaEventDestroy(S->ev_out);
     if (S->cstream) cudaStreamDestroy(S->cstream);
-    void* ptrs[] = {S->d_mask, S->d_diag, S->d_pinv, S->d_pinv32, S->d_r, S->d_p, S->d_q, S->d_z, S->d_x,
+    void* ptrs[] = {S->d_mask, S->d_dirichlet, S->d_diag, S->d_pinv, S->d_pinv32, S->d_r, S->d_p, S->d_q, S->d_z, S->d_x,
                     S->d_xs, S->f_r, S->f_p, S->f_q, S->f_z, S->f_x, S->d_scal, S->d_partials,
                     S->d_pair_neg, S->d_pair_pos, S->d_pair_normal};
     for (void* p : ptrs) dev_free(p, S->mesh->ctx->stream);

@@ -393,6 +393,10 @@ class Solver:
     def solve(self, b, x):
         check(C.lib().pl_solver_solve(self.handle, _ptr(b), _ptr(x)))
 
+    def insert_constrained(self, values, u) -> None:
+        """u[i] = values[i] at the constrained DOFs (pl_solver_insert_constrained)."""
+        check(C.lib().pl_solver_insert_constrained(self.handle, _ptr(values), _ptr(u)))
+
     def apply_fault_slip(self, iface: "IntegratorInterface", u) -> None:
         check(C.lib().pl_solver_apply_fault_slip(self.handle, iface.handle, _ptr(u)))
 

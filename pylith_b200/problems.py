@@ -65,8 +65,9 @@ class QuasistaticProblem:
         self.u = torch.zeros(n, dtype=torch.float64, device="cuda")
         self.F = torch.zeros_like(self.u)
         self.du = torch.zeros_like(self.u)
-        self._mask = torch.from_numpy(np.asarray(self.constrained, dtype=bool)).cuda()
-        self._bc = torch.from_numpy(np.asarray(self.bc_values, dtype=np.float64)).cuda()
+        self._bc = torch.from_numpy(np.ascontiguousarray(self.bc_values, dtype=np.float64)).cuda()
+        if self._bc.numel() < n:
+            raise ValueError(f"bc_values has {self._bc.numel()} entries, the solution {n}")
         self._setup_dt: Optional[float] = None
         self.history: List[StepStats] = []
 
@@ -83,9 +84,7 @@ class QuasistaticProblem:
         and the prescribed slip, F is the domain residual (the fault's lambda terms cancel in the
         reduced, slip-constrained space) and the solver is set up when its trigger fires. Returns
         (F, du): the solve is A du = F."""
-        import torch
-
-        self.u = torch.where(self._mask, self._bc, self.u)
+        self.solver.insert_constrained(self._bc, self.u)
         for iface in self.interfaces:
             self.solver.apply_fault_slip(iface, self.u)
         for i, ig in enumerate(self.domain):

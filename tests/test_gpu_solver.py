@@ -676,3 +676,28 @@ def test_reduced_fault_space_operator_matches_unfold_and_fold(ctx, monkeypatch, 
         (u1, i1), (u0, i0) = out[("1", prec)], out[("0", prec)]
         assert np.linalg.norm(u1 - u0) <= 1e-10 * np.linalg.norm(u0), prec
         assert abs(i1 - i0) <= 0.05 * i0 + 10, (prec, i1, i0)
+
+
+def test_insert_constrained_sets_only_the_constrained_dofs(ctx):
+    """pl_solver_insert_constrained: u takes the boundary values where the solver's mask is set
+    and keeps every other entry (Lagrange-multiplier DOFs of a fault mesh included)."""
+    import torch
+    from pylith_b200 import feassemble as FA
+
+    mesh = M.insert_fault_x(M.box_hex(4, 3, 3))
+    dm = FA.DeviceMesh(ctx, mesh)
+    mat = MAT.IsotropicLinearElasticity(*MAT.lognormal_elastic(mesh.num_cells, seed=1))
+    ig = mat.create_integrator(dm)
+    rng = np.random.default_rng(4)
+    cons = rng.random(3 * mesh.num_nodes) < 0.3
+    S = FA.Solver(dm, np.concatenate([cons, np.zeros(3 * mesh.num_lagrange, dtype=bool)]), [ig])
+    u0 = rng.standard_normal(dm.num_dof)
+    vals = rng.standard_normal(dm.num_dof)
+    u = torch.from_numpy(u0.copy()).cuda()
+    S.insert_constrained(torch.from_numpy(vals).cuda(), u)
+    ctx.synchronize()
+    got = u.cpu().numpy()
+    want = u0.copy()
+    want[:3 * mesh.num_nodes][cons] = vals[:3 * mesh.num_nodes][cons]
+    assert np.array_equal(got, want)
+    S.close()
