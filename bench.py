@@ -10,7 +10,7 @@ The L2 cache (126 MB) is flushed (256 MiB write) before every application, becau
 application's working set (~53 MB) would otherwise stay cached between applications.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pylith_b200|reference]
-  python bench.py --config c0|c1q2|c2|c3|c3tile|c3mg|c3bmg|c4  (the other configurations, one JSON line each)
+  python bench.py --config c0|c1link|c1q2|c2|c3|c3tile|c3mg|c3bmg|c4  (the other configurations, one JSON line each)
 
 Under torchrun (N > 1) the ranks share one mesh of N x 1.2 M cells (the same Delaunay box
 stretched N times along x, so every rank's part is the single-GPU workload: weak scaling), cut into
@@ -360,7 +360,7 @@ def main():
     ap.add_argument("--impl", default="pylith_b200")
     ap.add_argument("--cells", type=int, default=TARGET_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1q2", "c2", "c3", "c3tile", "c3mg", "c3bmg", "c4"])
+    ap.add_argument("--config", default="c1", choices=["c1", "c0", "c1link", "c1q2", "c2", "c3", "c3tile", "c3mg", "c3bmg", "c4"])
     ap.add_argument("--scale", type=float, default=1.0, help="size factor for the --config runs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -1134,7 +1134,93 @@ def config_c4(args):
                                        "freed memory for reuse)"}}
 
 
-CONFIGS = {"c0": config_c0, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c3tile": config_c3tile,
+def config_c1link(args):
+    """Where the end-to-end steps of the headline workload (1.2 M P1 tets, one step = u and v in,
+    residual and J v, r and J v out) spend their time on this box: each piece alone and the
+    pipelines, in microseconds per step over 40 steps, with host buffers from pl_host_alloc
+    and, for comparison, torch's pinned-memory cache."""
+    import ctypes
+
+    import torch
+
+    from pylith_b200 import _lib
+    from pylith_b200 import feassemble as FA
+    from pylith_b200 import materials as MAT
+
+    mesh = load_mesh(args.cells, seed=0)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=0)
+    ctx = FA.Context(0)
+    ig = MAT.IsotropicLinearElasticity(rho, mu, K).create_integrator(FA.DeviceMesh(ctx, mesh))
+    n = 3 * mesh.num_nodes
+
+    def host(*shape):
+        return torch.from_numpy(ctx.host_empty(shape))
+
+    hin = [host(2, n) for _ in range(2)]
+    hr, hjv = [host(n) for _ in range(2)], [host(n) for _ in range(2)]
+    for h in hin:
+        h.normal_()
+    din = [torch.empty(2, n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    dr = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    djv = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    main = torch.cuda.current_stream()
+    ctx.set_stream(s_comp.cuda_stream)
+    rt, lib = cudart(), _lib.lib()
+    P, S = ctypes.c_void_p, ctypes.c_size_t
+    steps = 40
+
+    def per_step(fn):
+        fn(4)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        fn(steps)
+        e1.record(main)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e3 / steps
+
+    def copies(do_in, do_out, src=None):
+        def fn(k):
+            for st in (s_in, s_out):
+                st.wait_stream(main)
+            for j in range(k):
+                i = j & 1
+                if do_in:
+                    p = src[i] if src is not None else hin[i].data_ptr()
+                    rt.cudaMemcpyAsync(P(din[i].data_ptr()), P(p), S(16 * n), 1, P(s_in.cuda_stream))
+                if do_out:
+                    rt.cudaMemcpyAsync(P(hr[i].data_ptr()), P(dr[i].data_ptr()), S(8 * n), 2, P(s_out.cuda_stream))
+                    rt.cudaMemcpyAsync(P(hjv[i].data_ptr()), P(djv[i].data_ptr()), S(8 * n), 2, P(s_out.cuda_stream))
+            for st in (s_in, s_out):
+                main.wait_stream(st)
+        return fn
+
+    def compute(k):
+        s_comp.wait_stream(main)
+        for j in range(k):
+            i = j & 1
+            lib.pl_compute_lhs_residual(ig.handle, 0.0, 0.0, P(din[i].data_ptr()), None, P(dr[i].data_ptr()), 0)
+            lib.pl_compute_lhs_jacobian_action(ig.handle, 0.0, 0.0, 0.0, P(din[i].data_ptr()),
+                                               P(din[i].data_ptr() + 8 * n), P(djv[i].data_ptr()), 0)
+        main.wait_stream(s_comp)
+
+    pinned = [torch.empty(2, n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    for t in pinned:
+        t.normal_()
+    out = {"in": per_step(copies(True, False)), "out": per_step(copies(False, True)),
+           "in_and_out": per_step(copies(True, True)), "kernels": per_step(compute)}
+    run = native_e2e_steps(ig, hin, din, dr, djv, hr, hjv, s_in, s_comp, s_out, n, main)
+    out["e2e_per_call"] = per_step(run)
+    out["in_from_torch_pinned"] = per_step(copies(True, False, [t.data_ptr() for t in pinned]))
+    ctx.set_stream(main.cuda_stream)
+    gbs = {k: 16 * n / (v * 1e-6) / 1e9 for k, v in out.items() if k.startswith("in") and k != "in_and_out"}
+    return {"config": "c1link", "dof": n, "bytes_in_per_step": 16 * n, "bytes_out_per_step": 16 * n,
+            "us_per_step": out, "h2d_gbs": gbs, "e2e_gdof_s": 2 * n / (out["e2e_per_call"] * 1e-6) / 1e9,
+            "host_buffers": f"pl_host_alloc (GPU NUMA node {ctx.numa_node})"}
+
+
+CONFIGS = {"c0": config_c0, "c1link": config_c1link, "c1q2": config_c1q2, "c2": config_c2, "c3": config_c3, "c3tile": config_c3tile,
            "c3mg": config_c3mg, "c3bmg": config_c3bmg, "c4": config_c4}
 
 
