@@ -21,6 +21,9 @@ from typing import List, Optional
 import numpy as np
 
 from . import feassemble as FA
+from ._lib import PylithB200Error
+
+PL_ERR_UNSUPPORTED = -7  # include/pylith_b200.h
 
 
 @dataclass
@@ -44,6 +47,7 @@ class QuasistaticProblem:
     precision: int = FA.Solver.FP64
     rtol: float = 1e-12
     inner_rtol: float = 1e-5
+    observers: list = field(default_factory=list)  # OutputObserver: written after every step
 
     def __post_init__(self):
         import torch
@@ -51,7 +55,9 @@ class QuasistaticProblem:
         self.dmesh = FA.DeviceMesh(self.ctx, self.mesh)
         self.domain: List[FA.IntegratorDomain] = []
         self.viscous: List[FA.IntegratorDomain] = []
+        self.domain_cells: List[np.ndarray] = []  # mesh cell ids of each domain integrator
         for mat, ids in self.materials:
+            self.domain_cells.append(np.arange(self.mesh.num_cells) if ids is None else np.asarray(ids))
             if hasattr(mat, "maxwell_time"):
                 ig = mat.create_integrator(self.dmesh, self.dt, ids)
                 self.viscous.append(ig)
@@ -107,11 +113,96 @@ class QuasistaticProblem:
         s = self.solver.stats()
         st = StepStats(t, s["iterations"], s["inner_iterations"], s["outer_iterations"], s["rel_residual"])
         self.history.append(st)
+        for obs in self.observers:  # poststep: notify the observers (TimeDependent.cc:490-538)
+            obs.update(self, t, len(self.history) - 1)
         return st
 
     def close(self) -> None:
-        """Releases the device objects (solver, integrators, mesh) now rather than at collection."""
+        """Releases the device objects (solver, integrators, mesh) now rather than at collection;
+        closes the observers' writers."""
+        for obs in self.observers:
+            obs.close()
         self.solver.close()
         for ig in self.domain + self.interfaces:
             ig.close()
         self.dmesh.close()
+
+
+@dataclass
+class OutputObserver:
+    """The reference's solution and material observers over one writer (OutputSolnDomain,
+    meshio/OutputSolnDomain.cc, and OutputPhysics, meshio/OutputPhysics.cc), triggered every
+    num_steps_skip + 1 steps (OutputTriggerStep::shouldWrite, meshio/OutputTriggerStep.cc:54-66:
+    a step is written when its index exceeds the last written one by more than num_steps_skip).
+
+    At a written step the solution's displacement goes out as a vertex field and, when
+    `derived` is set, every domain integrator's registered derived fields (cauchy_stress,
+    cauchy_strain: basis order 0, pl_compute_derived_field) as cell fields over the whole mesh,
+    each integrator filling its own cells. The writer is an output.DataWriterHDF5,
+    DataWriterHDF5Ext or DataWriterVTK (one file per step, into `directory`); it is opened on the
+    problem's mesh at the first update and closed by close()."""
+
+    writer: object
+    num_steps_skip: int = 0
+    derived: bool = True  # (integrators whose derived fields the device does not evaluate for
+    directory: str = "."  # their cell type, PL_ERR_UNSUPPORTED, are left out)
+    _step_wrote: int = -(1 << 30)
+    _opened: bool = False
+
+    def should_write(self, tindex: int) -> bool:
+        if tindex - self._step_wrote > self.num_steps_skip:
+            self._step_wrote = tindex
+            return True
+        return False
+
+    def _fields(self, problem, t: float):
+        import torch
+
+        nn = problem.mesh.num_nodes
+        vertex = [("displacement", problem.u[:3 * nn].reshape(nn, 3).cpu().numpy(), "vector")]
+        cell = []
+        if self.derived:
+            out = {}
+            for ig, ids in zip(problem.domain, problem.domain_cells):
+                names = getattr(ig, "derived_subfields", [])
+                if not names:
+                    continue
+                vals = torch.empty((len(ids), 6 * len(names)), dtype=torch.float64, device="cuda")
+                try:
+                    ig.compute_derived_field(t, problem.dt, problem.u, vals)
+                except PylithB200Error as e:
+                    if e.code != PL_ERR_UNSUPPORTED:
+                        raise
+                    continue  # no device evaluation of these fields for this cell type
+                v = vals.cpu().numpy()
+                for k, name in enumerate(names):
+                    full = out.setdefault(name, np.zeros((problem.mesh.num_cells, 6)))
+                    full[ids] = v[:, 6 * k:6 * k + 6]
+            cell = [(name, v, "tensor") for name, v in out.items()]
+        return vertex, cell
+
+    def update(self, problem, t: float, tindex: int) -> None:
+        if not self.should_write(tindex):
+            return
+        w = self.writer
+        if not self._opened:
+            w.open(problem.mesh)
+            self._opened = True
+        vertex, cell = self._fields(problem, t)
+        if hasattr(w, "open_time_step"):  # VTK: one file per step
+            w.open_time_step(t)
+            for name, v, vtype in vertex:
+                w.write_vertex_field(name, v, vector=vtype == "vector")
+            for name, v, _ in cell:
+                w.write_cell_field(name, v)
+            w.close_time_step(self.directory)
+        else:
+            for name, v, vtype in vertex:
+                w.write_vertex_field(t, name, v, vector_field_type=vtype)
+            for name, v, vtype in cell:
+                w.write_cell_field(t, name, v, vector_field_type=vtype)
+
+    def close(self) -> None:
+        if self._opened:
+            self.writer.close()
+            self._opened = False
