@@ -17,7 +17,6 @@ baseline alike. The baseline is the same stream served one at a time with the FP
 from __future__ import annotations
 
 import time
-from collections import deque
 from dataclasses import dataclass
 from typing import List, Optional
 
