@@ -247,6 +247,133 @@ class DataWriterVTK:
 # HDF5 output
 # ---------------------------------------------------------------------------------------------
 
+@dataclass
+class PointMesh:
+    """A mesh of points alone, one vertex cell per point (the point mesh of station output,
+    MeshOps::createFromPoints in topology/MeshOps.cc, used by OutputSolnPoints)."""
+
+    coords: np.ndarray  # float64 [npoints, 3]
+
+    @property
+    def num_nodes(self) -> int:
+        return int(len(self.coords))
+
+    @property
+    def num_cells(self) -> int:
+        return int(len(self.coords))
+
+
+def _q1_basis(xi: np.ndarray) -> np.ndarray:
+    """Trilinear basis on [0, 1]^3 in this package's Q1 corner order, [n][8]."""
+    x, y, z = xi[:, 0], xi[:, 1], xi[:, 2]
+    cols = []
+    for (a, b, c) in ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)):
+        cols.append((x if a else 1 - x) * (y if b else 1 - y) * (z if c else 1 - z))
+    return np.stack(cols, axis=1)
+
+
+def _q1_jacobian(X: np.ndarray, xi: np.ndarray) -> np.ndarray:
+    """d x / d xi of the trilinear map of corners X [n][8][3] at xi [n][3], [n][3][3]."""
+    x, y, z = xi[:, 0], xi[:, 1], xi[:, 2]
+    J = np.zeros((len(xi), 3, 3))
+    for k, (a, b, c) in enumerate(((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1),
+                                   (0, 1, 1))):
+        fx, fy, fz = (x if a else 1 - x), (y if b else 1 - y), (z if c else 1 - z)
+        dx, dy, dz = (1.0 if a else -1.0), (1.0 if b else -1.0), (1.0 if c else -1.0)
+        grad = np.stack([dx * fy * fz, fx * dy * fz, fx * fy * dz], axis=1)  # [n][3]
+        J += X[:, k, :, None] * grad[:, None, :]
+    return J
+
+
+def _q2_basis(xi: np.ndarray) -> np.ndarray:
+    """Triquadratic basis on [0, 1]^3, node (a, b, c) at index a + 3 b + 9 c, [n][27]."""
+    def lag(t):
+        return np.stack([2 * (t - 0.5) * (t - 1), -4 * t * (t - 1), 2 * t * (t - 0.5)], axis=1)
+
+    lx, ly, lz = lag(xi[:, 0]), lag(xi[:, 1]), lag(xi[:, 2])
+    return np.einsum("na,nb,nc->ncba", lx, ly, lz).reshape(len(xi), 27)
+
+
+class PointInterpolator:
+    """DMInterpolation for station output (OutputSolnPoints, meshio/OutputSolnPoints.cc:160-260):
+    each point is located once in a cell of the mesh on the host (cells nearest by centroid,
+    then the point's coordinates in the cell: barycentric for P1 tetrahedra, the inverse of the
+    trilinear corner map by Newton iterations for Q1 and Q2 hexahedra), and the solution's nodal
+    displacement is then interpolated with the cell's basis at the point on the device. A point
+    outside the mesh is an error, as DMInterpolationSetUp reports without ignoreOutsideDomain."""
+
+    def __init__(self, mesh, points, tol: float = 1e-9, device: str = "cuda"):
+        from scipy.spatial import cKDTree
+
+        pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+        corners = mesh.corner_nodes()
+        cent = mesh.coords[corners].mean(axis=1)
+        k = min(64, mesh.num_cells)
+        _, cand = cKDTree(cent).query(pts, k=k)
+        cand = np.asarray(cand).reshape(len(pts), k)
+        cell = np.full(len(pts), -1)
+        ref = np.zeros((len(pts), 3))
+        for j in range(k):
+            todo = np.flatnonzero(cell < 0)
+            if len(todo) == 0:
+                break
+            c = cand[todo, j]
+            xi = self._reference(mesh, corners[c], pts[todo])
+            if mesh.cell_type == M.CELL_TET4:
+                inside = (xi >= -tol).all(axis=1) & (xi.sum(axis=1) <= 1 + tol)
+            else:
+                inside = ((xi >= -tol) & (xi <= 1 + tol)).all(axis=1)
+            cell[todo[inside]] = c[inside]
+            ref[todo[inside]] = xi[inside]
+        if (cell < 0).any():
+            raise ValueError(f"{int((cell < 0).sum())} points are outside the mesh, e.g. {pts[cell < 0][0]}")
+        if mesh.cell_type == M.CELL_TET4:
+            w = np.concatenate([1 - ref.sum(axis=1, keepdims=True), ref], axis=1)
+        elif mesh.cell_type == M.CELL_HEX8:
+            w = _q1_basis(ref)
+        else:
+            w = _q2_basis(ref)
+        import torch
+
+        self.cells = cell
+        self.nodes = torch.from_numpy(mesh.cells[cell].astype(np.int64)).to(device)
+        self.weights = torch.from_numpy(w).to(device)
+
+    @staticmethod
+    def _reference(mesh, X_idx, pts):
+        X = mesh.coords[X_idx]  # [n][corners][3]
+        if mesh.cell_type == M.CELL_TET4:
+            A = np.transpose(X[:, 1:, :] - X[:, :1, :], (0, 2, 1))  # columns x_k - x_0
+            return np.linalg.solve(A, (pts - X[:, 0, :])[..., None])[..., 0]
+        xi = np.full((len(pts), 3), 0.5)
+        for _ in range(20):  # Newton on the trilinear map (exact in one step for affine cells)
+            r = np.einsum("nk,nkd->nd", _q1_basis(xi), X) - pts
+            xi = xi - np.linalg.solve(_q1_jacobian(X, xi), r[..., None])[..., 0]
+        return xi
+
+    def __call__(self, u):
+        """Displacement at the points, [npoints][3], from a device solution vector (3 DOFs per
+        mesh node first)."""
+        disp = u.reshape(-1, 3)  # mesh nodes first, then the fault's Lagrange-multiplier nodes
+        return (disp[self.nodes] * self.weights[..., None]).sum(dim=1)
+
+
+def read_points_list(path: str, comment: str = "#", delimiter: Optional[str] = None):
+    """Station names and coordinates from a points file as PyLith's PointsList reads it
+    (pylith/meshio/PointsList.py): one point per line, `name x y z`, fields split on whitespace
+    (or `delimiter`), lines starting with the comment delimiter skipped."""
+    names, coords = [], []
+    with open(path) as fh:
+        for line in fh:
+            line = line.strip()
+            if not line or line.startswith(comment):
+                continue
+            fields = line.split(delimiter)
+            names.append(fields[0].strip())
+            coords.append([float(v) for v in fields[1:4]])
+    return names, np.array(coords, dtype=np.float64).reshape(-1, 3)
+
+
 VECTOR_FIELD_TYPES = ("scalar", "vector", "tensor", "other", "multi_scalar", "multi_vector", "multi_tensor",
                       "multi_other")  # FieldBase::vectorFieldString (topology/FieldBase.cc:34-56)
 
@@ -305,6 +432,14 @@ class DataWriterHDF5:
         self._steps, self._tstamp_index = {}, 0
         w = H5.H5Writer(self.hdf5_filename())
         w.create_dataset("/geometry/vertices", np.asarray(mesh.coords, dtype=np.float64) * self.length_scale)
+        if isinstance(mesh, PointMesh):  # stations: vertex cells, the rank as a vertex field
+            n = mesh.num_nodes
+            w.create_dataset("/viz/topology/cells", np.arange(n, dtype=np.int32).reshape(n, 1),
+                             {"cell_corners": np.int32(1), "cell_dim": np.int32(0)})
+            w.create_dataset("/vertex_fields/partition_rank", np.zeros((n, 1)),
+                             {"vector_field_type": "scalar", "componentName0": "0"})
+            self._h5 = w
+            return
         corners = vtk_cells(mesh)[0].astype(np.int32)
         w.create_dataset("/viz/topology/cells", corners,
                          {"cell_corners": np.int32(corners.shape[1]), "cell_dim": np.int32(3)})

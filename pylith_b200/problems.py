@@ -206,3 +206,36 @@ class OutputObserver:
         if self._opened:
             self.writer.close()
             self._opened = False
+
+
+@dataclass
+class OutputPointsObserver:
+    """The reference's station observer (OutputSolnPoints, meshio/OutputSolnPoints.cc:110-140)
+    over one writer: every num_steps_skip + 1 steps (OutputTriggerStep) the displacement
+    interpolated at named points (output.PointInterpolator, the counterpart of DMInterpolation)
+    goes to a file of a point mesh, with the names in /stations written before the first step
+    (output.read_points_list reads PyLith's points files)."""
+
+    writer: object
+    names: list
+    points: np.ndarray
+    num_steps_skip: int = 0
+    _step_wrote: int = -(1 << 30)
+    _interp: Optional[object] = None
+
+    def update(self, problem, t: float, tindex: int) -> None:
+        if tindex - self._step_wrote <= self.num_steps_skip:
+            return
+        self._step_wrote = tindex
+        from . import output as OUT
+
+        if self._interp is None:
+            self._interp = OUT.PointInterpolator(problem.mesh, self.points)
+            self.writer.open(OUT.PointMesh(np.asarray(self.points, dtype=np.float64).reshape(-1, 3)))
+            self.writer.write_point_names(list(self.names))
+        disp = self._interp(problem.u).cpu().numpy()
+        self.writer.write_vertex_field(t, "displacement", disp, vector_field_type="vector")
+
+    def close(self) -> None:
+        if self._interp is not None:
+            self.writer.close()

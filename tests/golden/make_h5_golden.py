@@ -15,7 +15,7 @@ facts that do not come from the files' encoding:
     cell centroid's x (so that of x for vertices off the fault);
   * /time holds the tests' one time, 1.0, and each field's vector_field_type is its name.
 
-It then keeps, for the tet4 and hex8 vertex and cell files, every dataset (values, shapes) and
+It then keeps, for the tet4 and hex8 vertex, cell and station (points) files, every dataset (values, shapes) and
 attribute, and the SHA-256 of each file, so that tests/test_hdf5.py can check the writer in
 pylith_b200/output.py against them without the PyLith sources.
 
@@ -34,7 +34,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 from pylith_b200 import hdf5 as H5  # noqa: E402
 
-KEEP = ["tet4_vertex.h5", "tet4_cell.h5", "hex8_vertex.h5", "hex8_cell.h5"]
+KEEP = ["tet4_vertex.h5", "tet4_cell.h5", "hex8_vertex.h5", "hex8_cell.h5", "tet4_points_vertex.h5",
+        "hex8_points_vertex.h5"]
 MESH_CASES = {"tri3": 2, "quad4": 2, "tet4": 3, "hex8": 3}
 LENGTH_SCALE = 0.1
 CONSTANTS = (11.0, 13.0, 17.0)

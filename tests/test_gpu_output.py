@@ -107,3 +107,41 @@ def test_observer_writes_vtk_files_per_step(ctx, tmp_path):
     pts, conn, offs, types, cfields, pfields = OUT.read_vtu(str(tmp_path / "domain_t001.vtu"))
     assert np.array_equal(pfields["displacement"], d)
     assert np.array_equal(cfields["cauchy_stress.0"].ravel(), cell["cauchy_stress"][:, 0])
+
+
+def test_station_observer_interpolates_the_device_solution(ctx, tmp_path):
+    """OutputPointsObserver: the displacement at stations read from a points file, interpolated
+    on the device (exact for the uniform strain the boundaries impose on a homogeneous box),
+    written with the station names to a point-mesh HDF5 file."""
+    from pylith_b200 import hdf5 as H5
+    from pylith_b200 import output as OUT
+    from pylith_b200 import problems as P
+
+    pts_file = tmp_path / "points.txt"
+    pts_file.write_text("# stations\nZZ.1 -2200.0 +2100.0 -1000.0\nZZ.2 +100.0 +50.0 -1020.0\n"
+                        "ZZ.3 +1100.0 +3400.0 -3230.0\nZZ.44 0.0 0.0 -7999.0\n")
+    names, pts = OUT.read_points_list(str(pts_file))
+    mesh = M.box_tet_delaunay(3000, seed=4, lo=LO, hi=HI)
+    rho, mu, K = MAT.lognormal_elastic(mesh.num_cells, seed=2, sigma_log=0.0, density_spread=0.0)
+    cons = np.zeros((mesh.num_nodes, 3), dtype=bool)
+    for ax in range(3):
+        for sd in ("neg", "pos"):
+            cons[M.boundary_mask(mesh, ax, sd, LO, HI)] = True
+    X = mesh.coords
+    bc = np.stack([0 * X[:, 0], 0 * X[:, 1], E0 * (X[:, 2] - LO[2])], axis=1).ravel()
+    w = OUT.DataWriterHDF5(filename=str(tmp_path / "stations.h5"))
+    obs = P.OutputPointsObserver(w, names, pts)
+    prob = P.QuasistaticProblem(ctx, mesh, [(MAT.IsotropicLinearElasticity(rho, mu, K), None)], cons.ravel(), bc,
+                                rtol=1e-13, observers=[obs])
+    prob.step(1.0)
+    prob.step(2.0)
+    prob.close()
+    f = H5.H5File(str(tmp_path / "stations.h5"))
+    assert [s.decode() for s in f.dataset("/stations")] == names
+    assert f.dataset("/stations").dtype == np.dtype("S6")
+    d = f.dataset("/vertex_fields/displacement")
+    assert d.shape == (2, 4, 3)
+    want = np.stack([0 * pts[:, 0], 0 * pts[:, 1], E0 * (pts[:, 2] - LO[2])], axis=1)
+    np.testing.assert_allclose(d[1], want, rtol=0, atol=1e-9 * E0 * (HI[2] - LO[2]))
+    assert np.array_equal(f.dataset("/viz/topology/cells").ravel(), np.arange(4))
+    assert f.attrs("/viz/topology/cells") == {"cell_corners": 1, "cell_dim": 0}

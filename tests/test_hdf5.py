@@ -62,6 +62,40 @@ def test_writer_reproduces_the_reference_datasets(tmp_path, name):
         assert _attrs(f, p) == a, p
 
 
+@pytest.mark.parametrize("name", ["tet4_points_vertex.h5", "hex8_points_vertex.h5"])
+def test_station_output_reproduces_the_reference_datasets(tmp_path, name):
+    """Station output (TestDataWriterHDF5Points): a point mesh, its names in /stations, fields per
+    point; the layout and values must be the golden file's."""
+    ds, groups = _golden(name)
+    pts = ds["/geometry/vertices"][0]
+    names = [n.decode() for n in ds["/stations"][0]]
+    w = OUT.DataWriterHDF5(filename=str(tmp_path / name))
+    w.open(OUT.PointMesh(pts))
+    w.write_point_names(names)
+    for p, (v, a) in ds.items():
+        if p.startswith("/vertex_fields/") and "timestepping" in a:
+            w.write_vertex_field(1.0, p.rsplit("/", 1)[1], v[0], vector_field_type=a["vector_field_type"])
+    w.close()
+    f = H5.H5File(str(tmp_path / name))
+    paths = f.walk()
+    assert sorted(p for p in paths if f.is_group(p)) == sorted(groups)
+    assert sorted(p for p in paths if not f.is_group(p)) == sorted(ds)
+    for p, (v, a) in ds.items():
+        got = f.dataset(p)
+        assert got.dtype == v.dtype and got.shape == v.shape, p
+        assert np.array_equal(got, v), p
+        assert _attrs(f, p) == a, p
+    assert '<Topology TopologyType="Polyvertex" NumberOfElements="4">' in open(tmp_path / name.replace(".h5", ".xmf")).read()
+
+
+def test_points_list_reader(tmp_path):
+    p = tmp_path / "points.txt"
+    p.write_text("# Points for solution output\nZZ.1 -2200.0 +2100.0  -1000.0\n\nZZ.2  +100.0   +50.0  -1020.0\n")
+    names, xyz = OUT.read_points_list(str(p))
+    assert names == ["ZZ.1", "ZZ.2"]
+    assert np.array_equal(xyz, [[-2200.0, 2100.0, -1000.0], [100.0, 50.0, -1020.0]])
+
+
 def test_steps_times_and_growth(tmp_path):
     """The reference's step rule (DataWriterHDF5.cc:168-178): the k-th write of a field is its step
     k and the first field written at a new step adds that step's time (times the time scale). The
