@@ -313,7 +313,6 @@ static void context_free(pl_context c) {
     cudaStreamSynchronize(c->stream);
     dev_free(c->d_err, c->stream);
     dev_free(c->d_stage, c->stream);
-    if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     dev_pool_trim(c->device);
     delete c;

@@ -126,9 +126,7 @@ struct pl_context_s {
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     unsigned int* d_err = nullptr;
-    // staging buffers for the host-buffer entry points
-    double* h_pinned = nullptr;
-    size_t h_pinned_bytes = 0;
+    // staging buffer for the host-buffer entry points
     double* d_stage = nullptr;
     size_t d_stage_bytes = 0;
 };
