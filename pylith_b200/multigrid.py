@@ -4,7 +4,7 @@ x = x0 of cohesive cells), for the multigrid-preconditioned conjugate gradients 
 
 The reference preconditions its elasticity solves with algebraic multigrid (PETSc GAMG, fine-level
 smoother point-block Jacobi with faults; libsrc/pylith/materials/Elasticity.cc:298-330). The boxes
-of the configurations this build runs are structured, so the hierarchy here is geometric: every
+of the benchmarked configurations are structured, so the hierarchy here is geometric: every
 level is the same box with about half the cells per direction (exactly half while that keeps the
 fault plane a grid plane; otherwise the nearest count that does, so the grids need not be nested),
 re-discretised with the registered pointwise kernels on cell-averaged aux fields; the levels are

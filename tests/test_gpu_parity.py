@@ -363,7 +363,7 @@ def test_unknown_kernel_is_rejected(torch_cuda, ctx):
 
 
 def test_more_than_eight_constants_are_rejected(torch_cuda, ctx):
-    """Integrator::_setKernelConstants takes any number of constants; this build holds at most 8
+    """Integrator::_setKernelConstants takes any number of constants; the library holds at most 8
     (the kernels on the path use 1 or 6) and rejects more with PL_ERR_UNSUPPORTED instead of
     dropping the extra ones; the previous constants stay in place."""
     from pylith_b200 import _lib
