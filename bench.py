@@ -315,7 +315,7 @@ def cpu_baseline(mesh, mat, source: str, budget_s: float = 10.0):
     """Oracle cell loop on every host core: residual F(u) plus a second pass of the same loop
     standing in for J v (linear elasticity: F(u) = J u), repeated within a time budget."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O  # the checker; timed here as the CPU baseline only
+    import oracle as O  # the oracle; timed here as the CPU baseline only
 
     if source == "ref" and not O.ref_available():
         source = "oracle"

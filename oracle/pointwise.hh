@@ -1,6 +1,6 @@
 // ORACLE — test infrastructure only. Nothing in the product library includes,
 // links or calls this file; tests/, bench.py's CPU-baseline leg and smoke()
-// use it as the checker.
+// use it as the oracle.
 //
 // CPU restatement of the PyLith pointwise kernels on the residual/Jacobian hot
 // path, written against PETSc's pointwise-function signature

@@ -1,6 +1,6 @@
 """GPU parity: the CUDA cell loop (called through the C ABI) against the oracle on the same
-seeded meshes, fields and parameters. FP64 tolerance: relative L2 <= 1e-12 (the north-star
-bar); FP32 Jacobian action: relative L2 <= 1e-5."""
+seeded meshes, fields and parameters. FP64 tolerance: relative L2 <= 1e-12 (the FP64
+parity bar); FP32 Jacobian action: relative L2 <= 1e-5."""
 import numpy as np
 import pytest
 

@@ -1,4 +1,4 @@
-"""Pins the oracle (CPU restatement) before it is trusted as the checker.
+"""Pins the oracle (CPU restatement) before the GPU tests compare against it.
 
 1. Pointwise kernels: the restatement against golden vectors produced by the
    reference's own kernels (tests/golden/pointwise_golden.npz), and against
