@@ -651,6 +651,84 @@ PL_D void padjv_stage(const float* __restrict__ v32, const PipeArrays& A, int64_
         __pipeline_memcpy_async(&M.inc[8 * t], &A.inc[b * 4 * kTetBlockCells + 8 * t], 16);
 }
 
+// One cell of the FP32 Jacobian action over the padded layout: FP64 geometry (cofactors, 1/det)
+// from the staged coordinates X [3][ld], gradient and flux of the FP32 field V [3][ld] with the
+// isotropic tangent (lam, mu), and the element vector into column tc of sE [12][kTetBlockCells].
+PL_D void padjv_cell(const DomainParams& p, ushort4 lc, float lam, float mu, const double* X, const float* V, int ld,
+                     float* sE, int tc) {
+    const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
+    double Xc[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Xc[k][d] = X[d * ld + ln[k]];
+    double cof[3][3];
+    const double det = tet_cofactors(Xc, cof);
+    if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
+    const double rdet = 1.0 / det;
+    float inv[3][3], cf[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            inv[i][j] = (float)(cof[i][j] * rdet);
+            cf[i][j] = (float)(cof[i][j] * (1.0 / 6.0));
+        }
+    float s[3][3];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+        const float v0 = V[cc * ld + ln[0]];
+        const float g0 = V[cc * ld + ln[1]] - v0, g1 = V[cc * ld + ln[2]] - v0, g2 = V[cc * ld + ln[3]] - v0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s[cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
+    }
+    // flux f1 = -(lambda tr(e) I + 2 mu e), e = sym grad v
+    const float ltr = lam * (s[0][0] + s[1][1] + s[2][2]);
+    const float xy = -mu * (s[0][1] + s[1][0]), yz = -mu * (s[1][2] + s[2][1]), xz = -mu * (s[0][2] + s[2][0]);
+    const float f[3][3] = {{-(2.0f * mu * s[0][0] + ltr), xy, xz},
+                           {xy, -(2.0f * mu * s[1][1] + ltr), yz},
+                           {xz, yz, -(2.0f * mu * s[2][2] + ltr)}};
+    float e0[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+            const float v = f[cc][0] * cf[k][0] + f[cc][1] * cf[k][1] + f[cc][2] * cf[k][2];
+            e0[cc] -= v;
+            sE[((k + 1) * 3 + cc) * kTetBlockCells + tc] = v;
+        }
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + tc] = e0[cc];
+}
+
+// Node sums of block b from its element vectors sE and metadata M: owned nodes added, shared
+// nodes reduced into p.out32.
+PL_D void padjv_node_sums(const DomainParams& p, const PipeArrays& A, int64_t b, const float* sE, const PipeMeta& M) {
+    const int ns = A.slot_begin[b + 1] - A.slot_begin[b];
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        const int j0 = M.off[k], j1 = M.off[k + 1];
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+#pragma unroll 4
+        for (int j = j0; j < j1; ++j) {
+            const int e = M.inc[j];
+            r0 += sE[e];
+            r1 += sE[e + kTetBlockCells];
+            r2 += sE[e + 2 * kTetBlockCells];
+        }
+        const uint32_t id = M.ids[k];
+        float* o = p.out32 + 3 * (int64_t)(id & ~kSharedBit);
+        if (id & kSharedBit) {
+            red_add(o, r0);
+            red_add(o + 1, r1);
+            red_add(o + 2, r2);
+        } else {
+            o[0] += r0;
+            o[1] += r1;
+            o[2] += r2;
+        }
+    }
+}
+
 // FP32 Jacobian action of an isotropic tangent on the padded cell-block layout, in the shape of
 // k_tet_pad2: block b + G is staged with cp.async while block b is computed, geometry (cofactors,
 // 1/det) in FP64 per cell, field, gradient, flux, element vectors and node sums in FP32. The
@@ -722,79 +800,13 @@ __global__ void __launch_bounds__(kTetBlockCells, 4) k_tet_pad_jv32(DomainParams
         for (int k = 0; k < kMaxSlotsPerThread; ++k) nd_next[k] = nd_after[k];
         const double* X = reinterpret_cast<const double*>(nodeb + (it & 1) * nbytes);
         const float* V = reinterpret_cast<const float*>(nodeb + (it & 1) * nbytes + 3 * (size_t)ld * sizeof(double));
-        if (live) {
-            const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
-            double Xc[4][3];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) Xc[k][d] = X[d * ld + ln[k]];
-            double cof[3][3];
-            const double det = tet_cofactors(Xc, cof);
-            if (!(det > 0.0)) flag_error(p.err, CHECK_NONPOSITIVE_DETJ);
-            const double rdet = 1.0 / det;
-            float inv[3][3], cf[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    inv[i][j] = (float)(cof[i][j] * rdet);
-                    cf[i][j] = (float)(cof[i][j] * (1.0 / 6.0));
-                }
-            float s[3][3];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) {
-                const float v0 = V[cc * ld + ln[0]];
-                const float g0 = V[cc * ld + ln[1]] - v0, g1 = V[cc * ld + ln[2]] - v0, g2 = V[cc * ld + ln[3]] - v0;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) s[cc][d] = g0 * inv[0][d] + g1 * inv[1][d] + g2 * inv[2][d];
-            }
-            // flux f1 = -(lambda tr(e) I + 2 mu e), e = sym grad v
-            const float ltr = lam * (s[0][0] + s[1][1] + s[2][2]);
-            const float xy = -mu * (s[0][1] + s[1][0]), yz = -mu * (s[1][2] + s[2][1]), xz = -mu * (s[0][2] + s[2][0]);
-            const float f[3][3] = {{-(2.0f * mu * s[0][0] + ltr), xy, xz},
-                                   {xy, -(2.0f * mu * s[1][1] + ltr), yz},
-                                   {xz, yz, -(2.0f * mu * s[2][2] + ltr)}};
-            float e0[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    const float v = f[cc][0] * cf[k][0] + f[cc][1] * cf[k][1] + f[cc][2] * cf[k][2];
-                    e0[cc] -= v;
-                    sE[((k + 1) * 3 + cc) * kTetBlockCells + tc] = v;
-                }
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) sE[cc * kTetBlockCells + tc] = e0[cc];
-        }
+        if (live) padjv_cell(p, lc, lam, mu, X, V, ld, sE, tc);
         __syncthreads();
-        const PipeMeta M = pipe_meta(metab + (it & 1) * mb, ld);
-        const int ns = A.slot_begin[b + 1] - A.slot_begin[b];
-        for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-            const int j0 = M.off[k], j1 = M.off[k + 1];
-            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
-#pragma unroll 4
-            for (int j = j0; j < j1; ++j) {
-                const int e = M.inc[j];
-                r0 += sE[e];
-                r1 += sE[e + kTetBlockCells];
-                r2 += sE[e + 2 * kTetBlockCells];
-            }
-            const uint32_t id = M.ids[k];
-            float* o = p.out32 + 3 * (int64_t)(id & ~kSharedBit);
-            if (id & kSharedBit) {
-                red_add(o, r0);
-                red_add(o + 1, r1);
-                red_add(o + 2, r2);
-            } else {
-                o[0] += r0;
-                o[1] += r1;
-                o[2] += r2;
-            }
-        }
+        padjv_node_sums(p, A, b, sE, pipe_meta(metab + (it & 1) * mb, ld));
     }
     __pipeline_wait_prior(0);
 }
+
 
 // FP32 Jacobian action of isotropic linear elasticity on the cell blocks: geometry (cofactors,
 // 1/det) and the elastic tangent in FP64 per cell, the field, gradient, flux and element vectors
